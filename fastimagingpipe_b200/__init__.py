@@ -1,0 +1,210 @@
+"""B200-native snapshot imaging + tLISI trigger (FastImagingPipe's hot path).
+
+Python mirror of the reference's entry point over the C ABI of
+libfip_b200.so (include/fip.h):
+
+* ``FIpipe(vis_re, vis_im, B, V, num_baselines, image_size, num_snapshots,
+  cell_size, unit_size)`` -> tLISI matrix, the same arguments and meaning as
+  the reference's ``FIpipe`` (FIPkernels.cu:554-557; pipe_interface.cpp:181),
+  host arrays in, host array out;
+* ``Imager``: persistent device state for one image size, device-pointer
+  calls for snapshot imaging, the trigger, sequences and the FIpipe shape;
+* ``plane_project`` / ``collapse_visibilities``: the on-device preprocessing
+  (SVDPreprocessKernels.cu).
+
+The CUDA library is required: nothing here falls back to the CPU.  Device
+buffers may be passed as integer addresses or as objects exposing
+``data_ptr()`` (torch tensors).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfip_b200.so")
+CLI_PATH = os.path.join(_HERE, "bin", "sharedlibrary_gpu")
+
+FORM_PLAIN = 0
+FORM_PRECISE = 1
+STORE_F32, STORE_F16, STORE_BF16 = 0, 1, 2
+REPROJECT_GATHER, REPROJECT_SCATTER = 0, 1
+
+_lib = None
+
+
+class FipError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"fip status {status}: {message}")
+        self.status = status
+
+
+class ImagerConfig(ctypes.Structure):
+    _fields_ = [("image_size", ctypes.c_size_t), ("max_baselines", ctypes.c_size_t),
+                ("unit_size", ctypes.c_size_t), ("cell_size", ctypes.c_float),
+                ("form", ctypes.c_int), ("vis_storage", ctypes.c_int),
+                ("device", ctypes.c_int), ("reproject", ctypes.c_int)]
+
+
+def lib() -> ctypes.CDLL:
+    """Loads libfip_b200.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with "
+                              "`python -m fastimagingpipe_b200.build` (there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, sz, fp = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_float
+        L.fip_last_error.restype = ctypes.c_char_p
+        L.fip_status_string.restype = ctypes.c_char_p
+        L.fip_status_string.argtypes = [ctypes.c_int]
+        L.fip_version.restype = ctypes.c_char_p
+        L.fip_pipe.argtypes = [vp, vp, vp, vp, vp, sz, sz, sz, fp, sz]
+        L.fip_imager_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(ImagerConfig)]
+        L.fip_imager_destroy.argtypes = [vp]
+        L.fip_imager_device_bytes.argtypes = [vp]
+        L.fip_imager_device_bytes.restype = sz
+        L.fip_image_snapshot.argtypes = [vp, vp, vp, vp, vp, sz, vp, vp, vp]
+        L.fip_trigger.argtypes = [vp, vp, vp, vp, vp, vp, vp]
+        L.fip_pipe_device.argtypes = [vp, vp, vp, vp, vp, sz, vp, vp]
+        L.fip_imager_image.argtypes = [vp, ctypes.c_int]
+        L.fip_imager_image.restype = vp
+        L.fip_pipe_host.argtypes = [vp, vp, vp, vp, vp, sz, sz, vp]
+        L.fip_pixel_targets.argtypes = [vp, vp, vp, ctypes.c_int, vp]
+        L.fip_plane_project.argtypes = [vp, vp, sz, sz, vp, vp, vp]
+        L.fip_collapse_visibilities.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]
+        L.fip_image_sequence.argtypes = [vp, vp, vp, vp, vp, vp, sz, sz, vp, vp]
+        _lib = L
+    return _lib
+
+
+def _check(status: int):
+    if status != 0:
+        raise FipError(status, lib().fip_last_error().decode(errors="replace"))
+
+
+def _ptr(x) -> int:
+    if x is None:
+        return 0
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return int(x.data_ptr())
+    raise TypeError(f"expected a device address or a tensor, got {type(x)!r}")
+
+
+def _stream(s) -> int:
+    if s is None:
+        return 0
+    if isinstance(s, int):
+        return s
+    return int(getattr(s, "cuda_stream", s))
+
+
+def version() -> str:
+    return lib().fip_version().decode()
+
+
+def FIpipe(Visreal, Visimag, Bin, Vin, num_baselines: int, image_size: int,
+           num_snapshots: int, cell_size: float, unit_size: int) -> np.ndarray:
+    """The reference's FIpipe (FIPkernels.cu:554) on host arrays: images the
+    first three snapshots and returns the (N/T, N/T) tLISI matrix."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (Visreal, Visimag, Bin, Vin)]
+    nb, n, s, t = int(num_baselines), int(image_size), int(num_snapshots), int(unit_size)
+    if arrs[0].size < s * nb or arrs[1].size < s * nb or arrs[2].size < s * nb * 2 or \
+            arrs[3].size < s * 9:
+        raise ValueError("input arrays are smaller than num_snapshots x num_baselines")
+    u = n // t if t > 0 else 0
+    out = np.zeros((u, u), np.float32)
+    _check(lib().fip_pipe(*(a.ctypes.data for a in arrs), out.ctypes.data, nb, n, s,
+                          float(cell_size), t))
+    return out
+
+
+class Imager:
+    """Persistent imager (fip_imager) for one image size."""
+
+    def __init__(self, image_size: int, max_baselines: int, cell_size: float,
+                 unit_size: int = 0, form: int = FORM_PLAIN, vis_storage: int = STORE_F32,
+                 device: int = 0, reproject: int = REPROJECT_GATHER):
+        self.cfg = ImagerConfig(image_size, max_baselines, unit_size, cell_size, form,
+                                vis_storage, device, reproject)
+        h = ctypes.c_void_p()
+        _check(lib().fip_imager_create(ctypes.byref(h), ctypes.byref(self.cfg)))
+        self._h = h
+        self.image_size = image_size
+        self.unit_size = unit_size
+        self.max_baselines = max_baselines
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fip_imager_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def device_bytes(self) -> int:
+        return int(lib().fip_imager_device_bytes(self._h))
+
+    def image_snapshot(self, vis_re, vis_im, B, V, nb: int, image, image_max=None, stream=None):
+        _check(lib().fip_image_snapshot(self._h, _ptr(vis_re), _ptr(vis_im), _ptr(B), _ptr(V), nb,
+                                        _ptr(image), _ptr(image_max), _stream(stream)))
+
+    def trigger(self, I1, I2, I3, max3, result, stream=None):
+        _check(lib().fip_trigger(self._h, _ptr(I1), _ptr(I2), _ptr(I3), _ptr(max3), _ptr(result),
+                                 _stream(stream)))
+
+    def pipe_device(self, vis_re, vis_im, B, V, nb: int, result, stream=None):
+        _check(lib().fip_pipe_device(self._h, _ptr(vis_re), _ptr(vis_im), _ptr(B), _ptr(V), nb,
+                                     _ptr(result), _stream(stream)))
+
+    def image_ptr(self, k: int) -> int:
+        return int(lib().fip_imager_image(self._h, k) or 0)
+
+    def pipe_host(self, vis_re, vis_im, B, V, nb: int, num_snapshots: int = 3) -> np.ndarray:
+        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (vis_re, vis_im, B, V)]
+        u = self.image_size // self.unit_size
+        out = np.zeros((u, u), np.float32)
+        _check(lib().fip_pipe_host(self._h, *(a.ctypes.data for a in arrs), nb, num_snapshots,
+                                   out.ctypes.data))
+        return out
+
+    def pixel_targets(self, V, out, exact: bool = False, stream=None):
+        _check(lib().fip_pixel_targets(self._h, _ptr(V), _ptr(out), int(exact), _stream(stream)))
+
+    def image_sequence(self, vis_re, vis_im, B, V, nb_per_snapshot, nb_stride: int, results,
+                       stream=None):
+        nbs = np.ascontiguousarray(nb_per_snapshot, dtype=np.uint64)
+        _check(lib().fip_image_sequence(self._h, _ptr(vis_re), _ptr(vis_im), _ptr(B), _ptr(V),
+                                        nbs.ctypes.data, nb_stride, len(nbs), _ptr(results),
+                                        _stream(stream)))
+
+
+def plane_project(uvw, freqs, rows: int, chans: int, B, V, stream=None):
+    """Device plane fit: uvw [rows*3] m, freqs [chans] Hz -> B [rows*chans*2], V [9]."""
+    _check(lib().fip_plane_project(_ptr(uvw), _ptr(freqs), rows, chans, _ptr(B), _ptr(V),
+                                   _stream(stream)))
+
+
+def collapse_visibilities(v0r, v0i, v3r, v3i, f0, f3, w0, w3, out_re, out_im, ns: int,
+                          stream=None):
+    _check(lib().fip_collapse_visibilities(*(_ptr(x) for x in (v0r, v0i, v3r, v3i, f0, f3, w0,
+                                                               w3, out_re, out_im)), ns,
+                                           _stream(stream)))

@@ -1,0 +1,515 @@
+// Host orchestration and C ABI of libfip_b200.so.
+//
+// One fip_imager owns every device buffer of one image size (grid, bins,
+// images, staging), one cuFFT C2R plan and its streams, so repeated calls
+// allocate nothing.  The reference's FIpipe re-allocates ~19 buffers, creates
+// a cuFFT plan and three streams per call and returns 0 whatever happens
+// (FIPkernels.cu:583-861); FIpipe here keeps a small cache of imagers and
+// returns a status.
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/fip.h"
+#include "fip_common.cuh"
+#include "fip_kernels.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define FIP_CUDA(call)                                                                     \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return fail(e_ == cudaErrorMemoryAllocation ? FIP_ERR_NOMEM : FIP_ERR_CUDA,          \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                     \
+  } while (0)
+
+#define FIP_CUFFT(call)                                                                    \
+  do {                                                                                     \
+    cufftResult r_ = (call);                                                               \
+    if (r_ != CUFFT_SUCCESS)                                                               \
+      return fail(r_ == CUFFT_ALLOC_FAILED ? FIP_ERR_NOMEM : FIP_ERR_CUFFT,                \
+                  std::string(#call) + ": cufftResult " + std::to_string((int)r_));        \
+  } while (0)
+
+#define FIP_TRY(call)                  \
+  do {                                 \
+    int st_ = (call);                  \
+    if (st_ != FIP_OK) return st_;     \
+  } while (0)
+
+// Sets the device for the lifetime of a call and restores the caller's.
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = true;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) ok = cudaSetDevice(dev) == cudaSuccess;
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t count, size_t& total) {
+  total += count * sizeof(T);
+  return cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T));
+}
+
+}  // namespace
+
+struct fip_imager {
+  fip_imager_config cfg{};
+  FipGeom geo{};
+  size_t device_bytes = 0;
+  cudaStream_t stream = nullptr;     // compute stream of the host-buffer path
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_copied[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ev_used[3] = {nullptr, nullptr, nullptr};
+  cufftHandle plan = 0;
+  bool plan_ok = false;
+  float2* grid = nullptr;            // G x (G/2+1) complex; in-place C2R output
+  float* taper = nullptr;            // N/2 + 1
+  FipBins bins{};
+  float* images[3] = {nullptr, nullptr, nullptr};
+  float* maxima = nullptr;           // [3] device floats (written as max bits)
+  float* result = nullptr;           // U*U
+  float* stats = nullptr;
+  // Reduced-precision visibility storage (precision form).
+  void* q_re = nullptr;
+  void* q_im = nullptr;
+  float* q_scale = nullptr;
+  // Device and pinned staging of the host-buffer path, 3 snapshot slots.
+  float* d_vr = nullptr;
+  float* d_vi = nullptr;
+  float* d_B = nullptr;
+  float* d_V = nullptr;
+  float* h_vr = nullptr;
+  float* h_vi = nullptr;
+  float* h_B = nullptr;
+  float* h_V = nullptr;
+  float* h_result = nullptr;
+};
+
+static void imager_free(fip_imager* im) {
+  if (!im) return;
+  DeviceGuard g(im->cfg.device);
+  if (im->stream) cudaStreamSynchronize(im->stream);
+  if (im->copy_stream) cudaStreamSynchronize(im->copy_stream);
+  if (im->plan_ok) cufftDestroy(im->plan);
+  void* dptrs[] = {im->grid, im->taper, im->bins.count, im->bins.offset, im->bins.cursor,
+                   im->bins.entries, im->bins.work, im->bins.nwork, im->bins.bbox,
+                   im->images[0], im->images[1], im->images[2], im->maxima, im->result,
+                   im->stats, im->q_re, im->q_im, im->q_scale, im->d_vr, im->d_vi, im->d_B,
+                   im->d_V};
+  for (void* p : dptrs)
+    if (p) cudaFree(p);
+  void* hptrs[] = {im->h_vr, im->h_vi, im->h_B, im->h_V, im->h_result};
+  for (void* p : hptrs)
+    if (p) cudaFreeHost(p);
+  for (int k = 0; k < 3; ++k) {
+    if (im->ev_copied[k]) cudaEventDestroy(im->ev_copied[k]);
+    if (im->ev_used[k]) cudaEventDestroy(im->ev_used[k]);
+  }
+  if (im->stream) cudaStreamDestroy(im->stream);
+  if (im->copy_stream) cudaStreamDestroy(im->copy_stream);
+  delete im;
+}
+
+static int validate_sizes(size_t n, size_t t, float cell) {
+  if (n < 8 || n % 4 != 0)
+    return fail(FIP_ERR_ARG, "image_size must be a multiple of 4 and >= 8 (the reference's "
+                             "grid crop is misaligned when ceil(1.5 N) is odd)");
+  if (n > 32768) return fail(FIP_ERR_ARG, "image_size above 32768 is not supported");
+  if (t > n) return fail(FIP_ERR_ARG, "unit_size larger than image_size");
+  if (!(cell > 0.f) || !(cell < 1.f)) return fail(FIP_ERR_ARG, "cell_size must be in (0, 1) rad");
+  return FIP_OK;
+}
+
+extern "C" {
+
+const char* fip_last_error(void) { return g_last_error.c_str(); }
+
+const char* fip_version(void) { return "0.1.0"; }
+
+const char* fip_status_string(int s) {
+  switch (s) {
+    case FIP_OK: return "ok";
+    case FIP_ERR_ARG: return "invalid argument";
+    case FIP_ERR_CUDA: return "CUDA error";
+    case FIP_ERR_CUFFT: return "cuFFT error";
+    case FIP_ERR_NOMEM: return "out of memory";
+    case FIP_ERR_BUDGET: return "over the HBM budget";
+    case FIP_ERR_NOT_READY: return "not ready";
+    case FIP_ERR_STATE: return "invalid state";
+    default: return "unknown status";
+  }
+}
+
+int fip_imager_create(fip_imager** out, const fip_imager_config* cfg) {
+  if (!out || !cfg) return fail(FIP_ERR_ARG, "null argument");
+  *out = nullptr;
+  FIP_TRY(validate_sizes(cfg->image_size, cfg->unit_size, cfg->cell_size));
+  if (cfg->max_baselines == 0 || cfg->max_baselines > (1u << 28))
+    return fail(FIP_ERR_ARG, "max_baselines must be in [1, 2^28]");
+  if (cfg->form != FIP_FORM_PLAIN && cfg->form != FIP_FORM_PRECISE)
+    return fail(FIP_ERR_ARG, "unknown form");
+  if (cfg->vis_storage < 0 || cfg->vis_storage > 2) return fail(FIP_ERR_ARG, "unknown storage");
+  int ndev = 0;
+  FIP_CUDA(cudaGetDeviceCount(&ndev));
+  if (cfg->device < 0 || cfg->device >= ndev) return fail(FIP_ERR_ARG, "no such device");
+  DeviceGuard guard(cfg->device);
+  if (!guard.ok) return fail(FIP_ERR_CUDA, "cudaSetDevice failed");
+
+  fip_imager* im = new fip_imager();
+  im->cfg = *cfg;
+  FipGeom& geo = im->geo;
+  geo.n = (int)cfg->image_size;
+  geo.g = (int)ceilf(1.5f * (float)cfg->image_size);  // computeCeil(1.5 N) (FIPkernels.cu:583)
+  geo.hp = geo.g / 2 + 1;
+  geo.t = (int)cfg->unit_size;
+  geo.u = geo.t > 0 ? geo.n / geo.t : 0;
+  geo.tiles_r = (geo.g + FIP_GTILE - 1) / FIP_GTILE;
+  geo.tiles_c = (geo.hp + FIP_GTILE - 1) / FIP_GTILE;
+  geo.cell = cfg->cell_size;
+  const size_t n2 = (size_t)geo.n * geo.n;
+  const size_t nb = cfg->max_baselines;
+  const size_t ntiles = (size_t)geo.tiles_r * geo.tiles_c;
+  size_t& tot = im->device_bytes;
+
+  auto cleanup = [&](int code) {
+    std::string msg = g_last_error;
+    imager_free(im);
+    g_last_error = msg;
+    return code;
+  };
+#define FIP_ALLOC(call)                                                                      \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return cleanup(fail(e_ == cudaErrorMemoryAllocation ? FIP_ERR_NOMEM : FIP_ERR_CUDA,    \
+                          std::string(#call) + ": " + cudaGetErrorString(e_)));              \
+  } while (0)
+
+  FIP_ALLOC(cudaStreamCreateWithFlags(&im->stream, cudaStreamNonBlocking));
+  FIP_ALLOC(cudaStreamCreateWithFlags(&im->copy_stream, cudaStreamNonBlocking));
+  for (int k = 0; k < 3; ++k) {
+    FIP_ALLOC(cudaEventCreateWithFlags(&im->ev_copied[k], cudaEventDisableTiming));
+    FIP_ALLOC(cudaEventCreateWithFlags(&im->ev_used[k], cudaEventDisableTiming));
+  }
+  FIP_ALLOC(dalloc(&im->grid, (size_t)geo.g * geo.hp, tot));
+  FIP_ALLOC(dalloc(&im->taper, (size_t)geo.n / 2 + 1, tot));
+  im->bins.cap = 12 * nb;
+  im->bins.wcap = ntiles + im->bins.cap / FIP_GCHUNK + 1;
+  FIP_ALLOC(dalloc(&im->bins.count, ntiles, tot));
+  FIP_ALLOC(dalloc(&im->bins.offset, ntiles + 1, tot));
+  FIP_ALLOC(dalloc(&im->bins.cursor, ntiles, tot));
+  FIP_ALLOC(dalloc(&im->bins.entries, im->bins.cap, tot));
+  FIP_ALLOC(dalloc(&im->bins.work, im->bins.wcap, tot));
+  FIP_ALLOC(dalloc(&im->bins.nwork, 1, tot));
+  FIP_ALLOC(dalloc(&im->bins.bbox, 4, tot));
+  for (int k = 0; k < 3; ++k) FIP_ALLOC(dalloc(&im->images[k], n2, tot));
+  FIP_ALLOC(dalloc(&im->maxima, 3, tot));
+  FIP_ALLOC(dalloc(&im->result, std::max<size_t>((size_t)geo.u * geo.u, 1), tot));
+  if (cfg->form == FIP_FORM_PRECISE && cfg->vis_storage != FIP_STORE_F32) {
+    FIP_ALLOC(dalloc((uint16_t**)&im->q_re, nb, tot));
+    FIP_ALLOC(dalloc((uint16_t**)&im->q_im, nb, tot));
+    FIP_ALLOC(dalloc(&im->q_scale, 1, tot));
+  }
+  FIP_ALLOC(dalloc(&im->d_vr, 3 * nb, tot));
+  FIP_ALLOC(dalloc(&im->d_vi, 3 * nb, tot));
+  FIP_ALLOC(dalloc(&im->d_B, 3 * nb * 2, tot));
+  FIP_ALLOC(dalloc(&im->d_V, 27, tot));
+  FIP_ALLOC(cudaMallocHost((void**)&im->h_vr, 3 * nb * sizeof(float)));
+  FIP_ALLOC(cudaMallocHost((void**)&im->h_vi, 3 * nb * sizeof(float)));
+  FIP_ALLOC(cudaMallocHost((void**)&im->h_B, 3 * nb * 2 * sizeof(float)));
+  FIP_ALLOC(cudaMallocHost((void**)&im->h_V, 27 * sizeof(float)));
+  FIP_ALLOC(cudaMallocHost((void**)&im->h_result,
+                           std::max<size_t>((size_t)geo.u * geo.u, 1) * sizeof(float)));
+
+  {
+    cufftResult r = cufftCreate(&im->plan);
+    if (r != CUFFT_SUCCESS) return cleanup(fail(FIP_ERR_CUFFT, "cufftCreate failed"));
+    im->plan_ok = true;
+    size_t work = 0;
+    r = cufftMakePlan2d(im->plan, geo.g, geo.g, CUFFT_C2R, &work);
+    if (r != CUFFT_SUCCESS)
+      return cleanup(fail(r == CUFFT_ALLOC_FAILED ? FIP_ERR_NOMEM : FIP_ERR_CUFFT,
+                          "cufftMakePlan2d(C2R) failed: " + std::to_string((int)r)));
+    tot += work;
+  }
+  cudaError_t e = fip_launch_taper(im->taper, geo, im->stream);
+  if (e != cudaSuccess) return cleanup(fail(FIP_ERR_CUDA, cudaGetErrorString(e)));
+  e = cudaStreamSynchronize(im->stream);
+  if (e != cudaSuccess) return cleanup(fail(FIP_ERR_CUDA, cudaGetErrorString(e)));
+#undef FIP_ALLOC
+  *out = im;
+  return FIP_OK;
+}
+
+int fip_imager_destroy(fip_imager* im) {
+  imager_free(im);
+  return FIP_OK;
+}
+
+size_t fip_imager_device_bytes(const fip_imager* im) { return im ? im->device_bytes : 0; }
+
+static int image_snapshot_impl(fip_imager* im, const float* vr, const float* vi, const float* B,
+                               const float* V, size_t nb, float* image, float* image_max,
+                               cudaStream_t s) {
+  const FipGeom& geo = im->geo;
+  if (nb > im->cfg.max_baselines) return fail(FIP_ERR_ARG, "nb exceeds the imager's capacity");
+  if (nb == 0) return fail(FIP_ERR_ARG, "nb must be positive");
+  if (!vr || !vi || !B || !V || !image) return fail(FIP_ERR_ARG, "null device pointer");
+  const bool precise = im->cfg.form == FIP_FORM_PRECISE;
+  const void* gvr = vr;
+  const void* gvi = vi;
+  int vt = FIP_VIS_F32;
+  if (precise && im->cfg.vis_storage != FIP_STORE_F32) {
+    vt = im->cfg.vis_storage == FIP_STORE_F16 ? FIP_VIS_F16 : FIP_VIS_BF16;
+    FIP_CUDA(fip_launch_quantize(vr, vi, nb, vt, im->q_re, im->q_im, im->q_scale, s));
+    gvr = im->q_re;
+    gvi = im->q_im;
+  }
+  FIP_CUDA(fip_launch_bin(geo, B, (int)nb, im->bins, s));
+  FIP_CUDA(fip_launch_grid(geo, B, gvr, gvi, vt, im->q_scale, V, (int)nb, im->bins, im->grid,
+                           precise ? 1 : 0, s));
+  FIP_CUFFT(cufftSetStream(im->plan, s));
+  FIP_CUFFT(cufftExecC2R(im->plan, reinterpret_cast<cufftComplex*>(im->grid),
+                         reinterpret_cast<cufftReal*>(im->grid)));
+  const float* fft_out = reinterpret_cast<const float*>(im->grid);
+  if (image_max) FIP_CUDA(cudaMemsetAsync(image_max, 0, sizeof(float), s));
+  if (im->cfg.reproject == 1 && !precise) {
+    FIP_CUDA(fip_launch_reproject_scatter(geo, fft_out, im->taper, V, (int)nb, image, s));
+    if (image_max)
+      FIP_CUDA(fip_launch_image_max(image, (size_t)geo.n * geo.n,
+                                    reinterpret_cast<unsigned*>(image_max), s));
+  } else {
+    FIP_CUDA(fip_launch_reproject_gather(geo, fft_out, im->taper, V, (int)nb, image,
+                                         reinterpret_cast<unsigned*>(image_max), precise ? 1 : 0,
+                                         s));
+  }
+  return FIP_OK;
+}
+
+int fip_image_snapshot(fip_imager* im, const float* vis_re, const float* vis_im, const float* B,
+                       const float* V, size_t nb, float* image, float* image_max, void* stream) {
+  if (!im) return fail(FIP_ERR_ARG, "null imager");
+  DeviceGuard g(im->cfg.device);
+  return image_snapshot_impl(im, vis_re, vis_im, B, V, nb, image, image_max,
+                             (cudaStream_t)stream);
+}
+
+int fip_trigger(fip_imager* im, const float* I1, const float* I2, const float* I3,
+                const float* max3, float* result, void* stream) {
+  if (!im) return fail(FIP_ERR_ARG, "null imager");
+  if (im->geo.t <= 0) return fail(FIP_ERR_ARG, "imager has no trigger tile (unit_size 0)");
+  if (!I1 || !I2 || !I3 || !max3 || !result) return fail(FIP_ERR_ARG, "null device pointer");
+  DeviceGuard g(im->cfg.device);
+  FIP_CUDA(fip_launch_trigger(im->geo, I1, I2, I3, max3, im->stats, result,
+                              im->cfg.form == FIP_FORM_PRECISE ? 1 : 0, (cudaStream_t)stream));
+  return FIP_OK;
+}
+
+int fip_pipe_device(fip_imager* im, const float* vr, const float* vi, const float* B,
+                    const float* V, size_t nb, float* result, void* stream) {
+  if (!im) return fail(FIP_ERR_ARG, "null imager");
+  DeviceGuard g(im->cfg.device);
+  cudaStream_t s = (cudaStream_t)stream;
+  for (int k = 0; k < 3; ++k)
+    FIP_TRY(image_snapshot_impl(im, vr + (size_t)k * nb, vi + (size_t)k * nb,
+                                B + (size_t)k * nb * 2, V + (size_t)k * 9, nb, im->images[k],
+                                im->maxima + k, s));
+  if (im->geo.t > 0 && result)
+    FIP_CUDA(fip_launch_trigger(im->geo, im->images[0], im->images[1], im->images[2],
+                                im->maxima, im->stats, result,
+                                im->cfg.form == FIP_FORM_PRECISE ? 1 : 0, s));
+  return FIP_OK;
+}
+
+const float* fip_imager_image(const fip_imager* im, int k) {
+  if (!im || k < 0 || k > 2) return nullptr;
+  return im->images[k];
+}
+
+int fip_pipe_host(fip_imager* im, const float* vr, const float* vi, const float* B,
+                  const float* V, size_t nb, size_t nsnap, float* result) {
+  if (!im) return fail(FIP_ERR_ARG, "null imager");
+  if (!vr || !vi || !B || !V || !result) return fail(FIP_ERR_ARG, "null host pointer");
+  if (nsnap < 3)
+    return fail(FIP_ERR_ARG, "num_snapshots must be >= 3 (the pipeline images three snapshots)");
+  if (im->geo.t <= 0) return fail(FIP_ERR_ARG, "imager has no trigger tile (unit_size 0)");
+  DeviceGuard g(im->cfg.device);
+  cudaStream_t s = im->stream, cs = im->copy_stream;
+  // Per snapshot: host copy into pinned slot k (CPU), async H2D on the copy
+  // stream, then the compute stream images it while the CPU stages k+1.
+  for (int k = 0; k < 3; ++k) {
+    float* hvr = im->h_vr + (size_t)k * nb;
+    float* hvi = im->h_vi + (size_t)k * nb;
+    float* hB = im->h_B + (size_t)k * nb * 2;
+    float* hV = im->h_V + (size_t)k * 9;
+    std::memcpy(hvr, vr + (size_t)k * nb, nb * sizeof(float));
+    std::memcpy(hvi, vi + (size_t)k * nb, nb * sizeof(float));
+    std::memcpy(hB, B + (size_t)k * nb * 2, nb * 2 * sizeof(float));
+    std::memcpy(hV, V + (size_t)k * 9, 9 * sizeof(float));
+    float* dvr = im->d_vr + (size_t)k * nb;
+    float* dvi = im->d_vi + (size_t)k * nb;
+    float* dB = im->d_B + (size_t)k * nb * 2;
+    float* dV = im->d_V + (size_t)k * 9;
+    FIP_CUDA(cudaMemcpyAsync(dvr, hvr, nb * sizeof(float), cudaMemcpyHostToDevice, cs));
+    FIP_CUDA(cudaMemcpyAsync(dvi, hvi, nb * sizeof(float), cudaMemcpyHostToDevice, cs));
+    FIP_CUDA(cudaMemcpyAsync(dB, hB, nb * 2 * sizeof(float), cudaMemcpyHostToDevice, cs));
+    FIP_CUDA(cudaMemcpyAsync(dV, hV, 9 * sizeof(float), cudaMemcpyHostToDevice, cs));
+    FIP_CUDA(cudaEventRecord(im->ev_copied[k], cs));
+    FIP_CUDA(cudaStreamWaitEvent(s, im->ev_copied[k], 0));
+    FIP_TRY(image_snapshot_impl(im, dvr, dvi, dB, dV, nb, im->images[k], im->maxima + k, s));
+  }
+  FIP_CUDA(fip_launch_trigger(im->geo, im->images[0], im->images[1], im->images[2], im->maxima,
+                              im->stats, im->result, im->cfg.form == FIP_FORM_PRECISE ? 1 : 0,
+                              s));
+  const size_t uu = (size_t)im->geo.u * im->geo.u;
+  FIP_CUDA(cudaMemcpyAsync(im->h_result, im->result, uu * sizeof(float), cudaMemcpyDeviceToHost,
+                           s));
+  FIP_CUDA(cudaStreamSynchronize(s));
+  std::memcpy(result, im->h_result, uu * sizeof(float));
+  return FIP_OK;
+}
+
+int fip_pixel_targets(fip_imager* im, const float* V, float* out, int exact, void* stream) {
+  if (!im || !V || !out) return fail(FIP_ERR_ARG, "null argument");
+  DeviceGuard g(im->cfg.device);
+  FIP_CUDA(fip_launch_pixel_targets(im->geo, V, out, exact, (cudaStream_t)stream));
+  return FIP_OK;
+}
+
+int fip_image_sequence(fip_imager* im, const float* vr, const float* vi, const float* B,
+                       const float* V, const size_t* nb, size_t nb_stride, size_t nsnap,
+                       float* results, void* stream) {
+  if (!im || !nb) return fail(FIP_ERR_ARG, "null argument");
+  if (nsnap < 3) return fail(FIP_ERR_ARG, "num_snapshots must be >= 3");
+  if (im->geo.t <= 0) return fail(FIP_ERR_ARG, "imager has no trigger tile (unit_size 0)");
+  DeviceGuard g(im->cfg.device);
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t uu = (size_t)im->geo.u * im->geo.u;
+  for (size_t k = 0; k < nsnap; ++k) {
+    const int slot = (int)(k % 3);
+    FIP_TRY(image_snapshot_impl(im, vr + k * nb_stride, vi + k * nb_stride, B + k * nb_stride * 2,
+                                V + k * 9, nb[k], im->images[slot], im->maxima + slot, s));
+    if (k >= 2) {
+      // Ring slots a, b, c hold snapshots k-2, k-1, k.  The combine uses the
+      // maximum of the three maxima only, so the maxima keep ring order.
+      const int a = (int)((k - 2) % 3), b = (int)((k - 1) % 3), c = slot;
+      FIP_CUDA(fip_launch_trigger(im->geo, im->images[a], im->images[b], im->images[c],
+                                  im->maxima, im->stats, results + (k - 2) * uu,
+                                  im->cfg.form == FIP_FORM_PRECISE ? 1 : 0, s));
+    }
+  }
+  return FIP_OK;
+}
+
+int fip_plane_project(const float* uvw, const float* freqs, size_t rows, size_t chans, float* B,
+                      float* V, void* stream) {
+  if (!uvw || !freqs || !B || !V) return fail(FIP_ERR_ARG, "null device pointer");
+  if (rows == 0 || chans == 0) return fail(FIP_ERR_ARG, "empty measurement set");
+  FIP_CUDA(fip_launch_plane_project(uvw, freqs, rows, chans, nullptr, B, V,
+                                    (cudaStream_t)stream));
+  return FIP_OK;
+}
+
+int fip_collapse_visibilities(const float* v0r, const float* v0i, const float* v3r,
+                              const float* v3i, const uint8_t* f0, const uint8_t* f3,
+                              const float* w0, const float* w3, float* out_re, float* out_im,
+                              size_t ns, void* stream) {
+  if (!v0r || !v0i || !v3r || !v3i || !f0 || !f3 || !w0 || !w3 || !out_re || !out_im)
+    return fail(FIP_ERR_ARG, "null device pointer");
+  FIP_CUDA(fip_launch_collapse(v0r, v0i, v3r, v3i, f0, f3, w0, w3, out_re, out_im, ns,
+                               (cudaStream_t)stream));
+  return FIP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// FIpipe-compatible entry points with a small cache of imagers.
+// ---------------------------------------------------------------------------
+
+namespace {
+struct CacheEntry {
+  int device;
+  size_t n, nb, t;
+  float cell;
+  fip_imager* im;
+  unsigned long long last_use;
+};
+std::mutex g_cache_mu;
+std::vector<CacheEntry> g_cache;
+unsigned long long g_tick = 0;
+constexpr size_t kCacheMax = 2;
+}  // namespace
+
+int fip_pipe(const float* vis_re, const float* vis_im, const float* B, const float* V,
+             float* result, size_t num_baselines, size_t image_size, size_t num_snapshots,
+             float cell_size, size_t unit_size) {
+  if (!vis_re || !vis_im || !B || !V || !result) return fail(FIP_ERR_ARG, "null host pointer");
+  if (num_baselines == 0) return fail(FIP_ERR_ARG, "num_baselines must be positive");
+  if (unit_size == 0) return fail(FIP_ERR_ARG, "unit_size must be positive");
+  FIP_TRY(validate_sizes(image_size, unit_size, cell_size));
+  if (num_snapshots < 3)
+    return fail(FIP_ERR_ARG, "num_snapshots must be >= 3 (three snapshots are imaged)");
+  int dev = 0;
+  FIP_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_cache_mu);
+  fip_imager* im = nullptr;
+  for (auto& e : g_cache)
+    if (e.device == dev && e.n == image_size && e.nb == num_baselines && e.t == unit_size &&
+        e.cell == cell_size) {
+      im = e.im;
+      e.last_use = ++g_tick;
+    }
+  if (!im) {
+    if (g_cache.size() >= kCacheMax) {
+      auto it = std::min_element(g_cache.begin(), g_cache.end(),
+                                 [](const CacheEntry& a, const CacheEntry& b) {
+                                   return a.last_use < b.last_use;
+                                 });
+      imager_free(it->im);
+      g_cache.erase(it);
+    }
+    fip_imager_config cfg{};
+    cfg.image_size = image_size;
+    cfg.max_baselines = num_baselines;
+    cfg.unit_size = unit_size;
+    cfg.cell_size = cell_size;
+    cfg.form = FIP_FORM_PLAIN;
+    cfg.vis_storage = FIP_STORE_F32;
+    cfg.device = dev;
+    cfg.reproject = 0;
+    FIP_TRY(fip_imager_create(&im, &cfg));
+    g_cache.push_back(CacheEntry{dev, image_size, num_baselines, unit_size, cell_size, im,
+                                 ++g_tick});
+  }
+  return fip_pipe_host(im, vis_re, vis_im, B, V, num_baselines, num_snapshots, result);
+}
+
+}  // extern "C"
+
+int FIpipe(float* Visreal, float* Visimag, float* Bin, float* Vin, float* result_array,
+           size_t num_baselines, size_t image_size, size_t num_snapshots, float cell_size,
+           size_t unit_size) {
+  return fip_pipe(Visreal, Visimag, Bin, Vin, result_array, num_baselines, image_size,
+                  num_snapshots, cell_size, unit_size);
+}

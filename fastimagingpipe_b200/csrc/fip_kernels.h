@@ -1,0 +1,61 @@
+// Launchers of the device stages, shared by the host orchestration.
+// All launchers are asynchronous on `s` and return the launch status.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+
+#include "fip_common.cuh"
+
+// Scratch of the tile-binned gridder for one image size.
+struct FipBins {
+  unsigned* count;    // [ntiles] entries per grid tile
+  unsigned* offset;   // [ntiles + 1] exclusive scan of count
+  unsigned* cursor;   // [ntiles] scatter cursors
+  unsigned* entries;  // [cap] (vis << 1 | mirrored), grouped by tile
+  int4* work;         // [wcap] (tile, begin, end, single-chunk flag)
+  unsigned* nwork;    // [1] number of work items
+  unsigned* bbox;     // [4] occupied half-plane rows/cols (precision form)
+  size_t cap;         // capacity of entries
+  size_t wcap;        // capacity of work
+};
+
+enum FipVisType { FIP_VIS_F32 = 0, FIP_VIS_F16 = 1, FIP_VIS_BF16 = 2 };
+
+// ---- plain FP32 form (reference-faithful arithmetic, fip_plain.cu) ----
+cudaError_t fip_launch_taper(float* taper, const FipGeom& geo, cudaStream_t s);
+cudaError_t fip_launch_bin(const FipGeom& geo, const float* B, int nb, FipBins& bins,
+                           cudaStream_t s);
+cudaError_t fip_launch_grid(const FipGeom& geo, const float* B, const void* vr, const void* vi,
+                            int vis_type, const float* vis_scale, const float* V, int nb,
+                            const FipBins& bins, float2* grid, int compensated, cudaStream_t s);
+// Source-major reprojection: one thread per source pixel, atomics into a
+// zeroed destination (the reference's scheme, with correction fused).
+cudaError_t fip_launch_reproject_scatter(const FipGeom& geo, const float* fft_out,
+                                         const float* taper, const float* V, int nb, float* dst,
+                                         cudaStream_t s);
+// Destination-tile-major reprojection: every destination tile gathers its
+// candidate source pixels, splats in shared memory and is stored once.  Also
+// records the image maximum into *img_max (atomic max, caller zeroes it).
+cudaError_t fip_launch_reproject_gather(const FipGeom& geo, const float* fft_out,
+                                        const float* taper, const float* V, int nb, float* dst,
+                                        unsigned* img_max, int exact_targets, cudaStream_t s);
+cudaError_t fip_launch_image_max(const float* img, size_t count, unsigned* out, cudaStream_t s);
+// Trigger: per-tile statistics of (I1, I2, I3) then the tLISI combine.
+cudaError_t fip_launch_trigger(const FipGeom& geo, const float* I1, const float* I2,
+                               const float* I3, const float* max3, float* stats,
+                               float* result, int precise, cudaStream_t s);
+cudaError_t fip_launch_pixel_targets(const FipGeom& geo, const float* V, float* out,
+                                     int exact_targets, cudaStream_t s);
+
+// ---- plane projection (fip_precise.cu) ----
+cudaError_t fip_launch_plane_project(const float* uvw, const float* freqs, size_t rows,
+                                     size_t chans, double* work, float* B, float* V,
+                                     cudaStream_t s);
+cudaError_t fip_launch_collapse(const float* v0r, const float* v0i, const float* v3r,
+                                const float* v3i, const unsigned char* f0,
+                                const unsigned char* f3, const float* w0, const float* w3,
+                                float* out_re, float* out_im, size_t ns, cudaStream_t s);
+cudaError_t fip_launch_quantize(const float* vr, const float* vi, size_t nb, int vis_type,
+                                void* out_re, void* out_im, float* scale_out, cudaStream_t s);

@@ -1,0 +1,265 @@
+// IEEE-arithmetic stages (compiled without fast math): plane projection of
+// baseline uvw, Stokes-I collapse, and the reduced-precision visibility
+// storage of the precision form.
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "fip_common.cuh"
+#include "fip_kernels.h"
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kPlaneBlocks = 296;  // 2 x 148 SMs
+constexpr double kLight = 299792458.0;
+
+// Sample s = row + chan * rows (SVDPreprocessMain.cpp:36-38), in wavelengths
+// (SVDPreprocessKernels.cu:41-61), FP64.
+__device__ __forceinline__ void sample_lambda(const float* uvw, const float* freqs, size_t rows,
+                                              size_t s, double x[3]) {
+  const size_t r = s % rows, c = s / rows;
+  const double sc = (double)freqs[c] / kLight;
+  x[0] = (double)uvw[3 * r + 0] * sc;
+  x[1] = (double)uvw[3 * r + 1] * sc;
+  x[2] = (double)uvw[3 * r + 2] * sc;
+}
+
+// Block partial sums in FP64 (deterministic two-stage reduction).
+// MODE 0: sum x (3 values); MODE 1: centred second moments (6 values).
+template <int MODE>
+__global__ void k_plane_moments(const float* uvw, const float* freqs, size_t rows, size_t chans,
+                                const double* mean, double* partial) {
+  constexpr int K = MODE == 0 ? 3 : 6;
+  __shared__ double sh[K][kThreads];
+  double acc[K];
+  for (int k = 0; k < K; ++k) acc[k] = 0.0;
+  const size_t ns = rows * chans;
+  double m[3] = {0, 0, 0};
+  if (MODE == 1) {
+    m[0] = mean[0]; m[1] = mean[1]; m[2] = mean[2];
+  }
+  for (size_t s = blockIdx.x * (size_t)kThreads + threadIdx.x; s < ns;
+       s += (size_t)gridDim.x * kThreads) {
+    double x[3];
+    sample_lambda(uvw, freqs, rows, s, x);
+    if (MODE == 0) {
+      acc[0] += x[0]; acc[1] += x[1]; acc[2] += x[2];
+    } else {
+      const double a = x[0] - m[0], b = x[1] - m[1], c = x[2] - m[2];
+      acc[0] += a * a; acc[1] += a * b; acc[2] += a * c;
+      acc[3 % K] += b * b; acc[4 % K] += b * c; acc[5 % K] += c * c;
+    }
+  }
+  for (int k = 0; k < K; ++k) sh[k][threadIdx.x] = acc[k];
+  __syncthreads();
+  for (int d = kThreads / 2; d > 0; d >>= 1) {
+    if ((int)threadIdx.x < d)
+      for (int k = 0; k < K; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + d];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < K; ++k) partial[blockIdx.x * K + k] = sh[k][0];
+}
+
+template <int K>
+__global__ void k_plane_reduce(const double* partial, int nblocks, double scale, double* out) {
+  if (threadIdx.x < K) {
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += partial[b * K + threadIdx.x];
+    out[threadIdx.x] = s * scale;
+  }
+}
+
+// Cyclic Jacobi eigen-decomposition of the 3x3 covariance, then the basis
+// of the reference: principal axes in descending order, each signed so its
+// largest-magnitude component is positive (SVDPreprocessKernels.cu:115-206),
+// third row their cross product.
+__global__ void k_plane_basis(const double* cov6, double* basis_out, float* V) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double A[9] = {cov6[0], cov6[1], cov6[2], cov6[1], cov6[3], cov6[4], cov6[2], cov6[4], cov6[5]};
+  double Q[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  for (int sweep = 0; sweep < 64; ++sweep) {
+    const double off = A[1] * A[1] + A[2] * A[2] + A[5] * A[5];
+    if (off < 1e-300) break;
+    for (int p = 0; p < 2; ++p)
+      for (int q = p + 1; q < 3; ++q) {
+        const double apq = A[p * 3 + q];
+        if (fabs(apq) < 1e-300) continue;
+        const double app = A[p * 3 + p], aqq = A[q * 3 + q];
+        const double tau = (aqq - app) / (2.0 * apq);
+        const double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+        const double c = 1.0 / sqrt(1.0 + t * t), s = t * c;
+        for (int k = 0; k < 3; ++k) {
+          const double akp = A[k * 3 + p], akq = A[k * 3 + q];
+          A[k * 3 + p] = c * akp - s * akq;
+          A[k * 3 + q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < 3; ++k) {
+          const double apk = A[p * 3 + k], aqk = A[q * 3 + k];
+          A[p * 3 + k] = c * apk - s * aqk;
+          A[q * 3 + k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < 3; ++k) {
+          const double qkp = Q[k * 3 + p], qkq = Q[k * 3 + q];
+          Q[k * 3 + p] = c * qkp - s * qkq;
+          Q[k * 3 + q] = s * qkp + c * qkq;
+        }
+      }
+  }
+  const double d[3] = {A[0], A[4], A[8]};
+  int big = 0;
+  for (int k = 1; k < 3; ++k)
+    if (d[k] > d[big]) big = k;
+  int mid = -1;
+  for (int k = 0; k < 3; ++k)
+    if (k != big && (mid < 0 || d[k] > d[mid])) mid = k;
+  double b[6];
+  for (int a = 0; a < 3; ++a) {
+    b[a] = Q[a * 3 + big];
+    b[3 + a] = Q[a * 3 + mid];
+  }
+  for (int comp = 0; comp < 2; ++comp) {
+    int ma = 0;
+    double mv = fabs(b[comp * 3]);
+    for (int a = 1; a < 3; ++a)
+      if (fabs(b[comp * 3 + a]) > mv) {
+        mv = fabs(b[comp * 3 + a]);
+        ma = a;
+      }
+    if (b[comp * 3 + ma] < 0)
+      for (int a = 0; a < 3; ++a) b[comp * 3 + a] = -b[comp * 3 + a];
+  }
+  for (int k = 0; k < 6; ++k) basis_out[k] = b[k];
+  const double c0 = b[1] * b[5] - b[2] * b[4];
+  const double c1 = b[2] * b[3] - b[0] * b[5];
+  const double c2 = b[0] * b[4] - b[1] * b[3];
+  for (int k = 0; k < 6; ++k) V[k] = (float)b[k];
+  V[6] = (float)c0;
+  V[7] = (float)c1;
+  V[8] = (float)c2;
+}
+
+// B[s] = x_s . basis^T, uncentred (SVDPreprocessKernels.cu:142-165).
+__global__ void k_plane_projectB(const float* uvw, const float* freqs, size_t rows, size_t chans,
+                                 const double* basis, float* B) {
+  const size_t ns = rows * chans;
+  for (size_t s = blockIdx.x * (size_t)kThreads + threadIdx.x; s < ns;
+       s += (size_t)gridDim.x * kThreads) {
+    double x[3];
+    sample_lambda(uvw, freqs, rows, s, x);
+    B[2 * s + 0] = (float)(x[0] * basis[0] + x[1] * basis[1] + x[2] * basis[2]);
+    B[2 * s + 1] = (float)(x[0] * basis[3] + x[1] * basis[4] + x[2] * basis[5]);
+  }
+}
+
+// SVDPreprocessKernels.cu:208-237.
+__global__ void k_collapse(const float* v0r, const float* v0i, const float* v3r, const float* v3i,
+                           const unsigned char* f0, const unsigned char* f3, const float* w0,
+                           const float* w3, float* out_re, float* out_im, size_t ns) {
+  for (size_t s = blockIdx.x * (size_t)kThreads + threadIdx.x; s < ns;
+       s += (size_t)gridDim.x * kThreads) {
+    const float a = f0[s] ? 0.0f : w0[s];
+    const float b = f3[s] ? 0.0f : w3[s];
+    const float ws = a + b;
+    if (ws > 0.0f) {
+      out_re[s] = (v0r[s] * a + v3r[s] * b) / ws;
+      out_im[s] = (v0i[s] * a + v3i[s] * b) / ws;
+    } else {
+      out_re[s] = 0.0f;
+      out_im[s] = 0.0f;
+    }
+  }
+}
+
+// Per-snapshot max-abs of the visibilities (as float bits, values >= 0).
+__global__ void k_maxabs(const float* vr, const float* vi, size_t nb, unsigned* out) {
+  float m = 0.f;
+  for (size_t k = blockIdx.x * (size_t)kThreads + threadIdx.x; k < nb;
+       k += (size_t)gridDim.x * kThreads)
+    m = fmaxf(m, fmaxf(fabsf(vr[k]), fabsf(vi[k])));
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+// Scaled storage: the maximum maps to 2^14 (FP16 keeps 2^-24..65504), the
+// stored value is v / scale and the gridder multiplies by scale.
+template <int VT>
+__global__ void k_quantize(const float* vr, const float* vi, size_t nb, void* qr, void* qi,
+                           float* scale_io) {
+  const float mx = scale_io[0];  // max-abs bits written by k_maxabs
+  const float scale = mx > 0.f ? mx / 16384.0f : 1.0f;
+  const float inv = 1.0f / scale;
+  for (size_t k = blockIdx.x * (size_t)kThreads + threadIdx.x; k < nb;
+       k += (size_t)gridDim.x * kThreads) {
+    if (VT == FIP_VIS_F16) {
+      reinterpret_cast<__half*>(qr)[k] = __float2half_rn(vr[k] * inv);
+      reinterpret_cast<__half*>(qi)[k] = __float2half_rn(vi[k] * inv);
+    } else {
+      reinterpret_cast<__nv_bfloat16*>(qr)[k] = __float2bfloat16_rn(vr[k] * inv);
+      reinterpret_cast<__nv_bfloat16*>(qi)[k] = __float2bfloat16_rn(vi[k] * inv);
+    }
+  }
+}
+
+__global__ void k_store_scale(float* scale_io) {
+  const float mx = scale_io[0];
+  scale_io[0] = mx > 0.f ? mx / 16384.0f : 1.0f;
+}
+
+}  // namespace
+
+cudaError_t fip_launch_plane_project(const float* uvw, const float* freqs, size_t rows,
+                                     size_t chans, double* work, float* B, float* V,
+                                     cudaStream_t s) {
+  const size_t ns = rows * chans;
+  const int blocks = (int)std::min<size_t>(kPlaneBlocks, (ns + kThreads - 1) / kThreads);
+  double* w = work;
+  cudaError_t e = cudaSuccess;
+  bool own = false;
+  if (!w) {
+    e = cudaMallocAsync((void**)&w, (size_t)(blocks * 6 + 16) * sizeof(double), s);
+    if (e != cudaSuccess) return e;
+    own = true;
+  }
+  double* partial = w;
+  double* mean = w + blocks * 6;
+  double* cov = mean + 3;
+  double* basis = cov + 6;
+  k_plane_moments<0><<<blocks, kThreads, 0, s>>>(uvw, freqs, rows, chans, nullptr, partial);
+  k_plane_reduce<3><<<1, 32, 0, s>>>(partial, blocks, 1.0 / (double)ns, mean);
+  k_plane_moments<1><<<blocks, kThreads, 0, s>>>(uvw, freqs, rows, chans, mean, partial);
+  k_plane_reduce<6><<<1, 32, 0, s>>>(partial, blocks, 1.0, cov);
+  k_plane_basis<<<1, 32, 0, s>>>(cov, basis, V);
+  k_plane_projectB<<<blocks, kThreads, 0, s>>>(uvw, freqs, rows, chans, basis, B);
+  e = cudaGetLastError();
+  if (own) {
+    cudaError_t e2 = cudaFreeAsync(w, s);
+    if (e == cudaSuccess) e = e2;
+  }
+  return e;
+}
+
+cudaError_t fip_launch_collapse(const float* v0r, const float* v0i, const float* v3r,
+                                const float* v3i, const unsigned char* f0,
+                                const unsigned char* f3, const float* w0, const float* w3,
+                                float* out_re, float* out_im, size_t ns, cudaStream_t s) {
+  const int blocks = (int)std::min<size_t>(4 * 148, (ns + kThreads - 1) / kThreads + 1);
+  k_collapse<<<blocks, kThreads, 0, s>>>(v0r, v0i, v3r, v3i, f0, f3, w0, w3, out_re, out_im, ns);
+  return cudaGetLastError();
+}
+
+cudaError_t fip_launch_quantize(const float* vr, const float* vi, size_t nb, int vis_type,
+                                void* out_re, void* out_im, float* scale_out, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(scale_out, 0, sizeof(float), s);
+  if (e != cudaSuccess) return e;
+  const int blocks = (int)std::min<size_t>(4 * 148, (nb + kThreads - 1) / kThreads + 1);
+  k_maxabs<<<blocks, kThreads, 0, s>>>(vr, vi, nb, reinterpret_cast<unsigned*>(scale_out));
+  if (vis_type == FIP_VIS_F16)
+    k_quantize<FIP_VIS_F16><<<blocks, kThreads, 0, s>>>(vr, vi, nb, out_re, out_im, scale_out);
+  else
+    k_quantize<FIP_VIS_BF16><<<blocks, kThreads, 0, s>>>(vr, vi, nb, out_re, out_im, scale_out);
+  k_store_scale<<<1, 1, 0, s>>>(scale_out);
+  return cudaGetLastError();
+}

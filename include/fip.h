@@ -1,0 +1,176 @@
+/*
+ * fip.h -- C ABI of the B200-native snapshot imaging + tLISI trigger library
+ * (libfip_b200.so), a drop-in for FastImagingPipe's imaging/trigger path.
+ *
+ * All functions return 0 (FIP_OK) on success or a fip_status code; the
+ * message of the last failure on the calling thread is fip_last_error().
+ * Device pointers are plain CUDA device addresses; `stream` is a cudaStream_t
+ * (NULL = the legacy default stream).  No torch types cross this boundary.
+ */
+#ifndef FIP_B200_H
+#define FIP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+/*
+ * Drop-in replacement of the reference entry point, same C++ signature and
+ * therefore the same linker symbol (_Z6FIpipePfS_S_S_S_mmmfm on x86-64).
+ * Replaces: int FIpipe(...) declared at pipe_interface.cpp:8, defined at
+ * FIPkernels.cu:554-557.
+ * Inputs are caller-owned host arrays, snapshot-concatenated:
+ *   Visreal, Visimag [num_snapshots * num_baselines]
+ *   Bin              [num_snapshots * num_baselines * 2]  (row-major pairs)
+ *   Vin              [num_snapshots * 9]                  (row-major 3x3)
+ * result_array       [(image_size / unit_size)^2], row-major tLISI matrix.
+ * As in the reference, the first three snapshots are imaged and their tLISI
+ * computed (FIPkernels.cu:647, 806-851).  Returns 0 on success; unlike the
+ * reference (which always returns 0, FIPkernels.cu:861) a failure returns a
+ * fip_status code.  Inputs are never written (the reference copies them too).
+ */
+int FIpipe(float* Visreal, float* Visimag, float* Bin, float* Vin, float* result_array,
+           size_t num_baselines, size_t image_size, size_t num_snapshots, float cell_size,
+           size_t unit_size);
+extern "C" {
+#endif
+
+typedef enum {
+  FIP_OK = 0,
+  FIP_ERR_ARG = 1,         /* invalid argument or unsupported size */
+  FIP_ERR_CUDA = 2,        /* CUDA runtime error */
+  FIP_ERR_CUFFT = 3,       /* cuFFT error */
+  FIP_ERR_NOMEM = 4,       /* device or pinned allocation failed */
+  FIP_ERR_BUDGET = 5,      /* request exceeds the configured HBM budget */
+  FIP_ERR_NOT_READY = 6,   /* no result available yet */
+  FIP_ERR_STATE = 7        /* call out of order / object in an error state */
+} fip_status;
+
+/* Numerical form of an imager. */
+typedef enum {
+  /* Reference-faithful FP32: the reference's arithmetic (fast-math FP32
+   * pixel mapping, FP32 sums), B200 data movement. */
+  FIP_FORM_PLAIN = 0,
+  /* Precision form: exact closed-form reprojection, compensated FP32 grid
+   * and tLISI sums, FP64 tLISI combine; visibility storage per vis_storage. */
+  FIP_FORM_PRECISE = 1
+} fip_form;
+
+typedef enum { FIP_STORE_F32 = 0, FIP_STORE_F16 = 1, FIP_STORE_BF16 = 2 } fip_vis_storage;
+
+const char* fip_last_error(void);
+const char* fip_status_string(int status);
+/* Library version "major.minor.patch". */
+const char* fip_version(void);
+
+/*
+ * Status-returning variant of FIpipe with the same arguments (const inputs).
+ * Replaces FIPkernels.cu:554-862 for callers that check errors.
+ */
+int fip_pipe(const float* vis_re, const float* vis_im, const float* B, const float* V,
+             float* result, size_t num_baselines, size_t image_size, size_t num_snapshots,
+             float cell_size, size_t unit_size);
+
+/* ------------------------------------------------------------------------ */
+/* Imager: persistent device state for one image size (no per-call allocs). */
+/* ------------------------------------------------------------------------ */
+typedef struct fip_imager fip_imager;
+
+typedef struct {
+  size_t image_size;     /* N: image side; multiple of 4 */
+  size_t max_baselines;  /* capacity: visibilities per snapshot */
+  size_t unit_size;      /* T: trigger tile side (0 = no trigger) */
+  float cell_size;       /* radians per pixel */
+  int form;              /* fip_form */
+  int vis_storage;       /* fip_vis_storage (precision form only) */
+  int device;            /* CUDA device ordinal */
+  int reproject;         /* 0 = tile gather (default), 1 = source scatter */
+} fip_imager_config;
+
+int fip_imager_create(fip_imager** out, const fip_imager_config* cfg);
+int fip_imager_destroy(fip_imager* im);
+/* Bytes of device memory the imager holds. */
+size_t fip_imager_device_bytes(const fip_imager* im);
+
+/*
+ * Images one snapshot (device inputs): vis_re/vis_im [nb] FP32, B [nb*2],
+ * V [9] -> image [N*N] (device, row-major) and, if image_max is not NULL,
+ * max(0, max(image)) as a device float.  Stages: per-snapshot uv binning,
+ * binned gridding, in-place C2R FFT, fused correction + reprojection.
+ * Replaces the per-snapshot body of FIPkernels.cu:665-711.
+ */
+int fip_image_snapshot(fip_imager* im, const float* vis_re, const float* vis_im, const float* B,
+                       const float* V, size_t nb, float* image, float* image_max, void* stream);
+
+/*
+ * tLISI of three consecutive images (device): maxima max3 [3] as produced by
+ * fip_image_snapshot, result [U*U].  The inputs are not modified (the
+ * reference clamps I2 in place, FIPkernels.cu:836; the clamp here is local).
+ * Replaces FIPkernels.cu:806-851.
+ */
+int fip_trigger(fip_imager* im, const float* I1, const float* I2, const float* I3,
+                const float* max3, float* result, void* stream);
+
+/*
+ * FIpipe on device buffers with the imager's persistent state: snapshots
+ * 0..2 of the concatenated device inputs -> result [U*U] (device).  The
+ * three images and their maxima stay in the imager (fip_imager_image).
+ */
+int fip_pipe_device(fip_imager* im, const float* vis_re, const float* vis_im, const float* B,
+                    const float* V, size_t nb, float* result, void* stream);
+/* Device pointer to image k (0..2) of the last fip_pipe_device call. */
+const float* fip_imager_image(const fip_imager* im, int k);
+
+/*
+ * FIpipe through an imager with host buffers (pinned staging owned by the
+ * imager, copies overlapped with compute): the public e2e call.
+ */
+int fip_pipe_host(fip_imager* im, const float* vis_re, const float* vis_im, const float* B,
+                  const float* V, size_t nb, size_t num_snapshots, float* result);
+
+/* Per-pixel targets (LL, MM) of the reprojection, [N*N][2] (device), for
+ * tests: exact = 0 the plain form's FP32 chain, 1 the exact closed form. */
+int fip_pixel_targets(fip_imager* im, const float* V, float* out, int exact, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Plane projection and visibility preparation                               */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * Plane fit of one snapshot on the device: uvw [rows*3] metres, freqs
+ * [chans] Hz -> B [rows*chans*2] (sample s = row + chan*rows), V [9].
+ * FP64 mean/covariance/3x3 eigensolve, FP32 outputs.  Replaces
+ * preprocess_measurement_set_gpu's projection (SVDPreprocessKernels.cu:
+ * 304-425, SVDPreprocessGpu.h:46-49).  Synchronous on `stream`'s work only.
+ */
+int fip_plane_project(const float* uvw, const float* freqs, size_t rows, size_t chans, float* B,
+                      float* V, void* stream);
+
+/*
+ * Flag/weight Stokes-I collapse (device): weighted mean of polarisations 0
+ * and 3, 0 when both weights vanish.  Replaces collapse_visibility_kernel
+ * (SVDPreprocessKernels.cu:208-237).
+ */
+int fip_collapse_visibilities(const float* v0r, const float* v0i, const float* v3r,
+                              const float* v3i, const uint8_t* f0, const uint8_t* f3,
+                              const float* w0, const float* w3, float* out_re, float* out_im,
+                              size_t ns, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Batched stream of snapshots of one beam (precision/batching form).        */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * Images S consecutive snapshots of one beam in one call and returns the
+ * S-2 sliding-window tLISI matrices (triples k, k+1, k+2).  vis_re/vis_im
+ * [S*nb_stride], B [S*nb_stride*2], V [S*9], nb [S] (host array: per-snapshot
+ * visibility counts <= nb_stride) -> results [(S-2)*U*U] (device).
+ */
+int fip_image_sequence(fip_imager* im, const float* vis_re, const float* vis_im, const float* B,
+                       const float* V, const size_t* nb, size_t nb_stride, size_t num_snapshots,
+                       float* results, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FIP_B200_H */
