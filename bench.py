@@ -1,0 +1,417 @@
+#!/usr/bin/env python
+"""Benchmark of the snapshot imaging + tLISI trigger path on B200.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+Workload (one "step"): the reference shape -- 3 snapshots of 130,816
+baselines imaged at 4096 x 4096 (grid 6144, cell 7.2722e-6 rad) and their
+128 x 128 tLISI matrix (tile 32), i.e. one FIpipe call (FIPkernels.cu:554).
+Inputs are seeded synthetic snapshots with the benchmark's layout, sky and
+noise (fastimagingpipe_b200.synthetic.config_reference).
+
+Prints ONE JSON line.  `value` is snapshots/s of the plain FP32 form
+(reference-faithful arithmetic) with inputs resident in HBM, timed with CUDA
+events around each step (L2 flushed between steps, flush untimed), summed
+over the K steps, max over ranks.  `e2e` is the same metric through the
+drop-in FIpipe call with host buffers (host->device copies and the result
+read-back inside the timed region).  Multi-GPU: one independent beam per
+rank (no data-path collective), weak scaling.
+
+`--impl reference` runs the reference's own implementation of the path, the
+unmodified FIpipe of its FIPkernels.cu recompiled for sm_100a
+(oracle/_ref/libfipref.so, built by `make -C oracle ref`), on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = ("snapshots/s at 4096², 130816 bl, tLISI ≤1e-4 vs FP64 (vs plain FP32); "
+          "p99 latency")
+UNIT = "snapshots/s"
+SNAPS_PER_STEP = 3
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.dev)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(snap):
+    """The FP64 CPU oracle on one full step (3 snapshots + tLISI), all host
+    threads; returns (line, oracle tLISI)."""
+    import oracle
+    oracle.lib()
+    t0 = time.perf_counter()
+    res, _, _ = oracle.fipipe(snap, "f64")
+    dt = time.perf_counter() - t0
+    return ({"value": SNAPS_PER_STEP / dt, "unit": UNIT, "cores": oracle.num_threads(),
+             "kind": "port",
+             "sample": "one full step (3 snapshots at 4096^2, 130,816 baselines, tile 32) of "
+                       "the FP64 OpenMP CPU restatement (oracle/fip_oracle.c)",
+             "seconds": dt}, res)
+
+
+def algorithmic_bytes(stage, n, nb, band, t):
+    """Algorithmic bytes of one launch of a stage (the minimum it must move)."""
+    k1, k2 = band
+    u = n // t
+    if stage == "reproject":
+        return n * n * (4 + 8 + 4)      # pre + targets read, image written
+    if stage == "fft_rows":
+        return (k2 + 1) * n * 8 + n * n * 4
+    if stage == "fft_cols":
+        return (2 * k1 + 1) * (k2 + 1) * 8 + (k2 + 1) * n * 8
+    if stage == "targets":
+        return n * n * 8
+    if stage == "trigger":
+        return 3 * n * n * 4 + u * u * 4
+    if stage == "grid":
+        return nb * 16 + (2 * k1 + 1) * (k2 + 1) * 8
+    if stage == "bin":
+        return 2 * nb * 8
+    return None
+
+
+def run_reference(args, rank):
+    line = {"impl": "reference", "metric": METRIC, "unit": UNIT, "higher_is_better": True}
+    if rank != 0:
+        return None
+    from oracle import reference as ref
+    if not ref.available():
+        line["unavailable"] = "oracle/_ref/libfipref.so not built (make -C oracle ref)"
+        return line
+    from fastimagingpipe_b200 import synthetic
+    snap = synthetic.config_reference()
+    for _ in range(args.warmup):
+        ref.fipipe(snap)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ref.fipipe(snap)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = SNAPS_PER_STEP * args.steps / total
+    nb = snap.num_baselines
+    line.update({
+        "value": value, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded benchmark layout, sky and noise)",
+        "config": {"workload": "FIpipe: 3 snapshots x 130,816 baselines at 4096^2, tile 32",
+                   "image_size": 4096, "baselines": nb, "tile": 32, "snapshots_per_step": 3},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": "unmodified reference FIpipe (FIPkernels.cu) recompiled for "
+                                   "sm_100a, called with host buffers; one host thread drives "
+                                   "the GPU"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "latency_ms": {"p50": 1e3 * float(np.percentile(times, 50)),
+                       "p99": 1e3 * float(np.percentile(times, 99))},
+    })
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the extra forms")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = _env_int("RANK", 0)
+    world = _env_int("WORLD_SIZE", 1)
+    local = _env_int("LOCAL_RANK", 0)
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    if args.impl == "reference":
+        line = run_reference(args, rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    import fastimagingpipe_b200 as fip
+    from fastimagingpipe_b200 import synthetic
+
+    dev = torch.device("cuda", local)
+    snap = synthetic.config_reference(seed=1 + rank)
+    n, nb, t, cell = snap.image_size, snap.num_baselines, snap.unit_size, snap.cell_size
+    u = n // t
+    d = {k: torch.tensor(getattr(snap, k), device=dev) for k in ("vis_re", "vis_im", "B", "V")}
+    result = torch.zeros(u * u, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    im = fip.Imager(n, nb, cell, t, device=local)
+
+    def step():
+        im.pipe_device(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, result, stream=stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+
+    # ---- device-resident timing (plain FP32 form) ----
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = im.kernel_launches
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.zero_()  # write 256 MB (> 126 MB L2) between steps, untimed
+            starts[k].record(stream)
+            step()
+            ends[k].record(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    launches = im.kernel_launches - launches0
+    step_ms = [starts[k].elapsed_time(ends[k]) for k in range(args.steps)]
+    total_s = sum(step_ms) / 1e3
+    if dist is not None:
+        tt = torch.tensor([total_s], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_s = float(tt.item())
+    value = world * SNAPS_PER_STEP * args.steps / total_s
+
+    # ---- per-stage device times (roofline of the dominant kernel) ----
+    im.set_profiling(True)
+    with torch.cuda.stream(stream):
+        for _ in range(max(5, min(args.steps, 20))):
+            flush.zero_()
+            step()
+    torch.cuda.synchronize()
+    stages = im.stage_times()
+    im.set_profiling(False)
+    band = im.band()
+
+    # ---- end-to-end through the drop-in FIpipe (host buffers) ----
+    for _ in range(2):
+        fip.FIpipe(snap.vis_re, snap.vis_im, snap.B, snap.V, nb, n, 3, cell, t)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    e2e_steps = max(3, min(args.steps, 50))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_res = fip.FIpipe(snap.vis_re, snap.vis_im, snap.B, snap.V, nb, n, 3, cell, t)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        tt = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e_value = world * SNAPS_PER_STEP * e2e_steps / e2e_s
+    clk = clocks.stop()
+    h2d = SNAPS_PER_STEP * nb * (4 + 4 + 8) + SNAPS_PER_STEP * 9 * 4
+    d2h = u * u * 4
+
+    line = None
+    if rank == 0:
+        # Dominant HBM-bound kernel and its roofline (the reference-chain
+        # pixel mapping, k_targets, is bound by the SFU/conversion pipe, not
+        # by memory; it is reported beside it).
+        per_launch = {k: (ms / c if c else 0.0, c) for k, (ms, c) in stages.items()}
+        hbm_stages = [k for k in per_launch if per_launch[k][1] > 0 and k != "targets"]
+        dom = max(hbm_stages, key=lambda k: per_launch[k][0] * per_launch[k][1])
+        dom_ms = per_launch[dom][0]
+        alg = algorithmic_bytes(dom, n, nb, band, t)
+        peaks_path = os.path.join(REPO, "MEASURED_PEAKS.json")
+        peak, peak_src = 6650.0, "fallback"
+        if os.path.exists(peaks_path):
+            with open(peaks_path) as f:
+                peak, peak_src = float(json.load(f)["hbm_gbs"]), "measured"
+        achieved = alg / (dom_ms * 1e-3) / 1e9 if alg and dom_ms > 0 else None
+        traffic = None
+        tpath = os.path.join(REPO, "profiles", "dram_traffic.json")
+        if os.path.exists(tpath):
+            with open(tpath) as f:
+                traffic = json.load(f).get(dom)
+        roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
+                    "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                    "traffic": traffic, "peak_source": peak_src,
+                    "algorithmic_bytes_per_launch": alg, "avg_launch_ms": dom_ms,
+                    "compute_bound_kernel": {
+                        "kernel": "targets", "bound": "sfu/conversion pipe",
+                        "avg_launch_ms": per_launch.get("targets", (None,))[0]}}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded 512-antenna layout, 20-source sky + transient, noise 0.1)",
+            "config": {"workload": "FIpipe: 3 snapshots x 130,816 baselines at 4096^2 "
+                                   "(grid 6144), tile 32 -> 128x128 tLISI",
+                       "image_size": n, "baselines": nb, "tile": t, "snapshots_per_step": 3,
+                       "form": "plain FP32 (reference-faithful)",
+                       "l2": "flushed (256 MB write) between timed steps, flush untimed",
+                       "parallelism": f"{world} independent beam(s), one per GPU"},
+            "latency_ms": {"p50": float(np.percentile(step_ms, 50)),
+                           "p99": float(np.percentile(step_ms, 99))},
+            "clocks": clk,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "path": "FIpipe (C ABI drop-in) with host numpy buffers"},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "stages_ms_per_launch": {k: v[0] for k, v in per_launch.items() if v[1]},
+            "stages_note": "measured serialised (profiling run), per launch",
+            "uv_band": {"max_row": band[0], "max_col": band[1], "grid": im.grid_side},
+        }
+    # ---- extra forms (rank 0) ----
+    forms = {}
+    if rank == 0 and not args.no_forms:
+        for name, kw in (("precise_f16", dict(form=fip.FORM_PRECISE, vis_storage=fip.STORE_F16)),
+                         ("precise_f32", dict(form=fip.FORM_PRECISE, vis_storage=fip.STORE_F32))):
+            im2 = fip.Imager(n, nb, cell, t, device=local, **kw)
+            res2 = torch.zeros(u * u, device=dev)
+            with torch.cuda.stream(stream):
+                for _ in range(3):
+                    im2.pipe_device(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, res2,
+                                    stream=stream)
+            torch.cuda.synchronize()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            reps = 20
+            with torch.cuda.stream(stream):
+                ev0.record(stream)
+                for _ in range(reps):
+                    im2.pipe_device(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, res2,
+                                    stream=stream)
+                ev1.record(stream)
+            torch.cuda.synchronize()
+            forms[name] = {"value": SNAPS_PER_STEP * reps / (ev0.elapsed_time(ev1) / 1e3),
+                           "unit": UNIT, "tlisi": res2.cpu().numpy().reshape(u, u)}
+            im2.close()
+        # Streaming sequence: each new snapshot yields a sliding-window tLISI.
+        S = 30
+        vre = torch.cat([d["vis_re"]] * 10)
+        vim = torch.cat([d["vis_im"]] * 10)
+        Bs = torch.cat([d["B"]] * 10)
+        Vs = torch.cat([d["V"]] * 10)
+        seq_res = torch.zeros((S - 2) * u * u, device=dev)
+        nbs = np.full(S, nb, np.uint64)
+        with torch.cuda.stream(stream):
+            im.image_sequence(vre, vim, Bs, Vs, nbs, nb, seq_res, stream=stream)
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            im.image_sequence(vre, vim, Bs, Vs, nbs, nb, seq_res, stream=stream)
+            ev1.record(stream)
+        torch.cuda.synchronize()
+        forms["sequence_plain"] = {
+            "value": S / (ev0.elapsed_time(ev1) / 1e3), "unit": UNIT,
+            "note": "30 snapshots, sliding-window tLISI per snapshot (28 matrices)"}
+
+    # ---- CPU baseline and FP64 errors (rank 0, N = 1) ----
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb, ref64 = cpu_baseline(snap)
+        line["cpu_baseline"] = cb
+        plain = result.cpu().numpy().reshape(u, u)
+        line["tlisi_error_vs_fp64"] = {"plain": float(np.abs(plain - ref64).max())}
+        for name in ("precise_f16", "precise_f32"):
+            if name in forms:
+                line["tlisi_error_vs_fp64"][name] = float(
+                    np.abs(forms[name]["tlisi"] - ref64).max())
+        line["tlisi_error_vs_fp64"]["max_1_minus_tlisi_fp64"] = float((1 - ref64).max())
+    if line is not None:
+        for f in forms.values():
+            f.pop("tlisi", None)
+        if forms:
+            line["forms"] = forms
+        print(json.dumps(line), flush=True)
+    im.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

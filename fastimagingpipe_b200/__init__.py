@@ -76,6 +76,16 @@ def lib() -> ctypes.CDLL:
         L.fip_plane_project.argtypes = [vp, vp, sz, sz, vp, vp, vp]
         L.fip_collapse_visibilities.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]
         L.fip_image_sequence.argtypes = [vp, vp, vp, vp, vp, vp, sz, sz, vp, vp]
+        L.fip_imager_set_profiling.argtypes = [vp, ctypes.c_int]
+        L.fip_imager_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_double),
+                                             ctypes.POINTER(ctypes.c_long), ctypes.c_int]
+        L.fip_stage_name.argtypes = [ctypes.c_int]
+        L.fip_stage_name.restype = ctypes.c_char_p
+        L.fip_stage_count.restype = ctypes.c_int
+        L.fip_imager_kernel_launches.argtypes = [vp]
+        L.fip_imager_kernel_launches.restype = ctypes.c_ulonglong
+        L.fip_imager_band.argtypes = [vp, ctypes.POINTER(ctypes.c_uint), ctypes.POINTER(ctypes.c_uint)]
+        L.fip_imager_grid_side.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -162,6 +172,32 @@ class Imager:
     @property
     def device_bytes(self) -> int:
         return int(lib().fip_imager_device_bytes(self._h))
+
+    def set_profiling(self, enable: bool = True):
+        """Per-stage device timing with CUDA events (resets the totals)."""
+        _check(lib().fip_imager_set_profiling(self._h, int(enable)))
+
+    def stage_times(self) -> dict:
+        """{stage: (total_ms, launches)} accumulated since set_profiling(True)."""
+        n = int(lib().fip_stage_count())
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_long * n)()
+        _check(lib().fip_imager_stage_times(self._h, ms, cnt, n))
+        return {lib().fip_stage_name(k).decode(): (ms[k], cnt[k]) for k in range(n)}
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(lib().fip_imager_kernel_launches(self._h))
+
+    @property
+    def grid_side(self) -> int:
+        return int(lib().fip_imager_grid_side(self._h))
+
+    def band(self):
+        """(max |r1|, max half-plane column) of the last gridded snapshot."""
+        a, b = ctypes.c_uint(), ctypes.c_uint()
+        _check(lib().fip_imager_band(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return int(a.value), int(b.value)
 
     def image_snapshot(self, vis_re, vis_im, B, V, nb: int, image, image_max=None, stream=None):
         _check(lib().fip_image_snapshot(self._h, _ptr(vis_re), _ptr(vis_im), _ptr(B), _ptr(V), nb,

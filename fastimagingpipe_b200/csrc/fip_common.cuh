@@ -15,7 +15,7 @@
 
 // Grid tiles used by the binned gridder (cells of the half-plane grid).
 #define FIP_GTILE 64
-#define FIP_GCHUNK 512  // virtual visibilities per gridding work item
+#define FIP_GCHUNK 256  // virtual visibilities per gridding work item
 
 // Geometry of one image size.  The uv grid is the Hermitian half plane
 // G x (G/2+1) complex (row stride hp = G/2+1 complex = G+2 floats), which is
@@ -29,6 +29,8 @@ struct FipGeom {
   int tiles_r; // grid tiles along rows
   int tiles_c; // grid tiles along half-plane columns
   float cell;  // cell size (rad)
+  int layout;  // grid layout: 1 = band, column-major [col][row] (pruned FFT);
+               // 0 = full half plane, row-major (cuFFT C2R fallback)
 };
 
 // Snapshot descriptor for batched launches (device-resident arrays).

@@ -20,6 +20,7 @@
 #include "../../include/fip.h"
 #include "fip_common.cuh"
 #include "fip_kernels.h"
+#include <cmath>
 
 namespace {
 
@@ -72,6 +73,24 @@ cudaError_t dalloc(T** p, size_t count, size_t& total) {
   return cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T));
 }
 
+// Device-side stage timing (optional): an event pair per stage launch,
+// folded into per-stage totals when a call finishes.
+enum Stage {
+  ST_BIN, ST_GRID, ST_FFT_COLS, ST_FFT_ROWS, ST_TARGETS, ST_REPROJECT, ST_TRIGGER, ST_COUNT
+};
+const char* kStageNames[ST_COUNT] = {"bin",     "grid",      "fft_cols", "fft_rows",
+                                     "targets", "reproject", "trigger"};
+constexpr int kMaxPending = 64;
+
+struct StageTimer {
+  bool on = false;
+  cudaEvent_t ev[kMaxPending][2] = {};
+  int stage[kMaxPending] = {};
+  int pending = 0;
+  double total_ms[ST_COUNT] = {};
+  long count[ST_COUNT] = {};
+};
+
 }  // namespace
 
 struct fip_imager {
@@ -82,9 +101,17 @@ struct fip_imager {
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_copied[3] = {nullptr, nullptr, nullptr};
   cudaEvent_t ev_used[3] = {nullptr, nullptr, nullptr};
-  cufftHandle plan = 0;
+  cudaStream_t side = nullptr;       // pixel-mapping stream (overlaps gridding + FFT)
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cufftHandle plan = 0;              // cuFFT C2R fallback (grid side not 3 * 2^k)
   bool plan_ok = false;
-  float2* grid = nullptr;            // G x (G/2+1) complex; in-place C2R output
+  bool custom_fft = false;           // band-pruned FFT (fip_fft.cuh)
+  fipfft::Plan fft{};
+  float2* twiddles = nullptr;        // e^{+2 pi i k / G}, k < G
+  float2* colbuf = nullptr;          // column-pass output [G/2+1][N]
+  float* pre = nullptr;              // corrected pre-reprojection image [N*N]
+  float2* targets = nullptr;         // reference pixel mapping [N*N]
+  float2* grid = nullptr;            // uv grid (band layout, or C2R in place)
   float* taper = nullptr;            // N/2 + 1
   FipBins bins{};
   float* images[3] = {nullptr, nullptr, nullptr};
@@ -105,16 +132,64 @@ struct fip_imager {
   float* h_B = nullptr;
   float* h_V = nullptr;
   float* h_result = nullptr;
+  StageTimer timer;
+  unsigned long long launches = 0;   // kernels launched by this imager
+  // Calls may come on different streams; each call's stream first waits for
+  // the previous call's work (the imager's buffers are shared).
+  cudaEvent_t ev_done = nullptr;
+  bool done_recorded = false;
 };
+
+namespace {
+// Orders a call on stream s after every earlier call of the imager.
+int call_enter(fip_imager* im, cudaStream_t s) {
+  if (im->done_recorded) FIP_CUDA(cudaStreamWaitEvent(s, im->ev_done, 0));
+  return FIP_OK;
+}
+int call_leave(fip_imager* im, cudaStream_t s) {
+  FIP_CUDA(cudaEventRecord(im->ev_done, s));
+  im->done_recorded = true;
+  return FIP_OK;
+}
+
+// Opens a timed stage on stream s (no-op unless profiling is on).
+int stage_begin(fip_imager* im, int st, cudaStream_t s) {
+  StageTimer& t = im->timer;
+  if (!t.on || t.pending >= kMaxPending) return -1;
+  const int k = t.pending++;
+  t.stage[k] = st;
+  cudaEventRecord(t.ev[k][0], s);
+  return k;
+}
+void stage_end(fip_imager* im, int k, cudaStream_t s) {
+  if (k >= 0) cudaEventRecord(im->timer.ev[k][1], s);
+}
+// Folds finished stage timings into the totals (synchronises their events).
+void stage_collect(fip_imager* im) {
+  StageTimer& t = im->timer;
+  for (int k = 0; k < t.pending; ++k) {
+    float ms = 0.f;
+    cudaEventSynchronize(t.ev[k][1]);
+    if (cudaEventElapsedTime(&ms, t.ev[k][0], t.ev[k][1]) == cudaSuccess) {
+      t.total_ms[t.stage[k]] += ms;
+      t.count[t.stage[k]] += 1;
+    }
+  }
+  t.pending = 0;
+}
+}  // namespace
 
 static void imager_free(fip_imager* im) {
   if (!im) return;
   DeviceGuard g(im->cfg.device);
   if (im->stream) cudaStreamSynchronize(im->stream);
   if (im->copy_stream) cudaStreamSynchronize(im->copy_stream);
+  if (im->side) cudaStreamSynchronize(im->side);
   if (im->plan_ok) cufftDestroy(im->plan);
   void* dptrs[] = {im->grid, im->taper, im->bins.count, im->bins.offset, im->bins.cursor,
                    im->bins.entries, im->bins.work, im->bins.nwork, im->bins.bbox,
+                   im->bins.multi, im->bins.nmulti, im->twiddles, im->colbuf, im->pre,
+                   im->targets,
                    im->images[0], im->images[1], im->images[2], im->maxima, im->result,
                    im->stats, im->q_re, im->q_im, im->q_scale, im->d_vr, im->d_vi, im->d_B,
                    im->d_V};
@@ -127,8 +202,15 @@ static void imager_free(fip_imager* im) {
     if (im->ev_copied[k]) cudaEventDestroy(im->ev_copied[k]);
     if (im->ev_used[k]) cudaEventDestroy(im->ev_used[k]);
   }
+  for (int k = 0; k < kMaxPending; ++k)
+    for (int e = 0; e < 2; ++e)
+      if (im->timer.ev[k][e]) cudaEventDestroy(im->timer.ev[k][e]);
+  if (im->ev_done) cudaEventDestroy(im->ev_done);
+  if (im->ev_fork) cudaEventDestroy(im->ev_fork);
+  if (im->ev_join) cudaEventDestroy(im->ev_join);
   if (im->stream) cudaStreamDestroy(im->stream);
   if (im->copy_stream) cudaStreamDestroy(im->copy_stream);
+  if (im->side) cudaStreamDestroy(im->side);
   delete im;
 }
 
@@ -188,6 +270,8 @@ int fip_imager_create(fip_imager** out, const fip_imager_config* cfg) {
   geo.tiles_r = (geo.g + FIP_GTILE - 1) / FIP_GTILE;
   geo.tiles_c = (geo.hp + FIP_GTILE - 1) / FIP_GTILE;
   geo.cell = cfg->cell_size;
+  im->custom_fft = fip_fft_plan(geo.g, im->fft);
+  geo.layout = im->custom_fft ? 1 : 0;
   const size_t n2 = (size_t)geo.n * geo.n;
   const size_t nb = cfg->max_baselines;
   const size_t ntiles = (size_t)geo.tiles_r * geo.tiles_c;
@@ -209,11 +293,21 @@ int fip_imager_create(fip_imager** out, const fip_imager_config* cfg) {
 
   FIP_ALLOC(cudaStreamCreateWithFlags(&im->stream, cudaStreamNonBlocking));
   FIP_ALLOC(cudaStreamCreateWithFlags(&im->copy_stream, cudaStreamNonBlocking));
+  FIP_ALLOC(cudaStreamCreateWithFlags(&im->side, cudaStreamNonBlocking));
+  FIP_ALLOC(cudaEventCreateWithFlags(&im->ev_fork, cudaEventDisableTiming));
+  FIP_ALLOC(cudaEventCreateWithFlags(&im->ev_join, cudaEventDisableTiming));
+  FIP_ALLOC(cudaEventCreateWithFlags(&im->ev_done, cudaEventDisableTiming));
+  for (int k = 0; k < kMaxPending; ++k)
+    for (int e = 0; e < 2; ++e) FIP_ALLOC(cudaEventCreate(&im->timer.ev[k][e]));
   for (int k = 0; k < 3; ++k) {
     FIP_ALLOC(cudaEventCreateWithFlags(&im->ev_copied[k], cudaEventDisableTiming));
     FIP_ALLOC(cudaEventCreateWithFlags(&im->ev_used[k], cudaEventDisableTiming));
   }
   FIP_ALLOC(dalloc(&im->grid, (size_t)geo.g * geo.hp, tot));
+  if (cfg->reproject != 0 && cfg->reproject != 1) return cleanup(fail(FIP_ERR_ARG, "unknown reproject mode"));
+  if (cfg->reproject == 0 && !fip_gather_supported(geo, cfg->form == FIP_FORM_PRECISE))
+    return cleanup(fail(FIP_ERR_ARG, "cell_size too small for the tile-gather reprojection; "
+                                     "use reproject = 1"));
   FIP_ALLOC(dalloc(&im->taper, (size_t)geo.n / 2 + 1, tot));
   im->bins.cap = 12 * nb;
   im->bins.wcap = ntiles + im->bins.cap / FIP_GCHUNK + 1;
@@ -224,6 +318,21 @@ int fip_imager_create(fip_imager** out, const fip_imager_config* cfg) {
   FIP_ALLOC(dalloc(&im->bins.work, im->bins.wcap, tot));
   FIP_ALLOC(dalloc(&im->bins.nwork, 1, tot));
   FIP_ALLOC(dalloc(&im->bins.bbox, 4, tot));
+  FIP_ALLOC(dalloc(&im->bins.multi, ntiles, tot));
+  FIP_ALLOC(dalloc(&im->bins.nmulti, 1, tot));
+  FIP_ALLOC(dalloc(&im->pre, n2, tot));
+  if (cfg->form == FIP_FORM_PLAIN && cfg->reproject == 0) FIP_ALLOC(dalloc(&im->targets, n2, tot));
+  if (im->custom_fft) {
+    FIP_ALLOC(dalloc(&im->colbuf, (size_t)geo.hp * geo.n, tot));
+    FIP_ALLOC(dalloc(&im->twiddles, (size_t)geo.g, tot));
+    std::vector<float2> tw(geo.g);
+    for (int k = 0; k < geo.g; ++k) {
+      const double a = 2.0 * FIP_M_PI * (double)k / (double)geo.g;
+      tw[k] = make_float2((float)cos(a), (float)sin(a));
+    }
+    FIP_ALLOC(cudaMemcpy(im->twiddles, tw.data(), geo.g * sizeof(float2),
+                         cudaMemcpyHostToDevice));
+  }
   for (int k = 0; k < 3; ++k) FIP_ALLOC(dalloc(&im->images[k], n2, tot));
   FIP_ALLOC(dalloc(&im->maxima, 3, tot));
   FIP_ALLOC(dalloc(&im->result, std::max<size_t>((size_t)geo.u * geo.u, 1), tot));
@@ -243,7 +352,7 @@ int fip_imager_create(fip_imager** out, const fip_imager_config* cfg) {
   FIP_ALLOC(cudaMallocHost((void**)&im->h_result,
                            std::max<size_t>((size_t)geo.u * geo.u, 1) * sizeof(float)));
 
-  {
+  if (!im->custom_fft) {
     cufftResult r = cufftCreate(&im->plan);
     if (r != CUFFT_SUCCESS) return cleanup(fail(FIP_ERR_CUFFT, "cufftCreate failed"));
     im->plan_ok = true;
@@ -281,29 +390,78 @@ static int image_snapshot_impl(fip_imager* im, const float* vr, const float* vi,
   const void* gvr = vr;
   const void* gvi = vi;
   int vt = FIP_VIS_F32;
+  int k;
   if (precise && im->cfg.vis_storage != FIP_STORE_F32) {
     vt = im->cfg.vis_storage == FIP_STORE_F16 ? FIP_VIS_F16 : FIP_VIS_BF16;
+    k = stage_begin(im, ST_GRID, s);
     FIP_CUDA(fip_launch_quantize(vr, vi, nb, vt, im->q_re, im->q_im, im->q_scale, s));
+    stage_end(im, k, s);
+    im->launches += 3;
     gvr = im->q_re;
     gvi = im->q_im;
   }
+  const bool gather = im->cfg.reproject == 0;
+  const bool chain_targets = gather && !precise;
+  // The pixel mapping depends on V only: it runs beside gridding + FFT on
+  // the side stream (serialised on s when profiling, so every stage's time
+  // is its own).
+  const bool fork = chain_targets && !im->timer.on;
+  if (chain_targets) {
+    cudaStream_t ts = fork ? im->side : s;
+    if (fork) {
+      FIP_CUDA(cudaEventRecord(im->ev_fork, s));
+      FIP_CUDA(cudaStreamWaitEvent(im->side, im->ev_fork, 0));
+    }
+    k = stage_begin(im, ST_TARGETS, ts);
+    FIP_CUDA(fip_launch_targets(geo, V, im->targets, ts));
+    stage_end(im, k, ts);
+    im->launches += 1;
+    if (fork) FIP_CUDA(cudaEventRecord(im->ev_join, im->side));
+  }
+  k = stage_begin(im, ST_BIN, s);
   FIP_CUDA(fip_launch_bin(geo, B, (int)nb, im->bins, s));
+  stage_end(im, k, s);
+  k = stage_begin(im, ST_GRID, s);
   FIP_CUDA(fip_launch_grid(geo, B, gvr, gvi, vt, im->q_scale, V, (int)nb, im->bins, im->grid,
                            precise ? 1 : 0, s));
-  FIP_CUFFT(cufftSetStream(im->plan, s));
-  FIP_CUFFT(cufftExecC2R(im->plan, reinterpret_cast<cufftComplex*>(im->grid),
-                         reinterpret_cast<cufftReal*>(im->grid)));
-  const float* fft_out = reinterpret_cast<const float*>(im->grid);
+  stage_end(im, k, s);
+  im->launches += 5;  // bin count, scan, bin scatter, zero tiles, grid
+  if (im->custom_fft) {
+    k = stage_begin(im, ST_FFT_COLS, s);
+    FIP_CUDA(fip_launch_fft_cols(geo, im->grid, im->bins.bbox, im->colbuf, im->twiddles,
+                                 im->fft, s));
+    stage_end(im, k, s);
+    k = stage_begin(im, ST_FFT_ROWS, s);
+    FIP_CUDA(fip_launch_fft_rows(geo, im->colbuf, im->bins.bbox, im->taper, im->twiddles,
+                                 im->fft, im->pre, s));
+    im->launches += 2;
+  } else {
+    k = stage_begin(im, ST_FFT_ROWS, s);
+    FIP_CUFFT(cufftSetStream(im->plan, s));
+    FIP_CUFFT(cufftExecC2R(im->plan, reinterpret_cast<cufftComplex*>(im->grid),
+                           reinterpret_cast<cufftReal*>(im->grid)));
+    FIP_CUDA(fip_launch_correct_c2r(geo, reinterpret_cast<const float*>(im->grid), im->taper,
+                                    im->pre, s));
+    im->launches += 1;
+  }
+  stage_end(im, k, s);
   if (image_max) FIP_CUDA(cudaMemsetAsync(image_max, 0, sizeof(float), s));
-  if (im->cfg.reproject == 1 && !precise) {
-    FIP_CUDA(fip_launch_reproject_scatter(geo, fft_out, im->taper, V, (int)nb, image, s));
+  if (!gather) {
+    k = stage_begin(im, ST_REPROJECT, s);
+    FIP_CUDA(fip_launch_reproject_scatter(geo, im->pre, V, (int)nb, image, s));
     if (image_max)
       FIP_CUDA(fip_launch_image_max(image, (size_t)geo.n * geo.n,
                                     reinterpret_cast<unsigned*>(image_max), s));
+    stage_end(im, k, s);
+    im->launches += image_max ? 2 : 1;
   } else {
-    FIP_CUDA(fip_launch_reproject_gather(geo, fft_out, im->taper, V, (int)nb, image,
+    if (fork) FIP_CUDA(cudaStreamWaitEvent(s, im->ev_join, 0));
+    k = stage_begin(im, ST_REPROJECT, s);
+    FIP_CUDA(fip_launch_reproject_gather(geo, im->pre, im->targets, V, (int)nb, image,
                                          reinterpret_cast<unsigned*>(image_max), precise ? 1 : 0,
                                          s));
+    stage_end(im, k, s);
+    im->launches += 1;
   }
   return FIP_OK;
 }
@@ -312,8 +470,10 @@ int fip_image_snapshot(fip_imager* im, const float* vis_re, const float* vis_im,
                        const float* V, size_t nb, float* image, float* image_max, void* stream) {
   if (!im) return fail(FIP_ERR_ARG, "null imager");
   DeviceGuard g(im->cfg.device);
-  return image_snapshot_impl(im, vis_re, vis_im, B, V, nb, image, image_max,
-                             (cudaStream_t)stream);
+  cudaStream_t s = (cudaStream_t)stream;
+  FIP_TRY(call_enter(im, s));
+  FIP_TRY(image_snapshot_impl(im, vis_re, vis_im, B, V, nb, image, image_max, s));
+  return call_leave(im, s);
 }
 
 int fip_trigger(fip_imager* im, const float* I1, const float* I2, const float* I3,
@@ -322,8 +482,14 @@ int fip_trigger(fip_imager* im, const float* I1, const float* I2, const float* I
   if (im->geo.t <= 0) return fail(FIP_ERR_ARG, "imager has no trigger tile (unit_size 0)");
   if (!I1 || !I2 || !I3 || !max3 || !result) return fail(FIP_ERR_ARG, "null device pointer");
   DeviceGuard g(im->cfg.device);
+  FIP_TRY(call_enter(im, (cudaStream_t)stream));
+  const int k = stage_begin(im, ST_TRIGGER, (cudaStream_t)stream);
   FIP_CUDA(fip_launch_trigger(im->geo, I1, I2, I3, max3, im->stats, result,
                               im->cfg.form == FIP_FORM_PRECISE ? 1 : 0, (cudaStream_t)stream));
+  stage_end(im, k, (cudaStream_t)stream);
+  im->launches += 1;
+  FIP_TRY(call_leave(im, (cudaStream_t)stream));
+  if (im->timer.on) stage_collect(im);
   return FIP_OK;
 }
 
@@ -332,14 +498,21 @@ int fip_pipe_device(fip_imager* im, const float* vr, const float* vi, const floa
   if (!im) return fail(FIP_ERR_ARG, "null imager");
   DeviceGuard g(im->cfg.device);
   cudaStream_t s = (cudaStream_t)stream;
+  FIP_TRY(call_enter(im, s));
   for (int k = 0; k < 3; ++k)
     FIP_TRY(image_snapshot_impl(im, vr + (size_t)k * nb, vi + (size_t)k * nb,
                                 B + (size_t)k * nb * 2, V + (size_t)k * 9, nb, im->images[k],
                                 im->maxima + k, s));
-  if (im->geo.t > 0 && result)
+  if (im->geo.t > 0 && result) {
+    const int k = stage_begin(im, ST_TRIGGER, s);
     FIP_CUDA(fip_launch_trigger(im->geo, im->images[0], im->images[1], im->images[2],
                                 im->maxima, im->stats, result,
                                 im->cfg.form == FIP_FORM_PRECISE ? 1 : 0, s));
+    stage_end(im, k, s);
+    im->launches += 1;
+  }
+  FIP_TRY(call_leave(im, s));
+  if (im->timer.on) stage_collect(im);
   return FIP_OK;
 }
 
@@ -357,6 +530,8 @@ int fip_pipe_host(fip_imager* im, const float* vr, const float* vi, const float*
   if (im->geo.t <= 0) return fail(FIP_ERR_ARG, "imager has no trigger tile (unit_size 0)");
   DeviceGuard g(im->cfg.device);
   cudaStream_t s = im->stream, cs = im->copy_stream;
+  FIP_TRY(call_enter(im, s));
+  FIP_TRY(call_enter(im, cs));
   // Per snapshot: host copy into pinned slot k (CPU), async H2D on the copy
   // stream, then the compute stream images it while the CPU stages k+1.
   for (int k = 0; k < 3; ++k) {
@@ -380,21 +555,74 @@ int fip_pipe_host(fip_imager* im, const float* vr, const float* vi, const float*
     FIP_CUDA(cudaStreamWaitEvent(s, im->ev_copied[k], 0));
     FIP_TRY(image_snapshot_impl(im, dvr, dvi, dB, dV, nb, im->images[k], im->maxima + k, s));
   }
-  FIP_CUDA(fip_launch_trigger(im->geo, im->images[0], im->images[1], im->images[2], im->maxima,
-                              im->stats, im->result, im->cfg.form == FIP_FORM_PRECISE ? 1 : 0,
-                              s));
+  {
+    const int k = stage_begin(im, ST_TRIGGER, s);
+    FIP_CUDA(fip_launch_trigger(im->geo, im->images[0], im->images[1], im->images[2],
+                                im->maxima, im->stats, im->result,
+                                im->cfg.form == FIP_FORM_PRECISE ? 1 : 0, s));
+    stage_end(im, k, s);
+    im->launches += 1;
+  }
   const size_t uu = (size_t)im->geo.u * im->geo.u;
   FIP_CUDA(cudaMemcpyAsync(im->h_result, im->result, uu * sizeof(float), cudaMemcpyDeviceToHost,
                            s));
+  FIP_TRY(call_leave(im, s));
   FIP_CUDA(cudaStreamSynchronize(s));
   std::memcpy(result, im->h_result, uu * sizeof(float));
+  if (im->timer.on) stage_collect(im);
   return FIP_OK;
 }
+
+int fip_imager_set_profiling(fip_imager* im, int enable) {
+  if (!im) return fail(FIP_ERR_ARG, "null imager");
+  DeviceGuard g(im->cfg.device);
+  stage_collect(im);
+  im->timer.on = enable != 0;
+  for (int k = 0; k < ST_COUNT; ++k) {
+    im->timer.total_ms[k] = 0.0;
+    im->timer.count[k] = 0;
+  }
+  return FIP_OK;
+}
+
+int fip_imager_stage_times(fip_imager* im, double* total_ms, long* launches, int nstages) {
+  if (!im || !total_ms || !launches) return fail(FIP_ERR_ARG, "null argument");
+  DeviceGuard g(im->cfg.device);
+  stage_collect(im);
+  for (int k = 0; k < nstages && k < ST_COUNT; ++k) {
+    total_ms[k] = im->timer.total_ms[k];
+    launches[k] = im->timer.count[k];
+  }
+  return FIP_OK;
+}
+
+const char* fip_stage_name(int stage) {
+  return (stage >= 0 && stage < ST_COUNT) ? kStageNames[stage] : "";
+}
+
+int fip_stage_count(void) { return ST_COUNT; }
+
+unsigned long long fip_imager_kernel_launches(const fip_imager* im) {
+  return im ? im->launches : 0ull;
+}
+
+int fip_imager_band(fip_imager* im, unsigned* max_row, unsigned* max_col) {
+  if (!im || !max_row || !max_col) return fail(FIP_ERR_ARG, "null argument");
+  DeviceGuard g(im->cfg.device);
+  unsigned b[4] = {0, 0, 0, 0};
+  FIP_CUDA(cudaMemcpy(b, im->bins.bbox, sizeof(b), cudaMemcpyDeviceToHost));
+  *max_row = b[0];
+  *max_col = b[1];
+  return FIP_OK;
+}
+
+int fip_imager_grid_side(const fip_imager* im) { return im ? im->geo.g : 0; }
 
 int fip_pixel_targets(fip_imager* im, const float* V, float* out, int exact, void* stream) {
   if (!im || !V || !out) return fail(FIP_ERR_ARG, "null argument");
   DeviceGuard g(im->cfg.device);
   FIP_CUDA(fip_launch_pixel_targets(im->geo, V, out, exact, (cudaStream_t)stream));
+  im->launches += 1;
   return FIP_OK;
 }
 
@@ -407,6 +635,7 @@ int fip_image_sequence(fip_imager* im, const float* vr, const float* vi, const f
   DeviceGuard g(im->cfg.device);
   cudaStream_t s = (cudaStream_t)stream;
   const size_t uu = (size_t)im->geo.u * im->geo.u;
+  FIP_TRY(call_enter(im, s));
   for (size_t k = 0; k < nsnap; ++k) {
     const int slot = (int)(k % 3);
     FIP_TRY(image_snapshot_impl(im, vr + k * nb_stride, vi + k * nb_stride, B + k * nb_stride * 2,
@@ -415,11 +644,16 @@ int fip_image_sequence(fip_imager* im, const float* vr, const float* vi, const f
       // Ring slots a, b, c hold snapshots k-2, k-1, k.  The combine uses the
       // maximum of the three maxima only, so the maxima keep ring order.
       const int a = (int)((k - 2) % 3), b = (int)((k - 1) % 3), c = slot;
+      const int st = stage_begin(im, ST_TRIGGER, s);
       FIP_CUDA(fip_launch_trigger(im->geo, im->images[a], im->images[b], im->images[c],
                                   im->maxima, im->stats, results + (k - 2) * uu,
                                   im->cfg.form == FIP_FORM_PRECISE ? 1 : 0, s));
+      stage_end(im, st, s);
+      im->launches += 1;
     }
   }
+  FIP_TRY(call_leave(im, s));
+  if (im->timer.on) stage_collect(im);
   return FIP_OK;
 }
 

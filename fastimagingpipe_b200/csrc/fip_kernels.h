@@ -7,6 +7,7 @@
 #include <cuda_bf16.h>
 
 #include "fip_common.cuh"
+#include "fip_fft.cuh"
 
 // Scratch of the tile-binned gridder for one image size.
 struct FipBins {
@@ -16,7 +17,9 @@ struct FipBins {
   unsigned* entries;  // [cap] (vis << 1 | mirrored), grouped by tile
   int4* work;         // [wcap] (tile, begin, end, single-chunk flag)
   unsigned* nwork;    // [1] number of work items
-  unsigned* bbox;     // [4] occupied half-plane rows/cols (precision form)
+  unsigned* bbox;     // [4] occupied band: max |r1|, max half-plane column
+  unsigned* multi;    // [ntiles] tiles split over several work items
+  unsigned* nmulti;   // [1]
   size_t cap;         // capacity of entries
   size_t wcap;        // capacity of work
 };
@@ -30,19 +33,34 @@ cudaError_t fip_launch_bin(const FipGeom& geo, const float* B, int nb, FipBins& 
 cudaError_t fip_launch_grid(const FipGeom& geo, const float* B, const void* vr, const void* vi,
                             int vis_type, const float* vis_scale, const float* V, int nb,
                             const FipBins& bins, float2* grid, int compensated, cudaStream_t s);
+bool fip_fft_plan(int g, fipfft::Plan& p);
+// Band-pruned inverse FFT: column pass (band grid -> colbuf [G/2+1][N]) and
+// row pass with the crop + correction epilogue (colbuf -> pre [N*N]).
+cudaError_t fip_launch_fft_cols(const FipGeom& geo, const float2* grid, const unsigned* bbox,
+                                float2* colbuf, const float2* twiddles, const fipfft::Plan& plan,
+                                cudaStream_t s);
+cudaError_t fip_launch_fft_rows(const FipGeom& geo, const float2* colbuf, const unsigned* bbox,
+                                const float* taper, const float2* twiddles,
+                                const fipfft::Plan& plan, float* pre, cudaStream_t s);
+// Crop + correction of an in-place cuFFT C2R output -> pre [N*N].
+cudaError_t fip_launch_correct_c2r(const FipGeom& geo, const float* fft_out, const float* taper,
+                                   float* pre, cudaStream_t s);
+// The reference's pixel mapping of every source pixel -> targets [N*N].
+cudaError_t fip_launch_targets(const FipGeom& geo, const float* V, float2* targets,
+                               cudaStream_t s);
 // Source-major reprojection: one thread per source pixel, atomics into a
-// zeroed destination (the reference's scheme, with correction fused).
-cudaError_t fip_launch_reproject_scatter(const FipGeom& geo, const float* fft_out,
-                                         const float* taper, const float* V, int nb, float* dst,
-                                         cudaStream_t s);
+// zeroed destination (the reference's scheme).
+cudaError_t fip_launch_reproject_scatter(const FipGeom& geo, const float* pre, const float* V,
+                                         int nb, float* dst, cudaStream_t s);
 // Destination-tile-major reprojection: every destination tile gathers its
 // candidate source pixels, splats in shared memory and is stored once.  Also
 // records the image maximum into *img_max (atomic max, caller zeroes it).
-cudaError_t fip_launch_reproject_gather(const FipGeom& geo, const float* fft_out,
-                                        const float* taper, const float* V, int nb, float* dst,
+bool fip_gather_supported(const FipGeom& geo, int exact_targets);
+cudaError_t fip_launch_reproject_gather(const FipGeom& geo, const float* pre,
+                                        const float2* targets, const float* V, int nb, float* dst,
                                         unsigned* img_max, int exact_targets, cudaStream_t s);
 cudaError_t fip_launch_image_max(const float* img, size_t count, unsigned* out, cudaStream_t s);
-// Trigger: per-tile statistics of (I1, I2, I3) then the tLISI combine.
+// Trigger: per-tile statistics of (I1, I2, I3) and the tLISI combine.
 cudaError_t fip_launch_trigger(const FipGeom& geo, const float* I1, const float* I2,
                                const float* I3, const float* max3, float* stats,
                                float* result, int precise, cudaStream_t s);

@@ -2,18 +2,22 @@
 //
 // This translation unit is compiled with --use_fast_math, the flags of the
 // reference's CUDA build (reference Makefile:13), because the plain FP32 form
-// reproduces the reference's FP32 arithmetic (see fip_refmath.cuh).  Data
+// reproduces the reference's FP32 arithmetic (fip_refmath.cuh).  Data
 // movement is B200-native:
 //   * gridding bins every visibility by 64x64 tile of the Hermitian half-plane
-//     grid, accumulates each tile in shared memory and commits it once (plain
-//     128-bit stores for tiles owned by one work item, vector reductions only
-//     for the few dense tiles split over several);
-//   * the FFT is one in-place C2R transform (half the data of the reference's
-//     C2C) and the crop/checkerboard/correction pass is fused into the
-//     reprojection's source loads;
-//   * reprojection is destination-tile-major: each 32x32 output tile gathers
-//     its candidate source pixels, splats them in shared memory, stores the
-//     tile once and reports its maximum -- no global atomics, no memsets;
+//     uv grid, prefetches each work item's visibilities into shared memory,
+//     accumulates the tile there and commits it once (plain stores for tiles
+//     owned by one work item, vector reductions for the few dense tiles split
+//     over several); only tiles inside the occupied uv band are written;
+//   * the 2-D inverse FFT is band-pruned: column transforms run only over the
+//     occupied half-plane columns and keep only the N needed outputs; row
+//     transforms pack two real image rows into one complex transform and
+//     apply the grid correction in their epilogue (fip_fft.cuh);
+//   * the reference's pixel mapping (compute-bound) runs on a side stream
+//     while gridding and the FFT run, and reprojection is destination-tile
+//     major: each 64x64 output tile gathers its candidate source pixels,
+//     splats them in shared memory, stores the tile once and reports its
+//     maximum -- no global atomics, no memsets;
 //   * the trigger reads the three images once, in 128-bit loads, with
 //     warp-shuffle tile reductions.
 #include <cuda_runtime.h>
@@ -22,6 +26,7 @@
 #include <stdint.h>
 
 #include "fip_common.cuh"
+#include "fip_fft.cuh"
 #include "fip_kernels.h"
 #include "fip_refmath.cuh"
 
@@ -29,10 +34,8 @@ namespace {
 
 constexpr int kThreads = 256;
 
-__device__ __forceinline__ int wrap_mod(long v, int m) {
-  long r = v % m;
-  return (int)(r < 0 ? r + m : r);
-}
+// Grid row of signed row index v in [-G, G): v mod G without a division.
+__device__ __forceinline__ int wrap_row(int v, int g) { return v < 0 ? v + g : (v >= g ? v - g : v); }
 
 // ---------------------------------------------------------------------------
 // Taper (FIPkernels.cu:173-186)
@@ -62,9 +65,11 @@ __device__ __forceinline__ bool footprint(const float* B, int v, float scale, in
   return !(a0 > a1 || b0 > b1);
 }
 
-// Half-plane image of a virtual visibility: the direct one keeps taps with
-// r2 >= 0 at (r1 mod G, r2); the mirrored one (conjugate) keeps taps with
-// r2 <= 0 at (-r1 mod G, -r2).  Column range in half-plane columns.
+// Half-plane image of a virtual visibility.  The grid holds the Hermitian
+// part h(r) = (g(r) + conj g(-r)) / 2 of the reference's grid g, whose real
+// transform is the real part the reference keeps (FIPkernels.cu:266): the
+// direct copy keeps taps with r2 >= 0 at (r1 mod G, r2), the mirrored copy
+// (conjugated) keeps taps with r2 <= 0 at (-r1 mod G, -r2).
 __device__ __forceinline__ bool half_cols(const Footprint& f, int mir, int& c0, int& c1) {
   if (!mir) {
     if (f.b1 < 0) return false;
@@ -76,16 +81,27 @@ __device__ __forceinline__ bool half_cols(const Footprint& f, int mir, int& c0, 
   return true;
 }
 
-// Enumerate distinct tile rows touched by rows r1 in [a0,a1] (direct) or
-// -r1 (mirrored), modulo G.  At most 3.
+// Distinct tile rows touched by rows r1 in [a0,a1] (direct) or -r1
+// (mirrored), modulo G.  At most 3.
 __device__ __forceinline__ int tile_rows(const Footprint& f, int mir, int g, int* out) {
+  // Signed row range [lo, hi] (<= 9 rows) wraps into at most two segments.
+  const int lo = mir ? -f.a1 : f.a0, hi = mir ? -f.a0 : f.a1;
   int n = 0;
-  for (int r1 = f.a0; r1 <= f.a1; ++r1) {
-    int row = wrap_mod(mir ? -(long)r1 : (long)r1, g);
-    int tr = row / FIP_GTILE;
-    bool seen = false;
-    for (int k = 0; k < n; ++k) seen |= (out[k] == tr);
-    if (!seen && n < 3) out[n++] = tr;
+  auto add_segment = [&](int a, int b) {  // rows a..b within [0, g)
+    for (int tr = a / FIP_GTILE; tr <= b / FIP_GTILE && n < 3; ++tr) {
+      bool seen = false;
+      for (int k = 0; k < n; ++k) seen |= (out[k] == tr);
+      if (!seen) out[n++] = tr;
+    }
+  };
+  if (lo < 0 && hi >= 0) {
+    add_segment(lo + g, g - 1);
+    add_segment(0, hi);
+  } else if (hi >= g) {
+    add_segment(lo, g - 1);
+    add_segment(0, hi - g);
+  } else {
+    add_segment(wrap_row(lo, g), wrap_row(hi, g));
   }
   return n;
 }
@@ -101,17 +117,24 @@ __device__ __forceinline__ unsigned agg_inc(unsigned* cnt, unsigned key, unsigne
   return base + rank;
 }
 
-// pass 0: count entries per tile; pass 1: scatter entries.
+// pass 0: count entries per tile and record the occupied band
+// (bbox[0] = max |r1|, bbox[1] = max half-plane column); pass 1: scatter.
 template <int PASS>
 __global__ void k_bin(const float* __restrict__ B, int nb, float scale, int g, int tiles_c,
-                      unsigned* cnt, const unsigned* __restrict__ offset, unsigned* entries) {
+                      unsigned* cnt, const unsigned* __restrict__ offset, unsigned* entries,
+                      unsigned* bbox) {
   int v = blockIdx.x * blockDim.x + threadIdx.x;
   Footprint f;
   bool ok = v < nb && footprint(B, v, scale, g, f);
+  unsigned k1 = 0, k2 = 0;
+  if (ok) k1 = (unsigned)max(abs(f.a0), abs(f.a1));
   for (int mir = 0; mir < 2; ++mir) {
     int c0 = 0, c1 = -1, trs[3], ntr = 0;
     bool on = ok && half_cols(f, mir, c0, c1);
-    if (on) ntr = tile_rows(f, mir, g, trs);
+    if (on) {
+      ntr = tile_rows(f, mir, g, trs);
+      k2 = max(k2, (unsigned)c1);
+    }
     int tc0 = on ? c0 / FIP_GTILE : 0, tc1 = on ? c1 / FIP_GTILE : -1;
     // Up to 3 x 2 (tile-row, tile-col) pairs; every lane walks the same
     // 6 slots so the warp-aggregated atomics stay converged.
@@ -126,48 +149,130 @@ __global__ void k_bin(const float* __restrict__ B, int nb, float scale, int g, i
       }
     }
   }
+  if (PASS == 0) {
+    for (int o = 16; o > 0; o >>= 1) {
+      k1 = max(k1, __shfl_xor_sync(0xffffffffu, k1, o));
+      k2 = max(k2, __shfl_xor_sync(0xffffffffu, k2, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMax(&bbox[0], k1);
+      atomicMax(&bbox[1], k2);
+    }
+  }
 }
 
-// Exclusive scan of tile counts and construction of the work list.  One CTA.
-__global__ void k_bin_scan(const unsigned* __restrict__ cnt, int ntiles, unsigned* offset,
-                           unsigned* cursor, int4* work, unsigned* nwork, int wcap) {
-  __shared__ unsigned s_sum[kThreads];
-  __shared__ unsigned s_wsum[kThreads];
-  const int per = (ntiles + kThreads - 1) / kThreads;
-  const int beg = threadIdx.x * per, end = min(beg + per, ntiles);
-  unsigned local = 0, wlocal = 0;
-  for (int t = beg; t < end; ++t) {
-    local += cnt[t];
-    wlocal += (cnt[t] + FIP_GCHUNK - 1) / FIP_GCHUNK;
-  }
-  s_sum[threadIdx.x] = local;
-  s_wsum[threadIdx.x] = wlocal;
-  __syncthreads();
-  for (int d = 1; d < kThreads; d <<= 1) {
-    unsigned a = threadIdx.x >= d ? s_sum[threadIdx.x - d] : 0;
-    unsigned b = threadIdx.x >= d ? s_wsum[threadIdx.x - d] : 0;
-    __syncthreads();
-    s_sum[threadIdx.x] += a;
-    s_wsum[threadIdx.x] += b;
-    __syncthreads();
-  }
-  unsigned run = s_sum[threadIdx.x] - local, wrun = s_wsum[threadIdx.x] - wlocal;
-  for (int t = beg; t < end; ++t) {
-    offset[t] = run;
-    cursor[t] = 0;
-    unsigned c = cnt[t];
-    unsigned nchunk = (c + FIP_GCHUNK - 1) / FIP_GCHUNK;
-    for (unsigned k = 0; k < nchunk; ++k) {
-      if ((int)(wrun + k) < wcap)
-        work[wrun + k] = make_int4(t, (int)(run + k * FIP_GCHUNK),
-                                   (int)min(run + (k + 1) * FIP_GCHUNK, run + c), nchunk == 1);
+// Is grid tile t inside the band that the transform reads?
+__device__ __forceinline__ bool in_band(int t, int tiles_c, int g, int layout,
+                                        const unsigned* bbox) {
+  if (layout == 0) return true;
+  const int tr = t / tiles_c, tc = t % tiles_c;
+  const int k1 = (int)bbox[0], k2 = (int)bbox[1];
+  if (tc * FIP_GTILE > k2) return false;
+  const int r0 = tr * FIP_GTILE, r1 = min(r0 + FIP_GTILE, g) - 1;
+  return r0 <= k1 || r1 >= g - k1;
+}
+
+// Exclusive scans of tile counts, construction of the work list (every band
+// tile gets >= 1 item, so the band is fully written), and the list of tiles
+// split over several items (zeroed before their reductions).  One CTA of
+// kScanThreads walks the tiles in coalesced chunks.
+constexpr int kScanThreads = 1024;
+
+__device__ __forceinline__ uint3 block_exclusive_scan(uint3 v, uint3& total) {
+  __shared__ uint3 s_w[kScanThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint3 inc = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned a = __shfl_up_sync(0xffffffffu, inc.x, o);
+    const unsigned b = __shfl_up_sync(0xffffffffu, inc.y, o);
+    const unsigned c = __shfl_up_sync(0xffffffffu, inc.z, o);
+    if (lane >= o) {
+      inc.x += a;
+      inc.y += b;
+      inc.z += c;
     }
-    run += c;
-    wrun += nchunk;
   }
-  if (threadIdx.x == kThreads - 1) {
-    offset[ntiles] = run;
-    *nwork = min(wrun, (unsigned)wcap);
+  if (lane == 31) s_w[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    uint3 w = lane < kScanThreads / 32 ? s_w[lane] : make_uint3(0, 0, 0);
+    uint3 wi = w;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned a = __shfl_up_sync(0xffffffffu, wi.x, o);
+      const unsigned b = __shfl_up_sync(0xffffffffu, wi.y, o);
+      const unsigned c = __shfl_up_sync(0xffffffffu, wi.z, o);
+      if (lane >= o) {
+        wi.x += a;
+        wi.y += b;
+        wi.z += c;
+      }
+    }
+    if (lane < kScanThreads / 32) s_w[lane] = make_uint3(wi.x - w.x, wi.y - w.y, wi.z - w.z);
+  }
+  __syncthreads();
+  const uint3 base = s_w[warp];
+  uint3 ex = make_uint3(base.x + inc.x - v.x, base.y + inc.y - v.y, base.z + inc.z - v.z);
+  __shared__ uint3 s_total;
+  if (threadIdx.x == kScanThreads - 1) s_total = make_uint3(ex.x + v.x, ex.y + v.y, ex.z + v.z);
+  __syncthreads();
+  total = s_total;
+  __syncthreads();
+  return ex;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_bin_scan(
+    const unsigned* __restrict__ cnt, const unsigned* __restrict__ bbox, int ntiles, int tiles_c,
+    int g, int layout, unsigned* offset, unsigned* cursor, int4* work, unsigned* nwork, int wcap,
+    unsigned* multi, unsigned* nmulti) {
+  uint3 carry = make_uint3(0, 0, 0);
+  for (int base = 0; base < ntiles; base += kScanThreads) {
+    const int t = base + threadIdx.x;
+    unsigned c = 0, nch = 0;
+    if (t < ntiles) {
+      c = cnt[t];
+      nch = in_band(t, tiles_c, g, layout, bbox) ? max(1u, (c + FIP_GCHUNK - 1) / FIP_GCHUNK)
+                                                 : 0u;
+    }
+    uint3 total;
+    const uint3 ex = block_exclusive_scan(make_uint3(c, nch, nch > 1 ? 1u : 0u), total);
+    if (t < ntiles) {
+      const unsigned run = carry.x + ex.x, wrun = carry.y + ex.y;
+      offset[t] = run;
+      cursor[t] = 0;
+      for (unsigned k = 0; k < nch; ++k)
+        if ((int)(wrun + k) < wcap)
+          work[wrun + k] = make_int4(t, (int)(run + min(k * FIP_GCHUNK, c)),
+                                     (int)(run + min((k + 1) * FIP_GCHUNK, c)), nch == 1);
+      if (nch > 1) multi[carry.z + ex.z] = (unsigned)t;
+    }
+    carry.x += total.x;
+    carry.y += total.y;
+    carry.z += total.z;
+  }
+  if (threadIdx.x == 0) {
+    offset[ntiles] = carry.x;
+    *nwork = min(carry.y, (unsigned)wcap);
+    *nmulti = carry.z;
+  }
+}
+
+__device__ __forceinline__ size_t cell_index(int row, int col, int g, int hp, int layout) {
+  return layout ? (size_t)col * g + row : (size_t)row * hp + col;
+}
+
+// Zeroes the tiles that several work items reduce into.
+__global__ void k_zero_tiles(const unsigned* __restrict__ multi, const unsigned* __restrict__ nmulti,
+                             int tiles_c, int g, int hp, int layout, float2* __restrict__ grid) {
+  const unsigned nm = *nmulti;
+  for (unsigned w = blockIdx.x; w < nm; w += gridDim.x) {
+    const int t = (int)multi[w];
+    const int row0 = (t / tiles_c) * FIP_GTILE, col0 = (t % tiles_c) * FIP_GTILE;
+    for (int k = threadIdx.x; k < FIP_GTILE * FIP_GTILE; k += kThreads) {
+      const int lr = layout ? k % FIP_GTILE : k / FIP_GTILE;
+      const int lc = layout ? k / FIP_GTILE : k % FIP_GTILE;
+      const int row = row0 + lr, col = col0 + lc;
+      if (row < g && col < hp) grid[cell_index(row, col, g, hp, layout)] = make_float2(0.f, 0.f);
+    }
   }
 }
 
@@ -178,44 +283,62 @@ __device__ __forceinline__ float load_vis(const void* p, int v) {
   return __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(p)[v]);
 }
 
-// Persistent gridder: each work item is (tile, entry range).  Warps take one
-// virtual visibility at a time; lanes own taps.  COMP: Kahan-compensated
-// accumulation in shared memory (precision form).
+// Shared-memory layout of one gridding work item.
+constexpr int kTS = FIP_GTILE + 8;  // padded row stride: 4 tap rows x 8 columns hit 32 banks
+struct GridSmem {
+  float re[FIP_GTILE * kTS], im[FIP_GTILE * kTS];
+  float wr[FIP_GCHUNK], wi[FIP_GCHUNK];
+  int row0[FIP_GCHUNK];   // r1 of the first tap row (negated when mirrored)
+  int col0[FIP_GCHUNK];   // half-plane column of the first kept tap column
+  int meta[FIP_GCHUNK];   // nr | nc << 4 | mirrored << 8
+  float k1[FIP_GCHUNK][9], k2[FIP_GCHUNK][9];  // stride 9: conflict-free both ways
+};
+
+// Persistent gridder over work items (tile, entry range).  Phase 1 loads the
+// item's visibilities and their separable kernel values into shared memory
+// (all loads in flight at once); phase 2 lets each warp spread one
+// visibility's taps over its lanes into the shared tile; phase 3 commits.
+// COMP: Neumaier-compensated tile sums (precision form).
 template <int VT, bool COMP>
 __global__ void __launch_bounds__(kThreads) k_grid(const float* __restrict__ B, const void* vr,
                                                    const void* vi,
                                                    const float* __restrict__ vis_scale_p,
                                                    const float* __restrict__ V, float scale,
-                                                   int g, int hp, int tiles_c,
+                                                   int g, int hp, int tiles_c, int layout,
                                                    const unsigned* __restrict__ entries,
                                                    const int4* __restrict__ work,
                                                    const unsigned* __restrict__ nwork,
                                                    float2* __restrict__ grid) {
   extern __shared__ float4 s_raw[];
-  float2* s_tile = reinterpret_cast<float2*>(s_raw);                // [64*64]
-  float2* s_comp = s_tile + FIP_GTILE * FIP_GTILE;                  // [64*64] if COMP
+  GridSmem& S = *reinterpret_cast<GridSmem*>(s_raw);
+  float* s_cre = reinterpret_cast<float*>(reinterpret_cast<char*>(s_raw) + sizeof(GridSmem));
+  float* s_cim = s_cre + FIP_GTILE * kTS;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const float inten = fabs(V[0 * 3 + 0] * V[1 * 3 + 1] - V[0 * 3 + 1] * V[1 * 3 + 0]);
   const float vis_scale = vis_scale_p ? *vis_scale_p : 1.0f;
   const unsigned nw = *nwork;
   for (unsigned w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 item = work[w];
-    const int tile = item.x;
-    const int row0 = (tile / tiles_c) * FIP_GTILE, col0 = (tile % tiles_c) * FIP_GTILE;
-    for (int k = threadIdx.x; k < FIP_GTILE * FIP_GTILE; k += kThreads) {
-      s_tile[k] = make_float2(0.f, 0.f);
-      if (COMP) s_comp[k] = make_float2(0.f, 0.f);
+    const int tile = item.x, cnt = item.z - item.y;
+    const int trow0 = (tile / tiles_c) * FIP_GTILE, tcol0 = (tile % tiles_c) * FIP_GTILE;
+    for (int k = threadIdx.x; k < FIP_GTILE * kTS; k += kThreads) {
+      S.re[k] = 0.f;
+      S.im[k] = 0.f;
+      if (COMP) {
+        s_cre[k] = 0.f;
+        s_cim[k] = 0.f;
+      }
     }
-    __syncthreads();
-    for (int e = item.y + warp; e < item.z; e += kThreads / 32) {
-      const unsigned ent = entries[e];
+    // Phase 1.
+    for (int q = threadIdx.x; q < cnt; q += kThreads) {
+      const unsigned ent = entries[item.y + q];
       const int v = (int)(ent >> 1), mir = (int)(ent & 1);
       Footprint f;
       footprint(B, v, scale, g, f);
       int c0, c1;
       half_cols(f, mir, c0, c1);
       // Visibility weighting (FIPkernels.cu:188-195), halved for the
-      // Hermitian split, conjugated for the mirrored image.
+      // Hermitian split, conjugated for the mirrored copy.
       float wr, wi;
       if (VT == FIP_VIS_F32) {
         wr = load_vis<VT>(vr, v) / inten;
@@ -224,71 +347,74 @@ __global__ void __launch_bounds__(kThreads) k_grid(const float* __restrict__ B, 
         wr = (load_vis<VT>(vr, v) * vis_scale) / inten;
         wi = (load_vis<VT>(vi, v) * vis_scale) / inten;
       }
-      wr *= 0.5f;
-      wi = mir ? -0.5f * wi : 0.5f * wi;
-      // 1-D kernel values: lanes 0..15 rows, lanes 16..31 columns.
-      float kv = 0.f;
-      {
-        const float ihs = 1 / static_cast<float>(FIP_SUPPORT / 2);
-        if (lane < 16) {
-          int r = f.a0 + lane;
-          if (r <= f.a1) kv = fipref::es((static_cast<float>(r) - f.p1) * ihs);
-        } else {
-          int r = f.b0 + (lane - 16);
-          if (r <= f.b1) kv = fipref::es((static_cast<float>(r) - f.p2) * ihs);
+      S.wr[q] = 0.5f * wr;
+      S.wi[q] = mir ? -0.5f * wi : 0.5f * wi;
+      const int nr = f.a1 - f.a0 + 1, nc = c1 - c0 + 1;
+      S.row0[q] = mir ? -f.a0 : f.a0;
+      S.col0[q] = c0;
+      S.meta[q] = nr | (nc << 4) | (mir << 8);
+      const float ihs = 1 / static_cast<float>(FIP_SUPPORT / 2);
+#pragma unroll
+      for (int a = 0; a < 9; ++a)
+        if (a < nr) S.k1[q][a] = fipref::es((static_cast<float>(f.a0 + a) - f.p1) * ihs);
+      // Column taps in half-plane order c0..c1: original r2 = c (direct) or
+      // -c (mirrored).
+#pragma unroll
+      for (int b = 0; b < 9; ++b)
+        if (b < nc) {
+          const int r2 = mir ? -(c0 + b) : c0 + b;
+          S.k2[q][b] = fipref::es((static_cast<float>(r2) - f.p2) * ihs);
         }
-      }
-      const int nr = f.a1 - f.a0 + 1;
-      const int r2lo = mir ? -c1 : c0;  // original r2 range of the kept taps
-      const int nc = c1 - c0 + 1;
-      const int ntap = nr * nc;
-      for (int t0 = 0; t0 < ntap; t0 += 32) {
-        const int t = t0 + lane;
-        const int ia = t / nc, ib = t % nc;
-        const int r1 = f.a0 + min(ia, nr - 1);
-        const int r2 = r2lo + ib;
-        float k1 = __shfl_sync(0xffffffffu, kv, min(ia, nr - 1));
-        float k2 = __shfl_sync(0xffffffffu, kv, 16 + (r2 - f.b0));
-        if (t < ntap) {
-          const int row = wrap_mod(mir ? -(long)r1 : (long)r1, g);
-          const int col = mir ? -r2 : r2;
-          const int lr = row - row0, lc = col - col0;
-          if (lr >= 0 && lr < FIP_GTILE && lc >= 0 && lc < FIP_GTILE) {
-            const float kval = k1 * k2;
-            const float cr = wr * kval, ci = wi * kval;
-            float2* cell = &s_tile[lr * FIP_GTILE + lc];
-            if (!COMP) {
-              atomicAdd(&cell->x, cr);
-              atomicAdd(&cell->y, ci);
-            } else {
-              // Compensated add: old + c; the rounding error goes to s_comp.
-              float o = atomicAdd(&cell->x, cr);
-              float s = o + cr;
-              float err = (fabsf(o) >= fabsf(cr)) ? (o - s) + cr : (cr - s) + o;
-              atomicAdd(&s_comp[lr * FIP_GTILE + lc].x, err);
-              o = atomicAdd(&cell->y, ci);
-              s = o + ci;
-              err = (fabsf(o) >= fabsf(ci)) ? (o - s) + ci : (ci - s) + o;
-              atomicAdd(&s_comp[lr * FIP_GTILE + lc].y, err);
-            }
-          }
+    }
+    __syncthreads();
+    // Phase 2.
+    for (int q = warp; q < cnt; q += kThreads / 32) {
+      const int meta = S.meta[q];
+      const int nr = meta & 15, nc = (meta >> 4) & 15, mir = (meta >> 8) & 1;
+      const int per = 32 / nc;  // tap rows per warp step
+      const int ia0 = lane / nc, ib = lane - ia0 * nc;
+      if (ia0 >= per) continue;
+      const float wr = S.wr[q], wi = S.wi[q];
+      const int rbase = S.row0[q], col = S.col0[q] + ib;
+      const int lc = col - tcol0;
+      if ((unsigned)lc >= (unsigned)FIP_GTILE) continue;
+      const float k2 = S.k2[q][ib];
+      for (int ia = ia0; ia < nr; ia += per) {
+        const int row = wrap_row(mir ? rbase - ia : rbase + ia, g);
+        const int lr = row - trow0;
+        if ((unsigned)lr >= (unsigned)FIP_GTILE) continue;
+        const float kval = S.k1[q][ia] * k2;
+        const float cr = wr * kval, ci = wi * kval;
+        const int cell = lr * kTS + lc;
+        if (!COMP) {
+          atomicAdd(&S.re[cell], cr);
+          atomicAdd(&S.im[cell], ci);
+        } else {
+          float o = atomicAdd(&S.re[cell], cr);
+          float sm = o + cr;
+          float err = (fabsf(o) >= fabsf(cr)) ? (o - sm) + cr : (cr - sm) + o;
+          atomicAdd(&s_cre[cell], err);
+          o = atomicAdd(&S.im[cell], ci);
+          sm = o + ci;
+          err = (fabsf(o) >= fabsf(ci)) ? (o - sm) + ci : (ci - sm) + o;
+          atomicAdd(&s_cim[cell], err);
         }
       }
     }
     __syncthreads();
-    // Commit the tile: plain stores when this item owns the tile, vector
-    // reductions otherwise (grid pre-zeroed).
+    // Phase 3: commit in the layout's contiguous direction.
     const bool single = item.w != 0;
     for (int k = threadIdx.x; k < FIP_GTILE * FIP_GTILE; k += kThreads) {
-      const int lr = k / FIP_GTILE, lc = k % FIP_GTILE;
-      const int row = row0 + lr, col = col0 + lc;
+      const int lr = layout ? k % FIP_GTILE : k / FIP_GTILE;
+      const int lc = layout ? k / FIP_GTILE : k % FIP_GTILE;
+      const int row = trow0 + lr, col = tcol0 + lc;
       if (row < g && col < hp) {
-        float2 val = s_tile[k];
+        float2 val = make_float2(S.re[lr * kTS + lc], S.im[lr * kTS + lc]);
         if (COMP) {
-          val.x += s_comp[k].x;
-          val.y += s_comp[k].y;
+          val.x += s_cre[lr * kTS + lc];
+          val.y += s_cim[lr * kTS + lc];
         }
-        float2* dst = &grid[(size_t)row * hp + col];
+        float2* dst = &grid[cell_index(row, col, g, hp, layout)];
         if (single) {
           *dst = val;
         } else if (val.x != 0.f || val.y != 0.f) {
@@ -301,35 +427,141 @@ __global__ void __launch_bounds__(kThreads) k_grid(const float* __restrict__ B, 
 }
 
 // ---------------------------------------------------------------------------
-// Corrected source pixel (FIPkernels.cu:256-287 and :391-392), read from the
-// in-place C2R output: row (j - N/2) mod G, column (i - N/2) mod G, row stride
-// G + 2 floats.  The reference's checkerboard signs cancel against its
-// centred grid origin, so none is applied here.
+// Band-pruned inverse FFT (power-of-two images).
+// Column pass: P[c][yy] = sum_r1 H[c][r1 mod G] e^{+2 pi i y r1 / G},
+// y = yy - N/2, for the occupied half-plane columns c <= bbox[1] and rows
+// |r1| <= bbox[0].
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float source_value(const float* __restrict__ fft_out,
-                                              const float* __restrict__ ck, int n, int g,
-                                              int i, int j, float inv_nb) {
+__global__ void __launch_bounds__(768) k_fft_cols(const float2* __restrict__ H,
+                                                  const unsigned* __restrict__ bbox,
+                                                  float2* __restrict__ P, int n,
+                                                  fipfft::Plan plan,
+                                                  const float2* __restrict__ tw) {
+  extern __shared__ float2 s_fft[];
+  const int c = blockIdx.x;
+  const int k2 = (int)bbox[1];
+  if (c > k2) return;
+  const int g = plan.g;
+  const int k1 = min((int)bbox[0], g / 2);
+  const float2* col = H + (size_t)c * g;
+  // Stage the band rows [0, k1] and [g - k1, g) with coalesced loads.
+  for (int r = threadIdx.x; r <= k1; r += blockDim.x) s_fft[r] = col[r];
+  for (int r = g - k1 + threadIdx.x; r < g; r += blockDim.x)
+    if (r > k1) s_fft[r] = col[r];
+  __syncthreads();
+  float2* out = P + (size_t)c * n;
+  auto load = [&](int pos) -> float2 {
+    return (pos <= k1 || pos >= g - k1) ? s_fft[pos] : make_float2(0.f, 0.f);
+  };
+  auto store = [&](int yy, float2 v) { out[yy] = v; };
+  fipfft::run(plan, s_fft, tw, n, load, store);
+}
+
+// Row pass for image rows yy1 = 2b, yy2 = 2b+1: their Hermitian spectra
+// X1, X2 (the column-pass output, extended by X(-c) = conj X(c)) are packed as
+// Z = X1 + i X2 so one complex transform yields both real rows.  The epilogue
+// is the reference's crop/correction (FIPkernels.cu:256-287): the image pixel
+// is |out * 1/(taper|x| taper|y| norm^2)| (the checkerboard signs cancel
+// against the centred grid origin).
+__global__ void __launch_bounds__(768) k_fft_rows(const float2* __restrict__ P, const unsigned* __restrict__ bbox,
+                           const float* __restrict__ ck, float* __restrict__ pre, int n,
+                           fipfft::Plan plan, const float2* __restrict__ tw) {
+  extern __shared__ float2 s_fft[];
+  const int yy1 = 2 * blockIdx.x;
+  const int g = plan.g, half = g / 2, h = n / 2;
+  const int k2 = min((int)bbox[1], half);
+  const float norm = FIP_CONV_NORM;
+  const float cky1 = ck[abs(yy1 - h)], cky2 = ck[abs(yy1 + 1 - h)];
+  // Stage (X1[c], X2[c]) for c <= k2: one 16-byte load per column, all in
+  // flight at once (the column pass stores P[c][yy]).
+  float4* s_in = reinterpret_cast<float4*>(s_fft);
+  for (int c = threadIdx.x; c <= k2; c += blockDim.x)
+    s_in[c] = *reinterpret_cast<const float4*>(P + (size_t)c * n + yy1);
+  __syncthreads();
+  auto load = [&](int pos) -> float2 {
+    int c;
+    bool mirror = false;
+    if (pos <= k2 && pos <= half) {
+      c = pos;
+    } else if (pos >= g - k2 && pos > half) {
+      c = g - pos;
+      mirror = true;
+    } else {
+      return make_float2(0.f, 0.f);
+    }
+    const float4 ab = s_in[c];
+    float ay = ab.y, by = ab.w;
+    if (mirror) {
+      ay = -ay;
+      by = -by;
+    }
+    if (pos == 0 || pos == half) {
+      ay = 0.f;
+      by = 0.f;
+    }
+    return make_float2(ab.x - by, ay + ab.z);
+  };
+  float* row1 = pre + (size_t)yy1 * n;
+  float* row2 = row1 + n;
+  auto store = [&](int xx, float2 v) {
+    const int x = xx - h;
+    const float ckx = ck[abs(x)];
+    float p1 = v.x, p2 = v.y;
+    p1 *= 1 / (ckx * cky1 * norm * norm);
+    p2 *= 1 / (ckx * cky2 * norm * norm);
+    row1[xx] = fabs(p1);
+    row2[xx] = fabs(p2);
+  };
+  fipfft::run(plan, s_fft, tw, n, load, store);
+}
+
+// Crop + correction of the cuFFT C2R output (images whose grid side is not
+// 3 * 2^k): row (y mod G), column (x mod G), row stride G + 2 floats.
+__global__ void k_correct_c2r(const float* __restrict__ fft_out, const float* __restrict__ ck,
+                              int n, int g, float* __restrict__ pre) {
+  const int xx = blockIdx.x * blockDim.x + threadIdx.x, yy = blockIdx.y;
+  if (xx >= n) return;
   const int h = n / 2;
-  const long x = (long)i - h, y = (long)j - h;
+  const long x = (long)xx - h, y = (long)yy - h;
   const int row = (int)(y < 0 ? y + g : y), col = (int)(x < 0 ? x + g : x);
   float px = fft_out[(size_t)row * (size_t)(g + 2) + col];
   const float norm = FIP_CONV_NORM;
   px *= 1 / (ck[labs(x)] * ck[labs(y)] * norm * norm);
-  px = fabs(px);
-  return px * inv_nb;
+  pre[(size_t)yy * n + xx] = fabs(px);
 }
 
-// Source-major reprojection, the reference's scheme (FIPkernels.cu:378-413)
-// with the crop/correction fused: one thread per source pixel, four atomics.
-__global__ void k_reproject_scatter(const float* __restrict__ fft_out, const float* __restrict__ ck,
-                                    const float* __restrict__ V, int n, int g, int nb, float dc,
-                                    float* __restrict__ dst) {
+// ---------------------------------------------------------------------------
+// Reprojection (FIPkernels.cu:289-413).
+// ---------------------------------------------------------------------------
+
+// The reference's pixel mapping for every source pixel: targets[j*N + i] =
+// (LL, MM) of source column i, row j.  Compute-bound; overlapped with the
+// gridding and the FFT on a side stream.
+constexpr int kTargetsPerThread = 4;
+__global__ void k_targets(const float* __restrict__ V, int n, float dc, float2* __restrict__ tg) {
+  const int j = blockIdx.y;
+  const fipref::Frame fr{V[0], V[1], V[3], V[4], V[8], V[6], V[7], dc};
+#pragma unroll
+  for (int q = 0; q < kTargetsPerThread; ++q) {
+    const int i = (blockIdx.x * kTargetsPerThread + q) * blockDim.x + threadIdx.x;
+    if (i < n) {
+      float LL, MM;
+      fipref::pixel_target(fr, (size_t)i, (size_t)j, (size_t)n, LL, MM);
+      tg[(size_t)j * n + i] = make_float2(LL, MM);
+    }
+  }
+}
+
+// Source-major reprojection, the reference's own scheme (FIPkernels.cu:378-413):
+// one thread per source pixel, four atomics into a zeroed destination.
+__global__ void k_reproject_scatter(const float* __restrict__ pre, const float* __restrict__ V,
+                                    int n, int nb, float dc, float* __restrict__ dst) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= n || j >= n) return;
   fipref::Frame fr{V[0], V[1], V[3], V[4], V[8], V[6], V[7], dc};
   const float inv_nb = 1.0f / static_cast<float>(nb);
-  const float value = source_value(fft_out, ck, n, g, i, j, inv_nb);
+  const float value = pre[(size_t)j * n + i] * inv_nb;
   float LL, MM;
   fipref::pixel_target(fr, (size_t)i, (size_t)j, (size_t)n, LL, MM);
   const size_t half = n / 2;
@@ -344,38 +576,58 @@ __global__ void k_reproject_scatter(const float* __restrict__ fft_out, const flo
   }
 }
 
-// ---------------------------------------------------------------------------
-// Destination-tile-major reprojection.
-// ---------------------------------------------------------------------------
-constexpr int kDT = 32;          // destination tile side
-constexpr int kMaxRows = 192;    // candidate source rows per tile
+constexpr int kDT = 64;          // destination tile side
+constexpr int kMaxRows = 256;    // candidate source rows per tile
 
+// Exact map: LL = P1 - xi z / cell, MM = P2 + eta z / cell with
+// z = 1 - sqrt(1 - rho), rho = cell^2 ((P1 - 1)^2 + (P2 - 1)^2),
+// P = M (a, b) / |V22| -- the closed form of coordschange + p2p.
+template <typename T>
 struct ExactMap {
-  // LL = P1 - xi z / cell, MM = P2 + eta z / cell, z = 1 - sqrt(1 - rho),
-  // rho = cell^2 ((P1 - 1)^2 + (P2 - 1)^2), P = M (a, b) / |V22|.
-  double m00, m01, m10, m11;  // M / |V22|
-  double i00, i01, i10, i11;  // inverse of M / |V22|
-  double xi, eta, cell;
+  T m00, m01, m10, m11;  // M / |V22|
+  T i00, i01, i10, i11;  // its inverse
+  T xi, eta, cell;
 };
 
-__device__ __forceinline__ void exact_forward(const ExactMap& m, double a, double b, double& LL,
-                                              double& MM) {
-  double P1 = m.m00 * a + m.m01 * b, P2 = m.m10 * a + m.m11 * b;
-  double rho = m.cell * m.cell * ((P1 - 1) * (P1 - 1) + (P2 - 1) * (P2 - 1));
-  double zc = rho <= 1 ? (rho / (1 + sqrt(1 - rho))) / m.cell : 0.0;
+template <typename T>
+__device__ __forceinline__ ExactMap<T> make_map(const float* V, float cell) {
+  ExactMap<T> m;
+  const double a22 = fabs((double)V[8]);
+  const double m00 = -(double)V[0] / a22, m01 = (double)V[3] / a22;
+  const double m10 = -(double)V[1] / a22, m11 = (double)V[4] / a22;
+  const double det = m00 * m11 - m01 * m10;
+  m.m00 = (T)m00; m.m01 = (T)m01; m.m10 = (T)m10; m.m11 = (T)m11;
+  m.i00 = (T)(m11 / det); m.i01 = (T)(-m01 / det);
+  m.i10 = (T)(-m10 / det); m.i11 = (T)(m00 / det);
+  m.xi = (T)((double)V[6] / (double)V[8]);
+  m.eta = (T)((double)V[7] / (double)V[8]);
+  m.cell = (T)cell;
+  return m;
+}
+
+template <typename T>
+__device__ __forceinline__ T slant_over_cell(const ExactMap<T>& m, T P1, T P2) {
+  const T rho = m.cell * m.cell * ((P1 - 1) * (P1 - 1) + (P2 - 1) * (P2 - 1));
+  return rho <= 1 ? (rho / (1 + sqrt(1 - rho))) / m.cell : (T)0;
+}
+
+template <typename T>
+__device__ __forceinline__ void exact_forward(const ExactMap<T>& m, T a, T b, T& LL, T& MM) {
+  const T P1 = m.m00 * a + m.m01 * b, P2 = m.m10 * a + m.m11 * b;
+  const T zc = slant_over_cell(m, P1, P2);
   LL = P1 - m.xi * zc;
   MM = P2 + m.eta * zc;
 }
 
-// Source coordinates (a, b) relative to the centre whose exact target is
-// (LL, MM): fixed-point iteration on the slant term (a contraction for any
-// field smaller than a radian).
-__device__ __forceinline__ void exact_inverse(const ExactMap& m, double LL, double MM, double& a,
-                                              double& b) {
-  double P1 = LL, P2 = MM;
-  for (int it = 0; it < 12; ++it) {
-    double rho = m.cell * m.cell * ((P1 - 1) * (P1 - 1) + (P2 - 1) * (P2 - 1));
-    double zc = rho <= 1 ? (rho / (1 + sqrt(1 - rho))) / m.cell : 0.0;
+// Source (a, b), relative to the centre, of an exact target (LL, MM):
+// fixed-point iteration on the slant term, a contraction for any field
+// smaller than a radian.
+template <typename T>
+__device__ __forceinline__ void exact_inverse(const ExactMap<T>& m, T LL, T MM, T& a, T& b) {
+  T P1 = LL, P2 = MM;
+#pragma unroll
+  for (int it = 0; it < 6; ++it) {
+    const T zc = slant_over_cell(m, P1, P2);
     P1 = LL + m.xi * zc;
     P2 = MM - m.eta * zc;
   }
@@ -383,165 +635,170 @@ __device__ __forceinline__ void exact_inverse(const ExactMap& m, double LL, doub
   b = m.i10 * P1 + m.i11 * P2;
 }
 
-__device__ __forceinline__ ExactMap make_map(const float* V, float cell) {
-  ExactMap m;
-  const double a22 = fabs((double)V[8]);
-  m.m00 = -(double)V[0] / a22; m.m01 = (double)V[3] / a22;
-  m.m10 = -(double)V[1] / a22; m.m11 = (double)V[4] / a22;
-  const double det = m.m00 * m.m11 - m.m01 * m.m10;
-  m.i00 = m.m11 / det; m.i01 = -m.m01 / det;
-  m.i10 = -m.m10 / det; m.i11 = m.m00 / det;
-  m.xi = (double)V[6] / (double)V[8];
-  m.eta = (double)V[7] / (double)V[8];
-  m.cell = (double)cell;
-  return m;
+// Destination-tile-major reprojection.  The candidate source pixels of a
+// 64x64 destination tile are the integer points of the preimage of the tile
+// widened by the splat reach (1 pixel) and delta (the FP32 chain's deviation
+// from the exact map): per source row, one column interval.  Each candidate
+// is splatted (bilinear weights of FIPkernels.cu:394-410) into shared memory;
+// the tile is stored once and its maximum folded into *img_max.
+// EXACT: targets from the closed form in FP64 (precision form) instead of
+// the precomputed reference-chain targets.
+// Physical shared-memory column of destination pixel (row, col) in a tile:
+// an XOR swizzle of 4-column groups by the row, so the lanes of a warp
+// (neighbouring sources, mapped along an arbitrary direction) spread over the
+// banks while 4-column groups stay contiguous for 128-bit stores.
+__device__ __forceinline__ int tile_slot(int row, int col) {
+  return row * kDT + (col ^ ((row & 7) << 2));
 }
-
-// Precision-form target: the closed form in FP32 relative to a local origin
-// (a0, b0) whose exact target (L0, M0) is given in double.
-struct LocalMap {
-  float m00, m01, m10, m11;  // M / |V22| in float
-  float P10, P20;            // P at the local origin (absolute)
-  float L0f, M0f;            // P at the origin minus the destination origin
-  float xi, eta, cell;
-};
 
 template <bool EXACT>
 __global__ void __launch_bounds__(kThreads) k_reproject_gather(
-    const float* __restrict__ fft_out, const float* __restrict__ ck, const float* __restrict__ V,
-    int n, int g, int nb, float dc, float cell, float delta, float* __restrict__ dst,
-    unsigned* img_max) {
-  __shared__ float s_tile[kDT * kDT];
+    const float* __restrict__ pre, const float2* __restrict__ tg, const float* __restrict__ V,
+    int n, int nb, float cell, float delta, float* __restrict__ dst, unsigned* img_max) {
+  __shared__ __align__(16) float s_tile[kDT * kDT];
   __shared__ int s_ilo[kMaxRows];
-  __shared__ int s_scan[kMaxRows + 1];
-  __shared__ double s_q[4][2];
-  __shared__ int s_rows[2];
+  __shared__ int s_cnt[kMaxRows];
+  __shared__ float s_q[4][2];
   __shared__ float s_wmax[kThreads / 32];
 
   const int tiles = (n + kDT - 1) / kDT;
   const int tr = blockIdx.x / tiles, tc = blockIdx.x % tiles;
   const int r0 = tr * kDT, c0 = tc * kDT;
   const int h = n / 2;
-  const ExactMap m = make_map(V, cell);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
   for (int k = threadIdx.x; k < kDT * kDT; k += kThreads) s_tile[k] = 0.f;
-  // Preimage corners of the destination window widened by the splat reach
-  // (one pixel) and delta (the FP32 chain's deviation from exact).
   if (threadIdx.x < 4) {
-    const double Llo = (double)(c0 - h) - 1.0 - delta, Lhi = (double)(c0 + kDT - h) + delta;
-    const double Mlo = (double)(r0 - h) - 1.0 - delta, Mhi = (double)(r0 + kDT - h) + delta;
-    const double L = (threadIdx.x == 0 || threadIdx.x == 3) ? Llo : Lhi;
-    const double M = (threadIdx.x < 2) ? Mlo : Mhi;
-    double a, b;
-    exact_inverse(m, L, M, a, b);
+    const ExactMap<float> mf = make_map<float>(V, cell);
+    const float Llo = (float)(c0 - h) - 1.0f - delta, Lhi = (float)(c0 + kDT - h) + delta;
+    const float Mlo = (float)(r0 - h) - 1.0f - delta, Mhi = (float)(r0 + kDT - h) + delta;
+    const float L = (threadIdx.x == 0 || threadIdx.x == 3) ? Llo : Lhi;
+    const float M = (threadIdx.x < 2) ? Mlo : Mhi;
+    float a, b;
+    exact_inverse(mf, L, M, a, b);
     s_q[threadIdx.x][0] = a;
     s_q[threadIdx.x][1] = b;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double bmin = s_q[0][1], bmax = s_q[0][1];
-    for (int k = 1; k < 4; ++k) {
-      bmin = fmin(bmin, s_q[k][1]);
-      bmax = fmax(bmax, s_q[k][1]);
-    }
-    int jlo = (int)fmax(0.0, ceil(fmax(bmin + h - 1e-9, -1.0)));
-    int jhi = (int)fmin((double)(n - 1), floor(fmin(bmax + h + 1e-9, (double)n)));
-    if (jhi - jlo + 1 > kMaxRows) jhi = jlo + kMaxRows - 1;  // unreachable for delta < 40
-    s_rows[0] = jlo;
-    s_rows[1] = jhi;
+  float bmin = s_q[0][1], bmax = s_q[0][1];
+#pragma unroll
+  for (int k = 1; k < 4; ++k) {
+    bmin = fminf(bmin, s_q[k][1]);
+    bmax = fmaxf(bmax, s_q[k][1]);
   }
-  __syncthreads();
-  const int jlo = s_rows[0], jhi = s_rows[1];
+  const int jlo = (int)fmaxf(0.f, ceilf(fmaxf(bmin + h - 1e-3f, -1.f)));
+  int jhi = (int)fminf((float)(n - 1), floorf(fminf(bmax + h + 1e-3f, (float)n)));
+  jhi = min(jhi, jlo + kMaxRows - 1);
   const int nrows = max(0, jhi - jlo + 1);
+  // Column interval of every candidate row: the preimage quadrilateral
+  // intersected with the row.
   for (int r = threadIdx.x; r < nrows; r += kThreads) {
-    const double b = (double)(jlo + r - h);
-    double alo = 1e300, ahi = -1e300;
+    const float b = (float)(jlo + r - h);
+    float alo = 3e38f, ahi = -3e38f;
+#pragma unroll
     for (int k = 0; k < 4; ++k) {
-      const double ax = s_q[k][0], bx = s_q[k][1];
-      const double ay = s_q[(k + 1) & 3][0], by = s_q[(k + 1) & 3][1];
+      const float ax = s_q[k][0], bx = s_q[k][1];
+      const float ay = s_q[(k + 1) & 3][0], by = s_q[(k + 1) & 3][1];
       if ((bx <= b && b <= by) || (by <= b && b <= bx)) {
-        double a;
         if (by == bx) {
-          alo = fmin(alo, fmin(ax, ay));
-          ahi = fmax(ahi, fmax(ax, ay));
-          continue;
+          alo = fminf(alo, fminf(ax, ay));
+          ahi = fmaxf(ahi, fmaxf(ax, ay));
+        } else {
+          const float a = ax + (ay - ax) * ((b - bx) / (by - bx));
+          alo = fminf(alo, a);
+          ahi = fmaxf(ahi, a);
         }
-        a = ax + (ay - ax) * (b - bx) / (by - bx);
-        alo = fmin(alo, a);
-        ahi = fmax(ahi, a);
       }
     }
     int ilo = 0, ihi = -1;
     if (alo <= ahi) {
-      ilo = (int)fmax(0.0, ceil(fmax(alo + h - 1e-9, -1.0)));
-      ihi = (int)fmin((double)(n - 1), floor(fmin(ahi + h + 1e-9, (double)n)));
+      ilo = (int)fmaxf(0.f, ceilf(fmaxf(alo + h - 1e-3f, -1.f)));
+      ihi = (int)fminf((float)(n - 1), floorf(fminf(ahi + h + 1e-3f, (float)n)));
     }
     s_ilo[r] = ilo;
-    s_scan[r + 1] = ihi >= ilo ? ihi - ilo + 1 : 0;
+    s_cnt[r] = ihi >= ilo ? ihi - ilo + 1 : 0;
   }
-  if (threadIdx.x == 0) s_scan[0] = 0;
   __syncthreads();
-  if (threadIdx.x == 0)
-    for (int r = 0; r < nrows; ++r) s_scan[r + 1] += s_scan[r];
-  __syncthreads();
-  const int total = s_scan[nrows];
 
   const float inv_nb = 1.0f / static_cast<float>(nb);
-  fipref::Frame fr{V[0], V[1], V[3], V[4], V[8], V[6], V[7], dc};
   const size_t half = n / 2;
-  for (int k = threadIdx.x; k < total; k += kThreads) {
-    int lo = 0, hi = nrows - 1;
-    while (lo < hi) {
-      int mid = (lo + hi + 1) >> 1;
-      if (s_scan[mid] <= k) lo = mid; else hi = mid - 1;
-    }
-    const int j = jlo + lo;
-    const int i = s_ilo[lo] + (k - s_scan[lo]);
-    const float value = source_value(fft_out, ck, n, g, i, j, inv_nb);
-    float LL, MM;
-    long fl, cl, fm, cm;
+  const float lim = half - 1;  // the reference compares |LL| with size_t (N/2 - 1)
+  ExactMap<double> md;
+  if (EXACT) md = make_map<double>(V, cell);
+  // Warps own candidate rows, lanes walk each row's column interval, two
+  // candidates per lane per step with both loads issued up front.
+  auto splat = [&](int i, int j, float value, float2 t) {
+    int fl, cl, fm, cm;
     float wl1, wm1, wl0, wm0;
     if (!EXACT) {
-      fipref::pixel_target(fr, (size_t)i, (size_t)j, (size_t)n, LL, MM);
-      if (!(fabs(LL) < half - 1 && fabs(MM) < half - 1)) continue;
-      fl = fipref::floor_l(LL); cl = fipref::ceil_l(LL);
-      fm = fipref::floor_l(MM); cm = fipref::ceil_l(MM);
+      const float LL = t.x, MM = t.y;
+      if (!(fabs(LL) < lim && fabs(MM) < lim)) return;
+      fl = (int)floorf(LL); cl = (int)ceilf(LL);
+      fm = (int)floorf(MM); cm = (int)ceilf(MM);
+      // The reference's weight expressions (FIPkernels.cu:397-409).
       wl0 = 1 - LL + fl; wl1 = LL - fl;
       wm0 = 1 - MM + fm; wm1 = MM - fm;
     } else {
       double Ld, Md;
-      exact_forward(m, (double)(i - h), (double)(j - h), Ld, Md);
-      if (!(fabs(Ld) < (double)(half - 1) && fabs(Md) < (double)(half - 1))) continue;
-      double fld = floor(Ld), fmd = floor(Md);
-      fl = (long)fld; fm = (long)fmd;
-      cl = (long)ceil(Ld); cm = (long)ceil(Md);
+      exact_forward(md, (double)(i - h), (double)(j - h), Ld, Md);
+      if (!(fabs(Ld) < (double)(half - 1) && fabs(Md) < (double)(half - 1))) return;
+      const double fld = floor(Ld), fmd = floor(Md);
+      fl = (int)fld; fm = (int)fmd;
+      cl = (int)ceil(Ld); cm = (int)ceil(Md);
       wl1 = (float)(Ld - fld); wm1 = (float)(Md - fmd);
       wl0 = 1.0f - wl1; wm0 = 1.0f - wm1;
     }
     // Destination pixel (row h + m, column h + l), local to this tile.
-    const int lf = (int)(h + fl) - c0, lc = (int)(h + cl) - c0;
-    const int mf = (int)(h + fm) - r0, mc = (int)(h + cm) - r0;
+    const int lf = h + fl - c0, lc = h + cl - c0;
+    const int mf = h + fm - r0, mc = h + cm - r0;
     if ((unsigned)mf < (unsigned)kDT) {
-      if ((unsigned)lf < (unsigned)kDT) atomicAdd(&s_tile[mf * kDT + lf], wl0 * wm0 * value);
-      if ((unsigned)lc < (unsigned)kDT) atomicAdd(&s_tile[mf * kDT + lc], wl1 * wm0 * value);
+      if ((unsigned)lf < (unsigned)kDT) atomicAdd(&s_tile[tile_slot(mf, lf)], wl0 * wm0 * value);
+      if ((unsigned)lc < (unsigned)kDT) atomicAdd(&s_tile[tile_slot(mf, lc)], wl1 * wm0 * value);
     }
     if ((unsigned)mc < (unsigned)kDT) {
-      if ((unsigned)lf < (unsigned)kDT) atomicAdd(&s_tile[mc * kDT + lf], wl0 * wm1 * value);
-      if ((unsigned)lc < (unsigned)kDT) atomicAdd(&s_tile[mc * kDT + lc], wl1 * wm1 * value);
+      if ((unsigned)lf < (unsigned)kDT) atomicAdd(&s_tile[tile_slot(mc, lf)], wl0 * wm1 * value);
+      if ((unsigned)lc < (unsigned)kDT) atomicAdd(&s_tile[tile_slot(mc, lc)], wl1 * wm1 * value);
+    }
+  };
+  for (int r = warp; r < nrows; r += kThreads / 32) {
+    const int j = jlo + r, ilo = s_ilo[r], cnt = s_cnt[r];
+    const float* prow = pre + (size_t)j * n + ilo;
+    const float2* trow = EXACT ? nullptr : tg + (size_t)j * n + ilo;
+    for (int c = lane; c < cnt; c += 64) {
+      const bool two = c + 32 < cnt;
+      const float v0 = prow[c];
+      const float v1 = two ? prow[c + 32] : 0.f;
+      float2 t0 = make_float2(0.f, 0.f), t1 = make_float2(0.f, 0.f);
+      if (!EXACT) {
+        t0 = trow[c];
+        if (two) t1 = trow[c + 32];
+      }
+      splat(ilo + c, j, v0 * inv_nb, t0);
+      if (two) splat(ilo + c + 32, j, v1 * inv_nb, t1);
     }
   }
   __syncthreads();
   float vmax = 0.f;
-  for (int k = threadIdx.x; k < kDT * kDT; k += kThreads) {
-    const int rr = r0 + k / kDT, cc = c0 + k % kDT;
-    if (rr < n && cc < n) {
-      const float val = s_tile[k];
-      dst[(size_t)rr * n + cc] = val;
-      vmax = fmaxf(vmax, val);
+  for (int k = threadIdx.x; k < kDT * kDT / 4; k += kThreads) {
+    const int lr = (4 * k) / kDT, g4 = ((4 * k) % kDT) >> 2;
+    const int rr = r0 + lr, cc = c0 + 4 * g4;
+    const float4 val = *reinterpret_cast<const float4*>(&s_tile[tile_slot(lr, 4 * g4)]);
+    if (rr < n) {
+      if (cc + 3 < n && (n & 3) == 0) {
+        *reinterpret_cast<float4*>(&dst[(size_t)rr * n + cc]) = val;
+        vmax = fmaxf(vmax, fmaxf(fmaxf(val.x, val.y), fmaxf(val.z, val.w)));
+      } else {
+        const float vv[4] = {val.x, val.y, val.z, val.w};
+        for (int e = 0; e < 4; ++e)
+          if (cc + e < n) {
+            dst[(size_t)rr * n + cc + e] = vv[e];
+            vmax = fmaxf(vmax, vv[e]);
+          }
+      }
     }
   }
   for (int o = 16; o > 0; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
-  if ((threadIdx.x & 31) == 0) s_wmax[threadIdx.x >> 5] = vmax;
+  if (lane == 0) s_wmax[warp] = vmax;
   __syncthreads();
   if (threadIdx.x == 0 && img_max) {
     float b = 0.f;
@@ -560,7 +817,7 @@ __global__ void k_pixel_targets(const float* __restrict__ V, int n, float dc, fl
     fipref::Frame fr{V[0], V[1], V[3], V[4], V[8], V[6], V[7], dc};
     fipref::pixel_target(fr, (size_t)i, (size_t)j, (size_t)n, LL, MM);
   } else {
-    const ExactMap m = make_map(V, cell);
+    const ExactMap<double> m = make_map<double>(V, cell);
     double Ld, Md;
     exact_forward(m, (double)(i - n / 2), (double)(j - n / 2), Ld, Md);
     LL = (float)Ld;
@@ -570,7 +827,7 @@ __global__ void k_pixel_targets(const float* __restrict__ V, int n, float dc, fl
   out[2 * ((size_t)j * n + i) + 1] = MM;
 }
 
-// Maximum of non-negative floats (bit pattern order), NaN ignored.
+// Maximum of non-negative floats (bit-pattern order), NaN ignored.
 __global__ void k_image_max(const float* __restrict__ img, size_t count, unsigned* out) {
   float m = 0.f;
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < count;
@@ -652,6 +909,11 @@ __global__ void __launch_bounds__(kThreads) k_trigger(const float* __restrict__ 
       a.r += __shfl_xor_sync(0xffffffffu, a.r, o);
       a.m = fmaxf(a.m, __shfl_xor_sync(0xffffffffu, a.m, o));
     }
+    if (lane == 0) {
+      const float maxallval = max(max3[0], max(max3[1], max3[2]));
+      const size_t us = (size_t)t;
+      result[b] = 1 - (a.s / us / us) * a.m * (a.r / us / us) / maxallval / maxallval;
+    }
   } else {
     double s = (double)a.s + (double)a.sc, r = (double)a.r + (double)a.rc;
     for (int o = 16; o > 0; o >>= 1) {
@@ -659,25 +921,46 @@ __global__ void __launch_bounds__(kThreads) k_trigger(const float* __restrict__ 
       r += __shfl_xor_sync(0xffffffffu, r, o);
       a.m = fmaxf(a.m, __shfl_xor_sync(0xffffffffu, a.m, o));
     }
-    a.s = (float)s;
-    a.r = (float)r;
     if (lane == 0) {
-      double mx = fmax(fmax((double)max3[0], (double)max3[1]), (double)max3[2]);
-      double tt = (double)t;
+      const double mx = fmax(fmax((double)max3[0], (double)max3[1]), (double)max3[2]);
+      const double tt = (double)t;
       result[b] = (float)(1.0 - (s / tt / tt) * (double)a.m * (r / tt / tt) / mx / mx);
     }
-    return;
-  }
-  if (lane == 0) {
-    const float maxallval = max(max3[0], max(max3[1], max3[2]));
-    const size_t us = (size_t)t;
-    result[b] = 1 - (a.s / us / us) * a.m * (a.r / us / us) / maxallval / maxallval;
   }
 }
 
 inline float cell_degrees(float cell) { return (float)((double)cell / FIP_M_PI * 180); }
 
+inline int sm_count() {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------
+
+bool fip_fft_plan(int g, fipfft::Plan& p) {
+  if (g < 48 || g % 3 != 0) return false;
+  const int m = g / 3;
+  if (m & (m - 1)) return false;
+  int k = 0;
+  while ((1 << k) < m) ++k;
+  p.g = g;
+  p.m = m;
+  p.ts = m / fipfft::E;
+  p.nt = 3 * p.ts;
+  if (p.nt > 1024) return false;
+  int np = 0;
+  for (int q = 0; q < k / 4; ++q) p.r[np++] = 16;
+  if (k % 4) p.r[np++] = 1 << (k % 4);
+  p.np = np;
+  return np <= fipfft::kMaxPass;
+}
 
 cudaError_t fip_launch_taper(float* taper, const FipGeom& geo, cudaStream_t s) {
   const int cnt = geo.n / 2 + 1;
@@ -691,37 +974,37 @@ cudaError_t fip_launch_bin(const FipGeom& geo, const float* B, int nb, FipBins& 
   const int ntiles = geo.tiles_r * geo.tiles_c;
   const float scale = geo.cell * (float)(size_t)geo.g;  // r1r2_scale (FIPkernels.cu:584)
   cudaError_t e = cudaMemsetAsync(bins.count, 0, ntiles * sizeof(unsigned), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(bins.bbox, 0, 4 * sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
   const int blocks = (nb + kThreads - 1) / kThreads;
   if (nb > 0)
     k_bin<0><<<blocks, kThreads, 0, s>>>(B, nb, scale, geo.g, geo.tiles_c, bins.count, nullptr,
-                                         nullptr);
-  k_bin_scan<<<1, kThreads, 0, s>>>(bins.count, ntiles, bins.offset, bins.cursor, bins.work,
-                                    bins.nwork, (int)bins.wcap);
+                                         nullptr, bins.bbox);
+  k_bin_scan<<<1, kScanThreads, 0, s>>>(bins.count, bins.bbox, ntiles, geo.tiles_c, geo.g,
+                                    geo.layout, bins.offset, bins.cursor, bins.work, bins.nwork,
+                                    (int)bins.wcap, bins.multi, bins.nmulti);
   if (nb > 0)
     k_bin<1><<<blocks, kThreads, 0, s>>>(B, nb, scale, geo.g, geo.tiles_c, bins.cursor,
-                                         bins.offset, bins.entries);
+                                         bins.offset, bins.entries, nullptr);
   return cudaGetLastError();
 }
 
 cudaError_t fip_launch_grid(const FipGeom& geo, const float* B, const void* vr, const void* vi,
                             int vis_type, const float* vis_scale, const float* V, int nb,
                             const FipBins& bins, float2* grid, int compensated, cudaStream_t s) {
-  cudaError_t e = cudaMemsetAsync(grid, 0, (size_t)geo.g * geo.hp * sizeof(float2), s);
-  if (e != cudaSuccess) return e;
-  if (nb <= 0) return cudaSuccess;
   const float scale = geo.cell * (float)(size_t)geo.g;
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const size_t smem = (compensated ? 2 : 1) * FIP_GTILE * FIP_GTILE * sizeof(float2);
-  const int blocks = sms * (compensated ? 3 : 6);
+  const int sms = sm_count();
+  k_zero_tiles<<<sms, kThreads, 0, s>>>(bins.multi, bins.nmulti, geo.tiles_c, geo.g, geo.hp,
+                                        geo.layout, grid);
+  const size_t smem = sizeof(GridSmem) + (compensated ? 2 * FIP_GTILE * kTS * sizeof(float) : 0);
+  const int blocks = sms * (compensated ? 2 : 3);
 #define FIP_GRID_CASE(VT, C)                                                                    \
   do {                                                                                          \
     auto kern = k_grid<VT, C>;                                                                  \
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);         \
     kern<<<blocks, kThreads, smem, s>>>(B, vr, vi, vis_scale, V, scale, geo.g, geo.hp,          \
-                                        geo.tiles_c, bins.entries, bins.work, bins.nwork, grid); \
+                                        geo.tiles_c, geo.layout, bins.entries, bins.work,       \
+                                        bins.nwork, grid);                                      \
   } while (0)
   if (vis_type == FIP_VIS_F32) {
     if (compensated) FIP_GRID_CASE(FIP_VIS_F32, true); else FIP_GRID_CASE(FIP_VIS_F32, false);
@@ -731,17 +1014,60 @@ cudaError_t fip_launch_grid(const FipGeom& geo, const float* B, const void* vr, 
     if (compensated) FIP_GRID_CASE(FIP_VIS_BF16, true); else FIP_GRID_CASE(FIP_VIS_BF16, false);
   }
 #undef FIP_GRID_CASE
+  (void)nb;
   return cudaGetLastError();
 }
 
-cudaError_t fip_launch_reproject_scatter(const FipGeom& geo, const float* fft_out,
-                                         const float* taper, const float* V, int nb, float* dst,
-                                         cudaStream_t s) {
+static cudaError_t fft_smem_attr(const FipGeom& geo, size_t& smem) {
+  smem = (size_t)fipfft::smem_elems(geo.g) * sizeof(float2);
+  cudaError_t e = cudaFuncSetAttribute(k_fft_cols, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_fft_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return e;
+}
+
+cudaError_t fip_launch_fft_cols(const FipGeom& geo, const float2* grid, const unsigned* bbox,
+                                float2* colbuf, const float2* twiddles, const fipfft::Plan& plan,
+                                cudaStream_t s) {
+  size_t smem;
+  cudaError_t e = fft_smem_attr(geo, smem);
+  if (e != cudaSuccess) return e;
+  k_fft_cols<<<geo.hp, plan.nt, smem, s>>>(grid, bbox, colbuf, geo.n, plan, twiddles);
+  return cudaGetLastError();
+}
+
+cudaError_t fip_launch_fft_rows(const FipGeom& geo, const float2* colbuf, const unsigned* bbox,
+                                const float* taper, const float2* twiddles,
+                                const fipfft::Plan& plan, float* pre, cudaStream_t s) {
+  size_t smem;
+  cudaError_t e = fft_smem_attr(geo, smem);
+  if (e != cudaSuccess) return e;
+  k_fft_rows<<<geo.n / 2, plan.nt, smem, s>>>(colbuf, bbox, taper, pre, geo.n, plan, twiddles);
+  return cudaGetLastError();
+}
+
+cudaError_t fip_launch_correct_c2r(const FipGeom& geo, const float* fft_out, const float* taper,
+                                   float* pre, cudaStream_t s) {
+  dim3 bl((geo.n + kThreads - 1) / kThreads, geo.n);
+  k_correct_c2r<<<bl, kThreads, 0, s>>>(fft_out, taper, geo.n, geo.g, pre);
+  return cudaGetLastError();
+}
+
+cudaError_t fip_launch_targets(const FipGeom& geo, const float* V, float2* targets,
+                               cudaStream_t s) {
+  const int per = kThreads * kTargetsPerThread;
+  dim3 bl((geo.n + per - 1) / per, geo.n);
+  k_targets<<<bl, kThreads, 0, s>>>(V, geo.n, cell_degrees(geo.cell), targets);
+  return cudaGetLastError();
+}
+
+cudaError_t fip_launch_reproject_scatter(const FipGeom& geo, const float* pre, const float* V,
+                                         int nb, float* dst, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(dst, 0, (size_t)geo.n * geo.n * sizeof(float), s);
   if (e != cudaSuccess) return e;
   dim3 th(32, 8), bl((geo.n + 31) / 32, (geo.n + 7) / 8);
-  k_reproject_scatter<<<bl, th, 0, s>>>(fft_out, taper, V, geo.n, geo.g, nb,
-                                        cell_degrees(geo.cell), dst);
+  k_reproject_scatter<<<bl, th, 0, s>>>(pre, V, geo.n, nb, cell_degrees(geo.cell), dst);
   return cudaGetLastError();
 }
 
@@ -750,20 +1076,22 @@ cudaError_t fip_launch_reproject_scatter(const FipGeom& geo, const float* fft_ou
 // expressed in pixels (the chain evaluates cos(theta) ~ R in degrees).
 static float chain_delta(float cell) { return 0.5f + 8.0f * 4.76837158e-7f / cell; }
 
-cudaError_t fip_launch_reproject_gather(const FipGeom& geo, const float* fft_out,
-                                        const float* taper, const float* V, int nb, float* dst,
+bool fip_gather_supported(const FipGeom& geo, int exact_targets) {
+  return exact_targets || chain_delta(geo.cell) <= 40.f;
+}
+
+cudaError_t fip_launch_reproject_gather(const FipGeom& geo, const float* pre,
+                                        const float2* targets, const float* V, int nb, float* dst,
                                         unsigned* img_max, int exact_targets, cudaStream_t s) {
   const int tiles = (geo.n + kDT - 1) / kDT;
   const float delta = exact_targets ? 0.25f : chain_delta(geo.cell);
-  if (delta > 40.f) return cudaErrorInvalidValue;
+  if (!fip_gather_supported(geo, exact_targets)) return cudaErrorInvalidValue;
   if (exact_targets)
-    k_reproject_gather<true><<<tiles * tiles, kThreads, 0, s>>>(
-        fft_out, taper, V, geo.n, geo.g, nb, cell_degrees(geo.cell), geo.cell, delta, dst,
-        img_max);
+    k_reproject_gather<true><<<tiles * tiles, kThreads, 0, s>>>(pre, nullptr, V, geo.n, nb,
+                                                                 geo.cell, delta, dst, img_max);
   else
-    k_reproject_gather<false><<<tiles * tiles, kThreads, 0, s>>>(
-        fft_out, taper, V, geo.n, geo.g, nb, cell_degrees(geo.cell), geo.cell, delta, dst,
-        img_max);
+    k_reproject_gather<false><<<tiles * tiles, kThreads, 0, s>>>(pre, targets, V, geo.n, nb,
+                                                                  geo.cell, delta, dst, img_max);
   return cudaGetLastError();
 }
 

@@ -35,6 +35,41 @@ __constant__ float fip_quad_kernel[14] = {
 
 namespace fipref {
 
+// Correctly rounded double quotient x / d for the constant divisors of the
+// chain (180 and pi), by one Markstein correction of the product with the
+// rounded reciprocal: q0 = x * (1/d), e = x - q0 * d (exact with an FMA),
+// q = q0 + e * (1/d) (P. Markstein, "Computation of elementary functions on
+// the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990).  This
+// equals the IEEE division the reference performs (verified against the
+// reference's own targets), at three FP64 operations instead of a division.
+__device__ __forceinline__ double div_const(double x, double d, double rinv) {
+  const double q0 = x * rinv;
+  const double e = fma(-q0, d, x);
+  return fma(e, rinv, q0);
+}
+#define FIP_INV_180 (1.0 / 180.0)
+#define FIP_INV_PI (1.0 / FIP_M_PI)
+// (double)a * M_PI / 180.0, as the reference evaluates the degree-to-radian
+// conversion inside sinf/cosf arguments (FIPkernels.cu:96-97, 116, 135).
+__device__ __forceinline__ float deg_to_rad_arg(float a) {
+  return (float)div_const((double)a * FIP_M_PI, 180.0, FIP_INV_180);
+}
+// (double)(v * 180.0f) / M_PI, the radian-to-degree step of the reference's
+// atan2/acos/asin helpers (FIPkernels.cu:145, 157, 169).
+__device__ __forceinline__ float rad_to_deg_ret(float v180) {
+  return (float)div_const((double)v180, FIP_M_PI, FIP_INV_PI);
+}
+
+// fmodf(a, 90.0f) == 0, i.e. a is an exact multiple of 90.  fmod is exact,
+// so for |a| < 90 it equals a, and for 90 <= |a| < 180 it equals |a| - 90
+// (Sterbenz); only larger angles need the library call.
+__device__ __forceinline__ bool multiple_of_90(float a) {
+  const float m = fabsf(a);
+  if (m < 90.0f) return a == 0.0f;
+  if (m < 180.0f) return m == 90.0f;
+  return fmodf(a, 90.0f) == 0;
+}
+
 // computeCeil/computeFloor semantics (FIPkernels.cu:47-61): equal to
 // ceilf/floorf, returned as a signed integer.
 __device__ __forceinline__ long ceil_l(float v) { return v < 0 ? -(long)floorf(-v) : (long)ceilf(v); }
@@ -65,7 +100,7 @@ __device__ __forceinline__ float taper(size_t t, size_t g) {
 // Degree-based trigonometry with exact values at multiples of 90 degrees
 // (FIPkernels.cu:73-171).
 __device__ __forceinline__ void sincos_deg(float a, float& s, float& c) {
-  if (fmodf(a, 90.0f) == 0) {
+  if (multiple_of_90(a)) {
     int i = static_cast<int>(fabsf((float)floor_l(a / 90.0f + 0.5f))) % 4;
     switch (i) {
       case 0: s = 0.0f; c = 1.0f; break;
@@ -74,45 +109,46 @@ __device__ __forceinline__ void sincos_deg(float a, float& s, float& c) {
       default: s = (a > 0.0f) ? -1.0f : 1.0f; c = 0.0f; break;
     }
   } else {
-    s = sinf(a * FIP_M_PI / 180.0f);
-    c = cosf(a * FIP_M_PI / 180.0f);
+    const float arg = deg_to_rad_arg(a);
+    s = sinf(arg);
+    c = cosf(arg);
   }
 }
 
 __device__ __forceinline__ float sin_deg(float a) {
-  if (fmodf(a, 90.0f) == 0) {
+  if (multiple_of_90(a)) {
     int i = static_cast<int>(fabsf((float)floor_l(a / 90.0f - 0.5f))) % 4;
     return i == 0 ? 1.0f : (i == 2 ? -1.0f : 0.0f);
   }
-  return sinf(a * FIP_M_PI / 180.0f);
+  return sinf(deg_to_rad_arg(a));
 }
 
 __device__ __forceinline__ float cos_deg(float a) {
-  if (fmodf(a, 90.0f) == 0) {
+  if (multiple_of_90(a)) {
     int i = static_cast<int>(fabsf((float)floor_l(a / 90.0f + 0.5f))) % 4;
     return i == 0 ? 1.0f : (i == 2 ? -1.0f : 0.0f);
   }
-  return cosf(a * FIP_M_PI / 180.0f);
+  return cosf(deg_to_rad_arg(a));
 }
 
 __device__ __forceinline__ float atan2_deg(float y, float x) {
   if (y == 0.0f) return (x >= 0.0f) ? 0.0f : 180.0f;
   if (x == 0.0f) return (y > 0.0f) ? 90.0f : -90.0f;
-  return atan2f(y, x) * 180.0f / FIP_M_PI;
+  return rad_to_deg_ret(atan2f(y, x) * 180.0f);
 }
 
 __device__ __forceinline__ float acos_deg(float v) {
   if (v >= 1.0f && v - 1.0f < 1e-10) return 0.0f;
   if (v == 0.0f) return 90.0f;
   if (v <= -1.0f && v + 1.0f > -1e-10) return 180.0f;
-  return acosf(v) * 180.0f / FIP_M_PI;
+  return rad_to_deg_ret(acosf(v) * 180.0f);
 }
 
 __device__ __forceinline__ float asin_deg(float v) {
   if (v <= -1.0f && v + 1.0f > -1e-10) return -90.0f;
   if (v == 0.0f) return 0.0f;
   if (v >= 1.0f && v - 1.0f < 1e-10) return 90.0f;
-  return asinf(v) * 180.0f / FIP_M_PI;
+  return rad_to_deg_ret(asinf(v) * 180.0f);
 }
 
 // Per-snapshot constants of the pixel mapping.

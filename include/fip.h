@@ -128,6 +128,25 @@ const float* fip_imager_image(const fip_imager* im, int k);
 int fip_pipe_host(fip_imager* im, const float* vis_re, const float* vis_im, const float* B,
                   const float* V, size_t nb, size_t num_snapshots, float* result);
 
+/*
+ * Stage timing (the reference's cudaEvent "Time elapsed" prints,
+ * FIPkernels.cu:570-581, 766-770, 825-846, as data): when enabled, every
+ * stage launch is bracketed by CUDA events on its stream and the device time
+ * is accumulated per stage (fip_stage_name(k), k < fip_stage_count()).
+ * Enabling resets the totals.  Collection synchronises the recorded events.
+ */
+int fip_imager_set_profiling(fip_imager* im, int enable);
+int fip_imager_stage_times(fip_imager* im, double* total_ms, long* launches, int nstages);
+const char* fip_stage_name(int stage);
+int fip_stage_count(void);
+/* Number of kernels this imager has launched (library-owned kernels only). */
+unsigned long long fip_imager_kernel_launches(const fip_imager* im);
+/* Occupied uv band of the last gridded snapshot: max |r1| (grid rows) and
+ * max half-plane column, in grid cells (synchronous). */
+int fip_imager_band(fip_imager* im, unsigned* max_row, unsigned* max_col);
+/* Grid side G = ceil(1.5 N) (FIPkernels.cu:583). */
+int fip_imager_grid_side(const fip_imager* im);
+
 /* Per-pixel targets (LL, MM) of the reprojection, [N*N][2] (device), for
  * tests: exact = 0 the plain form's FP32 chain, 1 the exact closed form. */
 int fip_pixel_targets(fip_imager* im, const float* V, float* out, int exact, void* stream);

@@ -1,0 +1,357 @@
+"""GPU parity tests of the CUDA path (through the C ABI) against the oracles.
+
+Checkers:
+* the reference's own CUDA build (oracle/_ref/libfipref.so), run live when
+  present, and its golden fixtures (tests/golden/*.npz);
+* the FP64 CPU oracle (oracle/fip_oracle.c).
+
+Tolerances (the project's parity bar):
+* plain FP32 form vs the reference: pixel targets bit-identical, images
+  <= 1e-5 relative RMS (float-atomic summation order differs), tLISI <= 1e-4
+  absolute;
+* plain form vs FP64: the reference's own error level (images <= 1e-2
+  relative RMS, tLISI <= 2e-3);
+* precision form vs FP64: tLISI <= 1e-4 absolute, images <= 1e-4 relative RMS
+  (FP32 storage <= 3e-5).
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import fastimagingpipe_b200 as fip
+from fastimagingpipe_b200 import fits, synthetic
+import oracle
+from oracle import reference as ref
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def relrms(a, b):
+    return float(np.sqrt(((a - b) ** 2).mean() / (b ** 2).mean()))
+
+
+def to_dev(snap, dev):
+    import torch
+    return {k: torch.tensor(np.ascontiguousarray(getattr(snap, k)), device=dev)
+            for k in ("vis_re", "vis_im", "B", "V")}
+
+
+def run(snap, dev, **kw):
+    """Images the three snapshots and computes the trigger through the C ABI.
+    -> (tlisi [U,U], images [3,N,N], maxima [3])."""
+    import torch
+    n, nb, t = snap.image_size, snap.num_baselines, snap.unit_size
+    u = n // t
+    d = to_dev(snap, dev)
+    imgs = torch.zeros((3, n * n), device=dev)
+    mx = torch.zeros(3, device=dev)
+    res = torch.zeros(u * u, device=dev)
+    with fip.Imager(n, nb, snap.cell_size, t, **kw) as im:
+        for k in range(3):
+            im.image_snapshot(d["vis_re"][k * nb:], d["vis_im"][k * nb:], d["B"][2 * k * nb:],
+                              d["V"][9 * k:], nb, imgs[k], mx[k:])
+        im.trigger(imgs[0], imgs[1], imgs[2], mx, res)
+        torch.cuda.synchronize()
+    return (res.cpu().numpy().reshape(u, u), imgs.cpu().numpy().reshape(3, n, n),
+            mx.cpu().numpy())
+
+
+def targets(snap, dev, exact=False, k=0):
+    import torch
+    n = snap.image_size
+    out = torch.zeros(n * n * 2, device=dev)
+    V = torch.tensor(snap.V[9 * k:9 * k + 9], device=dev)
+    with fip.Imager(n, snap.num_baselines, snap.cell_size, snap.unit_size) as im:
+        im.pixel_targets(V, out, exact=exact)
+        torch.cuda.synchronize()
+    return out.cpu().numpy().reshape(n, n, 2)
+
+
+needs_ref = pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+
+
+@pytest.fixture(scope="module")
+def small():
+    return synthetic.config_small(transient_snapshot=2)
+
+
+@pytest.fixture(scope="module")
+def tiny():
+    return synthetic.config_tiny(transient_snapshot=2)
+
+
+# ---------------------------------------------------------------- reference
+
+def test_targets_bit_identical_to_reference_fixture(cuda, tiny):
+    g = np.load(os.path.join(GOLDEN, "reference_tiny.npz"))
+    assert np.array_equal(targets(tiny, cuda), g["targets0"])
+
+
+def test_small_against_reference_fixture(cuda, small):
+    g = np.load(os.path.join(GOLDEN, "reference_small.npz"))
+    res, imgs, mx = run(small, cuda)
+    pix = g["target_pixels"]
+    tg = targets(small, cuda)
+    assert np.array_equal(tg[pix[:, 0], pix[:, 1]], g["targets"])
+    assert np.abs(res - g["tlisi"]).max() <= 1e-4
+    assert np.allclose(mx, g["maxall"], rtol=1e-5)
+    for k in range(3):
+        r0, c0 = g["crop_origins"][k]
+        assert relrms(imgs[k][r0:r0 + 64, c0:c0 + 64], g["crops"][k]) <= 1e-5
+    assert np.allclose(imgs.sum(axis=2), g["row_sums"], rtol=1e-5, atol=1e-4)
+
+
+def test_tiny_images_against_reference_fixture(cuda, tiny):
+    g = np.load(os.path.join(GOLDEN, "reference_tiny.npz"))
+    res, imgs, mx = run(tiny, cuda)
+    for k in range(3):
+        assert relrms(imgs[k], g["images"][k]) <= 1e-5
+    assert np.abs(res - g["tlisi"]).max() <= 1e-4
+
+
+@needs_ref
+@pytest.mark.parametrize("cfg", ["tiny", "small", "fallback96"])
+def test_live_reference_parity(cuda, cfg):
+    snap = {"tiny": lambda: synthetic.config_tiny(transient_snapshot=2),
+            "small": lambda: synthetic.config_small(transient_snapshot=2),
+            "fallback96": lambda: synthetic.config_tiny(image_size=96, cell_size=1.6e-4,
+                                                        transient_snapshot=2)}[cfg]()
+    n, nb = snap.image_size, snap.num_baselines
+    assert np.array_equal(targets(snap, cuda, k=1), ref.pixel_targets(snap.V[9:18], n,
+                                                                       snap.cell_size))
+    res, imgs, mx = run(snap, cuda)
+    for k in range(3):
+        vr, vi, B, V = snap.snapshot(k)
+        rimg, _, rmx = ref.image_snapshot(vr, vi, B, V, nb, n, snap.cell_size)
+        assert relrms(imgs[k], rimg) <= 1e-5
+        assert mx[k] == pytest.approx(rmx, rel=1e-5)
+    assert np.abs(res - ref.fipipe(snap)).max() <= 1e-4
+
+
+@needs_ref
+def test_reference_shape_tlisi_matches_reference(cuda):
+    snap = synthetic.config_reference(transient_snapshot=2)
+    got = fip.FIpipe(snap.vis_re, snap.vis_im, snap.B, snap.V, snap.num_baselines,
+                     snap.image_size, 3, snap.cell_size, snap.unit_size)
+    want = ref.fipipe(snap)
+    assert np.abs(got - want).max() <= 1e-4
+    assert np.unravel_index(np.argmin(got), got.shape) == np.unravel_index(np.argmin(want),
+                                                                          got.shape)
+
+
+# ---------------------------------------------------------------- FP64 oracle
+
+def test_plain_form_vs_fp64(cuda, small):
+    res, imgs, mx = run(small, cuda)
+    r64, i64, m64 = oracle.fipipe(small, "f64", want_images=True)
+    for k in range(3):
+        assert relrms(imgs[k], i64[k]) <= 1e-2
+    assert np.abs(res - r64).max() <= 2e-3
+    assert np.unravel_index(np.argmin(res), res.shape) == np.unravel_index(np.argmin(r64),
+                                                                          res.shape)
+
+
+@pytest.mark.parametrize("storage,img_tol", [(fip.STORE_F32, 3e-5), (fip.STORE_F16, 2e-4),
+                                             (fip.STORE_BF16, 3e-3)])
+def test_precision_form_vs_fp64(cuda, small, storage, img_tol):
+    res, imgs, mx = run(small, cuda, form=fip.FORM_PRECISE, vis_storage=storage)
+    r64, i64, m64 = oracle.fipipe(small, "f64", want_images=True)
+    for k in range(3):
+        assert relrms(imgs[k], i64[k]) <= img_tol
+    assert np.abs(res - r64).max() <= 1e-4
+
+
+def test_exact_targets_vs_oracle(cuda, small):
+    tg = targets(small, cuda, exact=True)
+    o = oracle.pixel_targets(small.V[:9], small.image_size, small.cell_size, "f64")
+    assert np.abs(tg - o).max() <= 1e-4
+
+
+def test_cufft_fallback_size_vs_fp64(cuda):
+    snap = synthetic.config_tiny(image_size=100, cell_size=1.5e-4, unit_size=20,
+                                 transient_snapshot=2)
+    res, imgs, _ = run(snap, cuda, form=fip.FORM_PRECISE)
+    r64, i64, _ = oracle.fipipe(snap, "f64", want_images=True)
+    for k in range(3):
+        assert relrms(imgs[k], i64[k]) <= 3e-5
+    assert np.abs(res - r64).max() <= 1e-4
+
+
+# ---------------------------------------------------------------- internal consistency
+
+def test_gather_equals_scatter(cuda, small):
+    _, a, ma = run(small, cuda)
+    _, b, mb = run(small, cuda, reproject=fip.REPROJECT_SCATTER)
+    for k in range(3):
+        assert relrms(a[k], b[k]) <= 1e-6
+    assert np.allclose(ma, mb, rtol=1e-6)
+
+
+def test_host_and_device_entry_points_agree(cuda, tiny):
+    import torch
+    res, _, _ = run(tiny, cuda)
+    host = fip.FIpipe(tiny.vis_re, tiny.vis_im, tiny.B, tiny.V, tiny.num_baselines,
+                      tiny.image_size, 3, tiny.cell_size, tiny.unit_size)
+    assert np.abs(host - res).max() <= 1e-6
+    d = to_dev(tiny, cuda)
+    u = tiny.image_size // tiny.unit_size
+    out = torch.zeros(u * u, device=cuda)
+    with fip.Imager(tiny.image_size, tiny.num_baselines, tiny.cell_size, tiny.unit_size) as im:
+        im.pipe_device(d["vis_re"], d["vis_im"], d["B"], d["V"], tiny.num_baselines, out)
+        assert np.abs(im.pipe_host(tiny.vis_re, tiny.vis_im, tiny.B, tiny.V,
+                                   tiny.num_baselines) - res).max() <= 1e-6
+    assert np.abs(out.cpu().numpy().reshape(u, u) - res).max() <= 1e-6
+
+
+def test_sequence_matches_triples(cuda):
+    import torch
+    snap = synthetic.config_tiny(n_snap=5, transient_snapshot=3)
+    n, nb, t = snap.image_size, snap.num_baselines, snap.unit_size
+    u = n // t
+    d = to_dev(snap, cuda)
+    seq = torch.zeros(3 * u * u, device=cuda)
+    with fip.Imager(n, nb, snap.cell_size, t) as im:
+        im.image_sequence(d["vis_re"], d["vis_im"], d["B"], d["V"], [nb] * 5, nb, seq)
+        torch.cuda.synchronize()
+    seq = seq.cpu().numpy().reshape(3, u, u)
+    for k in range(3):
+        sub = synthetic.SnapshotSet(
+            vis_re=snap.vis_re[k * nb:(k + 3) * nb], vis_im=snap.vis_im[k * nb:(k + 3) * nb],
+            B=snap.B[2 * k * nb:2 * (k + 3) * nb], V=snap.V[9 * k:9 * (k + 3)],
+            num_baselines=nb, num_snapshots=3, image_size=n, cell_size=snap.cell_size,
+            unit_size=t, frequency_hz=snap.frequency_hz)
+        res, _, _ = run(sub, cuda)
+        assert np.abs(seq[k] - res).max() <= 1e-6
+
+
+# ---------------------------------------------------------------- edge cases
+
+def test_identical_snapshots_give_unit_tlisi(cuda):
+    snap = synthetic.config_tiny()
+    nb = snap.num_baselines
+    for a in (snap.vis_re, snap.vis_im):
+        a[nb:2 * nb] = a[:nb]
+        a[2 * nb:] = a[:nb]
+    snap.B[2 * nb:4 * nb] = snap.B[:2 * nb]
+    snap.B[4 * nb:] = snap.B[:2 * nb]
+    snap.V[9:18] = snap.V[:9]
+    snap.V[18:] = snap.V[:9]
+    res, _, _ = run(snap, cuda)
+    assert np.abs(res - 1.0).max() <= 1e-6
+
+
+def test_zero_visibilities_give_nan_like_reference(cuda):
+    snap = synthetic.config_tiny()
+    snap.vis_re[:] = 0
+    snap.vis_im[:] = 0
+    res, imgs, mx = run(snap, cuda)
+    assert np.all(mx == 0) and np.all(imgs == 0)
+    assert np.all(np.isnan(res))
+
+
+def test_flagged_zero_padded_baselines(cuda):
+    snap = synthetic.config_tiny(flag_fraction_max=0.3, transient_snapshot=2, seed=9)
+    res, imgs, _ = run(snap, cuda, form=fip.FORM_PRECISE)
+    r64, i64, _ = oracle.fipipe(snap, "f64", want_images=True)
+    assert np.abs(res - r64).max() <= 1e-4
+    for k in range(3):
+        assert relrms(imgs[k], i64[k]) <= 3e-5
+
+
+def test_single_baseline_and_ragged_tiles(cuda):
+    snap = synthetic.config_tiny(n_ant=2, unit_size=24, transient_snapshot=None)
+    assert snap.num_baselines == 1
+    res, imgs, _ = run(snap, cuda, form=fip.FORM_PRECISE)
+    r64, i64, _ = oracle.fipipe(snap, "f64", want_images=True)
+    assert res.shape == (5, 5)
+    assert np.allclose(res, r64, atol=1e-4, equal_nan=True)
+
+
+def test_invalid_sizes_raise(cuda):
+    with pytest.raises(fip.FipError):
+        fip.Imager(102, 10, 1e-3, 16)
+    with fip.Imager(64, 10, 1e-3, 16) as im:
+        import torch
+        z = torch.zeros(1000, device=cuda)
+        with pytest.raises(fip.FipError):
+            im.image_snapshot(z, z, z, z, 11, z)
+
+
+def test_profiling_and_launch_count(cuda, tiny):
+    import torch
+    d = to_dev(tiny, cuda)
+    u = tiny.image_size // tiny.unit_size
+    out = torch.zeros(u * u, device=cuda)
+    with fip.Imager(tiny.image_size, tiny.num_baselines, tiny.cell_size, tiny.unit_size) as im:
+        im.set_profiling(True)
+        before = im.kernel_launches
+        im.pipe_device(d["vis_re"], d["vis_im"], d["B"], d["V"], tiny.num_baselines, out)
+        st = im.stage_times()
+        assert im.kernel_launches - before >= 3 * 9 + 1
+        for k in ("bin", "grid", "fft_rows", "targets", "reproject", "trigger"):
+            assert st[k][1] >= 1 and st[k][0] > 0
+
+
+# ---------------------------------------------------------------- preprocessing
+
+def test_plane_projection_vs_oracle(cuda):
+    import torch
+    snap = synthetic.config_small()
+    rows = snap.num_baselines
+    freqs = np.array([130e6, 140e6, 150e6], np.float32)
+    uvw = snap.uvw_m[0].reshape(-1).astype(np.float32)
+    B = torch.zeros(rows * 3 * 2, device=cuda)
+    V = torch.zeros(9, device=cuda)
+    fip.plane_project(torch.tensor(uvw, device=cuda), torch.tensor(freqs, device=cuda), rows, 3,
+                      B, V)
+    torch.cuda.synchronize()
+    Bo, Vo = oracle.plane_fit(uvw.reshape(-1, 3), freqs)
+    assert np.allclose(V.cpu().numpy().reshape(3, 3), Vo, atol=1e-6)
+    assert np.allclose(B.cpu().numpy().reshape(-1, 2), Bo, rtol=1e-5, atol=1e-3)
+
+
+def test_collapse_vs_oracle(cuda):
+    import torch
+    rng = np.random.default_rng(3)
+    ns = 10000
+    arrs = [rng.standard_normal(ns).astype(np.float32) for _ in range(4)]
+    f0 = (rng.random(ns) < 0.3).astype(np.uint8)
+    f3 = (rng.random(ns) < 0.3).astype(np.uint8)
+    w0 = rng.random(ns).astype(np.float32)
+    w3 = rng.random(ns).astype(np.float32)
+    t = lambda a: torch.tensor(a, device=cuda)
+    o_re = torch.zeros(ns, device=cuda)
+    o_im = torch.zeros(ns, device=cuda)
+    fip.collapse_visibilities(*(t(a) for a in arrs), t(f0), t(f3), t(w0), t(w3), o_re, o_im, ns)
+    torch.cuda.synchronize()
+    w_re, w_im = oracle.collapse(*arrs, f0, f3, w0, w3)
+    assert np.allclose(o_re.cpu().numpy(), w_re, rtol=1e-6, atol=1e-6)
+    assert np.allclose(o_im.cpu().numpy(), w_im, rtol=1e-6, atol=1e-6)
+
+
+# ---------------------------------------------------------------- command line
+
+@pytest.mark.parametrize("with_freq", [True, False])
+def test_cli_end_to_end(cuda, tiny, tmp_path, with_freq):
+    nb, n = tiny.num_baselines, tiny.image_size
+    p = {k: str(tmp_path / f"{k}.fits") for k in ("vr", "vi", "B", "V")}
+    fits.write_image(p["vr"], tiny.vis_re[:, None])
+    fits.write_image(p["vi"], tiny.vis_im[:, None])
+    fits.write_image(p["B"], tiny.B.reshape(-1, 2))
+    fits.write_image(p["V"], tiny.V.reshape(-1, 3))
+    out = str(tmp_path / "out.fits")
+    args = [fip.CLI_PATH, p["vr"], p["vi"], p["B"], p["V"], str(n), str(nb)]
+    if with_freq:
+        args.append(str(tiny.frequency_hz))
+    args += [repr(tiny.cell_size), "3", str(tiny.unit_size), out]
+    r = subprocess.run(args, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    got = fits.read_image(out)
+    want = fip.FIpipe(tiny.vis_re, tiny.vis_im, tiny.B, tiny.V, nb, n, 3, tiny.cell_size,
+                      tiny.unit_size)
+    assert got.shape == want.shape
+    assert np.abs(got - want).max() <= 1e-6
