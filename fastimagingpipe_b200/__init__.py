@@ -86,6 +86,7 @@ def lib() -> ctypes.CDLL:
         L.fip_imager_kernel_launches.restype = ctypes.c_ulonglong
         L.fip_imager_band.argtypes = [vp, ctypes.POINTER(ctypes.c_uint), ctypes.POINTER(ctypes.c_uint)]
         L.fip_imager_grid_side.argtypes = [vp]
+        L.fip_grid_snapshot.argtypes = [vp, vp, vp, vp, vp, sz, vp, vp]
         _lib = L
     return _lib
 
@@ -202,6 +203,11 @@ class Imager:
     def image_snapshot(self, vis_re, vis_im, B, V, nb: int, image, image_max=None, stream=None):
         _check(lib().fip_image_snapshot(self._h, _ptr(vis_re), _ptr(vis_im), _ptr(B), _ptr(V), nb,
                                         _ptr(image), _ptr(image_max), _stream(stream)))
+
+    def grid_snapshot(self, vis_re, vis_im, B, V, nb: int, grid, stream=None):
+        """Gridding stage only: grid [G][G/2+1] complex (2 floats each)."""
+        _check(lib().fip_grid_snapshot(self._h, _ptr(vis_re), _ptr(vis_im), _ptr(B), _ptr(V),
+                                       nb, _ptr(grid), _stream(stream)))
 
     def trigger(self, I1, I2, I3, max3, result, stream=None):
         _check(lib().fip_trigger(self._h, _ptr(I1), _ptr(I2), _ptr(I3), _ptr(max3), _ptr(result),

@@ -93,6 +93,8 @@ struct StageTimer {
 
 }  // namespace
 
+int fip_set_error(int code, const std::string& msg) { return fail(code, msg); }
+
 struct fip_imager {
   fip_imager_config cfg{};
   FipGeom geo{};
@@ -473,6 +475,36 @@ int fip_image_snapshot(fip_imager* im, const float* vis_re, const float* vis_im,
   cudaStream_t s = (cudaStream_t)stream;
   FIP_TRY(call_enter(im, s));
   FIP_TRY(image_snapshot_impl(im, vis_re, vis_im, B, V, nb, image, image_max, s));
+  return call_leave(im, s);
+}
+
+int fip_grid_snapshot(fip_imager* im, const float* vis_re, const float* vis_im, const float* B,
+                      const float* V, size_t nb, float* grid, void* stream) {
+  if (!im) return fail(FIP_ERR_ARG, "null imager");
+  if (!vis_re || !vis_im || !B || !V || !grid) return fail(FIP_ERR_ARG, "null device pointer");
+  if (nb == 0 || nb > im->cfg.max_baselines)
+    return fail(FIP_ERR_ARG, "nb must be in [1, the imager's max_baselines]");
+  DeviceGuard g(im->cfg.device);
+  cudaStream_t s = (cudaStream_t)stream;
+  FIP_TRY(call_enter(im, s));
+  // Full half plane, row-major: every tile is written (zero where empty).
+  FipGeom geo = im->geo;
+  geo.layout = 0;
+  const bool precise = im->cfg.form == FIP_FORM_PRECISE;
+  const void* gvr = vis_re;
+  const void* gvi = vis_im;
+  int vt = FIP_VIS_F32;
+  if (precise && im->cfg.vis_storage != FIP_STORE_F32) {
+    vt = im->cfg.vis_storage == FIP_STORE_F16 ? FIP_VIS_F16 : FIP_VIS_BF16;
+    FIP_CUDA(fip_launch_quantize(vis_re, vis_im, nb, vt, im->q_re, im->q_im, im->q_scale, s));
+    im->launches += 3;
+    gvr = im->q_re;
+    gvi = im->q_im;
+  }
+  FIP_CUDA(fip_launch_bin(geo, B, (int)nb, im->bins, s));
+  FIP_CUDA(fip_launch_grid(geo, B, gvr, gvi, vt, im->q_scale, V, (int)nb, im->bins,
+                           reinterpret_cast<float2*>(grid), precise ? 1 : 0, s));
+  im->launches += 5;
   return call_leave(im, s);
 }
 

@@ -6,8 +6,13 @@
 #include <cuda_fp16.h>
 #include <cuda_bf16.h>
 
+#include <string>
+
 #include "fip_common.cuh"
 #include "fip_fft.cuh"
+
+// Records the calling thread's last error message and returns `code`.
+int fip_set_error(int code, const std::string& msg);
 
 // Scratch of the tile-binned gridder for one image size.
 struct FipBins {

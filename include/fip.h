@@ -103,6 +103,19 @@ int fip_image_snapshot(fip_imager* im, const float* vis_re, const float* vis_im,
                        const float* V, size_t nb, float* image, float* image_max, void* stream);
 
 /*
+ * The gridding stage alone (device): the visibilities of one snapshot,
+ * weighted by 1/|V00 V11 - V01 V10| and spread with the ES kernel, as the
+ * Hermitian half of the uv grid the reference builds (gridding +
+ * combineToComplex, FIPkernels.cu:188-254): grid [G][G/2+1] complex
+ * (interleaved float pairs, row-major, G = ceil(1.5 N)), holding
+ * h(r1, r2) = (g(r1, r2) + conj g(-r1, -r2)) / 2 at row r1 mod G, column
+ * r2 >= 0, where g is the reference's grid without its (-1)^(r1+r2)
+ * checkerboard.  This is the input layout of a C2R transform.
+ */
+int fip_grid_snapshot(fip_imager* im, const float* vis_re, const float* vis_im, const float* B,
+                      const float* V, size_t nb, float* grid, void* stream);
+
+/*
  * tLISI of three consecutive images (device): maxima max3 [3] as produced by
  * fip_image_snapshot, result [U*U].  The inputs are not modified (the
  * reference clamps I2 in place, FIPkernels.cu:836; the clamp here is local).

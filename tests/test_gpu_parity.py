@@ -181,6 +181,38 @@ def test_cufft_fallback_size_vs_fp64(cuda):
     assert np.abs(res - r64).max() <= 1e-4
 
 
+def hermitian_half_grid(snap, k=0):
+    """The oracle's checkerboarded grid (FIPkernels.cu:197-245) as the
+    half-plane Hermitian grid fip_grid_snapshot returns."""
+    vr, vi, B, V = snap.snapshot(k)
+    n = snap.image_size
+    g = oracle.grid_size(n)
+    gref = oracle.grid(B, vr, vi, V, snap.num_baselines, n, snap.cell_size)
+    r = np.arange(g) - g // 2
+    checker = np.where((r[:, None] + r[None, :]) % 2 == 0, 1.0, -1.0)
+    gw = np.fft.ifftshift(gref * checker)          # gw[r1 mod G, r2 mod G] = g(r1, r2)
+    gneg = np.roll(np.flip(gw, (0, 1)), 1, axis=(0, 1))  # g(-r1, -r2)
+    h = 0.5 * (gw + np.conj(gneg))
+    return h[:, : g // 2 + 1]
+
+
+@pytest.mark.parametrize("n", [512, 100])
+def test_grid_stage_vs_oracle(cuda, n):
+    import torch
+    snap = synthetic.config_small() if n == 512 else \
+        synthetic.config_tiny(image_size=100, cell_size=1.5e-4, unit_size=20)
+    g = oracle.grid_size(n)
+    d = to_dev(snap, cuda)
+    out = torch.zeros(g * (g // 2 + 1) * 2, device=cuda)
+    with fip.Imager(n, snap.num_baselines, snap.cell_size, snap.unit_size) as im:
+        im.grid_snapshot(d["vis_re"], d["vis_im"], d["B"], d["V"], snap.num_baselines, out)
+        torch.cuda.synchronize()
+    got = out.cpu().numpy().view(np.complex64).reshape(g, g // 2 + 1)
+    want = hermitian_half_grid(snap)
+    err = np.sqrt((np.abs(got - want) ** 2).mean() / (np.abs(want) ** 2).mean())
+    assert err <= 1e-5
+
+
 # ---------------------------------------------------------------- internal consistency
 
 def test_gather_equals_scatter(cuda, small):
