@@ -87,6 +87,7 @@ def lib() -> ctypes.CDLL:
         L.fip_imager_band.argtypes = [vp, ctypes.POINTER(ctypes.c_uint), ctypes.POINTER(ctypes.c_uint)]
         L.fip_imager_grid_side.argtypes = [vp]
         L.fip_grid_snapshot.argtypes = [vp, vp, vp, vp, vp, sz, vp, vp]
+        L.fip_grid_snapshot_noalloc.argtypes = [vp, vp, vp, vp, sz, sz, fp, vp, vp]
         _lib = L
     return _lib
 
@@ -237,6 +238,16 @@ class Imager:
         _check(lib().fip_image_sequence(self._h, _ptr(vis_re), _ptr(vis_im), _ptr(B), _ptr(V),
                                         nbs.ctypes.data, nb_stride, len(nbs), _ptr(results),
                                         _stream(stream)))
+
+
+def grid_snapshot_noalloc(vis_re, vis_im, B, V, nb: int, image_size: int, cell_size: float,
+                          grid, stream=None):
+    """Gridding of one snapshot that allocates nothing (for callers that cannot
+    allocate device memory): scratch in a fixed device array of the library;
+    nb <= 131072, image_size <= 4096.  Output as Imager.grid_snapshot."""
+    _check(lib().fip_grid_snapshot_noalloc(_ptr(vis_re), _ptr(vis_im), _ptr(B), _ptr(V), nb,
+                                           image_size, float(cell_size), _ptr(grid),
+                                           _stream(stream)))
 
 
 def plane_project(uvw, freqs, rows: int, chans: int, B, V, stream=None):

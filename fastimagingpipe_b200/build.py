@@ -29,6 +29,7 @@ UNITS = {
     "fip_plain.cu": ["--use_fast_math"],
     "fip_precise.cu": [],
     "fip_host.cu": [],
+    "fip_noalloc.cu": [],
 }
 HOST_CXX = ["fits_io.cpp"]
 

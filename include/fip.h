@@ -116,6 +116,24 @@ int fip_grid_snapshot(fip_imager* im, const float* vis_re, const float* vis_im, 
                       const float* V, size_t nb, float* grid, void* stream);
 
 /*
+ * fip_grid_snapshot without any allocation, for callers that cannot
+ * allocate device memory (fixed memory pools or arenas, plugins whose host
+ * application owns every device allocation, real-time loops that must not
+ * call the allocator).  No counterpart in the reference.  Same inputs and
+ * output grid as fip_grid_snapshot (FP32 visibilities, plain FP32 sums); the
+ * binning scratch is a fixed ~6.5 MB device array inside the library, held
+ * on every GPU that loads it until the process exits.  Limits: nb <= 131072
+ * and image_size <= 4096 (multiple of 4); larger requests return
+ * FIP_ERR_ARG.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress, with that device current); make that first
+ * call before any stream capture.  All calls share the array: calls whose
+ * work overlaps on the GPU race, so serialise them (one stream, or events).
+ */
+int fip_grid_snapshot_noalloc(const float* vis_re, const float* vis_im, const float* B,
+                              const float* V, size_t nb, size_t image_size, float cell_size,
+                              float* grid, void* stream);
+
+/*
  * tLISI of three consecutive images (device): maxima max3 [3] as produced by
  * fip_image_snapshot, result [U*U].  The inputs are not modified (the
  * reference clamps I2 in place, FIPkernels.cu:836; the clamp here is local).
