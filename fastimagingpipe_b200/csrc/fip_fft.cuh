@@ -1,13 +1,13 @@
-// Shared-memory FFT for lengths G = 3 * M, M = 2^k >= 16 (the grid sides of
+// Shared-memory FFT for lengths G = 3 * M, M = 2^k >= 8 (the grid sides of
 // power-of-two images: G = 1.5 N), exponent +i (the reference's
 // CUFFT_INVERSE, unnormalised), producing only the N outputs an image needs.
 //
 // One CTA computes one length-G transform as three interleaved length-M
 // transforms Z_s (inputs z[3n + s], s = 0, 1, 2) followed by the radix-3
 // recombination X[p] = sum_s e^{+2 pi i s p / G} Z_s[p mod M], evaluated only
-// for the requested outputs.  Each length-M transform runs on M / 16 threads
-// that keep 16 complex values in registers: radix-16 (or 8/4/2 for the last
-// factor) Stockham passes with table twiddles, exchanging values through
+// for the requested outputs.  Each length-M transform runs on M / E threads
+// that keep E (8 or 16) complex values in registers: radix-E (or smaller for
+// the last factor) Stockham passes with table twiddles, exchanging values through
 // shared memory padded by one element every 16 (conflict-free 64-bit
 // accesses).  The first pass reads its inputs through a caller functor,
 // straight from global memory; the recombination writes the outputs through
@@ -18,13 +18,13 @@
 
 namespace fipfft {
 
-constexpr int E = 16;       // complex values per thread
-constexpr int kMaxPass = 6;
+constexpr int kMaxPass = 8;
 
 struct Plan {
   int g;              // transform length G = 3 M
   int m;              // sub-transform length M
-  int ts;             // threads per sub-transform = M / 16
+  int e;              // complex values per thread (8 or 16)
+  int ts;             // threads per sub-transform = M / e
   int nt;             // threads = 3 * ts
   int np;             // passes of the sub-transform
   int r[kMaxPass];    // radices, r[0] first
@@ -116,12 +116,34 @@ __device__ __forceinline__ void dft<16>(float2* x) {
 template <int R>
 __host__ __device__ constexpr int log2c() { return R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : 4; }
 
+// w[k] = W^k for k < R, W = tw[step]: the power-of-two powers come from the
+// table (exact to rounding), the rest as products of at most three of them
+// (a few ulps), so one butterfly reads log2(R) table entries instead of R - 1.
+template <int R>
+__device__ __forceinline__ void twiddle_powers(float2 (&w)[R], const float2* __restrict__ tw,
+                                               int step) {
+  w[1] = __ldg(&tw[step]);
+  if (R > 2) w[2] = __ldg(&tw[2 * step]);
+  if (R > 4) w[4] = __ldg(&tw[4 * step]);
+  if (R > 8) w[8] = __ldg(&tw[8 * step]);
+  if (R > 2) w[3] = cmul(w[1], w[2]);
+  if (R > 4) {
+    w[5] = cmul(w[1], w[4]);
+    w[6] = cmul(w[2], w[4]);
+    w[7] = cmul(w[3], w[4]);
+  }
+  if (R > 8) {
+#pragma unroll
+    for (int k = 9; k < R; ++k) w[k] = cmul(w[k - 8], w[8]);
+  }
+}
+
 // Radix-R pass on a length-M sub-transform: butterfly j = lt + b * ts,
 // inputs at j + k M/R, twiddle e^{+2 pi i (j mod ns) k / (ns R)} read from
 // the length-G table (index 3 * ...), outputs at (j/ns) ns R + (j mod ns) +
 // m ns (Stockham, self-sorting).  ns and M are powers of two:
 // lns = log2 ns, lm = log2 M.
-template <int R>
+template <int R, int E>
 __device__ __forceinline__ void butterflies(float2 (&v)[E], const float2* __restrict__ tw, int lm,
                                             int lns, int lt, int ts) {
 #pragma unroll
@@ -130,14 +152,16 @@ __device__ __forceinline__ void butterflies(float2 (&v)[E], const float2* __rest
     if (lns > 0) {
       const int j = lt + b * ts;
       const int step = 3 * ((j & ((1 << lns) - 1)) << (lm - lns - log2c<R>()));
+      float2 w[R];
+      twiddle_powers<R>(w, tw, step);
 #pragma unroll
-      for (int k = 1; k < R; ++k) x[k] = cmul(x[k], __ldg(&tw[step * k]));
+      for (int k = 1; k < R; ++k) x[k] = cmul(x[k], w[k]);
     }
     dft<R>(x);
   }
 }
 
-template <int R>
+template <int R, int E>
 __device__ __forceinline__ void store_smem(const float2 (&v)[E], float2* sm, int lns, int lt,
                                            int ts) {
   const int ns = 1 << lns;
@@ -150,7 +174,7 @@ __device__ __forceinline__ void store_smem(const float2 (&v)[E], float2* sm, int
   }
 }
 
-template <int R>
+template <int R, int E>
 __device__ __forceinline__ void load_smem(float2 (&v)[E], const float2* sm, int m, int lt,
                                           int ts) {
 #pragma unroll
@@ -162,7 +186,7 @@ __device__ __forceinline__ void load_smem(float2 (&v)[E], const float2* sm, int 
 }
 
 // First pass inputs: sub-transform s element i is z[3 i + s].
-template <int R, class Load>
+template <int R, int E, class Load>
 __device__ __forceinline__ void first_load(float2 (&v)[E], int m, int s, int lt, int ts,
                                            Load& load) {
 #pragma unroll
@@ -173,18 +197,19 @@ __device__ __forceinline__ void first_load(float2 (&v)[E], int m, int s, int lt,
   }
 }
 
-#define FIPFFT_DISPATCH(RADIX, CALL)                  \
-  switch (RADIX) {                                    \
-    case 2: { constexpr int R_ = 2; CALL; } break;    \
-    case 4: { constexpr int R_ = 4; CALL; } break;    \
-    case 8: { constexpr int R_ = 8; CALL; } break;    \
-    default: { constexpr int R_ = 16; CALL; } break;  \
+// Radix dispatch; radices larger than E never occur (the plan keeps them <= E).
+#define FIPFFT_DISPATCH(RADIX, CALL)                              \
+  switch (RADIX) {                                                \
+    case 2: { constexpr int R_ = 2; CALL; } break;                \
+    case 4: { constexpr int R_ = 4; CALL; } break;                \
+    case 8: { constexpr int R_ = 8; CALL; } break;                \
+    default: { constexpr int R_ = (E >= 16 ? 16 : 8); CALL; } break; \
   }
 
 // Runs one transform.  load(n) returns input element n (0 <= n < G);
 // store(o, X) receives output p = (o - nout/2) mod G for o in [0, nout).
 // All threads of the CTA must call it; sm holds smem_elems(g) float2.
-template <class Load, class Store>
+template <int E, class Load, class Store>
 __device__ __forceinline__ void run(const Plan& p, float2* sm, const float2* __restrict__ tw,
                                     int nout, Load& load, Store& store) {
   const int tid = threadIdx.x;
@@ -194,17 +219,17 @@ __device__ __forceinline__ void run(const Plan& p, float2* sm, const float2* __r
   int lm = 0;
   while ((1 << lm) < m) ++lm;
   float2 v[E];
-  FIPFFT_DISPATCH(p.r[0], (first_load<R_>(v, m, s, lt, ts, load)));
+  FIPFFT_DISPATCH(p.r[0], (first_load<R_, E>(v, m, s, lt, ts, load)));
   // The loader may read a staging copy in sm; the first pass overwrites it.
   __syncthreads();
   int lns = 0;
   for (int q = 0; q < p.np; ++q) {
     const int r = p.r[q];
-    FIPFFT_DISPATCH(r, (butterflies<R_>(v, tw, lm, lns, lt, ts)));
-    FIPFFT_DISPATCH(r, (store_smem<R_>(v, sub, lns, lt, ts)));
+    FIPFFT_DISPATCH(r, (butterflies<R_, E>(v, tw, lm, lns, lt, ts)));
+    FIPFFT_DISPATCH(r, (store_smem<R_, E>(v, sub, lns, lt, ts)));
     __syncthreads();
     if (q + 1 < p.np) {
-      FIPFFT_DISPATCH(p.r[q + 1], (load_smem<R_>(v, sub, m, lt, ts)));
+      FIPFFT_DISPATCH(p.r[q + 1], (load_smem<R_, E>(v, sub, m, lt, ts)));
       __syncthreads();
     }
     lns += (r == 2 ? 1 : r == 4 ? 2 : r == 8 ? 3 : 4);

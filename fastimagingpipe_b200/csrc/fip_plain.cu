@@ -432,7 +432,8 @@ __global__ void __launch_bounds__(kThreads) k_grid(const float* __restrict__ B, 
 // y = yy - N/2, for the occupied half-plane columns c <= bbox[1] and rows
 // |r1| <= bbox[0].
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(768) k_fft_cols(const float2* __restrict__ H,
+template <int E>
+__global__ void __launch_bounds__(768, (E == 8 ? 2 : 1)) k_fft_cols(const float2* __restrict__ H,
                                                   const unsigned* __restrict__ bbox,
                                                   float2* __restrict__ P, int n,
                                                   fipfft::Plan plan,
@@ -444,17 +445,15 @@ __global__ void __launch_bounds__(768) k_fft_cols(const float2* __restrict__ H,
   const int g = plan.g;
   const int k1 = min((int)bbox[0], g / 2);
   const float2* col = H + (size_t)c * g;
-  // Stage the band rows [0, k1] and [g - k1, g) with coalesced loads.
-  for (int r = threadIdx.x; r <= k1; r += blockDim.x) s_fft[r] = col[r];
-  for (int r = g - k1 + threadIdx.x; r < g; r += blockDim.x)
-    if (r > k1) s_fft[r] = col[r];
+  // Stage the whole column densely: band rows [0, k1] and [g - k1, g) with
+  // coalesced loads, zeros elsewhere.
+  for (int r = threadIdx.x; r < g; r += blockDim.x)
+    s_fft[r] = (r <= k1 || r >= g - k1) ? col[r] : make_float2(0.f, 0.f);
   __syncthreads();
   float2* out = P + (size_t)c * n;
-  auto load = [&](int pos) -> float2 {
-    return (pos <= k1 || pos >= g - k1) ? s_fft[pos] : make_float2(0.f, 0.f);
-  };
+  auto load = [&](int pos) -> float2 { return s_fft[pos]; };
   auto store = [&](int yy, float2 v) { out[yy] = v; };
-  fipfft::run(plan, s_fft, tw, n, load, store);
+  fipfft::run<E>(plan, s_fft, tw, n, load, store);
 }
 
 // Row pass for image rows yy1 = 2b, yy2 = 2b+1: their Hermitian spectra
@@ -463,7 +462,8 @@ __global__ void __launch_bounds__(768) k_fft_cols(const float2* __restrict__ H,
 // is the reference's crop/correction (FIPkernels.cu:256-287): the image pixel
 // is |out * 1/(taper|x| taper|y| norm^2)| (the checkerboard signs cancel
 // against the centred grid origin).
-__global__ void __launch_bounds__(768) k_fft_rows(const float2* __restrict__ P, const unsigned* __restrict__ bbox,
+template <int E>
+__global__ void __launch_bounds__(768, (E == 8 ? 2 : 1)) k_fft_rows(const float2* __restrict__ P, const unsigned* __restrict__ bbox,
                            const float* __restrict__ ck, float* __restrict__ pre, int n,
                            fipfft::Plan plan, const float2* __restrict__ tw) {
   extern __shared__ float2 s_fft[];
@@ -472,35 +472,23 @@ __global__ void __launch_bounds__(768) k_fft_rows(const float2* __restrict__ P, 
   const int k2 = min((int)bbox[1], half);
   const float norm = FIP_CONV_NORM;
   const float cky1 = ck[abs(yy1 - h)], cky2 = ck[abs(yy1 + 1 - h)];
-  // Stage (X1[c], X2[c]) for c <= k2: one 16-byte load per column, all in
-  // flight at once (the column pass stores P[c][yy]).
-  float4* s_in = reinterpret_cast<float4*>(s_fft);
-  for (int c = threadIdx.x; c <= k2; c += blockDim.x)
-    s_in[c] = *reinterpret_cast<const float4*>(P + (size_t)c * n + yy1);
-  __syncthreads();
-  auto load = [&](int pos) -> float2 {
-    int c;
-    bool mirror = false;
-    if (pos <= k2 && pos <= half) {
-      c = pos;
-    } else if (pos >= g - k2 && pos > half) {
-      c = g - pos;
-      mirror = true;
-    } else {
-      return make_float2(0.f, 0.f);
-    }
-    const float4 ab = s_in[c];
+  // Stage Z[pos] = X1[pos] + i X2[pos] densely for pos < g, with
+  // X(g - c) = conj X(c): one 16-byte load per occupied column c (the column
+  // pass stores P[c][yy]), written at c and g - c; zeros elsewhere.
+  for (int pos = threadIdx.x; pos < g; pos += blockDim.x)
+    if (pos > k2 && pos < g - k2) s_fft[pos] = make_float2(0.f, 0.f);
+  for (int c = threadIdx.x; c <= k2; c += blockDim.x) {
+    const float4 ab = *reinterpret_cast<const float4*>(P + (size_t)c * n + yy1);
     float ay = ab.y, by = ab.w;
-    if (mirror) {
-      ay = -ay;
-      by = -by;
-    }
-    if (pos == 0 || pos == half) {
+    if (c == 0 || c == half) {  // self-conjugate bins are real
       ay = 0.f;
       by = 0.f;
     }
-    return make_float2(ab.x - by, ay + ab.z);
-  };
+    s_fft[c] = make_float2(ab.x - by, ay + ab.z);
+    if (c > 0 && g - c != c) s_fft[g - c] = make_float2(ab.x + by, ab.z - ay);  // conj X1 + i conj X2
+  }
+  __syncthreads();
+  auto load = [&](int pos) -> float2 { return s_fft[pos]; };
   float* row1 = pre + (size_t)yy1 * n;
   float* row2 = row1 + n;
   auto store = [&](int xx, float2 v) {
@@ -512,7 +500,7 @@ __global__ void __launch_bounds__(768) k_fft_rows(const float2* __restrict__ P, 
     row1[xx] = fabs(p1);
     row2[xx] = fabs(p2);
   };
-  fipfft::run(plan, s_fft, tw, n, load, store);
+  fipfft::run<E>(plan, s_fft, tw, n, load, store);
 }
 
 // Crop + correction of the cuFFT C2R output (images whose grid side is not
@@ -723,41 +711,65 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
   const float inv_nb = 1.0f / static_cast<float>(nb);
   const size_t half = n / 2;
   const float lim = half - 1;  // the reference compares |LL| with size_t (N/2 - 1)
-  ExactMap<double> md;
-  if (EXACT) md = make_map<double>(V, cell);
+  // Precision form: exact targets in FP32 around a per-tile origin (a0, b0),
+  // so offsets stay small; P at the origin and the destination-tile offset
+  // come from FP64.
+  ExactMap<float> mf;
+  float p10 = 0.f, p20 = 0.f, off1 = 0.f, off2 = 0.f;
+  int a0 = 0, b0 = 0;
+  if (EXACT) {
+    const ExactMap<double> md = make_map<double>(V, cell);
+    mf = make_map<float>(V, cell);
+    a0 = (int)rintf(0.25f * (s_q[0][0] + s_q[1][0] + s_q[2][0] + s_q[3][0]));
+    b0 = (int)rintf(0.25f * (s_q[0][1] + s_q[1][1] + s_q[2][1] + s_q[3][1]));
+    const double P1 = md.m00 * a0 + md.m01 * b0, P2 = md.m10 * a0 + md.m11 * b0;
+    p10 = (float)P1;
+    p20 = (float)P2;
+    off1 = (float)(P1 - (double)(c0 - h));
+    off2 = (float)(P2 - (double)(r0 - h));
+  }
   // Warps own candidate rows, lanes walk each row's column interval, two
   // candidates per lane per step with both loads issued up front.
   auto splat = [&](int i, int j, float value, float2 t) {
-    int fl, cl, fm, cm;
+    int fl, fm;
     float wl1, wm1, wl0, wm0;
     if (!EXACT) {
       const float LL = t.x, MM = t.y;
       if (!(fabs(LL) < lim && fabs(MM) < lim)) return;
-      fl = (int)floorf(LL); cl = (int)ceilf(LL);
-      fm = (int)floorf(MM); cm = (int)ceilf(MM);
+      fl = (int)floorf(LL);
+      fm = (int)floorf(MM);
+      const int cl = (int)ceilf(LL), cm = (int)ceilf(MM);
       // The reference's weight expressions (FIPkernels.cu:397-409).
       wl0 = 1 - LL + fl; wl1 = LL - fl;
       wm0 = 1 - MM + fm; wm1 = MM - fm;
+      fl += h - c0;
+      fm += h - r0;
+      // ceil == floor + 1 except on exact integers, where the far weight is 0.
+      if (cl == fl + c0 - h) wl1 = 0.f;
+      if (cm == fm + r0 - h) wm1 = 0.f;
     } else {
-      double Ld, Md;
-      exact_forward(md, (double)(i - h), (double)(j - h), Ld, Md);
-      if (!(fabs(Ld) < (double)(half - 1) && fabs(Md) < (double)(half - 1))) return;
-      const double fld = floor(Ld), fmd = floor(Md);
-      fl = (int)fld; fm = (int)fmd;
-      cl = (int)ceil(Ld); cm = (int)ceil(Md);
-      wl1 = (float)(Ld - fld); wm1 = (float)(Md - fmd);
+      const float da = (float)(i - h - a0), db = (float)(j - h - b0);
+      const float d1 = mf.m00 * da + mf.m01 * db, d2 = mf.m10 * da + mf.m11 * db;
+      const float zc = slant_over_cell(mf, p10 + d1, p20 + d2);
+      const float Lr = off1 + d1 - mf.xi * zc, Mr = off2 + d2 + mf.eta * zc;
+      if (!(fabsf(Lr + (float)(c0 - h)) < lim && fabsf(Mr + (float)(r0 - h)) < lim)) return;
+      const float flr = floorf(Lr), fmr = floorf(Mr);
+      fl = (int)flr;
+      fm = (int)fmr;
+      wl1 = Lr - flr; wm1 = Mr - fmr;
       wl0 = 1.0f - wl1; wm0 = 1.0f - wm1;
     }
-    // Destination pixel (row h + m, column h + l), local to this tile.
-    const int lf = h + fl - c0, lc = h + cl - c0;
-    const int mf = h + fm - r0, mc = h + cm - r0;
-    if ((unsigned)mf < (unsigned)kDT) {
-      if ((unsigned)lf < (unsigned)kDT) atomicAdd(&s_tile[tile_slot(mf, lf)], wl0 * wm0 * value);
-      if ((unsigned)lc < (unsigned)kDT) atomicAdd(&s_tile[tile_slot(mf, lc)], wl1 * wm0 * value);
+    // Local destination pixels (fm|fm+1, fl|fl+1) of this tile.
+    const int lc = fl + 1, mc = fm + 1;
+    if ((unsigned)fm < (unsigned)kDT) {
+      if ((unsigned)fl < (unsigned)kDT) atomicAdd(&s_tile[tile_slot(fm, fl)], wl0 * wm0 * value);
+      if ((unsigned)lc < (unsigned)kDT && wl1 != 0.f)
+        atomicAdd(&s_tile[tile_slot(fm, lc)], wl1 * wm0 * value);
     }
-    if ((unsigned)mc < (unsigned)kDT) {
-      if ((unsigned)lf < (unsigned)kDT) atomicAdd(&s_tile[tile_slot(mc, lf)], wl0 * wm1 * value);
-      if ((unsigned)lc < (unsigned)kDT) atomicAdd(&s_tile[tile_slot(mc, lc)], wl1 * wm1 * value);
+    if ((unsigned)mc < (unsigned)kDT && wm1 != 0.f) {
+      if ((unsigned)fl < (unsigned)kDT) atomicAdd(&s_tile[tile_slot(mc, fl)], wl0 * wm1 * value);
+      if ((unsigned)lc < (unsigned)kDT && wl1 != 0.f)
+        atomicAdd(&s_tile[tile_slot(mc, lc)], wl1 * wm1 * value);
     }
   };
   for (int r = warp; r < nrows; r += kThreads / 32) {
@@ -945,19 +957,23 @@ inline int sm_count() {
 // ---------------------------------------------------------------------------
 
 bool fip_fft_plan(int g, fipfft::Plan& p) {
-  if (g < 48 || g % 3 != 0) return false;
+  if (g < 24 || g % 3 != 0) return false;
   const int m = g / 3;
   if (m & (m - 1)) return false;
   int k = 0;
   while ((1 << k) < m) ++k;
+  // 8 values per thread up to M = 2048 (N = 4096), 16 beyond (<= 1024 threads).
+  const int le = (k <= 11) ? 3 : 4;
+  if (k < le) return false;
   p.g = g;
   p.m = m;
-  p.ts = m / fipfft::E;
+  p.e = 1 << le;
+  p.ts = m / p.e;
   p.nt = 3 * p.ts;
-  if (p.nt > 1024) return false;
+  if (p.nt > 768) return false;
   int np = 0;
-  for (int q = 0; q < k / 4; ++q) p.r[np++] = 16;
-  if (k % 4) p.r[np++] = 1 << (k % 4);
+  for (int q = 0; q < k / le; ++q) p.r[np++] = p.e;
+  if (k % le) p.r[np++] = 1 << (k % le);
   p.np = np;
   return np <= fipfft::kMaxPass;
 }
@@ -1018,12 +1034,14 @@ cudaError_t fip_launch_grid(const FipGeom& geo, const float* B, const void* vr, 
   return cudaGetLastError();
 }
 
+template <int E>
 static cudaError_t fft_smem_attr(const FipGeom& geo, size_t& smem) {
   smem = (size_t)fipfft::smem_elems(geo.g) * sizeof(float2);
-  cudaError_t e = cudaFuncSetAttribute(k_fft_cols, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(k_fft_cols<E>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_fft_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(k_fft_rows<E>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
   return e;
 }
 
@@ -1031,9 +1049,14 @@ cudaError_t fip_launch_fft_cols(const FipGeom& geo, const float2* grid, const un
                                 float2* colbuf, const float2* twiddles, const fipfft::Plan& plan,
                                 cudaStream_t s) {
   size_t smem;
-  cudaError_t e = fft_smem_attr(geo, smem);
-  if (e != cudaSuccess) return e;
-  k_fft_cols<<<geo.hp, plan.nt, smem, s>>>(grid, bbox, colbuf, geo.n, plan, twiddles);
+  cudaError_t e;
+  if (plan.e == 8) {
+    if ((e = fft_smem_attr<8>(geo, smem)) != cudaSuccess) return e;
+    k_fft_cols<8><<<geo.hp, plan.nt, smem, s>>>(grid, bbox, colbuf, geo.n, plan, twiddles);
+  } else {
+    if ((e = fft_smem_attr<16>(geo, smem)) != cudaSuccess) return e;
+    k_fft_cols<16><<<geo.hp, plan.nt, smem, s>>>(grid, bbox, colbuf, geo.n, plan, twiddles);
+  }
   return cudaGetLastError();
 }
 
@@ -1041,9 +1064,16 @@ cudaError_t fip_launch_fft_rows(const FipGeom& geo, const float2* colbuf, const 
                                 const float* taper, const float2* twiddles,
                                 const fipfft::Plan& plan, float* pre, cudaStream_t s) {
   size_t smem;
-  cudaError_t e = fft_smem_attr(geo, smem);
-  if (e != cudaSuccess) return e;
-  k_fft_rows<<<geo.n / 2, plan.nt, smem, s>>>(colbuf, bbox, taper, pre, geo.n, plan, twiddles);
+  cudaError_t e;
+  if (plan.e == 8) {
+    if ((e = fft_smem_attr<8>(geo, smem)) != cudaSuccess) return e;
+    k_fft_rows<8><<<geo.n / 2, plan.nt, smem, s>>>(colbuf, bbox, taper, pre, geo.n, plan,
+                                                   twiddles);
+  } else {
+    if ((e = fft_smem_attr<16>(geo, smem)) != cudaSuccess) return e;
+    k_fft_rows<16><<<geo.n / 2, plan.nt, smem, s>>>(colbuf, bbox, taper, pre, geo.n, plan,
+                                                    twiddles);
+  }
   return cudaGetLastError();
 }
 
