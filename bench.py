@@ -390,6 +390,26 @@ def main():
             "value": S / (ev0.elapsed_time(ev1) / 1e3), "unit": UNIT,
             "note": "30 snapshots, sliding-window tLISI per snapshot (28 matrices)"}
 
+    # ---- serving form: 4 beams, Poisson arrivals, HBM budget (rank 0) ----
+    if rank == 0 and not args.no_forms:
+        from fastimagingpipe_b200 import serving
+        beams = [synthetic.config_reference(n_ant=256, image_size=1024, cell_size=2.9089e-5,
+                                            n_snap=6, seed=11),
+                 synthetic.config_reference(image_size=2048, cell_size=1.4544e-5, n_snap=6,
+                                            seed=12),
+                 synthetic.config_reference(n_snap=6, seed=13),
+                 synthetic.config_reference(n_snap=6, seed=14)]
+        rates = [200.0, 100.0, 50.0, 20.0]
+        with fip.Server(150 << 30, slots=4, device=local) as sv:
+            ids = [sv.add_beam(s.image_size, s.num_baselines, s.cell_size, s.unit_size)
+                   for s in beams]
+            serving.run_poisson(sv, ids, beams, rates, 0.3, seed=1)  # warm-up
+            sres = serving.run_poisson(sv, ids, beams, rates, 3.0, seed=2)
+            sres["hbm_reserved_gb"] = sv.reserved_bytes / 2**30
+        sres["config"] = ("beams 1024^2/32,640 bl, 2048^2/130,816, 4096^2/130,816 x2; Poisson "
+                          "200/100/50/20 snapshots/s; HBM budget 150 GB; 4 slots; 3 s")
+        forms["serving"] = sres
+
     # ---- CPU baseline and FP64 errors (rank 0, N = 1) ----
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb, ref64 = cpu_baseline(snap)

@@ -88,6 +88,18 @@ def lib() -> ctypes.CDLL:
         L.fip_imager_grid_side.argtypes = [vp]
         L.fip_grid_snapshot.argtypes = [vp, vp, vp, vp, vp, sz, vp, vp]
         L.fip_grid_snapshot_noalloc.argtypes = [vp, vp, vp, vp, sz, sz, fp, vp, vp]
+        L.fip_server_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, sz, ctypes.c_int, sz]
+        L.fip_server_destroy.argtypes = [vp]
+        L.fip_server_add_beam.argtypes = [vp, ctypes.POINTER(ImagerConfig),
+                                          ctypes.POINTER(ctypes.c_int)]
+        L.fip_server_reserved_bytes.argtypes = [vp]
+        L.fip_server_reserved_bytes.restype = sz
+        L.fip_server_submit.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, sz,
+                                        ctypes.POINTER(ctypes.c_long)]
+        L.fip_server_wait.argtypes = [vp, ctypes.c_long, ctypes.c_double,
+                                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_long),
+                                      ctypes.POINTER(ctypes.c_int), vp, sz,
+                                      ctypes.POINTER(ctypes.c_double)]
         _lib = L
     return _lib
 
@@ -261,3 +273,67 @@ def collapse_visibilities(v0r, v0i, v3r, v3i, f0, f3, w0, w3, out_re, out_im, ns
     _check(lib().fip_collapse_visibilities(*(_ptr(x) for x in (v0r, v0i, v3r, v3i, f0, f3, w0,
                                                                w3, out_re, out_im)), ns,
                                            _stream(stream)))
+
+
+class Server:
+    """Multi-beam streaming server (fip_server): continuous batching of
+    snapshot requests, sliding-window tLISI per beam, HBM-budget admission."""
+
+    def __init__(self, hbm_budget_bytes: int, slots: int = 4, max_queue: int = 1024,
+                 device: int = 0):
+        h = ctypes.c_void_p()
+        _check(lib().fip_server_create(ctypes.byref(h), device, int(hbm_budget_bytes), slots,
+                                       max_queue))
+        self._h = h
+        self._beams = {}
+
+    def add_beam(self, image_size: int, max_baselines: int, cell_size: float, unit_size: int,
+                 form: int = FORM_PLAIN, vis_storage: int = STORE_F32,
+                 reproject: int = REPROJECT_GATHER) -> int:
+        cfg = ImagerConfig(image_size, max_baselines, unit_size, cell_size, form, vis_storage, 0,
+                           reproject)
+        bid = ctypes.c_int()
+        _check(lib().fip_server_add_beam(self._h, ctypes.byref(cfg), ctypes.byref(bid)))
+        self._beams[bid.value] = (image_size // unit_size) ** 2
+        return bid.value
+
+    @property
+    def reserved_bytes(self) -> int:
+        return int(lib().fip_server_reserved_bytes(self._h))
+
+    def submit(self, beam: int, vis_re, vis_im, B, V, nb: int) -> int:
+        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (vis_re, vis_im, B, V)]
+        rid = ctypes.c_long()
+        _check(lib().fip_server_submit(self._h, beam, *(a.ctypes.data for a in arrs), nb,
+                                       ctypes.byref(rid)))
+        return rid.value
+
+    def wait(self, request_id: int, timeout_ms: float = -1.0) -> dict:
+        beam, seq, has = ctypes.c_int(), ctypes.c_long(), ctypes.c_int()
+        lat = ctypes.c_double()
+        n = max(self._beams.values()) if self._beams else 1
+        buf = np.zeros(n, np.float32)
+        _check(lib().fip_server_wait(self._h, request_id, timeout_ms, ctypes.byref(beam),
+                                     ctypes.byref(seq), ctypes.byref(has), buf.ctypes.data, n,
+                                     ctypes.byref(lat)))
+        uu = self._beams[beam.value]
+        u = int(round(uu ** 0.5))
+        return {"beam": beam.value, "seq": seq.value, "latency_ms": lat.value,
+                "tlisi": buf[:uu].reshape(u, u).copy() if has.value else None}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fip_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

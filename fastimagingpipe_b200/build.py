@@ -30,6 +30,7 @@ UNITS = {
     "fip_precise.cu": [],
     "fip_host.cu": [],
     "fip_noalloc.cu": [],
+    "fip_server.cu": [],
 }
 HOST_CXX = ["fits_io.cpp"]
 

@@ -220,6 +220,39 @@ int fip_image_sequence(fip_imager* im, const float* vis_re, const float* vis_im,
                        const float* V, const size_t* nb, size_t nb_stride, size_t num_snapshots,
                        float* results, void* stream);
 
+/* ------------------------------------------------------------------------ */
+/* Multi-beam streaming server (serving form).                              */
+/* ------------------------------------------------------------------------ */
+/*
+ * Continuous batching of snapshot requests from several beams.  Each beam
+ * owns an imager and the ring of its last three images, so every snapshot
+ * from the third on yields the tLISI of the triple ending with it (the
+ * reference's trigger, FIPkernels.cu:806-851, applied as a sliding window).
+ * `slots` worker threads serve the oldest request whose beam is idle, so the
+ * work of different beams overlaps on the device while each beam stays in
+ * order.  Beams are admitted against `hbm_budget_bytes` (FIP_ERR_BUDGET when
+ * a beam's buffers do not fit); submit copies the host inputs and returns
+ * FIP_ERR_NOT_READY while the queue (max_queue requests) is full.  No
+ * counterpart in the reference, which images one FIpipe call at a time.
+ */
+typedef struct fip_server fip_server;
+int fip_server_create(fip_server** out, int device, size_t hbm_budget_bytes, int slots,
+                      size_t max_queue);
+int fip_server_destroy(fip_server* sv);
+/* cfg->device is ignored (the server's device is used). */
+int fip_server_add_beam(fip_server* sv, const fip_imager_config* cfg, int* beam_id);
+size_t fip_server_reserved_bytes(fip_server* sv);
+int fip_server_submit(fip_server* sv, int beam, const float* vis_re, const float* vis_im,
+                      const float* B, const float* V, size_t nb, long* request_id);
+/*
+ * Waits for a request (timeout_ms < 0: no limit) and returns its beam, its
+ * snapshot index within the beam, whether a tLISI matrix was produced (from
+ * the third snapshot on; copied to tlisi, tlisi_len floats) and the latency
+ * from submit to completion.
+ */
+int fip_server_wait(fip_server* sv, long request_id, double timeout_ms, int* beam, long* seq,
+                    int* has_tlisi, float* tlisi, size_t tlisi_len, double* latency_ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -98,6 +98,14 @@ def test_imager_config_validation_before_device():
     assert fip.lib().fip_imager_create(ctypes.byref(h), ctypes.byref(cfg)) == 1
 
 
+def test_server_rejects_bad_arguments():
+    h = ctypes.c_void_p()
+    L = fip.lib()
+    assert L.fip_server_create(ctypes.byref(h), 0, 1 << 30, 0, 16) == 1
+    assert L.fip_server_create(None, 0, 1 << 30, 1, 16) == 1
+    assert L.fip_server_destroy(None) == 0
+
+
 def test_python_mirror_validates_sizes():
     with pytest.raises(ValueError):
         fip.FIpipe(np.zeros(5), np.zeros(5), np.zeros(10), np.zeros(27), 10, 64, 3, 1e-3, 16)
