@@ -1,39 +1,46 @@
 // Shared-memory FFT for lengths G = 3 * M, M = 2^k >= 8 (the grid sides of
 // power-of-two images: G = 1.5 N), exponent +i (the reference's
-// CUFFT_INVERSE, unnormalised), producing only the N outputs an image needs.
+// CUFFT_INVERSE, unnormalised), for inputs z[c] supported on a band
+// lo <= c <= hi around 0 and the N = 2 M outputs X[p], -M <= p < M, that an
+// image keeps.
 //
-// One CTA computes one length-G transform as three interleaved length-M
-// transforms Z_s (inputs z[3n + s], s = 0, 1, 2) followed by the radix-3
-// recombination X[p] = sum_s e^{+2 pi i s p / G} Z_s[p mod M], evaluated only
-// for the requested outputs.  Each length-M transform runs on M / E threads
-// that keep E (8 or 16) complex values in registers: radix-E (or smaller for
-// the last factor) Stockham passes with table twiddles, exchanging values through
-// shared memory padded by one element every 16 (conflict-free 64-bit
-// accesses).  The first pass reads its inputs through a caller functor,
-// straight from global memory; the recombination writes the outputs through
-// another, in natural order.
+// One CTA computes one length-G transform by decimation in frequency by 3:
+// X[3 q + s] = sum_n y_s[n] e^{+2 pi i n q / M} with
+// y_s[n] = sum_{c = n mod M} z[c] w^{c s}, w = e^{+2 pi i / G}, so the three
+// length-M transforms Y_s need no recombination and the band folds into
+// them (a band narrower than M puts at most one input on each n).  Each
+// length-M transform runs on M / E threads that keep E (8 or 16) complex
+// values in registers: radix-E (or smaller for the last factor) Stockham
+// passes with table twiddles, exchanging values through shared memory padded
+// by one element every 16 (conflict-free 64-bit accesses).  The first pass
+// reads the band through a caller functor and applies w^{c s}; the last pass
+// leaves Y_s in shared memory in natural order, read back per output by
+// fetch().
 #pragma once
 
 #include <cuda_runtime.h>
 
 namespace fipfft {
 
-constexpr int kMaxPass = 8;
-
+// Transform shape chosen on the host; the kernels are instantiated per
+// (lm, le), so the passes, radices and index arithmetic are compile-time.
 struct Plan {
-  int g;              // transform length G = 3 M
-  int m;              // sub-transform length M
-  int e;              // complex values per thread (8 or 16)
-  int ts;             // threads per sub-transform = M / e
-  int nt;             // threads = 3 * ts
-  int np;             // passes of the sub-transform
-  int r[kMaxPass];    // radices, r[0] first
+  int g;   // transform length G = 3 M
+  int m;   // sub-transform length M = 2^lm
+  int lm;  // log2 M
+  int le;  // log2 of the complex values per thread (3 or 4)
+  int e;   // values per thread
+  int nt;  // threads = 3 M / e
 };
 
 // Padded shared-memory index.
 __device__ __forceinline__ int sidx(int i) { return i + (i >> 4); }
-// Shared-memory elements for length g.
-__host__ __device__ __forceinline__ int smem_elems(int g) { return g + g / 16 + 16; }
+// Distance between the three sub-transform buffers: the padded length plus 6
+// elements, so that outputs read across the buffers (fetch) start on
+// different banks.
+__host__ __device__ __forceinline__ int sub_stride(int m) { return m + m / 16 + 6; }
+// Shared-memory elements for length g (also >= g, for a staged band).
+__host__ __device__ __forceinline__ int smem_elems(int g) { return 3 * sub_stride(g / 3) + 16; }
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -185,68 +192,100 @@ __device__ __forceinline__ void load_smem(float2 (&v)[E], const float2* sm, int 
   }
 }
 
-// First pass inputs: sub-transform s element i is z[3 i + s].
-template <int R, int E, class Load>
-__device__ __forceinline__ void first_load(float2 (&v)[E], int m, int s, int lt, int ts,
-                                           Load& load) {
+// First-pass inputs of sub-transform s: element n is
+// y_s[n] = sum_{c = n + t M, lo <= c <= hi} z[c] w^{c s}.  WIDE: the band may
+// reach past +-M (t in -2..1); otherwise only t = -1, 0 can hit.
+template <int R, int E, int M, bool WIDE, class Load>
+__device__ __forceinline__ void first_load(float2 (&v)[E], int s, int lt, int lo, int hi,
+                                           const float2* __restrict__ tw, Load& load) {
+  constexpr int G = 3 * M, TS = M / E;
 #pragma unroll
   for (int b = 0; b < E / R; ++b) {
-    const int j = lt + b * ts;
+    const int j = lt + b * TS;
 #pragma unroll
-    for (int k = 0; k < R; ++k) v[b * R + k] = load(3 * (j + k * (m / R)) + s);
+    for (int k = 0; k < R; ++k) {
+      const int n = j + k * (M / R);
+      float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int t = (WIDE ? -2 : -1); t <= (WIDE ? 1 : 0); ++t) {
+        const int c = n + t * M;
+        if (c >= lo && c <= hi) {
+          float2 z = load(c);
+          if (s != 0) {
+            int e = c * s;
+            e += e < 0 ? G : 0;
+            e -= e >= G ? G : 0;
+            z = cmul(z, __ldg(&tw[e]));
+          }
+          acc = cadd(acc, z);
+        }
+      }
+      v[b * R + k] = acc;
+    }
   }
 }
 
-// Radix dispatch; radices larger than E never occur (the plan keeps them <= E).
-#define FIPFFT_DISPATCH(RADIX, CALL)                              \
-  switch (RADIX) {                                                \
-    case 2: { constexpr int R_ = 2; CALL; } break;                \
-    case 4: { constexpr int R_ = 4; CALL; } break;                \
-    case 8: { constexpr int R_ = 8; CALL; } break;                \
-    default: { constexpr int R_ = (E >= 16 ? 16 : 8); CALL; } break; \
-  }
+// log2 of the radix of pass q: LE for the full passes, the remainder last.
+template <int LM, int LE>
+__host__ __device__ constexpr int pass_lr(int q) {
+  return q < LM / LE ? LE : LM % LE;
+}
+template <int LM, int LE>
+__host__ __device__ constexpr int pass_count() {
+  return (LM + LE - 1) / LE;
+}
 
-// Runs one transform.  load(n) returns input element n (0 <= n < G);
-// store(o, X) receives output p = (o - nout/2) mod G for o in [0, nout).
-// All threads of the CTA must call it; sm holds smem_elems(g) float2.
-template <int E, class Load, class Store>
-__device__ __forceinline__ void run(const Plan& p, float2* sm, const float2* __restrict__ tw,
-                                    int nout, Load& load, Store& store) {
-  const int tid = threadIdx.x;
-  const int s = tid >= 2 * p.ts ? 2 : (tid >= p.ts ? 1 : 0);
-  const int lt = tid - s * p.ts, m = p.m, ts = p.ts;
-  float2* sub = sm + s * (m + m / 16);  // sidx(s * m) == s * (m + m / 16) for 16 | m
-  int lm = 0;
-  while ((1 << lm) < m) ++lm;
-  float2 v[E];
-  FIPFFT_DISPATCH(p.r[0], (first_load<R_, E>(v, m, s, lt, ts, load)));
-  // The loader may read a staging copy in sm; the first pass overwrites it.
-  __syncthreads();
-  int lns = 0;
-  for (int q = 0; q < p.np; ++q) {
-    const int r = p.r[q];
-    FIPFFT_DISPATCH(r, (butterflies<R_, E>(v, tw, lm, lns, lt, ts)));
-    FIPFFT_DISPATCH(r, (store_smem<R_, E>(v, sub, lns, lt, ts)));
+// Pass Q of the Stockham transform and the exchange before pass Q + 1.
+template <int LM, int LE, int Q>
+__device__ __forceinline__ void passes(float2 (&v)[1 << LE], float2* sub,
+                                       const float2* __restrict__ tw, int lt) {
+  constexpr int E = 1 << LE, M = 1 << LM, TS = M / E, NP = pass_count<LM, LE>();
+  if constexpr (Q < NP) {
+    constexpr int LNS = Q * LE, R = 1 << pass_lr<LM, LE>(Q);
+    butterflies<R, E>(v, tw, LM, LNS, lt, TS);
+    store_smem<R, E>(v, sub, LNS, lt, TS);
     __syncthreads();
-    if (q + 1 < p.np) {
-      FIPFFT_DISPATCH(p.r[q + 1], (load_smem<R_, E>(v, sub, m, lt, ts)));
+    if constexpr (Q + 1 < NP) {
+      load_smem<(1 << pass_lr<LM, LE>(Q + 1)), E>(v, sub, M, lt, TS);
       __syncthreads();
+      passes<LM, LE, Q + 1>(v, sub, tw, lt);
     }
-    lns += (r == 2 ? 1 : r == 4 ? 2 : r == 8 ? 3 : 4);
   }
-  // Radix-3 recombination for the requested outputs.
-  const int g = p.g, sub_stride = m + m / 16;
-  for (int o = tid; o < nout; o += p.nt) {
-    int pp = o - nout / 2;
-    if (pp < 0) pp += g;
-    const int qq = pp & (m - 1);
-    const float2 z0 = sm[sidx(qq)];
-    const float2 z1 = sm[sub_stride + sidx(qq)];
-    const float2 z2 = sm[2 * sub_stride + sidx(qq)];
-    const int p2 = (2 * pp) >= g ? 2 * pp - g : 2 * pp;
-    const float2 x = cadd(z0, cadd(cmul(z1, __ldg(&tw[pp])), cmul(z2, __ldg(&tw[p2]))));
-    store(o, x);
-  }
+}
+
+// Computes Y_s for s = 0, 1, 2 into sm (sub-transform s at s * sub_stride(M),
+// natural order), M = 2^LM, E = 2^LE values per thread, 3 M / E threads.
+// load(c) returns z[c] for lo <= c <= hi (-G/2 < lo <= 0 <= hi <= G/2); it
+// may read a staging copy in sm, which the first pass overwrites.  All threads
+// of the CTA must call it; sm holds smem_elems(3 M) float2.  Ends with a
+// barrier: sm is then ready for fetch().
+template <int LM, int LE, class Load>
+__device__ __forceinline__ void run(float2* sm, const float2* __restrict__ tw, int lo, int hi,
+                                    Load& load) {
+  constexpr int E = 1 << LE, M = 1 << LM, TS = M / E;
+  constexpr int R0 = 1 << pass_lr<LM, LE>(0);
+  const int tid = threadIdx.x;
+  const int s = tid >= 2 * TS ? 2 : (tid >= TS ? 1 : 0);
+  const int lt = tid - s * TS;
+  float2* sub = sm + s * sub_stride(M);
+  float2 v[E];
+  if (hi >= M || lo < -M)
+    first_load<R0, E, M, true>(v, s, lt, lo, hi, tw, load);
+  else
+    first_load<R0, E, M, false>(v, s, lt, lo, hi, tw, load);
+  __syncthreads();
+  passes<LM, LE, 0>(v, sub, tw, lt);
+}
+
+// Output o in [0, 2M) after run(): X[p] with p = o - M, i.e. Y_s[q] for
+// (p mod G) = 3 q + s.
+template <int LM>
+__device__ __forceinline__ float2 fetch(const float2* sm, int o) {
+  constexpr int M = 1 << LM;
+  int pp = o - M;
+  if (pp < 0) pp += 3 * M;
+  const int q = pp / 3, s = pp - 3 * q;
+  return sm[s * sub_stride(M) + sidx(q)];
 }
 
 }  // namespace fipfft

@@ -114,7 +114,7 @@ struct fip_imager {
   float* pre = nullptr;              // corrected pre-reprojection image [N*N]
   float2* targets = nullptr;         // reference pixel mapping [N*N]
   float2* grid = nullptr;            // uv grid (band layout, or C2R in place)
-  float* taper = nullptr;            // N/2 + 1
+  float* taper = nullptr;            // N/2 + 1 taper values, N/2 + 1 reciprocals
   FipBins bins{};
   float* images[3] = {nullptr, nullptr, nullptr};
   float* maxima = nullptr;           // [3] device floats (written as max bits)
@@ -310,7 +310,7 @@ int fip_imager_create(fip_imager** out, const fip_imager_config* cfg) {
   if (cfg->reproject == 0 && !fip_gather_supported(geo, cfg->form == FIP_FORM_PRECISE))
     return cleanup(fail(FIP_ERR_ARG, "cell_size too small for the tile-gather reprojection; "
                                      "use reproject = 1"));
-  FIP_ALLOC(dalloc(&im->taper, (size_t)geo.n / 2 + 1, tot));
+  FIP_ALLOC(dalloc(&im->taper, 2 * ((size_t)geo.n / 2 + 1), tot));
   im->bins.cap = 12 * nb;
   im->bins.wcap = ntiles + im->bins.cap / FIP_GCHUNK + 1;
   FIP_ALLOC(dalloc(&im->bins.count, ntiles, tot));
@@ -427,7 +427,7 @@ static int image_snapshot_impl(fip_imager* im, const float* vr, const float* vi,
   FIP_CUDA(fip_launch_grid(geo, B, gvr, gvi, vt, im->q_scale, V, (int)nb, im->bins, im->grid,
                            precise ? 1 : 0, s));
   stage_end(im, k, s);
-  im->launches += 5;  // bin count, scan, bin scatter, zero tiles, grid
+  im->launches += fip_bin_launches(geo) + 2;  // binning, zero tiles, grid
   if (im->custom_fft) {
     k = stage_begin(im, ST_FFT_COLS, s);
     FIP_CUDA(fip_launch_fft_cols(geo, im->grid, im->bins.bbox, im->colbuf, im->twiddles,
@@ -504,7 +504,7 @@ int fip_grid_snapshot(fip_imager* im, const float* vis_re, const float* vis_im, 
   FIP_CUDA(fip_launch_bin(geo, B, (int)nb, im->bins, s));
   FIP_CUDA(fip_launch_grid(geo, B, gvr, gvi, vt, im->q_scale, V, (int)nb, im->bins,
                            reinterpret_cast<float2*>(grid), precise ? 1 : 0, s));
-  im->launches += 5;
+  im->launches += fip_bin_launches(geo) + 2;
   return call_leave(im, s);
 }
 

@@ -35,10 +35,13 @@ enum FipVisType { FIP_VIS_F32 = 0, FIP_VIS_F16 = 1, FIP_VIS_BF16 = 2 };
 cudaError_t fip_launch_taper(float* taper, const FipGeom& geo, cudaStream_t s);
 cudaError_t fip_launch_bin(const FipGeom& geo, const float* B, int nb, FipBins& bins,
                            cudaStream_t s);
+// Kernels fip_launch_bin launches for nb > 0.
+int fip_bin_launches(const FipGeom& geo);
 cudaError_t fip_launch_grid(const FipGeom& geo, const float* B, const void* vr, const void* vi,
                             int vis_type, const float* vis_scale, const float* V, int nb,
                             const FipBins& bins, float2* grid, int compensated, cudaStream_t s);
-bool fip_fft_plan(int g, fipfft::Plan& p);
+// values_per_thread: 8 or 16 (0 = the default for the length).
+bool fip_fft_plan(int g, fipfft::Plan& p, int values_per_thread = 0);
 // Band-pruned inverse FFT: column pass (band grid -> colbuf [G/2+1][N]) and
 // row pass with the crop + correction epilogue (colbuf -> pre [N*N]).
 cudaError_t fip_launch_fft_cols(const FipGeom& geo, const float2* grid, const unsigned* bbox,

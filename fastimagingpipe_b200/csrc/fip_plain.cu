@@ -40,9 +40,15 @@ __device__ __forceinline__ int wrap_row(int v, int g) { return v < 0 ? v + g : (
 // ---------------------------------------------------------------------------
 // Taper (FIPkernels.cu:173-186)
 // ---------------------------------------------------------------------------
+// taper[t] for t <= N/2, then the reciprocal correction
+// taper[N/2 + 1 + t] = 1 / (taper[t] norm) that the row transform applies.
 __global__ void k_taper(float* taper, size_t n, size_t g) {
   size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (t < n / 2 + 1) taper[t] = fipref::taper(t, g);
+  if (t < n / 2 + 1) {
+    const float c = fipref::taper(t, g);
+    taper[t] = c;
+    taper[n / 2 + 1 + t] = (float)(1.0 / ((double)c * (double)FIP_CONV_NORM));
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -256,6 +262,218 @@ __global__ void __launch_bounds__(kScanThreads) k_bin_scan(
   }
 }
 
+// ---------------------------------------------------------------------------
+// Binning with per-CTA shared-memory histograms (grids of up to
+// kMaxSmemTiles tiles).  Each CTA takes a contiguous range of visibilities,
+// counts their tile entries in shared memory (native integer atomics,
+// warp-aggregated), and adds its non-zero counts to the global ones; the last
+// CTA to finish scans the tiles.  The scatter pass recounts its range,
+// reserves one slice of each tile's list with one global atomic per
+// (CTA, tile), and fills it through shared-memory cursors.
+// ---------------------------------------------------------------------------
+constexpr int kBinThreads = 512;
+constexpr int kMaxSmemTiles = 12288;  // 48 KB of counters
+
+// Visits every tile entry (tile, code) of visibility v (ok = v is valid);
+// all lanes of the warp must call it together.
+template <class F>
+__device__ __forceinline__ void for_each_entry(const float* B, int v, bool ok, float scale, int g,
+                                               int tiles_c, unsigned& k1, unsigned& k2, F&& f) {
+  Footprint fp;
+  ok = ok && footprint(B, v, scale, g, fp);
+  if (ok) k1 = max(k1, (unsigned)max(abs(fp.a0), abs(fp.a1)));
+  for (int mir = 0; mir < 2; ++mir) {
+    int c0 = 0, c1 = -1, trs[3], ntr = 0;
+    const bool on = ok && half_cols(fp, mir, c0, c1);
+    if (on) {
+      ntr = tile_rows(fp, mir, g, trs);
+      k2 = max(k2, (unsigned)c1);
+    }
+    const int tc0 = on ? c0 / FIP_GTILE : 0, tc1 = on ? c1 / FIP_GTILE : -1;
+    for (int s = 0; s < 6; ++s) {
+      const int kr = s >> 1, kc = s & 1;
+      const bool act = on && kr < ntr && tc0 + kc <= tc1;
+      const unsigned mask = __ballot_sync(0xffffffffu, act);
+      if (act) f((unsigned)(trs[kr] * tiles_c + tc0 + kc), ((unsigned)v << 1) | (unsigned)mir, mask);
+    }
+  }
+}
+
+template <int NT>
+__device__ __forceinline__ uint3 block_scan3(uint3 v, uint3& total) {
+  __shared__ uint3 s_w[NT / 32];
+  __shared__ uint3 s_total;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint3 inc = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned a = __shfl_up_sync(0xffffffffu, inc.x, o);
+    const unsigned b = __shfl_up_sync(0xffffffffu, inc.y, o);
+    const unsigned c = __shfl_up_sync(0xffffffffu, inc.z, o);
+    if (lane >= o) {
+      inc.x += a;
+      inc.y += b;
+      inc.z += c;
+    }
+  }
+  if (lane == 31) s_w[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    const uint3 w = lane < NT / 32 ? s_w[lane] : make_uint3(0, 0, 0);
+    uint3 wi = w;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned a = __shfl_up_sync(0xffffffffu, wi.x, o);
+      const unsigned b = __shfl_up_sync(0xffffffffu, wi.y, o);
+      const unsigned c = __shfl_up_sync(0xffffffffu, wi.z, o);
+      if (lane >= o) {
+        wi.x += a;
+        wi.y += b;
+        wi.z += c;
+      }
+    }
+    if (lane < NT / 32) s_w[lane] = make_uint3(wi.x - w.x, wi.y - w.y, wi.z - w.z);
+    if (lane == NT / 32 - 1) s_total = wi;
+  }
+  __syncthreads();
+  const uint3 base = s_w[warp];
+  total = s_total;
+  __syncthreads();
+  return make_uint3(base.x + inc.x - v.x, base.y + inc.y - v.y, base.z + inc.z - v.z);
+}
+
+// Tile scan run by one CTA of NT threads: offsets, cursors, the work list
+// (every band tile gets >= 1 item) and the list of tiles split over several
+// items.  cnt_s: the tile counts, in shared memory.
+template <int NT>
+__device__ __forceinline__ void scan_tiles(const unsigned* cnt_s, const unsigned* bbox, int ntiles,
+                                           int tiles_c, int g, int layout, unsigned* offset,
+                                           unsigned* cursor, int4* work, unsigned* nwork,
+                                           int wcap, unsigned* multi, unsigned* nmulti) {
+  constexpr int PER = 8;
+  uint3 carry = make_uint3(0, 0, 0);
+  for (int base = 0; base < ntiles; base += NT * PER) {
+    const int t0 = base + threadIdx.x * PER;
+    unsigned c[PER], nch[PER];
+    uint3 sum = make_uint3(0, 0, 0);
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int t = t0 + k;
+      c[k] = 0;
+      nch[k] = 0;
+      if (t < ntiles) {
+        c[k] = cnt_s[t];
+        nch[k] = in_band(t, tiles_c, g, layout, bbox) ? max(1u, (c[k] + FIP_GCHUNK - 1) / FIP_GCHUNK)
+                                                      : 0u;
+      }
+      sum.x += c[k];
+      sum.y += nch[k];
+      sum.z += nch[k] > 1 ? 1u : 0u;
+    }
+    uint3 total;
+    const uint3 ex = block_scan3<NT>(sum, total);
+    unsigned run = carry.x + ex.x, wrun = carry.y + ex.y, mrun = carry.z + ex.z;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int t = t0 + k;
+      if (t < ntiles) {
+        offset[t] = run;
+        cursor[t] = 0;
+        for (unsigned q = 0; q < nch[k]; ++q)
+          if ((int)(wrun + q) < wcap)
+            work[wrun + q] = make_int4(t, (int)(run + min(q * FIP_GCHUNK, c[k])),
+                                       (int)(run + min((q + 1) * FIP_GCHUNK, c[k])), nch[k] == 1);
+        if (nch[k] > 1) multi[mrun++] = (unsigned)t;
+        run += c[k];
+        wrun += nch[k];
+      }
+    }
+    carry.x += total.x;
+    carry.y += total.y;
+    carry.z += total.z;
+  }
+  if (threadIdx.x == 0) {
+    offset[ntiles] = carry.x;
+    *nwork = min(carry.y, (unsigned)wcap);
+    *nmulti = carry.z;
+  }
+}
+
+// Count pass + (last CTA) tile scan.  bbox[2] counts finished CTAs; count
+// and bbox are zero on entry.
+__global__ void __launch_bounds__(kBinThreads) k_bin_count(
+    const float* __restrict__ B, int nb, int per_cta, float scale, int g, int tiles_c, int ntiles,
+    int layout, unsigned* count, unsigned* bbox, unsigned* offset, unsigned* cursor, int4* work,
+    unsigned* nwork, int wcap, unsigned* multi, unsigned* nmulti) {
+  extern __shared__ unsigned s_hist[];
+  __shared__ unsigned s_k[2];
+  __shared__ bool s_last;
+  for (int t = threadIdx.x; t < ntiles; t += kBinThreads) s_hist[t] = 0;
+  if (threadIdx.x < 2) s_k[threadIdx.x] = 0;
+  __syncthreads();
+  const int v0 = blockIdx.x * per_cta, v1 = min(nb, v0 + per_cta);
+  unsigned k1 = 0, k2 = 0;
+  for (int base = v0; base < v1; base += kBinThreads) {
+    const int v = base + threadIdx.x;
+    for_each_entry(B, v, v < v1, scale, g, tiles_c, k1, k2,
+                   [&](unsigned tile, unsigned, unsigned mask) { agg_inc(s_hist, tile, mask); });
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    k1 = max(k1, __shfl_xor_sync(0xffffffffu, k1, o));
+    k2 = max(k2, __shfl_xor_sync(0xffffffffu, k2, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&s_k[0], k1);
+    atomicMax(&s_k[1], k2);
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < ntiles; t += kBinThreads)
+    if (s_hist[t]) atomicAdd(&count[t], s_hist[t]);
+  if (threadIdx.x == 0) {
+    atomicMax(&bbox[0], s_k[0]);
+    atomicMax(&bbox[1], s_k[1]);
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(&bbox[2], 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  // Last CTA: every count and the band are final (read from L2).
+  for (int t = threadIdx.x; t < ntiles; t += kBinThreads) s_hist[t] = __ldcg(&count[t]);
+  if (threadIdx.x < 2) s_k[threadIdx.x] = __ldcg(&bbox[threadIdx.x]);
+  __syncthreads();
+  scan_tiles<kBinThreads>(s_hist, s_k, ntiles, tiles_c, g, layout, offset, cursor, work, nwork,
+                          wcap, multi, nmulti);
+}
+
+// Scatter pass: entries of the CTA's visibility range into the tile lists.
+__global__ void __launch_bounds__(kBinThreads) k_bin_scatter(
+    const float* __restrict__ B, int nb, int per_cta, float scale, int g, int tiles_c, int ntiles,
+    const unsigned* __restrict__ offset, unsigned* cursor, unsigned* entries) {
+  extern __shared__ unsigned s_hist[];
+  for (int t = threadIdx.x; t < ntiles; t += kBinThreads) s_hist[t] = 0;
+  __syncthreads();
+  const int v0 = blockIdx.x * per_cta, v1 = min(nb, v0 + per_cta);
+  unsigned k1 = 0, k2 = 0;
+  for (int base = v0; base < v1; base += kBinThreads) {
+    const int v = base + threadIdx.x;
+    for_each_entry(B, v, v < v1, scale, g, tiles_c, k1, k2,
+                   [&](unsigned tile, unsigned, unsigned mask) { agg_inc(s_hist, tile, mask); });
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < ntiles; t += kBinThreads) {
+    const unsigned c = s_hist[t];
+    if (c) s_hist[t] = offset[t] + atomicAdd(&cursor[t], c);
+  }
+  __syncthreads();
+  for (int base = v0; base < v1; base += kBinThreads) {
+    const int v = base + threadIdx.x;
+    for_each_entry(B, v, v < v1, scale, g, tiles_c, k1, k2,
+                   [&](unsigned tile, unsigned code, unsigned mask) {
+                     entries[agg_inc(s_hist, tile, mask)] = code;
+                   });
+  }
+}
+
 __device__ __forceinline__ size_t cell_index(int row, int col, int g, int hp, int layout) {
   return layout ? (size_t)col * g + row : (size_t)row * hp + col;
 }
@@ -427,80 +645,98 @@ __global__ void __launch_bounds__(kThreads) k_grid(const float* __restrict__ B, 
 }
 
 // ---------------------------------------------------------------------------
-// Band-pruned inverse FFT (power-of-two images).
+// Band-pruned inverse FFT (power-of-two images), instantiated per
+// M = 2^LM = G / 3 and E = 2^LE values per thread (3 M / E threads).
 // Column pass: P[c][yy] = sum_r1 H[c][r1 mod G] e^{+2 pi i y r1 / G},
 // y = yy - N/2, for the occupied half-plane columns c <= bbox[1] and rows
 // |r1| <= bbox[0].
 // ---------------------------------------------------------------------------
-template <int E>
-__global__ void __launch_bounds__(768, (E == 8 ? 2 : 1)) k_fft_cols(const float2* __restrict__ H,
-                                                  const unsigned* __restrict__ bbox,
-                                                  float2* __restrict__ P, int n,
-                                                  fipfft::Plan plan,
-                                                  const float2* __restrict__ tw) {
+template <int LM, int LE>
+__host__ __device__ constexpr int fft_threads() { return 3 << (LM - LE); }
+template <int LM, int LE>
+__host__ __device__ constexpr int fft_min_blocks() {
+  return fft_threads<LM, LE>() >= 768 && LE == 4 ? 1 : 2;
+}
+
+template <int LM, int LE>
+__global__ void __launch_bounds__(fft_threads<LM, LE>(), fft_min_blocks<LM, LE>())
+    k_fft_cols(const float2* __restrict__ H, const unsigned* __restrict__ bbox,
+               float2* __restrict__ P, const float2* __restrict__ tw) {
+  constexpr int M = 1 << LM, g = 3 * M, half = g / 2, n = 2 * M, NT = fft_threads<LM, LE>();
   extern __shared__ float2 s_fft[];
   const int c = blockIdx.x;
   const int k2 = (int)bbox[1];
   if (c > k2) return;
-  const int g = plan.g;
-  const int k1 = min((int)bbox[0], g / 2);
+  const int k1 = min((int)bbox[0], half);
+  // Row band [lo, hi]; row -G/2 is row +G/2 (counted once).
+  const int lo = (k1 == half) ? 1 - k1 : -k1, hi = k1;
   const float2* col = H + (size_t)c * g;
-  // Stage the whole column densely: band rows [0, k1] and [g - k1, g) with
-  // coalesced loads, zeros elsewhere.
-  for (int r = threadIdx.x; r < g; r += blockDim.x)
-    s_fft[r] = (r <= k1 || r >= g - k1) ? col[r] : make_float2(0.f, 0.f);
+  // Stage the band densely (coalesced): s_fft[r - lo] = H[c][r mod G].
+  for (int i = threadIdx.x; i <= hi - lo; i += NT) {
+    const int r = i + lo;
+    s_fft[i] = col[r < 0 ? r + g : r];
+  }
   __syncthreads();
-  float2* out = P + (size_t)c * n;
-  auto load = [&](int pos) -> float2 { return s_fft[pos]; };
-  auto store = [&](int yy, float2 v) { out[yy] = v; };
-  fipfft::run<E>(plan, s_fft, tw, n, load, store);
+  auto load = [&](int r) -> float2 { return s_fft[r - lo]; };
+  fipfft::run<LM, LE>(s_fft, tw, lo, hi, load);
+  float4* out = reinterpret_cast<float4*>(P + (size_t)c * n);
+  for (int o2 = threadIdx.x; o2 < n / 2; o2 += NT) {
+    const float2 a = fipfft::fetch<LM>(s_fft, 2 * o2);
+    const float2 b = fipfft::fetch<LM>(s_fft, 2 * o2 + 1);
+    out[o2] = make_float4(a.x, a.y, b.x, b.y);
+  }
 }
 
 // Row pass for image rows yy1 = 2b, yy2 = 2b+1: their Hermitian spectra
 // X1, X2 (the column-pass output, extended by X(-c) = conj X(c)) are packed as
 // Z = X1 + i X2 so one complex transform yields both real rows.  The epilogue
 // is the reference's crop/correction (FIPkernels.cu:256-287): the image pixel
-// is |out * 1/(taper|x| taper|y| norm^2)| (the checkerboard signs cancel
-// against the centred grid origin).
-template <int E>
-__global__ void __launch_bounds__(768, (E == 8 ? 2 : 1)) k_fft_rows(const float2* __restrict__ P, const unsigned* __restrict__ bbox,
-                           const float* __restrict__ ck, float* __restrict__ pre, int n,
-                           fipfft::Plan plan, const float2* __restrict__ tw) {
+// is |out| / (taper|x| taper|y| norm^2) (the checkerboard signs cancel
+// against the centred grid origin), applied as a product of the reciprocal
+// table rck[t] = 1 / (taper[t] norm).
+template <int LM, int LE>
+__global__ void __launch_bounds__(fft_threads<LM, LE>(), fft_min_blocks<LM, LE>())
+    k_fft_rows(const float2* __restrict__ P, const unsigned* __restrict__ bbox,
+               const float* __restrict__ rck, float* __restrict__ pre,
+               const float2* __restrict__ tw) {
+  constexpr int M = 1 << LM, g = 3 * M, half = g / 2, n = 2 * M, h = M, NT = fft_threads<LM, LE>();
   extern __shared__ float2 s_fft[];
   const int yy1 = 2 * blockIdx.x;
-  const int g = plan.g, half = g / 2, h = n / 2;
   const int k2 = min((int)bbox[1], half);
-  const float norm = FIP_CONV_NORM;
-  const float cky1 = ck[abs(yy1 - h)], cky2 = ck[abs(yy1 + 1 - h)];
-  // Stage Z[pos] = X1[pos] + i X2[pos] densely for pos < g, with
-  // X(g - c) = conj X(c): one 16-byte load per occupied column c (the column
-  // pass stores P[c][yy]), written at c and g - c; zeros elsewhere.
-  for (int pos = threadIdx.x; pos < g; pos += blockDim.x)
-    if (pos > k2 && pos < g - k2) s_fft[pos] = make_float2(0.f, 0.f);
-  for (int c = threadIdx.x; c <= k2; c += blockDim.x) {
+  // Column band [lo, hi]; column -G/2 is column +G/2 (counted once).
+  const int lo = (k2 == half) ? 1 - k2 : -k2, hi = k2;
+  // Stage Z[c] = X1[c] + i X2[c] at s_fft[c - lo], with X(-c) = conj X(c):
+  // one 16-byte load per occupied column c (the column pass stores
+  // P[c][yy]), written at c and -c.
+  for (int c = threadIdx.x; c <= k2; c += NT) {
     const float4 ab = *reinterpret_cast<const float4*>(P + (size_t)c * n + yy1);
     float ay = ab.y, by = ab.w;
     if (c == 0 || c == half) {  // self-conjugate bins are real
       ay = 0.f;
       by = 0.f;
     }
-    s_fft[c] = make_float2(ab.x - by, ay + ab.z);
-    if (c > 0 && g - c != c) s_fft[g - c] = make_float2(ab.x + by, ab.z - ay);  // conj X1 + i conj X2
+    s_fft[c - lo] = make_float2(ab.x - by, ay + ab.z);
+    if (c > 0 && -c >= lo) s_fft[-c - lo] = make_float2(ab.x + by, ab.z - ay);  // conj X1 + i conj X2
   }
   __syncthreads();
-  auto load = [&](int pos) -> float2 { return s_fft[pos]; };
-  float* row1 = pre + (size_t)yy1 * n;
-  float* row2 = row1 + n;
-  auto store = [&](int xx, float2 v) {
-    const int x = xx - h;
-    const float ckx = ck[abs(x)];
-    float p1 = v.x, p2 = v.y;
-    p1 *= 1 / (ckx * cky1 * norm * norm);
-    p2 *= 1 / (ckx * cky2 * norm * norm);
-    row1[xx] = fabs(p1);
-    row2[xx] = fabs(p2);
-  };
-  fipfft::run<E>(plan, s_fft, tw, n, load, store);
+  auto load = [&](int c) -> float2 { return s_fft[c - lo]; };
+  fipfft::run<LM, LE>(s_fft, tw, lo, hi, load);
+  const float ry1 = rck[abs(yy1 - h)], ry2 = rck[abs(yy1 + 1 - h)];
+  float4* row1 = reinterpret_cast<float4*>(pre + (size_t)yy1 * n);
+  float4* row2 = reinterpret_cast<float4*>(pre + (size_t)(yy1 + 1) * n);
+  for (int o4 = threadIdx.x; o4 < n / 4; o4 += NT) {
+    float a[4], b[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int o = 4 * o4 + e;
+      const float2 v = fipfft::fetch<LM>(s_fft, o);
+      const float rx = rck[abs(o - h)];
+      a[e] = fabsf(v.x * (rx * ry1));
+      b[e] = fabsf(v.y * (rx * ry2));
+    }
+    row1[o4] = make_float4(a[0], a[1], a[2], a[3]);
+    row2[o4] = make_float4(b[0], b[1], b[2], b[3]);
+  }
 }
 
 // Crop + correction of the cuFFT C2R output (images whose grid side is not
@@ -956,26 +1192,26 @@ inline int sm_count() {
 // Launchers
 // ---------------------------------------------------------------------------
 
-bool fip_fft_plan(int g, fipfft::Plan& p) {
-  if (g < 24 || g % 3 != 0) return false;
+bool fip_fft_plan(int g, fipfft::Plan& p, int values_per_thread) {
+  if (g < 48 || g % 3 != 0) return false;
   const int m = g / 3;
   if (m & (m - 1)) return false;
-  int k = 0;
-  while ((1 << k) < m) ++k;
-  // 8 values per thread up to M = 2048 (N = 4096), 16 beyond (<= 1024 threads).
-  const int le = (k <= 11) ? 3 : 4;
-  if (k < le) return false;
+  int lm = 0;
+  while ((1 << lm) < m) ++lm;
+  // Instantiated: 8 values per thread for M = 2^4..2^11, 16 for 2^5..2^12
+  // (<= 768 threads).  Default: 8 up to M = 2048 (N = 4096), 16 beyond.
+  int le = (lm <= 11) ? 3 : 4;
+  if (values_per_thread == 8) le = 3;
+  if (values_per_thread == 16) le = 4;
+  if (le == 3 && (lm < 4 || lm > 11)) return false;
+  if (le == 4 && (lm < 5 || lm > 12)) return false;
   p.g = g;
   p.m = m;
+  p.lm = lm;
+  p.le = le;
   p.e = 1 << le;
-  p.ts = m / p.e;
-  p.nt = 3 * p.ts;
-  if (p.nt > 768) return false;
-  int np = 0;
-  for (int q = 0; q < k / le; ++q) p.r[np++] = p.e;
-  if (k % le) p.r[np++] = 1 << (k % le);
-  p.np = np;
-  return np <= fipfft::kMaxPass;
+  p.nt = 3 * (m >> le);
+  return true;
 }
 
 cudaError_t fip_launch_taper(float* taper, const FipGeom& geo, cudaStream_t s) {
@@ -985,6 +1221,10 @@ cudaError_t fip_launch_taper(float* taper, const FipGeom& geo, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+int fip_bin_launches(const FipGeom& geo) {
+  return geo.tiles_r * geo.tiles_c <= kMaxSmemTiles ? 2 : 3;
+}
+
 cudaError_t fip_launch_bin(const FipGeom& geo, const float* B, int nb, FipBins& bins,
                            cudaStream_t s) {
   const int ntiles = geo.tiles_r * geo.tiles_c;
@@ -992,6 +1232,20 @@ cudaError_t fip_launch_bin(const FipGeom& geo, const float* B, int nb, FipBins& 
   cudaError_t e = cudaMemsetAsync(bins.count, 0, ntiles * sizeof(unsigned), s);
   if (e == cudaSuccess) e = cudaMemsetAsync(bins.bbox, 0, 4 * sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
+  if (ntiles <= kMaxSmemTiles) {
+    const int cta = max(1, min(sm_count(), (nb + kBinThreads - 1) / kBinThreads));
+    const int per_cta = (nb + cta - 1) / cta;
+    const size_t smem = (size_t)ntiles * sizeof(unsigned);
+    k_bin_count<<<cta, kBinThreads, smem, s>>>(B, nb, per_cta, scale, geo.g, geo.tiles_c, ntiles,
+                                                geo.layout, bins.count, bins.bbox, bins.offset,
+                                                bins.cursor, bins.work, bins.nwork,
+                                                (int)bins.wcap, bins.multi, bins.nmulti);
+    if (nb > 0)
+      k_bin_scatter<<<cta, kBinThreads, smem, s>>>(B, nb, per_cta, scale, geo.g, geo.tiles_c,
+                                                    ntiles, bins.offset, bins.cursor,
+                                                    bins.entries);
+    return cudaGetLastError();
+  }
   const int blocks = (nb + kThreads - 1) / kThreads;
   if (nb > 0)
     k_bin<0><<<blocks, kThreads, 0, s>>>(B, nb, scale, geo.g, geo.tiles_c, bins.count, nullptr,
@@ -1034,47 +1288,80 @@ cudaError_t fip_launch_grid(const FipGeom& geo, const float* B, const void* vr, 
   return cudaGetLastError();
 }
 
-template <int E>
-static cudaError_t fft_smem_attr(const FipGeom& geo, size_t& smem) {
-  smem = (size_t)fipfft::smem_elems(geo.g) * sizeof(float2);
-  cudaError_t e = cudaFuncSetAttribute(k_fft_cols<E>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+// The transforms' dynamic shared memory depends on the grid side.  Their
+// limit is raised to the device's opt-in maximum, the same value for every
+// caller, so imagers of different sizes launching from concurrent host threads
+// never lower it under one another's launch.
+static cudaError_t fft_smem_attr(const void* fn, int g, size_t& smem) {
+  smem = (size_t)fipfft::smem_elems(g) * sizeof(float2);
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_fft_rows<E>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
-  return e;
+    e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  if (smem > (size_t)optin) return cudaErrorInvalidConfiguration;
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
 }
+
+template <int LM, int LE>
+static cudaError_t launch_cols(const FipGeom& geo, const float2* grid, const unsigned* bbox,
+                               float2* colbuf, const float2* tw, cudaStream_t s) {
+  size_t smem;
+  cudaError_t e = fft_smem_attr((const void*)k_fft_cols<LM, LE>, geo.g, smem);
+  if (e != cudaSuccess) return e;
+  k_fft_cols<LM, LE><<<geo.hp, fft_threads<LM, LE>(), smem, s>>>(grid, bbox, colbuf, tw);
+  return cudaGetLastError();
+}
+
+template <int LM, int LE>
+static cudaError_t launch_rows(const FipGeom& geo, const float2* colbuf, const unsigned* bbox,
+                               const float* taper, const float2* tw, float* pre,
+                               cudaStream_t s) {
+  size_t smem;
+  cudaError_t e = fft_smem_attr((const void*)k_fft_rows<LM, LE>, geo.g, smem);
+  if (e != cudaSuccess) return e;
+  k_fft_rows<LM, LE><<<geo.n / 2, fft_threads<LM, LE>(), smem, s>>>(
+      colbuf, bbox, taper + geo.n / 2 + 1, pre, tw);
+  return cudaGetLastError();
+}
+
+// Calls F<LM, LE> for the plan's instantiation.
+#define FIP_FFT_SWITCH(PLAN, CALL)                                      \
+  do {                                                                  \
+    const int key_ = (PLAN).lm * 8 + (PLAN).le;                         \
+    switch (key_) {                                                     \
+      case 4 * 8 + 3: { constexpr int LM_ = 4, LE_ = 3; return CALL; }  \
+      case 5 * 8 + 3: { constexpr int LM_ = 5, LE_ = 3; return CALL; }  \
+      case 6 * 8 + 3: { constexpr int LM_ = 6, LE_ = 3; return CALL; }  \
+      case 7 * 8 + 3: { constexpr int LM_ = 7, LE_ = 3; return CALL; }  \
+      case 8 * 8 + 3: { constexpr int LM_ = 8, LE_ = 3; return CALL; }  \
+      case 9 * 8 + 3: { constexpr int LM_ = 9, LE_ = 3; return CALL; }  \
+      case 10 * 8 + 3: { constexpr int LM_ = 10, LE_ = 3; return CALL; } \
+      case 11 * 8 + 3: { constexpr int LM_ = 11, LE_ = 3; return CALL; } \
+      case 5 * 8 + 4: { constexpr int LM_ = 5, LE_ = 4; return CALL; }  \
+      case 6 * 8 + 4: { constexpr int LM_ = 6, LE_ = 4; return CALL; }  \
+      case 7 * 8 + 4: { constexpr int LM_ = 7, LE_ = 4; return CALL; }  \
+      case 8 * 8 + 4: { constexpr int LM_ = 8, LE_ = 4; return CALL; }  \
+      case 9 * 8 + 4: { constexpr int LM_ = 9, LE_ = 4; return CALL; }  \
+      case 10 * 8 + 4: { constexpr int LM_ = 10, LE_ = 4; return CALL; } \
+      case 11 * 8 + 4: { constexpr int LM_ = 11, LE_ = 4; return CALL; } \
+      case 12 * 8 + 4: { constexpr int LM_ = 12, LE_ = 4; return CALL; } \
+      default: return cudaErrorInvalidValue;                             \
+    }                                                                   \
+  } while (0)
 
 cudaError_t fip_launch_fft_cols(const FipGeom& geo, const float2* grid, const unsigned* bbox,
                                 float2* colbuf, const float2* twiddles, const fipfft::Plan& plan,
                                 cudaStream_t s) {
-  size_t smem;
-  cudaError_t e;
-  if (plan.e == 8) {
-    if ((e = fft_smem_attr<8>(geo, smem)) != cudaSuccess) return e;
-    k_fft_cols<8><<<geo.hp, plan.nt, smem, s>>>(grid, bbox, colbuf, geo.n, plan, twiddles);
-  } else {
-    if ((e = fft_smem_attr<16>(geo, smem)) != cudaSuccess) return e;
-    k_fft_cols<16><<<geo.hp, plan.nt, smem, s>>>(grid, bbox, colbuf, geo.n, plan, twiddles);
-  }
-  return cudaGetLastError();
+  if (plan.g != geo.g) return cudaErrorInvalidValue;
+  FIP_FFT_SWITCH(plan, (launch_cols<LM_, LE_>(geo, grid, bbox, colbuf, twiddles, s)));
 }
 
 cudaError_t fip_launch_fft_rows(const FipGeom& geo, const float2* colbuf, const unsigned* bbox,
                                 const float* taper, const float2* twiddles,
                                 const fipfft::Plan& plan, float* pre, cudaStream_t s) {
-  size_t smem;
-  cudaError_t e;
-  if (plan.e == 8) {
-    if ((e = fft_smem_attr<8>(geo, smem)) != cudaSuccess) return e;
-    k_fft_rows<8><<<geo.n / 2, plan.nt, smem, s>>>(colbuf, bbox, taper, pre, geo.n, plan,
-                                                   twiddles);
-  } else {
-    if ((e = fft_smem_attr<16>(geo, smem)) != cudaSuccess) return e;
-    k_fft_rows<16><<<geo.n / 2, plan.nt, smem, s>>>(colbuf, bbox, taper, pre, geo.n, plan,
-                                                    twiddles);
-  }
-  return cudaGetLastError();
+  if (plan.g != geo.g) return cudaErrorInvalidValue;
+  FIP_FFT_SWITCH(plan, (launch_rows<LM_, LE_>(geo, colbuf, bbox, taper, twiddles, pre, s)));
 }
 
 cudaError_t fip_launch_correct_c2r(const FipGeom& geo, const float* fft_out, const float* taper,
