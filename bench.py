@@ -225,6 +225,7 @@ def main():
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.Stream(device=dev)
     im = fip.Imager(n, nb, cell, t, device=local)
+    tuning = im.autotune(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, stream=stream)
 
     def step():
         im.pipe_device(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, result, stream=stream)
@@ -344,6 +345,7 @@ def main():
             "stages_ms_per_launch": {k: v[0] for k, v in per_launch.items() if v[1]},
             "stages_note": "measured serialised (profiling run), per launch",
             "uv_band": {"max_row": band[0], "max_col": band[1], "grid": im.grid_side},
+            "autotune": tuning,
         }
     # ---- extra forms (rank 0) ----
     forms = {}
@@ -351,6 +353,7 @@ def main():
         for name, kw in (("precise_f16", dict(form=fip.FORM_PRECISE, vis_storage=fip.STORE_F16)),
                          ("precise_f32", dict(form=fip.FORM_PRECISE, vis_storage=fip.STORE_F32))):
             im2 = fip.Imager(n, nb, cell, t, device=local, **kw)
+            im2.autotune(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, stream=stream)
             res2 = torch.zeros(u * u, device=dev)
             with torch.cuda.stream(stream):
                 for _ in range(3):

@@ -86,6 +86,8 @@ def lib() -> ctypes.CDLL:
         L.fip_imager_kernel_launches.restype = ctypes.c_ulonglong
         L.fip_imager_band.argtypes = [vp, ctypes.POINTER(ctypes.c_uint), ctypes.POINTER(ctypes.c_uint)]
         L.fip_imager_grid_side.argtypes = [vp]
+        L.fip_imager_autotune.argtypes = [vp, vp, vp, vp, vp, sz, vp]
+        L.fip_imager_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.fip_grid_snapshot.argtypes = [vp, vp, vp, vp, vp, sz, vp, vp]
         L.fip_grid_snapshot_noalloc.argtypes = [vp, vp, vp, vp, sz, sz, fp, vp, vp]
         L.fip_server_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, sz, ctypes.c_int, sz]
@@ -206,6 +208,19 @@ class Imager:
     @property
     def grid_side(self) -> int:
         return int(lib().fip_imager_grid_side(self._h))
+
+    def autotune(self, vis_re, vis_im, B, V, nb: int, stream=None) -> dict:
+        """Times the transform's values per thread and the gridder's CTAs per SM on
+        this snapshot (device buffers) and keeps the fastest; returns the choice.
+        Overwrites the trigger ring: call it before a run of snapshots."""
+        _check(lib().fip_imager_autotune(self._h, _ptr(vis_re), _ptr(vis_im), _ptr(B), _ptr(V),
+                                         nb, _stream(stream)))
+        return self.tuning()
+
+    def tuning(self) -> dict:
+        e, c = ctypes.c_int(), ctypes.c_int()
+        _check(lib().fip_imager_tuning(self._h, ctypes.byref(e), ctypes.byref(c)))
+        return {"fft_values_per_thread": int(e.value), "grid_ctas_per_sm": int(c.value)}
 
     def band(self):
         """(max |r1|, max half-plane column) of the last gridded snapshot."""

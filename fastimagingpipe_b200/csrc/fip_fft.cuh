@@ -39,8 +39,12 @@ __device__ __forceinline__ int sidx(int i) { return i + (i >> 4); }
 // elements, so that outputs read across the buffers (fetch) start on
 // different banks.
 __host__ __device__ __forceinline__ int sub_stride(int m) { return m + m / 16 + 6; }
-// Shared-memory elements for length g (also >= g, for a staged band).
-__host__ __device__ __forceinline__ int smem_elems(int g) { return 3 * sub_stride(g / 3) + 16; }
+// Shared memory: two buffers of three sub-transforms (passes alternate
+// between them, so a pass's stores never wait for the previous pass's loads);
+// the input band is staged in the second (stage_offset), which the first
+// pass does not write.
+__host__ __device__ __forceinline__ int stage_offset(int g) { return 3 * sub_stride(g / 3); }
+__host__ __device__ __forceinline__ int smem_elems(int g) { return 6 * sub_stride(g / 3) + 16; }
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -235,30 +239,31 @@ __host__ __device__ constexpr int pass_count() {
   return (LM + LE - 1) / LE;
 }
 
-// Pass Q of the Stockham transform and the exchange before pass Q + 1.
+// Pass Q of the Stockham transform: butterflies, stores into buffer Q & 1,
+// and the loads of pass Q + 1 from it.
 template <int LM, int LE, int Q>
-__device__ __forceinline__ void passes(float2 (&v)[1 << LE], float2* sub,
+__device__ __forceinline__ void passes(float2 (&v)[1 << LE], float2* sm, int s,
                                        const float2* __restrict__ tw, int lt) {
   constexpr int E = 1 << LE, M = 1 << LM, TS = M / E, NP = pass_count<LM, LE>();
   if constexpr (Q < NP) {
     constexpr int LNS = Q * LE, R = 1 << pass_lr<LM, LE>(Q);
+    float2* sub = sm + (Q & 1) * stage_offset(3 * M) + s * sub_stride(M);
     butterflies<R, E>(v, tw, LM, LNS, lt, TS);
     store_smem<R, E>(v, sub, LNS, lt, TS);
     __syncthreads();
     if constexpr (Q + 1 < NP) {
       load_smem<(1 << pass_lr<LM, LE>(Q + 1)), E>(v, sub, M, lt, TS);
-      __syncthreads();
-      passes<LM, LE, Q + 1>(v, sub, tw, lt);
+      passes<LM, LE, Q + 1>(v, sm, s, tw, lt);
     }
   }
 }
 
-// Computes Y_s for s = 0, 1, 2 into sm (sub-transform s at s * sub_stride(M),
-// natural order), M = 2^LM, E = 2^LE values per thread, 3 M / E threads.
-// load(c) returns z[c] for lo <= c <= hi (-G/2 < lo <= 0 <= hi <= G/2); it
-// may read a staging copy in sm, which the first pass overwrites.  All threads
-// of the CTA must call it; sm holds smem_elems(3 M) float2.  Ends with a
-// barrier: sm is then ready for fetch().
+// Computes Y_s for s = 0, 1, 2 into sm (natural order; see fetch), M = 2^LM,
+// E = 2^LE values per thread, 3 M / E threads.  load(c) returns z[c] for
+// lo <= c <= hi (-G/2 < lo <= 0 <= hi <= G/2); it may read a staging copy at
+// sm + stage_offset(G) (written before a barrier).  All threads of the CTA
+// must call it; sm holds smem_elems(G) float2.  Ends with a barrier: sm is
+// then ready for fetch().
 template <int LM, int LE, class Load>
 __device__ __forceinline__ void run(float2* sm, const float2* __restrict__ tw, int lo, int hi,
                                     Load& load) {
@@ -267,25 +272,24 @@ __device__ __forceinline__ void run(float2* sm, const float2* __restrict__ tw, i
   const int tid = threadIdx.x;
   const int s = tid >= 2 * TS ? 2 : (tid >= TS ? 1 : 0);
   const int lt = tid - s * TS;
-  float2* sub = sm + s * sub_stride(M);
   float2 v[E];
   if (hi >= M || lo < -M)
     first_load<R0, E, M, true>(v, s, lt, lo, hi, tw, load);
   else
     first_load<R0, E, M, false>(v, s, lt, lo, hi, tw, load);
-  __syncthreads();
-  passes<LM, LE, 0>(v, sub, tw, lt);
+  passes<LM, LE, 0>(v, sm, s, tw, lt);
 }
 
 // Output o in [0, 2M) after run(): X[p] with p = o - M, i.e. Y_s[q] for
-// (p mod G) = 3 q + s.
-template <int LM>
+// (p mod G) = 3 q + s, in the buffer of the last pass.
+template <int LM, int LE>
 __device__ __forceinline__ float2 fetch(const float2* sm, int o) {
   constexpr int M = 1 << LM;
+  constexpr int last = (pass_count<LM, LE>() - 1) & 1;
   int pp = o - M;
   if (pp < 0) pp += 3 * M;
   const int q = pp / 3, s = pp - 3 * q;
-  return sm[s * sub_stride(M) + sidx(q)];
+  return sm[last * stage_offset(3 * M) + s * sub_stride(M) + sidx(q)];
 }
 
 }  // namespace fipfft

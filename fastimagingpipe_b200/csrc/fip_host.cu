@@ -109,6 +109,7 @@ struct fip_imager {
   bool plan_ok = false;
   bool custom_fft = false;           // band-pruned FFT (fip_fft.cuh)
   fipfft::Plan fft{};
+  int grid_ctas_per_sm = 0;          // persistent gridder CTAs per SM (0 = most that fit)
   float2* twiddles = nullptr;        // e^{+2 pi i k / G}, k < G
   float2* colbuf = nullptr;          // column-pass output [G/2+1][N]
   float* pre = nullptr;              // corrected pre-reprojection image [N*N]
@@ -425,7 +426,7 @@ static int image_snapshot_impl(fip_imager* im, const float* vr, const float* vi,
   stage_end(im, k, s);
   k = stage_begin(im, ST_GRID, s);
   FIP_CUDA(fip_launch_grid(geo, B, gvr, gvi, vt, im->q_scale, V, (int)nb, im->bins, im->grid,
-                           precise ? 1 : 0, s));
+                           precise ? 1 : 0, s, im->grid_ctas_per_sm));
   stage_end(im, k, s);
   im->launches += fip_bin_launches(geo) + 2;  // binning, zero tiles, grid
   if (im->custom_fft) {
@@ -443,7 +444,7 @@ static int image_snapshot_impl(fip_imager* im, const float* vr, const float* vi,
     FIP_CUFFT(cufftExecC2R(im->plan, reinterpret_cast<cufftComplex*>(im->grid),
                            reinterpret_cast<cufftReal*>(im->grid)));
     FIP_CUDA(fip_launch_correct_c2r(geo, reinterpret_cast<const float*>(im->grid), im->taper,
-                                    im->pre, s));
+                                    im->pre, im->bins.bbox + 3, s));
     im->launches += 1;
   }
   stage_end(im, k, s);
@@ -459,7 +460,8 @@ static int image_snapshot_impl(fip_imager* im, const float* vr, const float* vi,
   } else {
     if (fork) FIP_CUDA(cudaStreamWaitEvent(s, im->ev_join, 0));
     k = stage_begin(im, ST_REPROJECT, s);
-    FIP_CUDA(fip_launch_reproject_gather(geo, im->pre, im->targets, V, (int)nb, image,
+    FIP_CUDA(fip_launch_reproject_gather(geo, im->pre, im->targets, V, (int)nb,
+                                         im->bins.bbox + 3, image,
                                          reinterpret_cast<unsigned*>(image_max), precise ? 1 : 0,
                                          s));
     stage_end(im, k, s);
@@ -503,7 +505,8 @@ int fip_grid_snapshot(fip_imager* im, const float* vis_re, const float* vis_im, 
   }
   FIP_CUDA(fip_launch_bin(geo, B, (int)nb, im->bins, s));
   FIP_CUDA(fip_launch_grid(geo, B, gvr, gvi, vt, im->q_scale, V, (int)nb, im->bins,
-                           reinterpret_cast<float2*>(grid), precise ? 1 : 0, s));
+                           reinterpret_cast<float2*>(grid), precise ? 1 : 0, s,
+                           im->grid_ctas_per_sm));
   im->launches += fip_bin_launches(geo) + 2;
   return call_leave(im, s);
 }
@@ -655,6 +658,108 @@ int fip_pixel_targets(fip_imager* im, const float* V, float* out, int exact, voi
   DeviceGuard g(im->cfg.device);
   FIP_CUDA(fip_launch_pixel_targets(im->geo, V, out, exact, (cudaStream_t)stream));
   im->launches += 1;
+  return FIP_OK;
+}
+
+namespace {
+struct EventPair {
+  cudaEvent_t a = nullptr, b = nullptr;
+  ~EventPair() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+}  // namespace
+
+int fip_imager_autotune(fip_imager* im, const float* vr, const float* vi, const float* B,
+                        const float* V, size_t nb, void* stream) {
+  if (!im) return fail(FIP_ERR_ARG, "null imager");
+  DeviceGuard g(im->cfg.device);
+  if (!g.ok) return fail(FIP_ERR_CUDA, "cudaSetDevice failed");
+  cudaStream_t s = (cudaStream_t)stream;
+  FIP_TRY(call_enter(im, s));
+  // One full snapshot leaves this snapshot's bins, band and grid in place.
+  FIP_TRY(image_snapshot_impl(im, vr, vi, B, V, nb, im->images[0], im->maxima, s));
+  const FipGeom& geo = im->geo;
+  const bool precise = im->cfg.form == FIP_FORM_PRECISE;
+  const void* gvr = vr;
+  const void* gvi = vi;
+  int vt = FIP_VIS_F32;
+  if (precise && im->cfg.vis_storage != FIP_STORE_F32) {
+    vt = im->cfg.vis_storage == FIP_STORE_F16 ? FIP_VIS_F16 : FIP_VIS_BF16;
+    gvr = im->q_re;
+    gvi = im->q_im;
+  }
+  EventPair ev;
+  FIP_CUDA(cudaEventCreate(&ev.a));
+  FIP_CUDA(cudaEventCreate(&ev.b));
+  // Best of three timed repetitions after one untimed.
+  auto timed = [&](auto&& launch, float& ms) -> int {
+    ms = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+      FIP_CUDA(cudaEventRecord(ev.a, s));
+      FIP_CUDA(launch());
+      FIP_CUDA(cudaEventRecord(ev.b, s));
+      FIP_CUDA(cudaEventSynchronize(ev.b));
+      float t = 0.f;
+      FIP_CUDA(cudaEventElapsedTime(&t, ev.a, ev.b));
+      if (rep > 0) ms = std::min(ms, t);
+    }
+    return FIP_OK;
+  };
+  if (im->custom_fft) {
+    float best = 1e30f;
+    fipfft::Plan chosen = im->fft;
+    for (int vpt : {8, 16}) {
+      fipfft::Plan p{};
+      if (!fip_fft_plan(geo.g, p, vpt)) continue;
+      float ms = 0.f;
+      FIP_TRY(timed(
+          [&]() -> cudaError_t {
+            cudaError_t e = fip_launch_fft_cols(geo, im->grid, im->bins.bbox, im->colbuf,
+                                                im->twiddles, p, s);
+            if (e != cudaSuccess) return e;
+            return fip_launch_fft_rows(geo, im->colbuf, im->bins.bbox, im->taper, im->twiddles,
+                                       p, im->pre, s);
+          },
+          ms));
+      if (ms < best) {
+        best = ms;
+        chosen = p;
+      }
+    }
+    im->fft = chosen;
+  }
+  {
+    float best = 1e30f;
+    int chosen = 0;
+    for (int c = 1; c <= fip_grid_max_ctas_per_sm(precise ? 1 : 0); ++c) {
+      float ms = 0.f;
+      FIP_TRY(timed(
+          [&]() -> cudaError_t {
+            return fip_launch_grid(geo, B, gvr, gvi, vt, im->q_scale, V, (int)nb, im->bins,
+                                   im->grid, precise ? 1 : 0, s, c);
+          },
+          ms));
+      if (ms < best) {
+        best = ms;
+        chosen = c;
+      }
+    }
+    im->grid_ctas_per_sm = chosen;
+  }
+  FIP_TRY(call_leave(im, s));
+  FIP_CUDA(cudaStreamSynchronize(s));
+  return FIP_OK;
+}
+
+int fip_imager_tuning(const fip_imager* im, int* fft_values_per_thread, int* grid_ctas_per_sm) {
+  if (!im) return fail(FIP_ERR_ARG, "null imager");
+  if (fft_values_per_thread) *fft_values_per_thread = im->custom_fft ? im->fft.e : 0;
+  if (grid_ctas_per_sm)
+    *grid_ctas_per_sm = im->grid_ctas_per_sm > 0
+                            ? im->grid_ctas_per_sm
+                            : fip_grid_max_ctas_per_sm(im->cfg.form == FIP_FORM_PRECISE ? 1 : 0);
   return FIP_OK;
 }
 

@@ -22,7 +22,8 @@ struct FipBins {
   unsigned* entries;  // [cap] (vis << 1 | mirrored), grouped by tile
   int4* work;         // [wcap] (tile, begin, end, single-chunk flag)
   unsigned* nwork;    // [1] number of work items
-  unsigned* bbox;     // [4] occupied band: max |r1|, max half-plane column
+  unsigned* bbox;     // [4] max |r1|, max half-plane column, (unused),
+                      // image maximum (float bits, set by the transform)
   unsigned* multi;    // [ntiles] tiles split over several work items
   unsigned* nmulti;   // [1]
   size_t cap;         // capacity of entries
@@ -37,9 +38,13 @@ cudaError_t fip_launch_bin(const FipGeom& geo, const float* B, int nb, FipBins& 
                            cudaStream_t s);
 // Kernels fip_launch_bin launches for nb > 0.
 int fip_bin_launches(const FipGeom& geo);
+// ctas_per_sm: persistent gridder CTAs per SM (0 = the most that fit,
+// fip_grid_max_ctas_per_sm).
 cudaError_t fip_launch_grid(const FipGeom& geo, const float* B, const void* vr, const void* vi,
                             int vis_type, const float* vis_scale, const float* V, int nb,
-                            const FipBins& bins, float2* grid, int compensated, cudaStream_t s);
+                            const FipBins& bins, float2* grid, int compensated, cudaStream_t s,
+                            int ctas_per_sm = 0);
+int fip_grid_max_ctas_per_sm(int compensated);
 // values_per_thread: 8 or 16 (0 = the default for the length).
 bool fip_fft_plan(int g, fipfft::Plan& p, int values_per_thread = 0);
 // Band-pruned inverse FFT: column pass (band grid -> colbuf [G/2+1][N]) and
@@ -47,12 +52,14 @@ bool fip_fft_plan(int g, fipfft::Plan& p, int values_per_thread = 0);
 cudaError_t fip_launch_fft_cols(const FipGeom& geo, const float2* grid, const unsigned* bbox,
                                 float2* colbuf, const float2* twiddles, const fipfft::Plan& plan,
                                 cudaStream_t s);
-cudaError_t fip_launch_fft_rows(const FipGeom& geo, const float2* colbuf, const unsigned* bbox,
+// Also folds the image maximum into bbox[3] (float bits, zeroed by the
+// binning), which the gather reprojection reads.
+cudaError_t fip_launch_fft_rows(const FipGeom& geo, const float2* colbuf, unsigned* bbox,
                                 const float* taper, const float2* twiddles,
                                 const fipfft::Plan& plan, float* pre, cudaStream_t s);
 // Crop + correction of an in-place cuFFT C2R output -> pre [N*N].
 cudaError_t fip_launch_correct_c2r(const FipGeom& geo, const float* fft_out, const float* taper,
-                                   float* pre, cudaStream_t s);
+                                   float* pre, unsigned* pre_max, cudaStream_t s);
 // The reference's pixel mapping of every source pixel -> targets [N*N].
 cudaError_t fip_launch_targets(const FipGeom& geo, const float* V, float2* targets,
                                cudaStream_t s);
@@ -64,9 +71,11 @@ cudaError_t fip_launch_reproject_scatter(const FipGeom& geo, const float* pre, c
 // candidate source pixels, splats in shared memory and is stored once.  Also
 // records the image maximum into *img_max (atomic max, caller zeroes it).
 bool fip_gather_supported(const FipGeom& geo, int exact_targets);
+// pre_max: maximum of pre (float bits), from the transform's epilogue.
 cudaError_t fip_launch_reproject_gather(const FipGeom& geo, const float* pre,
-                                        const float2* targets, const float* V, int nb, float* dst,
-                                        unsigned* img_max, int exact_targets, cudaStream_t s);
+                                        const float2* targets, const float* V, int nb,
+                                        const unsigned* pre_max, float* dst, unsigned* img_max,
+                                        int exact_targets, cudaStream_t s);
 cudaError_t fip_launch_image_max(const float* img, size_t count, unsigned* out, cudaStream_t s);
 // Trigger: per-tile statistics of (I1, I2, I3) and the tLISI combine.
 cudaError_t fip_launch_trigger(const FipGeom& geo, const float* I1, const float* I2,

@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(kScanThreads) k_bin_scan(
 // reserves one slice of each tile's list with one global atomic per
 // (CTA, tile), and fills it through shared-memory cursors.
 // ---------------------------------------------------------------------------
-constexpr int kBinThreads = 512;
+constexpr int kBinThreads = 256;
 constexpr int kMaxSmemTiles = 12288;  // 48 KB of counters
 
 // Visits every tile entry (tile, code) of visibility v (ok = v is valid);
@@ -397,15 +397,13 @@ __device__ __forceinline__ void scan_tiles(const unsigned* cnt_s, const unsigned
   }
 }
 
-// Count pass + (last CTA) tile scan.  bbox[2] counts finished CTAs; count
-// and bbox are zero on entry.
+// Count pass: per-CTA shared-memory counts added to count[], and the
+// occupied band (bbox[0], bbox[1]).  count and bbox are zero on entry.
 __global__ void __launch_bounds__(kBinThreads) k_bin_count(
     const float* __restrict__ B, int nb, int per_cta, float scale, int g, int tiles_c, int ntiles,
-    int layout, unsigned* count, unsigned* bbox, unsigned* offset, unsigned* cursor, int4* work,
-    unsigned* nwork, int wcap, unsigned* multi, unsigned* nmulti) {
+    unsigned* count, unsigned* bbox) {
   extern __shared__ unsigned s_hist[];
   __shared__ unsigned s_k[2];
-  __shared__ bool s_last;
   for (int t = threadIdx.x; t < ntiles; t += kBinThreads) s_hist[t] = 0;
   if (threadIdx.x < 2) s_k[threadIdx.x] = 0;
   __syncthreads();
@@ -431,18 +429,20 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_count(
     atomicMax(&bbox[0], s_k[0]);
     atomicMax(&bbox[1], s_k[1]);
   }
-  __threadfence();
+}
+
+// Tile scan over the final counts, one CTA of kScanThreads.
+__global__ void __launch_bounds__(kScanThreads) k_bin_scan_tiles(
+    const unsigned* __restrict__ count, const unsigned* __restrict__ bbox, int ntiles,
+    int tiles_c, int g, int layout, unsigned* offset, unsigned* cursor, int4* work,
+    unsigned* nwork, int wcap, unsigned* multi, unsigned* nmulti) {
+  extern __shared__ unsigned s_cnt[];
+  __shared__ unsigned s_k[2];
+  for (int t = threadIdx.x; t < ntiles; t += kScanThreads) s_cnt[t] = count[t];
+  if (threadIdx.x < 2) s_k[threadIdx.x] = bbox[threadIdx.x];
   __syncthreads();
-  if (threadIdx.x == 0) s_last = atomicAdd(&bbox[2], 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  // Last CTA: every count and the band are final (read from L2).
-  for (int t = threadIdx.x; t < ntiles; t += kBinThreads) s_hist[t] = __ldcg(&count[t]);
-  if (threadIdx.x < 2) s_k[threadIdx.x] = __ldcg(&bbox[threadIdx.x]);
-  __syncthreads();
-  scan_tiles<kBinThreads>(s_hist, s_k, ntiles, tiles_c, g, layout, offset, cursor, work, nwork,
-                          wcap, multi, nmulti);
+  scan_tiles<kScanThreads>(s_cnt, s_k, ntiles, tiles_c, g, layout, offset, cursor, work, nwork,
+                           wcap, multi, nmulti);
 }
 
 // Scatter pass: entries of the CTA's visibility range into the tile lists.
@@ -644,6 +644,21 @@ __global__ void __launch_bounds__(kThreads) k_grid(const float* __restrict__ B, 
   }
 }
 
+// Block-wide maximum of non-negative v, folded into *out (float bits) with
+// one atomic per CTA.  All threads of the CTA must call it.
+__device__ __forceinline__ void block_max_to(float v, unsigned* out) {
+  __shared__ float s_m[32];
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) s_m[warp] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float m = 0.f;
+    for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) m = fmaxf(m, s_m[w]);
+    atomicMax(out, __float_as_uint(m));
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Band-pruned inverse FFT (power-of-two images), instantiated per
 // M = 2^LM = G / 3 and E = 2^LE values per thread (3 M / E threads).
@@ -671,18 +686,19 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), fft_min_blocks<LM, LE>(
   // Row band [lo, hi]; row -G/2 is row +G/2 (counted once).
   const int lo = (k1 == half) ? 1 - k1 : -k1, hi = k1;
   const float2* col = H + (size_t)c * g;
-  // Stage the band densely (coalesced): s_fft[r - lo] = H[c][r mod G].
+  // Stage the band densely (coalesced): st[r - lo] = H[c][r mod G].
+  float2* st = s_fft + fipfft::stage_offset(g);
   for (int i = threadIdx.x; i <= hi - lo; i += NT) {
     const int r = i + lo;
-    s_fft[i] = col[r < 0 ? r + g : r];
+    st[i] = col[r < 0 ? r + g : r];
   }
   __syncthreads();
-  auto load = [&](int r) -> float2 { return s_fft[r - lo]; };
+  auto load = [&](int r) -> float2 { return st[r - lo]; };
   fipfft::run<LM, LE>(s_fft, tw, lo, hi, load);
   float4* out = reinterpret_cast<float4*>(P + (size_t)c * n);
   for (int o2 = threadIdx.x; o2 < n / 2; o2 += NT) {
-    const float2 a = fipfft::fetch<LM>(s_fft, 2 * o2);
-    const float2 b = fipfft::fetch<LM>(s_fft, 2 * o2 + 1);
+    const float2 a = fipfft::fetch<LM, LE>(s_fft, 2 * o2);
+    const float2 b = fipfft::fetch<LM, LE>(s_fft, 2 * o2 + 1);
     out[o2] = make_float4(a.x, a.y, b.x, b.y);
   }
 }
@@ -696,7 +712,7 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), fft_min_blocks<LM, LE>(
 // table rck[t] = 1 / (taper[t] norm).
 template <int LM, int LE>
 __global__ void __launch_bounds__(fft_threads<LM, LE>(), fft_min_blocks<LM, LE>())
-    k_fft_rows(const float2* __restrict__ P, const unsigned* __restrict__ bbox,
+    k_fft_rows(const float2* __restrict__ P, unsigned* bbox,
                const float* __restrict__ rck, float* __restrict__ pre,
                const float2* __restrict__ tw) {
   constexpr int M = 1 << LM, g = 3 * M, half = g / 2, n = 2 * M, h = M, NT = fft_threads<LM, LE>();
@@ -705,9 +721,10 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), fft_min_blocks<LM, LE>(
   const int k2 = min((int)bbox[1], half);
   // Column band [lo, hi]; column -G/2 is column +G/2 (counted once).
   const int lo = (k2 == half) ? 1 - k2 : -k2, hi = k2;
-  // Stage Z[c] = X1[c] + i X2[c] at s_fft[c - lo], with X(-c) = conj X(c):
+  // Stage Z[c] = X1[c] + i X2[c] at st[c - lo], with X(-c) = conj X(c):
   // one 16-byte load per occupied column c (the column pass stores
   // P[c][yy]), written at c and -c.
+  float2* st = s_fft + fipfft::stage_offset(g);
   for (int c = threadIdx.x; c <= k2; c += NT) {
     const float4 ab = *reinterpret_cast<const float4*>(P + (size_t)c * n + yy1);
     float ay = ab.y, by = ab.w;
@@ -715,43 +732,52 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), fft_min_blocks<LM, LE>(
       ay = 0.f;
       by = 0.f;
     }
-    s_fft[c - lo] = make_float2(ab.x - by, ay + ab.z);
-    if (c > 0 && -c >= lo) s_fft[-c - lo] = make_float2(ab.x + by, ab.z - ay);  // conj X1 + i conj X2
+    st[c - lo] = make_float2(ab.x - by, ay + ab.z);
+    if (c > 0 && -c >= lo) st[-c - lo] = make_float2(ab.x + by, ab.z - ay);  // conj X1 + i conj X2
   }
   __syncthreads();
-  auto load = [&](int c) -> float2 { return s_fft[c - lo]; };
+  auto load = [&](int c) -> float2 { return st[c - lo]; };
   fipfft::run<LM, LE>(s_fft, tw, lo, hi, load);
   const float ry1 = rck[abs(yy1 - h)], ry2 = rck[abs(yy1 + 1 - h)];
   float4* row1 = reinterpret_cast<float4*>(pre + (size_t)yy1 * n);
   float4* row2 = reinterpret_cast<float4*>(pre + (size_t)(yy1 + 1) * n);
+  float vmax = 0.f;
   for (int o4 = threadIdx.x; o4 < n / 4; o4 += NT) {
     float a[4], b[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       const int o = 4 * o4 + e;
-      const float2 v = fipfft::fetch<LM>(s_fft, o);
+      const float2 v = fipfft::fetch<LM, LE>(s_fft, o);
       const float rx = rck[abs(o - h)];
       a[e] = fabsf(v.x * (rx * ry1));
       b[e] = fabsf(v.y * (rx * ry2));
+      vmax = fmaxf(vmax, fmaxf(a[e], b[e]));
     }
     row1[o4] = make_float4(a[0], a[1], a[2], a[3]);
     row2[o4] = make_float4(b[0], b[1], b[2], b[3]);
   }
+  // Image maximum (bbox[3], float bits; zeroed by the binning), which
+  // scales the reprojection's fixed-point sums.
+  block_max_to(vmax, &bbox[3]);
 }
 
 // Crop + correction of the cuFFT C2R output (images whose grid side is not
 // 3 * 2^k): row (y mod G), column (x mod G), row stride G + 2 floats.
 __global__ void k_correct_c2r(const float* __restrict__ fft_out, const float* __restrict__ ck,
-                              int n, int g, float* __restrict__ pre) {
+                              int n, int g, float* __restrict__ pre, unsigned* pre_max) {
   const int xx = blockIdx.x * blockDim.x + threadIdx.x, yy = blockIdx.y;
-  if (xx >= n) return;
-  const int h = n / 2;
-  const long x = (long)xx - h, y = (long)yy - h;
-  const int row = (int)(y < 0 ? y + g : y), col = (int)(x < 0 ? x + g : x);
-  float px = fft_out[(size_t)row * (size_t)(g + 2) + col];
-  const float norm = FIP_CONV_NORM;
-  px *= 1 / (ck[labs(x)] * ck[labs(y)] * norm * norm);
-  pre[(size_t)yy * n + xx] = fabs(px);
+  float v = 0.f;
+  if (xx < n) {
+    const int h = n / 2;
+    const long x = (long)xx - h, y = (long)yy - h;
+    const int row = (int)(y < 0 ? y + g : y), col = (int)(x < 0 ? x + g : x);
+    float px = fft_out[(size_t)row * (size_t)(g + 2) + col];
+    const float norm = FIP_CONV_NORM;
+    px *= 1 / (ck[labs(x)] * ck[labs(y)] * norm * norm);
+    v = fabs(px);
+    pre[(size_t)yy * n + xx] = v;
+  }
+  block_max_to(v, pre_max);
 }
 
 // ---------------------------------------------------------------------------
@@ -801,7 +827,8 @@ __global__ void k_reproject_scatter(const float* __restrict__ pre, const float* 
 }
 
 constexpr int kDT = 64;          // destination tile side
-constexpr int kMaxRows = 256;    // candidate source rows per tile
+constexpr int kMaxRows = 256;    // candidate source rows per tile (one per thread)
+static_assert(kMaxRows == kThreads, "the gather numbers rows one per thread");
 
 // Exact map: LL = P1 - xi z / cell, MM = P2 + eta z / cell with
 // z = 1 - sqrt(1 - rho), rho = cell^2 ((P1 - 1)^2 + (P2 - 1)^2),
@@ -878,10 +905,12 @@ __device__ __forceinline__ int tile_slot(int row, int col) {
 template <bool EXACT>
 __global__ void __launch_bounds__(kThreads) k_reproject_gather(
     const float* __restrict__ pre, const float2* __restrict__ tg, const float* __restrict__ V,
-    int n, int nb, float cell, float delta, float* __restrict__ dst, unsigned* img_max) {
-  __shared__ __align__(16) float s_tile[kDT * kDT];
+    int n, int nb, float cell, float delta, const unsigned* __restrict__ pre_max,
+    float* __restrict__ dst, unsigned* img_max) {
+  __shared__ __align__(16) unsigned s_tile[kDT * kDT];
   __shared__ int s_ilo[kMaxRows];
-  __shared__ int s_cnt[kMaxRows];
+  __shared__ int s_off[kMaxRows + 1];
+  __shared__ int s_wsum[kThreads / 32];
   __shared__ float s_q[4][2];
   __shared__ float s_wmax[kThreads / 32];
 
@@ -891,7 +920,7 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
   const int h = n / 2;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
-  for (int k = threadIdx.x; k < kDT * kDT; k += kThreads) s_tile[k] = 0.f;
+  for (int k = threadIdx.x; k < kDT * kDT; k += kThreads) s_tile[k] = 0u;
   if (threadIdx.x < 4) {
     const ExactMap<float> mf = make_map<float>(V, cell);
     const float Llo = (float)(c0 - h) - 1.0f - delta, Lhi = (float)(c0 + kDT - h) + delta;
@@ -914,39 +943,67 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
   int jhi = (int)fminf((float)(n - 1), floorf(fminf(bmax + h + 1e-3f, (float)n)));
   jhi = min(jhi, jlo + kMaxRows - 1);
   const int nrows = max(0, jhi - jlo + 1);
-  // Column interval of every candidate row: the preimage quadrilateral
-  // intersected with the row.
-  for (int r = threadIdx.x; r < nrows; r += kThreads) {
-    const float b = (float)(jlo + r - h);
-    float alo = 3e38f, ahi = -3e38f;
+  // Column interval of every candidate row (the preimage quadrilateral
+  // intersected with the row), one row per thread, and the exclusive prefix
+  // of the interval lengths: candidates are then numbered 0 .. total-1 row by
+  // row, so every warp step splats 32 candidates whatever the row lengths.
+  int cnt = 0;
+  {
+    const int r = threadIdx.x;
+    if (r < nrows) {
+      const float b = (float)(jlo + r - h);
+      float alo = 3e38f, ahi = -3e38f;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const float ax = s_q[k][0], bx = s_q[k][1];
-      const float ay = s_q[(k + 1) & 3][0], by = s_q[(k + 1) & 3][1];
-      if ((bx <= b && b <= by) || (by <= b && b <= bx)) {
-        if (by == bx) {
-          alo = fminf(alo, fminf(ax, ay));
-          ahi = fmaxf(ahi, fmaxf(ax, ay));
-        } else {
-          const float a = ax + (ay - ax) * ((b - bx) / (by - bx));
-          alo = fminf(alo, a);
-          ahi = fmaxf(ahi, a);
+      for (int k = 0; k < 4; ++k) {
+        const float ax = s_q[k][0], bx = s_q[k][1];
+        const float ay = s_q[(k + 1) & 3][0], by = s_q[(k + 1) & 3][1];
+        if ((bx <= b && b <= by) || (by <= b && b <= bx)) {
+          if (by == bx) {
+            alo = fminf(alo, fminf(ax, ay));
+            ahi = fmaxf(ahi, fmaxf(ax, ay));
+          } else {
+            const float a = ax + (ay - ax) * ((b - bx) / (by - bx));
+            alo = fminf(alo, a);
+            ahi = fmaxf(ahi, a);
+          }
         }
       }
+      int ilo = 0, ihi = -1;
+      if (alo <= ahi) {
+        ilo = (int)fmaxf(0.f, ceilf(fmaxf(alo + h - 1e-3f, -1.f)));
+        ihi = (int)fminf((float)(n - 1), floorf(fminf(ahi + h + 1e-3f, (float)n)));
+      }
+      s_ilo[r] = ilo;
+      cnt = ihi >= ilo ? ihi - ilo + 1 : 0;
     }
-    int ilo = 0, ihi = -1;
-    if (alo <= ahi) {
-      ilo = (int)fmaxf(0.f, ceilf(fmaxf(alo + h - 1e-3f, -1.f)));
-      ihi = (int)fminf((float)(n - 1), floorf(fminf(ahi + h + 1e-3f, (float)n)));
+    int inc = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
     }
-    s_ilo[r] = ilo;
-    s_cnt[r] = ihi >= ilo ? ihi - ilo + 1 : 0;
+    if (lane == 31) s_wsum[warp] = inc;
+    __syncthreads();
+    int wbase = 0;
+    for (int w = 0; w < warp; ++w) wbase += s_wsum[w];
+    if (r < kMaxRows) s_off[r] = wbase + inc - cnt;
+    if (r == kThreads - 1) s_off[kMaxRows] = wbase + inc;
   }
   __syncthreads();
+  const int total = s_off[kMaxRows];
+  // Rows past nrows have no candidates: their offsets equal total.
 
   const float inv_nb = 1.0f / static_cast<float>(nb);
   const size_t half = n / 2;
   const float lim = half - 1;  // the reference compares |LL| with size_t (N/2 - 1)
+  // Fixed-point tile sums: a source's splat value v / nb is carried as
+  // v * 2^28 / max(pre).  Every contribution is <= 2^28 and the bilinear
+  // weights landing on one pixel sum to a few units at most (the map never
+  // contracts), far below 2^32, so the shared-memory sums are native integer
+  // atomics, exact and independent of their order; the tile is converted
+  // back once.  Resolution 2^-28 of the image maximum.
+  const float pmax = __uint_as_float(*pre_max);
+  const float qk = pmax > 0.f ? 268435456.0f / pmax : 0.f;
+  const float deq = pmax * inv_nb * (1.0f / 268435456.0f);
   // Precision form: exact targets in FP32 around a per-tile origin (a0, b0),
   // so offsets stay small; P at the origin and the destination-tile offset
   // come from FP64.
@@ -964,9 +1021,11 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
     off1 = (float)(P1 - (double)(c0 - h));
     off2 = (float)(P2 - (double)(r0 - h));
   }
-  // Warps own candidate rows, lanes walk each row's column interval, two
-  // candidates per lane per step with both loads issued up front.
-  auto splat = [&](int i, int j, float value, float2 t) {
+  auto add = [&](int row, int col, float w) {
+    const unsigned q = __float2uint_rn(w);
+    if (q) atomicAdd(&s_tile[tile_slot(row, col)], q);
+  };
+  auto splat = [&](int i, int j, float vq, float2 t) {
     int fl, fm;
     float wl1, wm1, wl0, wm0;
     if (!EXACT) {
@@ -998,39 +1057,47 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
     // Local destination pixels (fm|fm+1, fl|fl+1) of this tile.
     const int lc = fl + 1, mc = fm + 1;
     if ((unsigned)fm < (unsigned)kDT) {
-      if ((unsigned)fl < (unsigned)kDT) atomicAdd(&s_tile[tile_slot(fm, fl)], wl0 * wm0 * value);
-      if ((unsigned)lc < (unsigned)kDT && wl1 != 0.f)
-        atomicAdd(&s_tile[tile_slot(fm, lc)], wl1 * wm0 * value);
+      if ((unsigned)fl < (unsigned)kDT) add(fm, fl, wl0 * wm0 * vq);
+      if ((unsigned)lc < (unsigned)kDT) add(fm, lc, wl1 * wm0 * vq);
     }
-    if ((unsigned)mc < (unsigned)kDT && wm1 != 0.f) {
-      if ((unsigned)fl < (unsigned)kDT) atomicAdd(&s_tile[tile_slot(mc, fl)], wl0 * wm1 * value);
-      if ((unsigned)lc < (unsigned)kDT && wl1 != 0.f)
-        atomicAdd(&s_tile[tile_slot(mc, lc)], wl1 * wm1 * value);
+    if ((unsigned)mc < (unsigned)kDT) {
+      if ((unsigned)fl < (unsigned)kDT) add(mc, fl, wl0 * wm1 * vq);
+      if ((unsigned)lc < (unsigned)kDT) add(mc, lc, wl1 * wm1 * vq);
     }
   };
-  for (int r = warp; r < nrows; r += kThreads / 32) {
-    const int j = jlo + r, ilo = s_ilo[r], cnt = s_cnt[r];
-    const float* prow = pre + (size_t)j * n + ilo;
-    const float2* trow = EXACT ? nullptr : tg + (size_t)j * n + ilo;
-    for (int c = lane; c < cnt; c += 64) {
-      const bool two = c + 32 < cnt;
-      const float v0 = prow[c];
-      const float v1 = two ? prow[c + 32] : 0.f;
-      float2 t0 = make_float2(0.f, 0.f), t1 = make_float2(0.f, 0.f);
-      if (!EXACT) {
-        t0 = trow[c];
-        if (two) t1 = trow[c + 32];
-      }
-      splat(ilo + c, j, v0 * inv_nb, t0);
-      if (two) splat(ilo + c + 32, j, v1 * inv_nb, t1);
+  // Warp step: candidates f0 + lane and f0 + 32 + lane, loads issued first.
+  int ra = 0, rb = 0;
+  for (int f0 = warp * 64; f0 < total; f0 += kThreads * 2) {
+    const int fa = f0 + lane, fb = fa + 32;
+    const bool va = fa < total, vb = fb < total;
+    if (va)
+      while (s_off[ra + 1] <= fa) ++ra;
+    if (rb < ra) rb = ra;
+    if (vb)
+      while (s_off[rb + 1] <= fb) ++rb;
+    const int ja = jlo + ra, ia = s_ilo[ra] + (fa - s_off[ra]);
+    const int jb = jlo + rb, ib = s_ilo[rb] + (fb - s_off[rb]);
+    float pa = 0.f, pb = 0.f;
+    float2 ta = make_float2(0.f, 0.f), tb = make_float2(0.f, 0.f);
+    if (va) {
+      pa = pre[(size_t)ja * n + ia];
+      if (!EXACT) ta = tg[(size_t)ja * n + ia];
     }
+    if (vb) {
+      pb = pre[(size_t)jb * n + ib];
+      if (!EXACT) tb = tg[(size_t)jb * n + ib];
+    }
+    if (va) splat(ia, ja, pa * qk, ta);
+    if (vb) splat(ib, jb, pb * qk, tb);
   }
   __syncthreads();
   float vmax = 0.f;
   for (int k = threadIdx.x; k < kDT * kDT / 4; k += kThreads) {
     const int lr = (4 * k) / kDT, g4 = ((4 * k) % kDT) >> 2;
     const int rr = r0 + lr, cc = c0 + 4 * g4;
-    const float4 val = *reinterpret_cast<const float4*>(&s_tile[tile_slot(lr, 4 * g4)]);
+    const uint4 q = *reinterpret_cast<const uint4*>(&s_tile[tile_slot(lr, 4 * g4)]);
+    const float4 val = make_float4((float)q.x * deq, (float)q.y * deq, (float)q.z * deq,
+                                   (float)q.w * deq);
     if (rr < n) {
       if (cc + 3 < n && (n & 3) == 0) {
         *reinterpret_cast<float4*>(&dst[(size_t)rr * n + cc]) = val;
@@ -1221,9 +1288,7 @@ cudaError_t fip_launch_taper(float* taper, const FipGeom& geo, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-int fip_bin_launches(const FipGeom& geo) {
-  return geo.tiles_r * geo.tiles_c <= kMaxSmemTiles ? 2 : 3;
-}
+int fip_bin_launches(const FipGeom&) { return 3; }
 
 cudaError_t fip_launch_bin(const FipGeom& geo, const float* B, int nb, FipBins& bins,
                            cudaStream_t s) {
@@ -1233,13 +1298,16 @@ cudaError_t fip_launch_bin(const FipGeom& geo, const float* B, int nb, FipBins& 
   if (e == cudaSuccess) e = cudaMemsetAsync(bins.bbox, 0, 4 * sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
   if (ntiles <= kMaxSmemTiles) {
-    const int cta = max(1, min(sm_count(), (nb + kBinThreads - 1) / kBinThreads));
+    const int cta = max(1, min(8 * sm_count(), (nb + kBinThreads - 1) / kBinThreads));
     const int per_cta = (nb + cta - 1) / cta;
     const size_t smem = (size_t)ntiles * sizeof(unsigned);
-    k_bin_count<<<cta, kBinThreads, smem, s>>>(B, nb, per_cta, scale, geo.g, geo.tiles_c, ntiles,
-                                                geo.layout, bins.count, bins.bbox, bins.offset,
-                                                bins.cursor, bins.work, bins.nwork,
-                                                (int)bins.wcap, bins.multi, bins.nmulti);
+    if (nb > 0)
+      k_bin_count<<<cta, kBinThreads, smem, s>>>(B, nb, per_cta, scale, geo.g, geo.tiles_c,
+                                                  ntiles, bins.count, bins.bbox);
+    k_bin_scan_tiles<<<1, kScanThreads, smem, s>>>(bins.count, bins.bbox, ntiles, geo.tiles_c,
+                                                    geo.g, geo.layout, bins.offset, bins.cursor,
+                                                    bins.work, bins.nwork, (int)bins.wcap,
+                                                    bins.multi, bins.nmulti);
     if (nb > 0)
       k_bin_scatter<<<cta, kBinThreads, smem, s>>>(B, nb, per_cta, scale, geo.g, geo.tiles_c,
                                                     ntiles, bins.offset, bins.cursor,
@@ -1259,15 +1327,19 @@ cudaError_t fip_launch_bin(const FipGeom& geo, const float* B, int nb, FipBins& 
   return cudaGetLastError();
 }
 
+int fip_grid_max_ctas_per_sm(int compensated) { return compensated ? 2 : 3; }
+
 cudaError_t fip_launch_grid(const FipGeom& geo, const float* B, const void* vr, const void* vi,
                             int vis_type, const float* vis_scale, const float* V, int nb,
-                            const FipBins& bins, float2* grid, int compensated, cudaStream_t s) {
+                            const FipBins& bins, float2* grid, int compensated, cudaStream_t s,
+                            int ctas_per_sm) {
   const float scale = geo.cell * (float)(size_t)geo.g;
   const int sms = sm_count();
   k_zero_tiles<<<sms, kThreads, 0, s>>>(bins.multi, bins.nmulti, geo.tiles_c, geo.g, geo.hp,
                                         geo.layout, grid);
   const size_t smem = sizeof(GridSmem) + (compensated ? 2 * FIP_GTILE * kTS * sizeof(float) : 0);
-  const int blocks = sms * (compensated ? 2 : 3);
+  const int most = fip_grid_max_ctas_per_sm(compensated);
+  const int blocks = sms * (ctas_per_sm > 0 ? min(ctas_per_sm, most) : most);
 #define FIP_GRID_CASE(VT, C)                                                                    \
   do {                                                                                          \
     auto kern = k_grid<VT, C>;                                                                  \
@@ -1289,9 +1361,10 @@ cudaError_t fip_launch_grid(const FipGeom& geo, const float* B, const void* vr, 
 }
 
 // The transforms' dynamic shared memory depends on the grid side.  Their
-// limit is raised to the device's opt-in maximum, the same value for every
-// caller, so imagers of different sizes launching from concurrent host threads
-// never lower it under one another's launch.
+// limit is raised to the most the device allows next to the kernel's static
+// shared memory, the same value for every caller, so imagers of different
+// sizes launching from concurrent host threads never lower it under one
+// another's launch.
 static cudaError_t fft_smem_attr(const void* fn, int g, size_t& smem) {
   smem = (size_t)fipfft::smem_elems(g) * sizeof(float2);
   int dev = 0, optin = 0;
@@ -1299,8 +1372,12 @@ static cudaError_t fft_smem_attr(const void* fn, int g, size_t& smem) {
   if (e == cudaSuccess)
     e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (e != cudaSuccess) return e;
-  if (smem > (size_t)optin) return cudaErrorInvalidConfiguration;
-  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  cudaFuncAttributes fa{};
+  e = cudaFuncGetAttributes(&fa, fn);
+  if (e != cudaSuccess) return e;
+  const int most = optin - (int)fa.sharedSizeBytes;  // static + dynamic <= opt-in maximum
+  if (smem > (size_t)most) return cudaErrorInvalidConfiguration;
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
 }
 
 template <int LM, int LE>
@@ -1314,7 +1391,7 @@ static cudaError_t launch_cols(const FipGeom& geo, const float2* grid, const uns
 }
 
 template <int LM, int LE>
-static cudaError_t launch_rows(const FipGeom& geo, const float2* colbuf, const unsigned* bbox,
+static cudaError_t launch_rows(const FipGeom& geo, const float2* colbuf, unsigned* bbox,
                                const float* taper, const float2* tw, float* pre,
                                cudaStream_t s) {
   size_t smem;
@@ -1357,7 +1434,7 @@ cudaError_t fip_launch_fft_cols(const FipGeom& geo, const float2* grid, const un
   FIP_FFT_SWITCH(plan, (launch_cols<LM_, LE_>(geo, grid, bbox, colbuf, twiddles, s)));
 }
 
-cudaError_t fip_launch_fft_rows(const FipGeom& geo, const float2* colbuf, const unsigned* bbox,
+cudaError_t fip_launch_fft_rows(const FipGeom& geo, const float2* colbuf, unsigned* bbox,
                                 const float* taper, const float2* twiddles,
                                 const fipfft::Plan& plan, float* pre, cudaStream_t s) {
   if (plan.g != geo.g) return cudaErrorInvalidValue;
@@ -1365,9 +1442,9 @@ cudaError_t fip_launch_fft_rows(const FipGeom& geo, const float2* colbuf, const 
 }
 
 cudaError_t fip_launch_correct_c2r(const FipGeom& geo, const float* fft_out, const float* taper,
-                                   float* pre, cudaStream_t s) {
+                                   float* pre, unsigned* pre_max, cudaStream_t s) {
   dim3 bl((geo.n + kThreads - 1) / kThreads, geo.n);
-  k_correct_c2r<<<bl, kThreads, 0, s>>>(fft_out, taper, geo.n, geo.g, pre);
+  k_correct_c2r<<<bl, kThreads, 0, s>>>(fft_out, taper, geo.n, geo.g, pre, pre_max);
   return cudaGetLastError();
 }
 
@@ -1398,17 +1475,18 @@ bool fip_gather_supported(const FipGeom& geo, int exact_targets) {
 }
 
 cudaError_t fip_launch_reproject_gather(const FipGeom& geo, const float* pre,
-                                        const float2* targets, const float* V, int nb, float* dst,
-                                        unsigned* img_max, int exact_targets, cudaStream_t s) {
+                                        const float2* targets, const float* V, int nb,
+                                        const unsigned* pre_max, float* dst, unsigned* img_max,
+                                        int exact_targets, cudaStream_t s) {
   const int tiles = (geo.n + kDT - 1) / kDT;
   const float delta = exact_targets ? 0.25f : chain_delta(geo.cell);
   if (!fip_gather_supported(geo, exact_targets)) return cudaErrorInvalidValue;
   if (exact_targets)
-    k_reproject_gather<true><<<tiles * tiles, kThreads, 0, s>>>(pre, nullptr, V, geo.n, nb,
-                                                                 geo.cell, delta, dst, img_max);
+    k_reproject_gather<true><<<tiles * tiles, kThreads, 0, s>>>(
+        pre, nullptr, V, geo.n, nb, geo.cell, delta, pre_max, dst, img_max);
   else
-    k_reproject_gather<false><<<tiles * tiles, kThreads, 0, s>>>(pre, targets, V, geo.n, nb,
-                                                                  geo.cell, delta, dst, img_max);
+    k_reproject_gather<false><<<tiles * tiles, kThreads, 0, s>>>(
+        pre, targets, V, geo.n, nb, geo.cell, delta, pre_max, dst, img_max);
   return cudaGetLastError();
 }
 

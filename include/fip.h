@@ -178,6 +178,17 @@ int fip_imager_band(fip_imager* im, unsigned* max_row, unsigned* max_col);
 /* Grid side G = ceil(1.5 N) (FIPkernels.cu:583). */
 int fip_imager_grid_side(const fip_imager* im);
 
+/* Autotuner (no counterpart in the reference).  Images the given snapshot
+ * once (device buffers, as fip_image_snapshot), then times the launch shapes
+ * that do not change the arithmetic beyond rounding -- the transform's complex
+ * values per thread (8 or 16) and the persistent gridder's CTAs per SM -- on
+ * that snapshot's band and bins, and keeps the fastest for later calls.
+ * Synchronous; overwrites the imager's trigger ring, so call it before a run
+ * of snapshots, not inside one.  fip_imager_tuning reports the choice. */
+int fip_imager_autotune(fip_imager* im, const float* vis_re, const float* vis_im,
+                        const float* B, const float* V, size_t nb, void* stream);
+int fip_imager_tuning(const fip_imager* im, int* fft_values_per_thread, int* grid_ctas_per_sm);
+
 /* Per-pixel targets (LL, MM) of the reprojection, [N*N][2] (device), for
  * tests: exact = 0 the plain form's FP32 chain, 1 the exact closed form. */
 int fip_pixel_targets(fip_imager* im, const float* V, float* out, int exact, void* stream);

@@ -329,6 +329,25 @@ def test_profiling_and_launch_count(cuda, tiny):
             assert st[k][1] >= 1 and st[k][0] > 0
 
 
+@pytest.mark.parametrize("form", ["plain", "precise"])
+def test_autotune_keeps_results(cuda, small, form):
+    """The autotuner only picks launch shapes: results stay within rounding."""
+    import torch
+    kw = {} if form == "plain" else dict(form=fip.FORM_PRECISE, vis_storage=fip.STORE_F16)
+    n, nb, t = small.image_size, small.num_baselines, small.unit_size
+    u = n // t
+    d = to_dev(small, cuda)
+    before, after = torch.zeros(u * u, device=cuda), torch.zeros(u * u, device=cuda)
+    with fip.Imager(n, nb, small.cell_size, t, **kw) as im:
+        im.pipe_device(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, before)
+        choice = im.autotune(d["vis_re"], d["vis_im"], d["B"], d["V"], nb)
+        assert choice["fft_values_per_thread"] in (8, 16)
+        assert 1 <= choice["grid_ctas_per_sm"] <= 3
+        im.pipe_device(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, after)
+        torch.cuda.synchronize()
+    assert np.abs(after.cpu().numpy() - before.cpu().numpy()).max() <= 1e-5
+
+
 # ---------------------------------------------------------------- preprocessing
 
 def test_plane_projection_vs_oracle(cuda):
