@@ -181,6 +181,75 @@ def run_reference(args, rank):
     return line
 
 
+def run_batching(fip, synthetic, torch, dev, local, per_call=16, calls_per_size=2,
+                 distinct=4):
+    """Times the batching form: for each image size (4096^2 and 2048^2) a Batch of
+    `per_call` snapshots per call, `calls_per_size` calls, the two sizes on two
+    streams at once (64 snapshots in all).  `distinct` seeded snapshots per size are
+    generated and cycled (input generation on the host is the slow part)."""
+    out = {}
+    sizes = (4096, 2048)
+    data = {}
+    for n in sizes:
+        snaps = synthetic.config_batching(n, n_snap=distinct, n_chan=8, seed=20 + n)
+        d = [{k: torch.tensor(getattr(x, k), device=dev) for k in ("vis_re", "vis_im", "B", "V")}
+             for x in snaps]
+        data[n] = (snaps, d)
+    total = len(sizes) * per_call * calls_per_size
+    for name, kw in (("batching_plain", {}),
+                     ("batching_precise_f16", dict(form=fip.FORM_PRECISE,
+                                                   vis_storage=fip.STORE_F16))):
+        batches, streams, res, args_of = {}, {}, {}, {}
+        for n in sizes:
+            snaps, d = data[n]
+            idx = [k % distinct for k in range(per_call)]
+            a = ([d[i]["vis_re"] for i in idx], [d[i]["vis_im"] for i in idx],
+                 [d[i]["B"] for i in idx], [d[i]["V"] for i in idx], [snaps[i].nb for i in idx])
+            nbmax = max(x.nb for x in snaps)
+            b = fip.Batch(n, nbmax, snaps[0].cell_size, 32, per_call, device=local, **kw)
+            tuning = b.autotune(*a)
+            u = n // 32
+            batches[n], args_of[n] = b, a
+            streams[n] = torch.cuda.Stream(device=dev)
+            res[n] = torch.zeros((per_call * calls_per_size, u * u), device=dev)
+            out.setdefault("autotune", {})[f"{name}_{n}"] = tuning
+        def run_all():
+            got = {}
+            for c in range(calls_per_size):
+                for n in sizes:
+                    with torch.cuda.stream(streams[n]):
+                        got[n] = got.get(n, 0) + batches[n].image(
+                            *args_of[n], res[n][got.get(n, 0):], stream=streams[n])
+            return got
+        for n in sizes:
+            batches[n].reset()
+        run_all()  # warm-up: instantiates the graphs
+        torch.cuda.synchronize()
+        for n in sizes:
+            batches[n].reset()
+        l0 = sum(b.kernel_launches for b in batches.values())
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record()
+        for n in sizes:
+            streams[n].wait_event(ev0)
+        run_all()
+        for n in sizes:
+            torch.cuda.current_stream().wait_stream(streams[n])
+        ev1.record()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        out[name] = {"value": total / (ms / 1e3), "unit": UNIT, "snapshots": total,
+                     "gpu_launches": sum(b.kernel_launches for b in batches.values()) - l0,
+                     "hbm_gb": sum(b.device_bytes for b in batches.values()) / 2**30,
+                     "config": f"{total} snapshots x 8 channels (130-150 MHz), 0-30 % flagged, "
+                               f"half 4096^2 / half 2048^2, tile 32, {per_call} per call, "
+                               "two sizes on two streams, CUDA graph per call"}
+        for b in batches.values():
+            b.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -392,6 +461,11 @@ def main():
         forms["sequence_plain"] = {
             "value": S / (ev0.elapsed_time(ev1) / 1e3), "unit": UNIT,
             "note": "30 snapshots, sliding-window tLISI per snapshot (28 matrices)"}
+
+    # ---- batching form: 64 snapshots x 8 channels (130-150 MHz), 0-30 % flagged,
+    # half at 2048^2 and half at 4096^2 (fixed field of view), tile 32 ----
+    if rank == 0 and not args.no_forms:
+        forms.update(run_batching(fip, synthetic, torch, dev, local))
 
     # ---- serving form: 4 beams, Poisson arrivals, HBM budget (rank 0) ----
     if rank == 0 and not args.no_forms:

@@ -87,6 +87,16 @@ def lib() -> ctypes.CDLL:
         L.fip_imager_band.argtypes = [vp, ctypes.POINTER(ctypes.c_uint), ctypes.POINTER(ctypes.c_uint)]
         L.fip_imager_grid_side.argtypes = [vp]
         L.fip_imager_autotune.argtypes = [vp, vp, vp, vp, vp, sz, vp]
+        L.fip_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(ImagerConfig), sz]
+        L.fip_batch_destroy.argtypes = [vp]
+        L.fip_batch_device_bytes.argtypes = [vp]
+        L.fip_batch_device_bytes.restype = sz
+        L.fip_batch_kernel_launches.argtypes = [vp]
+        L.fip_batch_kernel_launches.restype = ctypes.c_ulonglong
+        L.fip_batch_reset.argtypes = [vp]
+        L.fip_batch_image.argtypes = [vp, vp, vp, vp, vp, vp, sz, vp, ctypes.POINTER(sz), vp]
+        L.fip_batch_autotune.argtypes = [vp, vp, vp, vp, vp, vp, sz, vp]
+        L.fip_batch_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.fip_imager_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.fip_grid_snapshot.argtypes = [vp, vp, vp, vp, vp, sz, vp, vp]
         L.fip_grid_snapshot_noalloc.argtypes = [vp, vp, vp, vp, sz, sz, fp, vp, vp]
@@ -265,6 +275,82 @@ class Imager:
         _check(lib().fip_image_sequence(self._h, _ptr(vis_re), _ptr(vis_im), _ptr(B), _ptr(V),
                                         nbs.ctypes.data, nb_stride, len(nbs), _ptr(results),
                                         _stream(stream)))
+
+
+class Batch:
+    """Batching form (fip_batch): many snapshots of one power-of-two image size per
+    call, one persistent gridding launch and one batched transform per call,
+    replayed as a CUDA graph; the batch carries the sequence's last two images so
+    every snapshot with two predecessors yields a tLISI matrix."""
+
+    def __init__(self, image_size: int, max_baselines: int, cell_size: float, unit_size: int,
+                 max_snapshots: int, form: int = FORM_PLAIN, vis_storage: int = STORE_F32,
+                 device: int = 0):
+        self.cfg = ImagerConfig(image_size, max_baselines, unit_size, cell_size, form,
+                                vis_storage, device, REPROJECT_GATHER)
+        h = ctypes.c_void_p()
+        _check(lib().fip_batch_create(ctypes.byref(h), ctypes.byref(self.cfg), max_snapshots))
+        self._h = h
+        self.image_size = image_size
+        self.unit_size = unit_size
+        self.max_snapshots = max_snapshots
+
+    @staticmethod
+    def _arrays(vis_re, vis_im, B, V, nb):
+        count = len(nb)
+        if not (len(vis_re) == len(vis_im) == len(B) == len(V) == count):
+            raise ValueError("one vis_re, vis_im, B, V and nb per snapshot")
+        ptrs = lambda xs: (ctypes.c_void_p * count)(*[_ptr(x) for x in xs])
+        return (ptrs(vis_re), ptrs(vis_im), ptrs(B), ptrs(V),
+                (ctypes.c_size_t * count)(*[int(n) for n in nb]), count)
+
+    def image(self, vis_re, vis_im, B, V, nb, results, stream=None) -> int:
+        """Images len(nb) snapshots (per-snapshot device buffers); writes the tLISI
+        matrices of the snapshots with two predecessors to `results` (U*U each, in
+        order) and returns their number."""
+        a = self._arrays(vis_re, vis_im, B, V, nb)
+        nr = ctypes.c_size_t()
+        _check(lib().fip_batch_image(self._h, *a, _ptr(results), ctypes.byref(nr),
+                                     _stream(stream)))
+        return int(nr.value)
+
+    def autotune(self, vis_re, vis_im, B, V, nb, stream=None) -> dict:
+        _check(lib().fip_batch_autotune(self._h, *self._arrays(vis_re, vis_im, B, V, nb),
+                                        _stream(stream)))
+        return self.tuning()
+
+    def tuning(self) -> dict:
+        e, c = ctypes.c_int(), ctypes.c_int()
+        _check(lib().fip_batch_tuning(self._h, ctypes.byref(e), ctypes.byref(c)))
+        return {"fft_values_per_thread": int(e.value), "grid_ctas_per_sm": int(c.value)}
+
+    def reset(self):
+        _check(lib().fip_batch_reset(self._h))
+
+    @property
+    def device_bytes(self) -> int:
+        return int(lib().fip_batch_device_bytes(self._h))
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(lib().fip_batch_kernel_launches(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fip_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def grid_snapshot_noalloc(vis_re, vis_im, B, V, nb: int, image_size: int, cell_size: float,

@@ -33,12 +33,15 @@ struct FipGeom {
                // 0 = full half plane, row-major (cuFFT C2R fallback)
 };
 
-// Snapshot descriptor for batched launches (device-resident arrays).
-struct FipSnapDesc {
-  const void* vis_re;   // float or half/bf16 depending on storage
-  const void* vis_im;
-  const float* B;       // [nb][2]
-  const float* V;       // [9]
-  int nb;               // visibilities of this snapshot
-  float vis_scale;      // multiplier for reduced-precision storage (1 for FP32)
+// Batched launches: at most FIP_MAX_BATCH snapshots of one image size.
+#define FIP_MAX_BATCH 64
+
+// Per-snapshot inputs of a batched gridding launch (a kernel parameter).
+struct FipGridBatch {
+  int count;
+  const float* B[FIP_MAX_BATCH];          // [nb][2]
+  const void* vr[FIP_MAX_BATCH];          // float, or half/bf16 for reduced storage
+  const void* vi[FIP_MAX_BATCH];
+  const float* V[FIP_MAX_BATCH];          // [9]
+  const float* vis_scale[FIP_MAX_BATCH];  // reduced-storage scale, or null
 };

@@ -878,6 +878,477 @@ int fip_pipe(const float* vis_re, const float* vis_im, const float* B, const flo
 
 }  // extern "C"
 
+
+// ---------------------------------------------------------------------------
+// Batching form: many snapshots of one image size per call, imaged with one
+// persistent gridding launch and one batched transform for the whole batch,
+// the per-snapshot stages (binning, pixel mapping, reprojection) on parallel
+// branches, the trigger batched over the sequence, all captured as one CUDA
+// graph per call shape.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kBranches = 4;
+}  // namespace
+
+struct fip_batch {
+  fip_imager_config cfg{};
+  FipGeom geo{};
+  int smax = 0;                       // snapshots per call at most
+  size_t device_bytes = 0;
+  fipfft::Plan fft{};
+  int grid_ctas_per_sm = 0;
+  float2* twiddles = nullptr;
+  float* taper = nullptr;
+  // Per-snapshot scratch, snapshot k at base + k * stride.
+  size_t ntiles = 0, cap = 0, wcap = 0, n2 = 0, grid_elems = 0, col_elems = 0;
+  unsigned* count = nullptr;          // [smax][ntiles]
+  unsigned* offset = nullptr;         // [smax][ntiles + 1]
+  unsigned* cursor = nullptr;         // [smax][ntiles]
+  unsigned* entries = nullptr;        // [smax][cap]
+  int4* work = nullptr;               // [smax][wcap]
+  unsigned* nwork = nullptr;          // [smax]
+  unsigned* bbox = nullptr;           // [smax][4]
+  unsigned* multi = nullptr;          // [smax][ntiles]
+  unsigned* nmulti = nullptr;         // [smax]
+  float2* grid = nullptr;             // [smax][G (G/2+1)]
+  float2* colbuf = nullptr;           // [smax][(G/2+1) N]
+  float* pre = nullptr;               // [smax][N N]
+  float2* targets = nullptr;          // [smax][N N] (plain form)
+  void* q_re = nullptr;               // [smax][max_baselines] (reduced storage)
+  void* q_im = nullptr;
+  float* q_scale = nullptr;           // [smax]
+  // Linear ring: slots 0, 1 carry the sequence's last two images, the call's
+  // snapshots go to slots 2 .. count + 1.
+  float* images = nullptr;            // [smax + 2][N N]
+  float* maxima = nullptr;            // [smax + 2]
+  int carried = 0;
+  cudaStream_t branch[kBranches] = {};
+  cudaEvent_t fork = nullptr;
+  cudaEvent_t join[kBranches] = {};
+  cudaGraphExec_t exec = nullptr;
+  unsigned long long launches = 0;
+
+  FipBins bins(int k) const {
+    FipBins b{};
+    b.count = count + k * ntiles;
+    b.offset = offset + k * (ntiles + 1);
+    b.cursor = cursor + k * ntiles;
+    b.entries = entries + k * cap;
+    b.work = work + k * wcap;
+    b.nwork = nwork + k;
+    b.bbox = bbox + 4 * k;
+    b.multi = multi + k * ntiles;
+    b.nmulti = nmulti + k;
+    b.cap = cap;
+    b.wcap = wcap;
+    return b;
+  }
+};
+
+namespace {
+void batch_free(fip_batch* b) {
+  if (!b) return;
+  DeviceGuard g(b->cfg.device);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  void* ptrs[] = {b->twiddles, b->taper, b->count, b->offset, b->cursor, b->entries, b->work,
+                  b->nwork, b->bbox, b->multi, b->nmulti, b->grid, b->colbuf, b->pre,
+                  b->targets, b->q_re, b->q_im, b->q_scale, b->images, b->maxima};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  for (int k = 0; k < kBranches; ++k) {
+    if (b->branch[k]) cudaStreamDestroy(b->branch[k]);
+    if (b->join[k]) cudaEventDestroy(b->join[k]);
+  }
+  if (b->fork) cudaEventDestroy(b->fork);
+  delete b;
+}
+
+// Captures the work of one call into a graph (stream s in capture mode).
+int batch_record(fip_batch* b, const float* const* vr, const float* const* vi,
+                 const float* const* B, const float* const* V, const size_t* nb, int count,
+                 int first_result, float* results, cudaStream_t s) {
+  const FipGeom& geo = b->geo;
+  const bool precise = b->cfg.form == FIP_FORM_PRECISE;
+  const bool reduced = precise && b->cfg.vis_storage != FIP_STORE_F32;
+  const int vt = !reduced ? FIP_VIS_F32
+                          : (b->cfg.vis_storage == FIP_STORE_F16 ? FIP_VIS_F16 : FIP_VIS_BF16);
+  const size_t qsz = 2;  // bytes per reduced-storage value
+  unsigned long long launches = 0;
+  // Per snapshot, on the branches: storage conversion, binning, pixel mapping.
+  FIP_CUDA(cudaEventRecord(b->fork, s));
+  for (int i = 0; i < kBranches; ++i) FIP_CUDA(cudaStreamWaitEvent(b->branch[i], b->fork, 0));
+  FipGridBatch in{};
+  in.count = count;
+  for (int k = 0; k < count; ++k) {
+    cudaStream_t bs = b->branch[k % kBranches];
+    in.B[k] = B[k];
+    in.V[k] = V[k];
+    in.vr[k] = vr[k];
+    in.vi[k] = vi[k];
+    in.vis_scale[k] = nullptr;
+    if (reduced) {
+      void* qr = static_cast<char*>(b->q_re) + k * b->cfg.max_baselines * qsz;
+      void* qi = static_cast<char*>(b->q_im) + k * b->cfg.max_baselines * qsz;
+      FIP_CUDA(fip_launch_quantize(vr[k], vi[k], nb[k], vt, qr, qi, b->q_scale + k, bs));
+      in.vr[k] = qr;
+      in.vi[k] = qi;
+      in.vis_scale[k] = b->q_scale + k;
+      launches += 3;
+    }
+    FipBins bins = b->bins(k);
+    FIP_CUDA(fip_launch_bin(geo, B[k], (int)nb[k], bins, bs));
+    launches += fip_bin_launches(geo);
+    if (!precise) {
+      FIP_CUDA(fip_launch_targets(geo, V[k], b->targets + k * b->n2, bs));
+      launches += 1;
+    }
+  }
+  for (int i = 0; i < kBranches; ++i) {
+    FIP_CUDA(cudaEventRecord(b->join[i], b->branch[i]));
+    FIP_CUDA(cudaStreamWaitEvent(s, b->join[i], 0));
+  }
+  // One persistent gridding launch and one batched transform for the batch.
+  FIP_CUDA(fip_launch_grid_batch(geo, in, vt, b->multi, b->ntiles, b->nmulti, b->entries, b->cap,
+                                 b->work, b->wcap, b->nwork, b->grid, b->grid_elems,
+                                 precise ? 1 : 0, s, b->grid_ctas_per_sm));
+  FIP_CUDA(fip_launch_fft_cols(geo, b->grid, b->bbox, b->colbuf, b->twiddles, b->fft, s, count,
+                               b->grid_elems, b->col_elems));
+  FIP_CUDA(fip_launch_fft_rows(geo, b->colbuf, b->bbox, b->taper, b->twiddles, b->fft, b->pre, s,
+                               count, b->col_elems, b->n2));
+  launches += 4;
+  // Reprojection per snapshot on the branches, into ring slots 2 .. count+1.
+  FIP_CUDA(cudaMemsetAsync(b->maxima + 2, 0, count * sizeof(float), s));
+  FIP_CUDA(cudaEventRecord(b->fork, s));
+  for (int i = 0; i < kBranches; ++i) FIP_CUDA(cudaStreamWaitEvent(b->branch[i], b->fork, 0));
+  for (int k = 0; k < count; ++k) {
+    cudaStream_t bs = b->branch[k % kBranches];
+    FIP_CUDA(fip_launch_reproject_gather(
+        geo, b->pre + k * b->n2, precise ? nullptr : b->targets + k * b->n2, V[k], (int)nb[k],
+        b->bbox + 4 * k + 3, b->images + (k + 2) * b->n2,
+        reinterpret_cast<unsigned*>(b->maxima + k + 2), precise ? 1 : 0, bs));
+    launches += 1;
+  }
+  for (int i = 0; i < kBranches; ++i) {
+    FIP_CUDA(cudaEventRecord(b->join[i], b->branch[i]));
+    FIP_CUDA(cudaStreamWaitEvent(s, b->join[i], 0));
+  }
+  // Sliding-window trigger: snapshot k (slot k + 2) with two predecessors.
+  const int ntrig = count - first_result;
+  if (ntrig > 0 && geo.t > 0) {
+    FIP_CUDA(fip_launch_trigger_batch(geo, b->images + first_result * b->n2,
+                                      b->maxima + first_result, ntrig, results,
+                                      precise ? 1 : 0, s));
+    launches += 1;
+  }
+  // Carry the last two images (and maxima) to slots 0, 1.
+  for (int slot = 0; slot < 2; ++slot) {
+    const int from = count + slot;  // slots count, count + 1 (count >= 1)
+    if (from == slot) continue;
+    FIP_CUDA(cudaMemcpyAsync(b->images + slot * b->n2, b->images + from * b->n2,
+                             b->n2 * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    FIP_CUDA(cudaMemcpyAsync(b->maxima + slot, b->maxima + from, sizeof(float),
+                             cudaMemcpyDeviceToDevice, s));
+  }
+  b->launches += launches;
+  return FIP_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int fip_batch_create(fip_batch** out, const fip_imager_config* cfg, size_t max_snapshots) {
+  if (!out || !cfg) return fail(FIP_ERR_ARG, "null argument");
+  *out = nullptr;
+  FIP_TRY(validate_sizes(cfg->image_size, cfg->unit_size, cfg->cell_size));
+  if (max_snapshots < 1 || max_snapshots > FIP_MAX_BATCH)
+    return fail(FIP_ERR_ARG, "max_snapshots must be in [1, 64]");
+  if (cfg->max_baselines == 0 || cfg->max_baselines > (1u << 24))
+    return fail(FIP_ERR_ARG, "max_baselines must be in [1, 2^24]");
+  if (cfg->form != FIP_FORM_PLAIN && cfg->form != FIP_FORM_PRECISE)
+    return fail(FIP_ERR_ARG, "unknown form");
+  if (cfg->vis_storage < 0 || cfg->vis_storage > 2) return fail(FIP_ERR_ARG, "unknown storage");
+  if (cfg->reproject != 0) return fail(FIP_ERR_ARG, "the batching form reprojects by tile gather");
+  int ndev = 0;
+  FIP_CUDA(cudaGetDeviceCount(&ndev));
+  if (cfg->device < 0 || cfg->device >= ndev) return fail(FIP_ERR_ARG, "no such device");
+  DeviceGuard guard(cfg->device);
+  if (!guard.ok) return fail(FIP_ERR_CUDA, "cudaSetDevice failed");
+
+  fip_batch* b = new fip_batch();
+  b->cfg = *cfg;
+  b->smax = (int)max_snapshots;
+  FipGeom& geo = b->geo;
+  geo.n = (int)cfg->image_size;
+  geo.g = (int)ceilf(1.5f * (float)cfg->image_size);  // FIPkernels.cu:583
+  geo.hp = geo.g / 2 + 1;
+  geo.t = (int)cfg->unit_size;
+  geo.u = geo.t > 0 ? geo.n / geo.t : 0;
+  geo.tiles_r = (geo.g + FIP_GTILE - 1) / FIP_GTILE;
+  geo.tiles_c = (geo.hp + FIP_GTILE - 1) / FIP_GTILE;
+  geo.cell = cfg->cell_size;
+  geo.layout = 1;
+  auto cleanup = [&](int code) {
+    std::string msg = g_last_error;
+    batch_free(b);
+    g_last_error = msg;
+    return code;
+  };
+  if (!fip_fft_plan(geo.g, b->fft))
+    return cleanup(fail(FIP_ERR_ARG, "the batching form needs a power-of-two image size "
+                                     "(band-pruned transform)"));
+  if (!fip_gather_supported(geo, cfg->form == FIP_FORM_PRECISE))
+    return cleanup(fail(FIP_ERR_ARG, "cell_size too small for the tile-gather reprojection"));
+#define FIP_BALLOC(call)                                                                     \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return cleanup(fail(e_ == cudaErrorMemoryAllocation ? FIP_ERR_NOMEM : FIP_ERR_CUDA,    \
+                          std::string(#call) + ": " + cudaGetErrorString(e_)));              \
+  } while (0)
+  const size_t S = max_snapshots, nb = cfg->max_baselines;
+  size_t& tot = b->device_bytes;
+  b->ntiles = (size_t)geo.tiles_r * geo.tiles_c;
+  b->cap = 12 * nb;
+  b->wcap = b->ntiles + b->cap / FIP_GCHUNK + 1;
+  b->n2 = (size_t)geo.n * geo.n;
+  b->grid_elems = (size_t)geo.g * geo.hp;
+  b->col_elems = (size_t)geo.hp * geo.n;
+  FIP_BALLOC(dalloc(&b->count, S * b->ntiles, tot));
+  FIP_BALLOC(dalloc(&b->offset, S * (b->ntiles + 1), tot));
+  FIP_BALLOC(dalloc(&b->cursor, S * b->ntiles, tot));
+  FIP_BALLOC(dalloc(&b->entries, S * b->cap, tot));
+  FIP_BALLOC(dalloc(&b->work, S * b->wcap, tot));
+  FIP_BALLOC(dalloc(&b->nwork, S, tot));
+  FIP_BALLOC(dalloc(&b->bbox, 4 * S, tot));
+  FIP_BALLOC(dalloc(&b->multi, S * b->ntiles, tot));
+  FIP_BALLOC(dalloc(&b->nmulti, S, tot));
+  FIP_BALLOC(dalloc(&b->grid, S * b->grid_elems, tot));
+  FIP_BALLOC(dalloc(&b->colbuf, S * b->col_elems, tot));
+  FIP_BALLOC(dalloc(&b->pre, S * b->n2, tot));
+  if (cfg->form == FIP_FORM_PLAIN) FIP_BALLOC(dalloc(&b->targets, S * b->n2, tot));
+  if (cfg->form == FIP_FORM_PRECISE && cfg->vis_storage != FIP_STORE_F32) {
+    FIP_BALLOC(dalloc((uint16_t**)&b->q_re, S * nb, tot));
+    FIP_BALLOC(dalloc((uint16_t**)&b->q_im, S * nb, tot));
+    FIP_BALLOC(dalloc(&b->q_scale, S, tot));
+  }
+  FIP_BALLOC(dalloc(&b->images, (S + 2) * b->n2, tot));
+  FIP_BALLOC(dalloc(&b->maxima, S + 2, tot));
+  FIP_BALLOC(dalloc(&b->taper, 2 * ((size_t)geo.n / 2 + 1), tot));
+  FIP_BALLOC(dalloc(&b->twiddles, (size_t)geo.g, tot));
+  {
+    std::vector<float2> tw(geo.g);
+    for (int k = 0; k < geo.g; ++k) {
+      const double a = 2.0 * FIP_M_PI * (double)k / (double)geo.g;
+      tw[k] = make_float2((float)cos(a), (float)sin(a));
+    }
+    FIP_BALLOC(cudaMemcpy(b->twiddles, tw.data(), geo.g * sizeof(float2),
+                          cudaMemcpyHostToDevice));
+  }
+  for (int k = 0; k < kBranches; ++k) {
+    FIP_BALLOC(cudaStreamCreateWithFlags(&b->branch[k], cudaStreamNonBlocking));
+    FIP_BALLOC(cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming));
+  }
+  FIP_BALLOC(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+  FIP_BALLOC(fip_launch_taper(b->taper, geo, b->branch[0]));
+  FIP_BALLOC(cudaStreamSynchronize(b->branch[0]));
+#undef FIP_BALLOC
+  *out = b;
+  return FIP_OK;
+}
+
+int fip_batch_destroy(fip_batch* b) {
+  batch_free(b);
+  return FIP_OK;
+}
+
+size_t fip_batch_device_bytes(const fip_batch* b) { return b ? b->device_bytes : 0; }
+
+unsigned long long fip_batch_kernel_launches(const fip_batch* b) { return b ? b->launches : 0; }
+
+int fip_batch_reset(fip_batch* b) {
+  if (!b) return fail(FIP_ERR_ARG, "null batch");
+  b->carried = 0;
+  return FIP_OK;
+}
+
+int fip_batch_image(fip_batch* b, const float* const* vis_re, const float* const* vis_im,
+                    const float* const* B, const float* const* V, const size_t* nb, size_t count,
+                    float* results, size_t* nresults, void* stream) {
+  if (!b || !vis_re || !vis_im || !B || !V || !nb) return fail(FIP_ERR_ARG, "null argument");
+  if (count < 1 || count > (size_t)b->smax)
+    return fail(FIP_ERR_ARG, "count must be in [1, max_snapshots]");
+  for (size_t k = 0; k < count; ++k) {
+    if (!vis_re[k] || !vis_im[k] || !B[k] || !V[k]) return fail(FIP_ERR_ARG, "null device pointer");
+    if (nb[k] == 0 || nb[k] > b->cfg.max_baselines)
+      return fail(FIP_ERR_ARG, "nb must be in [1, max_baselines]");
+  }
+  const int first = std::max(0, 2 - b->carried);
+  const int ntrig = std::max(0, (int)count - first);
+  if (ntrig > 0 && b->geo.t > 0 && !results) return fail(FIP_ERR_ARG, "null results");
+  DeviceGuard g(b->cfg.device);
+  if (!g.ok) return fail(FIP_ERR_CUDA, "cudaSetDevice failed");
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaStream_t cs = s;
+  // The legacy default stream cannot be captured: record on a branch then.
+  if (s == nullptr || s == cudaStreamLegacy) cs = b->branch[0];
+  if (cs != s) {
+    FIP_CUDA(cudaEventRecord(b->fork, s));
+    FIP_CUDA(cudaStreamWaitEvent(cs, b->fork, 0));
+  }
+  cudaGraph_t graph = nullptr;
+  FIP_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+  const int st = batch_record(b, vis_re, vis_im, B, V, nb, (int)count, first, results, cs);
+  cudaError_t e = cudaStreamEndCapture(cs, &graph);
+  if (st != FIP_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return st;
+  }
+  if (e != cudaSuccess) return fail(FIP_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
+  // Re-use the executable graph when the call's shape is unchanged (only
+  // pointers, sizes and launch extents differ); instantiate otherwise.
+  bool updated = false;
+  if (b->exec) {
+    cudaGraphExecUpdateResultInfo info{};
+    updated = cudaGraphExecUpdate(b->exec, graph, &info) == cudaSuccess;
+    if (!updated) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(b->exec);
+      b->exec = nullptr;
+    }
+  }
+  if (!updated) {
+    e = cudaGraphInstantiate(&b->exec, graph, 0);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(graph);
+      b->exec = nullptr;
+      return fail(FIP_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    }
+  }
+  cudaGraphDestroy(graph);
+  FIP_CUDA(cudaGraphLaunch(b->exec, cs));
+  if (cs != s) {
+    FIP_CUDA(cudaEventRecord(b->fork, cs));
+    FIP_CUDA(cudaStreamWaitEvent(s, b->fork, 0));
+  }
+  b->carried = std::min(2, b->carried + (int)count);
+  if (nresults) *nresults = (b->geo.t > 0) ? (size_t)ntrig : 0;
+  return FIP_OK;
+}
+
+int fip_batch_autotune(fip_batch* b, const float* const* vis_re, const float* const* vis_im,
+                       const float* const* B, const float* const* V, const size_t* nb,
+                       size_t count, void* stream) {
+  if (!b) return fail(FIP_ERR_ARG, "null batch");
+  const int first = std::max(0, 2 - b->carried);
+  float* res = nullptr;
+  const int ntrig = std::max(0, (int)count - first);
+  if (ntrig > 0 && b->geo.t > 0) {
+    FIP_CUDA(cudaMalloc(&res, (size_t)ntrig * b->geo.u * b->geo.u * sizeof(float)));
+  }
+  size_t nr = 0;
+  int st = fip_batch_image(b, vis_re, vis_im, B, V, nb, count, res, &nr, stream);
+  DeviceGuard g(b->cfg.device);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (st == FIP_OK) st = cudaStreamSynchronize(s) == cudaSuccess ? FIP_OK : fail(FIP_ERR_CUDA, "sync");
+  if (res) cudaFree(res);
+  if (st != FIP_OK) return st;
+  // The bins, bands and grids of these snapshots are now in place: time the
+  // launch shapes on them.
+  const FipGeom& geo = b->geo;
+  const bool precise = b->cfg.form == FIP_FORM_PRECISE;
+  const bool reduced = precise && b->cfg.vis_storage != FIP_STORE_F32;
+  const int vt = !reduced ? FIP_VIS_F32
+                          : (b->cfg.vis_storage == FIP_STORE_F16 ? FIP_VIS_F16 : FIP_VIS_BF16);
+  FipGridBatch in{};
+  in.count = (int)count;
+  for (size_t k = 0; k < count; ++k) {
+    in.B[k] = B[k];
+    in.V[k] = V[k];
+    in.vr[k] = reduced ? static_cast<const void*>(static_cast<char*>(b->q_re) + k * b->cfg.max_baselines * 2)
+                       : vis_re[k];
+    in.vi[k] = reduced ? static_cast<const void*>(static_cast<char*>(b->q_im) + k * b->cfg.max_baselines * 2)
+                       : vis_im[k];
+    in.vis_scale[k] = reduced ? b->q_scale + k : nullptr;
+  }
+  EventPair ev;
+  FIP_CUDA(cudaEventCreate(&ev.a));
+  FIP_CUDA(cudaEventCreate(&ev.b));
+  auto timed = [&](auto&& launch, float& ms) -> int {
+    ms = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+      FIP_CUDA(cudaEventRecord(ev.a, s));
+      FIP_CUDA(launch());
+      FIP_CUDA(cudaEventRecord(ev.b, s));
+      FIP_CUDA(cudaEventSynchronize(ev.b));
+      float t = 0.f;
+      FIP_CUDA(cudaEventElapsedTime(&t, ev.a, ev.b));
+      if (rep > 0) ms = std::min(ms, t);
+    }
+    return FIP_OK;
+  };
+  {
+    float best = 1e30f;
+    fipfft::Plan chosen = b->fft;
+    for (int vpt : {8, 16}) {
+      fipfft::Plan p{};
+      if (!fip_fft_plan(geo.g, p, vpt)) continue;
+      float ms = 0.f;
+      FIP_TRY(timed(
+          [&]() -> cudaError_t {
+            cudaError_t e = fip_launch_fft_cols(geo, b->grid, b->bbox, b->colbuf, b->twiddles, p,
+                                                s, (int)count, b->grid_elems, b->col_elems);
+            if (e != cudaSuccess) return e;
+            return fip_launch_fft_rows(geo, b->colbuf, b->bbox, b->taper, b->twiddles, p, b->pre,
+                                       s, (int)count, b->col_elems, b->n2);
+          },
+          ms));
+      if (ms < best) {
+        best = ms;
+        chosen = p;
+      }
+    }
+    b->fft = chosen;
+  }
+  {
+    float best = 1e30f;
+    int chosen = 0;
+    for (int c = 1; c <= fip_grid_max_ctas_per_sm(precise ? 1 : 0); ++c) {
+      float ms = 0.f;
+      FIP_TRY(timed(
+          [&]() -> cudaError_t {
+            return fip_launch_grid_batch(geo, in, vt, b->multi, b->ntiles, b->nmulti, b->entries,
+                                         b->cap, b->work, b->wcap, b->nwork, b->grid,
+                                         b->grid_elems, precise ? 1 : 0, s, c);
+          },
+          ms));
+      if (ms < best) {
+        best = ms;
+        chosen = c;
+      }
+    }
+    b->grid_ctas_per_sm = chosen;
+  }
+  // The shapes changed: the next call instantiates a new graph.
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  b->carried = 0;
+  return FIP_OK;
+}
+
+int fip_batch_tuning(const fip_batch* b, int* fft_values_per_thread, int* grid_ctas_per_sm) {
+  if (!b) return fail(FIP_ERR_ARG, "null batch");
+  if (fft_values_per_thread) *fft_values_per_thread = b->fft.e;
+  if (grid_ctas_per_sm)
+    *grid_ctas_per_sm = b->grid_ctas_per_sm > 0
+                            ? b->grid_ctas_per_sm
+                            : fip_grid_max_ctas_per_sm(b->cfg.form == FIP_FORM_PRECISE ? 1 : 0);
+  return FIP_OK;
+}
+
+}  // extern "C"
+
 int FIpipe(float* Visreal, float* Visimag, float* Bin, float* Vin, float* result_array,
            size_t num_baselines, size_t image_size, size_t num_snapshots, float cell_size,
            size_t unit_size) {

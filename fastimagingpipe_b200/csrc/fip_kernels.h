@@ -45,18 +45,31 @@ cudaError_t fip_launch_grid(const FipGeom& geo, const float* B, const void* vr, 
                             const FipBins& bins, float2* grid, int compensated, cudaStream_t s,
                             int ctas_per_sm = 0);
 int fip_grid_max_ctas_per_sm(int compensated);
+// One persistent gridding launch over a batch of snapshots (plus the zeroing
+// of their split tiles): snapshot k's inputs in in.*[k], its bins and grid at
+// base + k * stride, its item count nwork[k] and split-tile count nmulti[k].
+cudaError_t fip_launch_grid_batch(const FipGeom& geo, const FipGridBatch& in, int vis_type,
+                                  const unsigned* multi, size_t multi_stride,
+                                  const unsigned* nmulti, const unsigned* entries,
+                                  size_t entries_stride, const int4* work, size_t work_stride,
+                                  const unsigned* nwork, float2* grid, size_t grid_stride,
+                                  int compensated, cudaStream_t s, int ctas_per_sm = 0);
 // values_per_thread: 8 or 16 (0 = the default for the length).
 bool fip_fft_plan(int g, fipfft::Plan& p, int values_per_thread = 0);
 // Band-pruned inverse FFT: column pass (band grid -> colbuf [G/2+1][N]) and
 // row pass with the crop + correction epilogue (colbuf -> pre [N*N]).
+// Batched (batch > 1): snapshot k's grid, bbox (4 words) and colbuf at
+// base + k * stride.
 cudaError_t fip_launch_fft_cols(const FipGeom& geo, const float2* grid, const unsigned* bbox,
                                 float2* colbuf, const float2* twiddles, const fipfft::Plan& plan,
-                                cudaStream_t s);
+                                cudaStream_t s, int batch = 1, size_t grid_stride = 0,
+                                size_t col_stride = 0);
 // Also folds the image maximum into bbox[3] (float bits, zeroed by the
 // binning), which the gather reprojection reads.
 cudaError_t fip_launch_fft_rows(const FipGeom& geo, const float2* colbuf, unsigned* bbox,
                                 const float* taper, const float2* twiddles,
-                                const fipfft::Plan& plan, float* pre, cudaStream_t s);
+                                const fipfft::Plan& plan, float* pre, cudaStream_t s,
+                                int batch = 1, size_t col_stride = 0, size_t pre_stride = 0);
 // Crop + correction of an in-place cuFFT C2R output -> pre [N*N].
 cudaError_t fip_launch_correct_c2r(const FipGeom& geo, const float* fft_out, const float* taper,
                                    float* pre, unsigned* pre_max, cudaStream_t s);
@@ -81,6 +94,10 @@ cudaError_t fip_launch_image_max(const float* img, size_t count, unsigned* out, 
 cudaError_t fip_launch_trigger(const FipGeom& geo, const float* I1, const float* I2,
                                const float* I3, const float* max3, float* stats,
                                float* result, int precise, cudaStream_t s);
+// Batched trigger over a linear ring of images (stride N*N): triple k is
+// images k, k+1, k+2 with maxima[k .. k+2], result k at results + k * U*U.
+cudaError_t fip_launch_trigger_batch(const FipGeom& geo, const float* images, const float* maxima,
+                                     int count, float* results, int precise, cudaStream_t s);
 cudaError_t fip_launch_pixel_targets(const FipGeom& geo, const float* V, float* out,
                                      int exact_targets, cudaStream_t s);
 

@@ -342,12 +342,16 @@ __device__ __forceinline__ uint3 block_scan3(uint3 v, uint3& total) {
 
 // Tile scan run by one CTA of NT threads: offsets, cursors, the work list
 // (every band tile gets >= 1 item) and the list of tiles split over several
-// items.  cnt_s: the tile counts, in shared memory.
+// items.  cnt_s: the tile counts; wp_s: [ntiles + 1] scratch for the work
+// prefix (both shared memory).  The work items are written in a second,
+// parallel sweep (one thread per item, its tile found by bisection), so a
+// tile with thousands of entries does not serialise on one thread.
 template <int NT>
-__device__ __forceinline__ void scan_tiles(const unsigned* cnt_s, const unsigned* bbox, int ntiles,
-                                           int tiles_c, int g, int layout, unsigned* offset,
-                                           unsigned* cursor, int4* work, unsigned* nwork,
-                                           int wcap, unsigned* multi, unsigned* nmulti) {
+__device__ __forceinline__ void scan_tiles(const unsigned* cnt_s, unsigned* wp_s,
+                                           const unsigned* bbox, int ntiles, int tiles_c, int g,
+                                           int layout, unsigned* offset, unsigned* cursor,
+                                           int4* work, unsigned* nwork, int wcap,
+                                           unsigned* multi, unsigned* nmulti) {
   constexpr int PER = 8;
   uint3 carry = make_uint3(0, 0, 0);
   for (int base = 0; base < ntiles; base += NT * PER) {
@@ -377,10 +381,7 @@ __device__ __forceinline__ void scan_tiles(const unsigned* cnt_s, const unsigned
       if (t < ntiles) {
         offset[t] = run;
         cursor[t] = 0;
-        for (unsigned q = 0; q < nch[k]; ++q)
-          if ((int)(wrun + q) < wcap)
-            work[wrun + q] = make_int4(t, (int)(run + min(q * FIP_GCHUNK, c[k])),
-                                       (int)(run + min((q + 1) * FIP_GCHUNK, c[k])), nch[k] == 1);
+        wp_s[t] = wrun;
         if (nch[k] > 1) multi[mrun++] = (unsigned)t;
         run += c[k];
         wrun += nch[k];
@@ -392,8 +393,23 @@ __device__ __forceinline__ void scan_tiles(const unsigned* cnt_s, const unsigned
   }
   if (threadIdx.x == 0) {
     offset[ntiles] = carry.x;
+    wp_s[ntiles] = carry.y;
     *nwork = min(carry.y, (unsigned)wcap);
     *nmulti = carry.z;
+  }
+  __syncthreads();
+  const unsigned nw = min(carry.y, (unsigned)wcap);
+  for (unsigned w = threadIdx.x; w < nw; w += NT) {
+    int lo = 0, hi = ntiles - 1;  // last tile with wp_s[t] <= w
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (wp_s[mid] <= w) lo = mid; else hi = mid - 1;
+    }
+    const int t = lo;
+    const unsigned q = w - wp_s[t], nch = wp_s[t + 1] - wp_s[t], c = cnt_s[t];
+    const unsigned run = offset[t];
+    work[w] = make_int4(t, (int)(run + min(q * FIP_GCHUNK, c)),
+                        (int)(run + min((q + 1) * FIP_GCHUNK, c)), nch == 1);
   }
 }
 
@@ -436,13 +452,13 @@ __global__ void __launch_bounds__(kScanThreads) k_bin_scan_tiles(
     const unsigned* __restrict__ count, const unsigned* __restrict__ bbox, int ntiles,
     int tiles_c, int g, int layout, unsigned* offset, unsigned* cursor, int4* work,
     unsigned* nwork, int wcap, unsigned* multi, unsigned* nmulti) {
-  extern __shared__ unsigned s_cnt[];
+  extern __shared__ unsigned s_cnt[];  // [ntiles] counts, then [ntiles + 1] work prefix
   __shared__ unsigned s_k[2];
   for (int t = threadIdx.x; t < ntiles; t += kScanThreads) s_cnt[t] = count[t];
   if (threadIdx.x < 2) s_k[threadIdx.x] = bbox[threadIdx.x];
   __syncthreads();
-  scan_tiles<kScanThreads>(s_cnt, s_k, ntiles, tiles_c, g, layout, offset, cursor, work, nwork,
-                           wcap, multi, nmulti);
+  scan_tiles<kScanThreads>(s_cnt, s_cnt + ntiles, s_k, ntiles, tiles_c, g, layout, offset,
+                           cursor, work, nwork, wcap, multi, nmulti);
 }
 
 // Scatter pass: entries of the CTA's visibility range into the tile lists.
@@ -479,9 +495,14 @@ __device__ __forceinline__ size_t cell_index(int row, int col, int g, int hp, in
 }
 
 // Zeroes the tiles that several work items reduce into.
+// Batched launches: snapshot blockIdx.y, its lists at multi + y * multi_stride,
+// nmulti[y], its grid at grid + y * grid_stride.
 __global__ void k_zero_tiles(const unsigned* __restrict__ multi, const unsigned* __restrict__ nmulti,
-                             int tiles_c, int g, int hp, int layout, float2* __restrict__ grid) {
-  const unsigned nm = *nmulti;
+                             int tiles_c, int g, int hp, int layout, float2* __restrict__ grid,
+                             size_t multi_stride, size_t grid_stride) {
+  multi += blockIdx.y * multi_stride;
+  grid += blockIdx.y * grid_stride;
+  const unsigned nm = nmulti[blockIdx.y];
   for (unsigned w = blockIdx.x; w < nm; w += gridDim.x) {
     const int t = (int)multi[w];
     const int row0 = (t / tiles_c) * FIP_GTILE, col0 = (t % tiles_c) * FIP_GTILE;
@@ -512,11 +533,130 @@ struct GridSmem {
   float k1[FIP_GCHUNK][9], k2[FIP_GCHUNK][9];  // stride 9: conflict-free both ways
 };
 
-// Persistent gridder over work items (tile, entry range).  Phase 1 loads the
-// item's visibilities and their separable kernel values into shared memory
-// (all loads in flight at once); phase 2 lets each warp spread one
-// visibility's taps over its lanes into the shared tile; phase 3 commits.
+// One gridding work item (tile, entry range) of one snapshot.  Phase 1
+// loads the item's visibilities and their separable kernel values into
+// shared memory (all loads in flight at once); phase 2 lets each warp spread
+// one visibility's taps over its lanes into the shared tile; phase 3 commits.
 // COMP: Neumaier-compensated tile sums (precision form).
+template <int VT, bool COMP>
+__device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_cim,
+                                          const float* __restrict__ B, const void* vr,
+                                          const void* vi, float vis_scale, float inten,
+                                          float scale, int g, int hp, int tiles_c, int layout,
+                                          const unsigned* __restrict__ entries, int4 item,
+                                          float2* __restrict__ grid) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int tile = item.x, cnt = item.z - item.y;
+  const int trow0 = (tile / tiles_c) * FIP_GTILE, tcol0 = (tile % tiles_c) * FIP_GTILE;
+  for (int k = threadIdx.x; k < FIP_GTILE * kTS; k += kThreads) {
+    S.re[k] = 0.f;
+    S.im[k] = 0.f;
+    if (COMP) {
+      s_cre[k] = 0.f;
+      s_cim[k] = 0.f;
+    }
+  }
+  // Phase 1.
+  for (int q = threadIdx.x; q < cnt; q += kThreads) {
+    const unsigned ent = entries[item.y + q];
+    const int v = (int)(ent >> 1), mir = (int)(ent & 1);
+    Footprint f;
+    footprint(B, v, scale, g, f);
+    int c0, c1;
+    half_cols(f, mir, c0, c1);
+    // Visibility weighting (FIPkernels.cu:188-195), halved for the
+    // Hermitian split, conjugated for the mirrored copy.
+    float wr, wi;
+    if (VT == FIP_VIS_F32) {
+      wr = load_vis<VT>(vr, v) / inten;
+      wi = load_vis<VT>(vi, v) / inten;
+    } else {
+      wr = (load_vis<VT>(vr, v) * vis_scale) / inten;
+      wi = (load_vis<VT>(vi, v) * vis_scale) / inten;
+    }
+    S.wr[q] = 0.5f * wr;
+    S.wi[q] = mir ? -0.5f * wi : 0.5f * wi;
+    const int nr = f.a1 - f.a0 + 1, nc = c1 - c0 + 1;
+    S.row0[q] = mir ? -f.a0 : f.a0;
+    S.col0[q] = c0;
+    S.meta[q] = nr | (nc << 4) | (mir << 8);
+    const float ihs = 1 / static_cast<float>(FIP_SUPPORT / 2);
+#pragma unroll
+    for (int a = 0; a < 9; ++a)
+      if (a < nr) S.k1[q][a] = fipref::es((static_cast<float>(f.a0 + a) - f.p1) * ihs);
+    // Column taps in half-plane order c0..c1: original r2 = c (direct) or
+    // -c (mirrored).
+#pragma unroll
+    for (int b = 0; b < 9; ++b)
+      if (b < nc) {
+        const int r2 = mir ? -(c0 + b) : c0 + b;
+        S.k2[q][b] = fipref::es((static_cast<float>(r2) - f.p2) * ihs);
+      }
+  }
+  __syncthreads();
+  // Phase 2.
+  for (int q = warp; q < cnt; q += kThreads / 32) {
+    const int meta = S.meta[q];
+    const int nr = meta & 15, nc = (meta >> 4) & 15, mir = (meta >> 8) & 1;
+    const int per = 32 / nc;  // tap rows per warp step
+    const int ia0 = lane / nc, ib = lane - ia0 * nc;
+    if (ia0 >= per) continue;
+    const float wr = S.wr[q], wi = S.wi[q];
+    const int rbase = S.row0[q], col = S.col0[q] + ib;
+    const int lc = col - tcol0;
+    if ((unsigned)lc >= (unsigned)FIP_GTILE) continue;
+    const float k2 = S.k2[q][ib];
+    for (int ia = ia0; ia < nr; ia += per) {
+      const int row = wrap_row(mir ? rbase - ia : rbase + ia, g);
+      const int lr = row - trow0;
+      if ((unsigned)lr >= (unsigned)FIP_GTILE) continue;
+      const float kval = S.k1[q][ia] * k2;
+      const float cr = wr * kval, ci = wi * kval;
+      const int cell = lr * kTS + lc;
+      if (!COMP) {
+        atomicAdd(&S.re[cell], cr);
+        atomicAdd(&S.im[cell], ci);
+      } else {
+        float o = atomicAdd(&S.re[cell], cr);
+        float sm = o + cr;
+        float err = (fabsf(o) >= fabsf(cr)) ? (o - sm) + cr : (cr - sm) + o;
+        atomicAdd(&s_cre[cell], err);
+        o = atomicAdd(&S.im[cell], ci);
+        sm = o + ci;
+        err = (fabsf(o) >= fabsf(ci)) ? (o - sm) + ci : (ci - sm) + o;
+        atomicAdd(&s_cim[cell], err);
+      }
+    }
+  }
+  __syncthreads();
+  // Phase 3: commit in the layout's contiguous direction.
+  const bool single = item.w != 0;
+  for (int k = threadIdx.x; k < FIP_GTILE * FIP_GTILE; k += kThreads) {
+    const int lr = layout ? k % FIP_GTILE : k / FIP_GTILE;
+    const int lc = layout ? k / FIP_GTILE : k % FIP_GTILE;
+    const int row = trow0 + lr, col = tcol0 + lc;
+    if (row < g && col < hp) {
+      float2 val = make_float2(S.re[lr * kTS + lc], S.im[lr * kTS + lc]);
+      if (COMP) {
+        val.x += s_cre[lr * kTS + lc];
+        val.y += s_cim[lr * kTS + lc];
+      }
+      float2* dst = &grid[cell_index(row, col, g, hp, layout)];
+      if (single) {
+        *dst = val;
+      } else if (val.x != 0.f || val.y != 0.f) {
+        atomicAdd(dst, val);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ float plane_intensity(const float* V) {
+  return fabs(V[0 * 3 + 0] * V[1 * 3 + 1] - V[0 * 3 + 1] * V[1 * 3 + 0]);
+}
+
+// Persistent gridder over the work items of one snapshot.
 template <int VT, bool COMP>
 __global__ void __launch_bounds__(kThreads) k_grid(const float* __restrict__ B, const void* vr,
                                                    const void* vi,
@@ -531,116 +671,50 @@ __global__ void __launch_bounds__(kThreads) k_grid(const float* __restrict__ B, 
   GridSmem& S = *reinterpret_cast<GridSmem*>(s_raw);
   float* s_cre = reinterpret_cast<float*>(reinterpret_cast<char*>(s_raw) + sizeof(GridSmem));
   float* s_cim = s_cre + FIP_GTILE * kTS;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const float inten = fabs(V[0 * 3 + 0] * V[1 * 3 + 1] - V[0 * 3 + 1] * V[1 * 3 + 0]);
+  const float inten = plane_intensity(V);
   const float vis_scale = vis_scale_p ? *vis_scale_p : 1.0f;
   const unsigned nw = *nwork;
-  for (unsigned w = blockIdx.x; w < nw; w += gridDim.x) {
-    const int4 item = work[w];
-    const int tile = item.x, cnt = item.z - item.y;
-    const int trow0 = (tile / tiles_c) * FIP_GTILE, tcol0 = (tile % tiles_c) * FIP_GTILE;
-    for (int k = threadIdx.x; k < FIP_GTILE * kTS; k += kThreads) {
-      S.re[k] = 0.f;
-      S.im[k] = 0.f;
-      if (COMP) {
-        s_cre[k] = 0.f;
-        s_cim[k] = 0.f;
-      }
+  for (unsigned w = blockIdx.x; w < nw; w += gridDim.x)
+    grid_item<VT, COMP>(S, s_cre, s_cim, B, vr, vi, vis_scale, inten, scale, g, hp, tiles_c,
+                        layout, entries, work[w], grid);
+}
+
+// Persistent gridder over the work items of a batch of snapshots (one launch
+// for the batch): snapshot k reads in.*[k] and its bins and grid at
+// base + k * stride.
+template <int VT, bool COMP>
+__global__ void __launch_bounds__(kThreads) k_grid_batch(const FipGridBatch in, float scale,
+                                                         int g, int hp, int tiles_c, int layout,
+                                                         const unsigned* __restrict__ entries,
+                                                         size_t entries_stride,
+                                                         const int4* __restrict__ work,
+                                                         size_t work_stride,
+                                                         const unsigned* __restrict__ nwork,
+                                                         float2* __restrict__ grid,
+                                                         size_t grid_stride) {
+  extern __shared__ float4 s_raw[];
+  __shared__ unsigned s_first[FIP_MAX_BATCH + 1];  // prefix of the snapshots' item counts
+  GridSmem& S = *reinterpret_cast<GridSmem*>(s_raw);
+  float* s_cre = reinterpret_cast<float*>(reinterpret_cast<char*>(s_raw) + sizeof(GridSmem));
+  float* s_cim = s_cre + FIP_GTILE * kTS;
+  if (threadIdx.x == 0) {
+    unsigned acc = 0;
+    for (int k = 0; k < in.count; ++k) {
+      s_first[k] = acc;
+      acc += nwork[k];
     }
-    // Phase 1.
-    for (int q = threadIdx.x; q < cnt; q += kThreads) {
-      const unsigned ent = entries[item.y + q];
-      const int v = (int)(ent >> 1), mir = (int)(ent & 1);
-      Footprint f;
-      footprint(B, v, scale, g, f);
-      int c0, c1;
-      half_cols(f, mir, c0, c1);
-      // Visibility weighting (FIPkernels.cu:188-195), halved for the
-      // Hermitian split, conjugated for the mirrored copy.
-      float wr, wi;
-      if (VT == FIP_VIS_F32) {
-        wr = load_vis<VT>(vr, v) / inten;
-        wi = load_vis<VT>(vi, v) / inten;
-      } else {
-        wr = (load_vis<VT>(vr, v) * vis_scale) / inten;
-        wi = (load_vis<VT>(vi, v) * vis_scale) / inten;
-      }
-      S.wr[q] = 0.5f * wr;
-      S.wi[q] = mir ? -0.5f * wi : 0.5f * wi;
-      const int nr = f.a1 - f.a0 + 1, nc = c1 - c0 + 1;
-      S.row0[q] = mir ? -f.a0 : f.a0;
-      S.col0[q] = c0;
-      S.meta[q] = nr | (nc << 4) | (mir << 8);
-      const float ihs = 1 / static_cast<float>(FIP_SUPPORT / 2);
-#pragma unroll
-      for (int a = 0; a < 9; ++a)
-        if (a < nr) S.k1[q][a] = fipref::es((static_cast<float>(f.a0 + a) - f.p1) * ihs);
-      // Column taps in half-plane order c0..c1: original r2 = c (direct) or
-      // -c (mirrored).
-#pragma unroll
-      for (int b = 0; b < 9; ++b)
-        if (b < nc) {
-          const int r2 = mir ? -(c0 + b) : c0 + b;
-          S.k2[q][b] = fipref::es((static_cast<float>(r2) - f.p2) * ihs);
-        }
-    }
-    __syncthreads();
-    // Phase 2.
-    for (int q = warp; q < cnt; q += kThreads / 32) {
-      const int meta = S.meta[q];
-      const int nr = meta & 15, nc = (meta >> 4) & 15, mir = (meta >> 8) & 1;
-      const int per = 32 / nc;  // tap rows per warp step
-      const int ia0 = lane / nc, ib = lane - ia0 * nc;
-      if (ia0 >= per) continue;
-      const float wr = S.wr[q], wi = S.wi[q];
-      const int rbase = S.row0[q], col = S.col0[q] + ib;
-      const int lc = col - tcol0;
-      if ((unsigned)lc >= (unsigned)FIP_GTILE) continue;
-      const float k2 = S.k2[q][ib];
-      for (int ia = ia0; ia < nr; ia += per) {
-        const int row = wrap_row(mir ? rbase - ia : rbase + ia, g);
-        const int lr = row - trow0;
-        if ((unsigned)lr >= (unsigned)FIP_GTILE) continue;
-        const float kval = S.k1[q][ia] * k2;
-        const float cr = wr * kval, ci = wi * kval;
-        const int cell = lr * kTS + lc;
-        if (!COMP) {
-          atomicAdd(&S.re[cell], cr);
-          atomicAdd(&S.im[cell], ci);
-        } else {
-          float o = atomicAdd(&S.re[cell], cr);
-          float sm = o + cr;
-          float err = (fabsf(o) >= fabsf(cr)) ? (o - sm) + cr : (cr - sm) + o;
-          atomicAdd(&s_cre[cell], err);
-          o = atomicAdd(&S.im[cell], ci);
-          sm = o + ci;
-          err = (fabsf(o) >= fabsf(ci)) ? (o - sm) + ci : (ci - sm) + o;
-          atomicAdd(&s_cim[cell], err);
-        }
-      }
-    }
-    __syncthreads();
-    // Phase 3: commit in the layout's contiguous direction.
-    const bool single = item.w != 0;
-    for (int k = threadIdx.x; k < FIP_GTILE * FIP_GTILE; k += kThreads) {
-      const int lr = layout ? k % FIP_GTILE : k / FIP_GTILE;
-      const int lc = layout ? k / FIP_GTILE : k % FIP_GTILE;
-      const int row = trow0 + lr, col = tcol0 + lc;
-      if (row < g && col < hp) {
-        float2 val = make_float2(S.re[lr * kTS + lc], S.im[lr * kTS + lc]);
-        if (COMP) {
-          val.x += s_cre[lr * kTS + lc];
-          val.y += s_cim[lr * kTS + lc];
-        }
-        float2* dst = &grid[cell_index(row, col, g, hp, layout)];
-        if (single) {
-          *dst = val;
-        } else if (val.x != 0.f || val.y != 0.f) {
-          atomicAdd(dst, val);
-        }
-      }
-    }
-    __syncthreads();
+    s_first[in.count] = acc;
+  }
+  __syncthreads();
+  const unsigned total = s_first[in.count];
+  int k = 0;
+  for (unsigned w = blockIdx.x; w < total; w += gridDim.x) {
+    while (s_first[k + 1] <= w) ++k;  // items are visited in increasing order
+    const float inten = plane_intensity(in.V[k]);
+    const float vis_scale = in.vis_scale[k] ? *in.vis_scale[k] : 1.0f;
+    grid_item<VT, COMP>(S, s_cre, s_cim, in.B[k], in.vr[k], in.vi[k], vis_scale, inten, scale,
+                        g, hp, tiles_c, layout, entries + k * entries_stride,
+                        work[k * work_stride + (w - s_first[k])], grid + k * grid_stride);
   }
 }
 
@@ -676,9 +750,14 @@ __host__ __device__ constexpr int fft_min_blocks() {
 template <int LM, int LE>
 __global__ void __launch_bounds__(fft_threads<LM, LE>(), fft_min_blocks<LM, LE>())
     k_fft_cols(const float2* __restrict__ H, const unsigned* __restrict__ bbox,
-               float2* __restrict__ P, const float2* __restrict__ tw) {
+               float2* __restrict__ P, const float2* __restrict__ tw, size_t grid_stride,
+               size_t col_stride) {
   constexpr int M = 1 << LM, g = 3 * M, half = g / 2, n = 2 * M, NT = fft_threads<LM, LE>();
   extern __shared__ float2 s_fft[];
+  // Batched launches: snapshot blockIdx.y.
+  H += blockIdx.y * grid_stride;
+  P += blockIdx.y * col_stride;
+  bbox += 4 * blockIdx.y;
   const int c = blockIdx.x;
   const int k2 = (int)bbox[1];
   if (c > k2) return;
@@ -714,9 +793,13 @@ template <int LM, int LE>
 __global__ void __launch_bounds__(fft_threads<LM, LE>(), fft_min_blocks<LM, LE>())
     k_fft_rows(const float2* __restrict__ P, unsigned* bbox,
                const float* __restrict__ rck, float* __restrict__ pre,
-               const float2* __restrict__ tw) {
+               const float2* __restrict__ tw, size_t col_stride, size_t pre_stride) {
   constexpr int M = 1 << LM, g = 3 * M, half = g / 2, n = 2 * M, h = M, NT = fft_threads<LM, LE>();
   extern __shared__ float2 s_fft[];
+  // Batched launches: snapshot blockIdx.y.
+  P += blockIdx.y * col_stride;
+  pre += blockIdx.y * pre_stride;
+  bbox += 4 * blockIdx.y;
   const int yy1 = 2 * blockIdx.x;
   const int k2 = min((int)bbox[1], half);
   // Column band [lo, hi]; column -G/2 is column +G/2 (counted once).
@@ -1030,18 +1113,16 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
     float wl1, wm1, wl0, wm0;
     if (!EXACT) {
       const float LL = t.x, MM = t.y;
-      if (!(fabs(LL) < lim && fabs(MM) < lim)) return;
-      fl = (int)floorf(LL);
-      fm = (int)floorf(MM);
-      const int cl = (int)ceilf(LL), cm = (int)ceilf(MM);
-      // The reference's weight expressions (FIPkernels.cu:397-409).
-      wl0 = 1 - LL + fl; wl1 = LL - fl;
-      wm0 = 1 - MM + fm; wm1 = MM - fm;
-      fl += h - c0;
-      fm += h - r0;
-      // ceil == floor + 1 except on exact integers, where the far weight is 0.
-      if (cl == fl + c0 - h) wl1 = 0.f;
-      if (cm == fm + r0 - h) wm1 = 0.f;
+      if (!(fabsf(LL) < lim && fabsf(MM) < lim)) return;
+      const float flf = floorf(LL), fmf = floorf(MM);
+      // The reference's weight expressions (FIPkernels.cu:397-409).  Its far
+      // pixel is ceil(LL), equal to floor(LL) + 1 except on exact integers,
+      // where the far weight LL - floor(LL) is 0: splatting the far weight at
+      // floor + 1 adds the same sums.
+      wl0 = 1 - LL + flf; wl1 = LL - flf;
+      wm0 = 1 - MM + fmf; wm1 = MM - fmf;
+      fl = (int)flf + (h - c0);
+      fm = (int)fmf + (h - r0);
     } else {
       const float da = (float)(i - h - a0), db = (float)(j - h - b0);
       const float d1 = mf.m00 * da + mf.m01 * db, d2 = mf.m10 * da + mf.m11 * db;
@@ -1192,7 +1273,15 @@ __global__ void __launch_bounds__(kThreads) k_trigger(const float* __restrict__ 
                                                       const float* __restrict__ I3,
                                                       const float* __restrict__ max3, int n,
                                                       int t, int u, int vec,
-                                                      float* __restrict__ result) {
+                                                      float* __restrict__ result,
+                                                      size_t img_stride, size_t res_stride) {
+  // Batched launches: triple blockIdx.y is images y, y+1, y+2 of a linear ring
+  // (stride img_stride) with maxima max3[y .. y+2].
+  I1 += blockIdx.y * img_stride;
+  I2 += blockIdx.y * img_stride;
+  I3 += blockIdx.y * img_stride;
+  max3 += blockIdx.y;
+  result += blockIdx.y * res_stride;
   const int lane = threadIdx.x & 31;
   const int b = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
   if (b >= u * u) return;
@@ -1304,7 +1393,12 @@ cudaError_t fip_launch_bin(const FipGeom& geo, const float* B, int nb, FipBins& 
     if (nb > 0)
       k_bin_count<<<cta, kBinThreads, smem, s>>>(B, nb, per_cta, scale, geo.g, geo.tiles_c,
                                                   ntiles, bins.count, bins.bbox);
-    k_bin_scan_tiles<<<1, kScanThreads, smem, s>>>(bins.count, bins.bbox, ntiles, geo.tiles_c,
+    const size_t scan_smem = (2 * (size_t)ntiles + 1) * sizeof(unsigned);
+    cudaError_t ea = cudaFuncSetAttribute(k_bin_scan_tiles,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)((2 * (size_t)kMaxSmemTiles + 1) * sizeof(unsigned)));
+    if (ea != cudaSuccess) return ea;
+    k_bin_scan_tiles<<<1, kScanThreads, scan_smem, s>>>(bins.count, bins.bbox, ntiles, geo.tiles_c,
                                                     geo.g, geo.layout, bins.offset, bins.cursor,
                                                     bins.work, bins.nwork, (int)bins.wcap,
                                                     bins.multi, bins.nmulti);
@@ -1336,7 +1430,7 @@ cudaError_t fip_launch_grid(const FipGeom& geo, const float* B, const void* vr, 
   const float scale = geo.cell * (float)(size_t)geo.g;
   const int sms = sm_count();
   k_zero_tiles<<<sms, kThreads, 0, s>>>(bins.multi, bins.nmulti, geo.tiles_c, geo.g, geo.hp,
-                                        geo.layout, grid);
+                                        geo.layout, grid, 0, 0);
   const size_t smem = sizeof(GridSmem) + (compensated ? 2 * FIP_GTILE * kTS * sizeof(float) : 0);
   const int most = fip_grid_max_ctas_per_sm(compensated);
   const int blocks = sms * (ctas_per_sm > 0 ? min(ctas_per_sm, most) : most);
@@ -1357,6 +1451,40 @@ cudaError_t fip_launch_grid(const FipGeom& geo, const float* B, const void* vr, 
   }
 #undef FIP_GRID_CASE
   (void)nb;
+  return cudaGetLastError();
+}
+
+cudaError_t fip_launch_grid_batch(const FipGeom& geo, const FipGridBatch& in, int vis_type,
+                                  const unsigned* multi, size_t multi_stride,
+                                  const unsigned* nmulti, const unsigned* entries,
+                                  size_t entries_stride, const int4* work, size_t work_stride,
+                                  const unsigned* nwork, float2* grid, size_t grid_stride,
+                                  int compensated, cudaStream_t s, int ctas_per_sm) {
+  if (in.count < 1 || in.count > FIP_MAX_BATCH) return cudaErrorInvalidValue;
+  const float scale = geo.cell * (float)(size_t)geo.g;
+  const int sms = sm_count();
+  k_zero_tiles<<<dim3(sms, in.count), kThreads, 0, s>>>(multi, nmulti, geo.tiles_c, geo.g,
+                                                         geo.hp, geo.layout, grid, multi_stride,
+                                                         grid_stride);
+  const size_t smem = sizeof(GridSmem) + (compensated ? 2 * FIP_GTILE * kTS * sizeof(float) : 0);
+  const int most = fip_grid_max_ctas_per_sm(compensated);
+  const int blocks = sms * (ctas_per_sm > 0 ? min(ctas_per_sm, most) : most);
+#define FIP_GRID_CASE(VT, C)                                                                   \
+  do {                                                                                         \
+    auto kern = k_grid_batch<VT, C>;                                                           \
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);        \
+    kern<<<blocks, kThreads, smem, s>>>(in, scale, geo.g, geo.hp, geo.tiles_c, geo.layout,     \
+                                        entries, entries_stride, work, work_stride, nwork,     \
+                                        grid, grid_stride);                                    \
+  } while (0)
+  if (vis_type == FIP_VIS_F32) {
+    if (compensated) FIP_GRID_CASE(FIP_VIS_F32, true); else FIP_GRID_CASE(FIP_VIS_F32, false);
+  } else if (vis_type == FIP_VIS_F16) {
+    if (compensated) FIP_GRID_CASE(FIP_VIS_F16, true); else FIP_GRID_CASE(FIP_VIS_F16, false);
+  } else {
+    if (compensated) FIP_GRID_CASE(FIP_VIS_BF16, true); else FIP_GRID_CASE(FIP_VIS_BF16, false);
+  }
+#undef FIP_GRID_CASE
   return cudaGetLastError();
 }
 
@@ -1382,23 +1510,26 @@ static cudaError_t fft_smem_attr(const void* fn, int g, size_t& smem) {
 
 template <int LM, int LE>
 static cudaError_t launch_cols(const FipGeom& geo, const float2* grid, const unsigned* bbox,
-                               float2* colbuf, const float2* tw, cudaStream_t s) {
+                               float2* colbuf, const float2* tw, cudaStream_t s, int batch,
+                               size_t grid_stride, size_t col_stride) {
   size_t smem;
   cudaError_t e = fft_smem_attr((const void*)k_fft_cols<LM, LE>, geo.g, smem);
   if (e != cudaSuccess) return e;
-  k_fft_cols<LM, LE><<<geo.hp, fft_threads<LM, LE>(), smem, s>>>(grid, bbox, colbuf, tw);
+  k_fft_cols<LM, LE><<<dim3(geo.hp, batch), fft_threads<LM, LE>(), smem, s>>>(
+      grid, bbox, colbuf, tw, grid_stride, col_stride);
   return cudaGetLastError();
 }
 
 template <int LM, int LE>
 static cudaError_t launch_rows(const FipGeom& geo, const float2* colbuf, unsigned* bbox,
                                const float* taper, const float2* tw, float* pre,
-                               cudaStream_t s) {
+                               cudaStream_t s, int batch, size_t col_stride,
+                               size_t pre_stride) {
   size_t smem;
   cudaError_t e = fft_smem_attr((const void*)k_fft_rows<LM, LE>, geo.g, smem);
   if (e != cudaSuccess) return e;
-  k_fft_rows<LM, LE><<<geo.n / 2, fft_threads<LM, LE>(), smem, s>>>(
-      colbuf, bbox, taper + geo.n / 2 + 1, pre, tw);
+  k_fft_rows<LM, LE><<<dim3(geo.n / 2, batch), fft_threads<LM, LE>(), smem, s>>>(
+      colbuf, bbox, taper + geo.n / 2 + 1, pre, tw, col_stride, pre_stride);
   return cudaGetLastError();
 }
 
@@ -1429,16 +1560,20 @@ static cudaError_t launch_rows(const FipGeom& geo, const float2* colbuf, unsigne
 
 cudaError_t fip_launch_fft_cols(const FipGeom& geo, const float2* grid, const unsigned* bbox,
                                 float2* colbuf, const float2* twiddles, const fipfft::Plan& plan,
-                                cudaStream_t s) {
-  if (plan.g != geo.g) return cudaErrorInvalidValue;
-  FIP_FFT_SWITCH(plan, (launch_cols<LM_, LE_>(geo, grid, bbox, colbuf, twiddles, s)));
+                                cudaStream_t s, int batch, size_t grid_stride,
+                                size_t col_stride) {
+  if (plan.g != geo.g || batch < 1 || batch > 65535) return cudaErrorInvalidValue;
+  FIP_FFT_SWITCH(plan, (launch_cols<LM_, LE_>(geo, grid, bbox, colbuf, twiddles, s, batch,
+                                              grid_stride, col_stride)));
 }
 
 cudaError_t fip_launch_fft_rows(const FipGeom& geo, const float2* colbuf, unsigned* bbox,
                                 const float* taper, const float2* twiddles,
-                                const fipfft::Plan& plan, float* pre, cudaStream_t s) {
-  if (plan.g != geo.g) return cudaErrorInvalidValue;
-  FIP_FFT_SWITCH(plan, (launch_rows<LM_, LE_>(geo, colbuf, bbox, taper, twiddles, pre, s)));
+                                const fipfft::Plan& plan, float* pre, cudaStream_t s, int batch,
+                                size_t col_stride, size_t pre_stride) {
+  if (plan.g != geo.g || batch < 1 || batch > 65535) return cudaErrorInvalidValue;
+  FIP_FFT_SWITCH(plan, (launch_rows<LM_, LE_>(geo, colbuf, bbox, taper, twiddles, pre, s, batch,
+                                              col_stride, pre_stride)));
 }
 
 cudaError_t fip_launch_correct_c2r(const FipGeom& geo, const float* fft_out, const float* taper,
@@ -1506,10 +1641,29 @@ cudaError_t fip_launch_trigger(const FipGeom& geo, const float* I1, const float*
                   ((((uintptr_t)I1) | ((uintptr_t)I2) | ((uintptr_t)I3)) & 15) == 0;
   if (precise)
     k_trigger<true><<<blocks, kThreads, 0, s>>>(I1, I2, I3, max3, geo.n, geo.t, geo.u, vec,
-                                                result);
+                                                result, 0, 0);
   else
     k_trigger<false><<<blocks, kThreads, 0, s>>>(I1, I2, I3, max3, geo.n, geo.t, geo.u, vec,
-                                                 result);
+                                                 result, 0, 0);
+  return cudaGetLastError();
+}
+
+cudaError_t fip_launch_trigger_batch(const FipGeom& geo, const float* images, const float* maxima,
+                                     int count, float* results, int precise, cudaStream_t s) {
+  const int tiles = geo.u * geo.u;
+  if (tiles == 0 || count <= 0) return cudaSuccess;
+  if (count > 65535) return cudaErrorInvalidValue;
+  const size_t n2 = (size_t)geo.n * geo.n;
+  const dim3 blocks((tiles + kThreads / 32 - 1) / (kThreads / 32), count);
+  const int vec = (geo.t % 4 == 0) && (geo.n % 4 == 0) && ((uintptr_t)images & 15) == 0;
+  if (precise)
+    k_trigger<true><<<blocks, kThreads, 0, s>>>(images, images + n2, images + 2 * n2, maxima,
+                                                geo.n, geo.t, geo.u, vec, results, n2,
+                                                (size_t)tiles);
+  else
+    k_trigger<false><<<blocks, kThreads, 0, s>>>(images, images + n2, images + 2 * n2, maxima,
+                                                 geo.n, geo.t, geo.u, vec, results, n2,
+                                                 (size_t)tiles);
   return cudaGetLastError();
 }
 

@@ -216,3 +216,77 @@ def config_tiny(seed: int = 3, **kw) -> SnapshotSet:
     args = dict(n_ant=48, radius_m=1000.0, image_size=128, cell_size=1.2e-4, unit_size=16)
     args.update(kw)
     return make_snapshots(seed=seed, **args)
+
+
+@dataclasses.dataclass
+class MfsSnapshot:
+    """One multi-frequency snapshot: the unflagged samples of every baseline
+    and channel (sample index = baseline + channel * baselines, the
+    preprocessing's MFS order, SVDPreprocessMain.cpp:32-34), their projected
+    coordinates B [nb, 2] and the plane basis V [3, 3]."""
+
+    vis_re: np.ndarray
+    vis_im: np.ndarray
+    B: np.ndarray
+    V: np.ndarray
+    image_size: int
+    cell_size: float
+    unit_size: int
+
+    @property
+    def nb(self) -> int:
+        return int(self.vis_re.shape[0])
+
+
+def make_mfs_snapshots(n_ant: int, radius_m: float, image_size: int, cell_size: float,
+                       unit_size: int, *, n_snap: int, freqs_hz, core_fraction: float = 0.0,
+                       core_radius_m: float = 0.0, n_sources: int = 20,
+                       transient_flux: float = 5.0, transient_snapshot: Optional[int] = None,
+                       noise_sigma: float = 0.1, dec_deg: float = -30.0, lat_deg: float = -26.7,
+                       hour_angle0_h: float = 1.5, dt_s: float = 10.0,
+                       flag_fraction_max: float = 0.3, source_extent: float = 0.4,
+                       seed: int = 1) -> list:
+    """Seeded multi-channel snapshots with a uniform random 0..flag_fraction_max
+    of their samples flagged and dropped (so nb differs between snapshots)."""
+    rng = np.random.default_rng(seed)
+    enu = antenna_layout(n_ant, radius_m, rng, core_fraction, core_radius_m)
+    xyz = enu_to_equatorial(baseline_vectors(enu), math.radians(lat_deg))
+    fov = image_size * cell_size
+    half = 0.5 * fov * source_extent
+    lm = rng.uniform(-half, half, size=(n_sources, 2))
+    flux = rng.lognormal(mean=0.0, sigma=1.0, size=n_sources)
+    sources = np.column_stack([lm, flux])
+    t_lm = rng.uniform(-half, half, size=2)
+    transient = np.array([[t_lm[0], t_lm[1], transient_flux]])
+    out = []
+    for k in range(n_snap):
+        ha = 2.0 * np.pi * (hour_angle0_h * 3600.0 + k * dt_s) / SIDEREAL_DAY_S
+        uvw = uvw_from_xyz(xyz, ha, math.radians(dec_deg))
+        uvw_l = np.concatenate([uvw * (f / C_LIGHT) for f in freqs_hz])
+        vis = point_source_vis(uvw_l, sources)
+        if transient_snapshot is not None and k == transient_snapshot and transient_flux != 0:
+            vis = vis + point_source_vis(uvw_l, transient)
+        n = uvw_l.shape[0]
+        vis = vis + noise_sigma * (rng.standard_normal(n) + 1j * rng.standard_normal(n))
+        B, V = plane_fit(uvw_l)
+        keep = rng.random(n) >= rng.uniform(0.0, flag_fraction_max)
+        out.append(MfsSnapshot(vis_re=np.ascontiguousarray(vis.real[keep], np.float32),
+                               vis_im=np.ascontiguousarray(vis.imag[keep], np.float32),
+                               B=np.ascontiguousarray(B[keep], np.float32).reshape(-1),
+                               V=V.astype(np.float32).reshape(-1), image_size=image_size,
+                               cell_size=cell_size, unit_size=unit_size))
+    return out
+
+
+def config_batching(image_size: int = 4096, n_snap: int = 8, n_chan: int = 8, seed: int = 1,
+                    **kw) -> list:
+    """The batching form's inputs for one image size: 512 antennas (40 km,
+    half within 1 km), n_chan channels over 130-150 MHz, 0-30 % of each
+    snapshot's samples flagged, tile 32, cell scaled so that the field of view
+    is that of 4096 x 7.2722e-6 rad."""
+    freqs = np.linspace(130e6, 150e6, n_chan)
+    args = dict(n_ant=512, radius_m=20000.0, core_fraction=0.5, core_radius_m=1000.0,
+                image_size=image_size, cell_size=7.2722e-6 * 4096 / image_size, unit_size=32,
+                n_snap=n_snap, freqs_hz=freqs, flag_fraction_max=0.3)
+    args.update(kw)
+    return make_mfs_snapshots(seed=seed, **args)

@@ -189,6 +189,37 @@ int fip_imager_autotune(fip_imager* im, const float* vis_re, const float* vis_im
                         const float* B, const float* V, size_t nb, void* stream);
 int fip_imager_tuning(const fip_imager* im, int* fft_values_per_thread, int* grid_ctas_per_sm);
 
+/* ---- Batching form (no counterpart in the reference) ----------------------
+ * Many snapshots of one image size per call: one persistent gridding launch
+ * and one batched band-pruned transform for the whole batch, the
+ * per-snapshot stages (binning, pixel mapping, reprojection) on parallel
+ * branches, and the sliding-window trigger batched over the sequence, all
+ * captured as one CUDA graph per call and re-launched with updated arguments.
+ * Snapshot k of a call: device buffers vis_re[k], vis_im[k] ([nb[k]]),
+ * B[k] ([nb[k]][2]), V[k] ([9]); nb may differ between snapshots (flagged
+ * visibilities dropped).  The batch keeps the sequence's last two images, so
+ * every snapshot with two predecessors (in this call or the previous ones)
+ * yields a tLISI matrix (U*U floats, in order, at results); *nresults gets
+ * their number.  Asynchronous on `stream`.  The image size must be a power of
+ * two (the band-pruned transform); cfg->reproject must be 0. */
+typedef struct fip_batch fip_batch;
+int fip_batch_create(fip_batch** out, const fip_imager_config* cfg, size_t max_snapshots);
+int fip_batch_destroy(fip_batch* b);
+size_t fip_batch_device_bytes(const fip_batch* b);
+unsigned long long fip_batch_kernel_launches(const fip_batch* b);
+/* Starts a new sequence (forgets the carried images). */
+int fip_batch_reset(fip_batch* b);
+int fip_batch_image(fip_batch* b, const float* const* vis_re, const float* const* vis_im,
+                    const float* const* B, const float* const* V, const size_t* nb, size_t count,
+                    float* results, size_t* nresults, void* stream);
+/* Autotuner of the batch's launch shapes (transform values per thread,
+ * gridder CTAs per SM) on a representative call; synchronous; resets the
+ * sequence. */
+int fip_batch_autotune(fip_batch* b, const float* const* vis_re, const float* const* vis_im,
+                       const float* const* B, const float* const* V, const size_t* nb,
+                       size_t count, void* stream);
+int fip_batch_tuning(const fip_batch* b, int* fft_values_per_thread, int* grid_ctas_per_sm);
+
 /* Per-pixel targets (LL, MM) of the reprojection, [N*N][2] (device), for
  * tests: exact = 0 the plain form's FP32 chain, 1 the exact closed form. */
 int fip_pixel_targets(fip_imager* im, const float* V, float* out, int exact, void* stream);

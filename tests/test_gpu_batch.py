@@ -1,0 +1,146 @@
+"""GPU tests of the batching form (fip_batch): one persistent gridding launch
+and one batched transform per call, replayed as a CUDA graph, against the
+per-snapshot path and the FP64 oracle.
+
+Tolerances: batch vs the per-snapshot path 1e-5 absolute in tLISI (the same
+kernels; float-atomic gridding sums may round in another order); precision
+form vs FP64 1e-4 absolute (the parity bar of the precision form).
+"""
+import numpy as np
+import pytest
+
+import fastimagingpipe_b200 as fip
+from fastimagingpipe_b200 import synthetic
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def mfs(n_snap=6, seed=5):
+    # 64 antennas, 2 channels, 0-30 % flagged: uneven nb per snapshot.
+    return synthetic.config_batching(512, n_snap=n_snap, n_chan=2, n_ant=64, radius_m=1500.0,
+                                     core_fraction=0.0, transient_snapshot=3, seed=seed)
+
+
+def dev(snaps, cuda):
+    import torch
+    return [{k: torch.tensor(getattr(s, k), device=cuda) for k in ("vis_re", "vis_im", "B", "V")}
+            for s in snaps]
+
+
+def per_snapshot(snaps, d, cuda, **kw):
+    """Sliding-window tLISI through the per-snapshot entry points."""
+    import torch
+    s0 = snaps[0]
+    n, t = s0.image_size, s0.unit_size
+    u = n // t
+    nbmax = max(s.nb for s in snaps)
+    imgs = torch.zeros((len(snaps), n * n), device=cuda)
+    mx = torch.zeros(len(snaps), device=cuda)
+    out = []
+    with fip.Imager(n, nbmax, s0.cell_size, t, **kw) as im:
+        for k, s in enumerate(snaps):
+            im.image_snapshot(d[k]["vis_re"], d[k]["vis_im"], d[k]["B"], d[k]["V"], s.nb,
+                              imgs[k], mx[k:])
+        for k in range(2, len(snaps)):
+            r = torch.zeros(u * u, device=cuda)
+            im.trigger(imgs[k - 2], imgs[k - 1], imgs[k], mx[k - 2:], r)
+            out.append(r)
+        torch.cuda.synchronize()
+    return np.stack([r.cpu().numpy().reshape(u, u) for r in out])
+
+
+def batched(snaps, d, cuda, calls, **kw):
+    import torch
+    s0 = snaps[0]
+    n, t = s0.image_size, s0.unit_size
+    u = n // t
+    nbmax = max(s.nb for s in snaps)
+    res = torch.zeros((len(snaps), u * u), device=cuda)
+    got = 0
+    with fip.Batch(n, nbmax, s0.cell_size, t, max(calls), **kw) as b:
+        k = 0
+        for c in calls:
+            part = d[k:k + c]
+            got += b.image([p["vis_re"] for p in part], [p["vis_im"] for p in part],
+                           [p["B"] for p in part], [p["V"] for p in part],
+                           [s.nb for s in snaps[k:k + c]], res[got:])
+            k += c
+        torch.cuda.synchronize()
+        launches = b.kernel_launches
+    assert got == len(snaps) - 2
+    return res[:got].cpu().numpy().reshape(got, u, u), launches
+
+
+@pytest.mark.parametrize("kw", [{}, dict(form=fip.FORM_PRECISE, vis_storage=fip.STORE_F16)])
+def test_batch_matches_per_snapshot_path(cuda, kw):
+    snaps = mfs()
+    d = dev(snaps, cuda)
+    ref = per_snapshot(snaps, d, cuda, **kw)
+    got, launches = batched(snaps, d, cuda, [6], **kw)
+    assert launches > 0
+    assert np.abs(got - ref).max() <= 1e-5
+
+
+def test_batch_carries_the_sequence_across_calls(cuda):
+    snaps = mfs()
+    d = dev(snaps, cuda)
+    one, _ = batched(snaps, d, cuda, [6])
+    split, _ = batched(snaps, d, cuda, [2, 1, 3])
+    assert np.abs(one - split).max() <= 1e-5
+
+
+def test_batch_graph_replay_with_new_inputs(cuda):
+    """The executable graph is re-used across calls of one shape: results must
+    follow the new inputs, not the captured ones."""
+    import torch
+    a, b2 = mfs(seed=5), mfs(seed=9)
+    da, db = dev(a, cuda), dev(b2, cuda)
+    ref_b = per_snapshot(b2, db, cuda)
+    s0 = a[0]
+    u = s0.image_size // s0.unit_size
+    nbmax = max(s.nb for s in a + b2)
+    with fip.Batch(s0.image_size, nbmax, s0.cell_size, s0.unit_size, 6) as b:
+        res = torch.zeros((4, u * u), device=cuda)
+        for snaps, d in ((a, da), (b2, db)):
+            b.reset()
+            b.image([p["vis_re"] for p in d], [p["vis_im"] for p in d], [p["B"] for p in d],
+                    [p["V"] for p in d], [s.nb for s in snaps], res)
+        torch.cuda.synchronize()
+    assert np.abs(res.cpu().numpy().reshape(4, u, u) - ref_b).max() <= 1e-5
+
+
+def test_batch_precision_form_vs_fp64(cuda):
+    small = synthetic.config_small(transient_snapshot=2)
+    nb = small.num_baselines
+    import torch
+    d = [{"vis_re": torch.tensor(small.vis_re[k * nb:(k + 1) * nb], device=cuda),
+          "vis_im": torch.tensor(small.vis_im[k * nb:(k + 1) * nb], device=cuda),
+          "B": torch.tensor(small.B[2 * k * nb:2 * (k + 1) * nb], device=cuda),
+          "V": torch.tensor(small.V[9 * k:9 * (k + 1)], device=cuda)} for k in range(3)]
+    u = small.image_size // small.unit_size
+    res = torch.zeros(u * u, device=cuda)
+    with fip.Batch(small.image_size, nb, small.cell_size, small.unit_size, 3,
+                   form=fip.FORM_PRECISE, vis_storage=fip.STORE_F16) as b:
+        tuning = b.autotune([p["vis_re"] for p in d], [p["vis_im"] for p in d],
+                            [p["B"] for p in d], [p["V"] for p in d], [nb] * 3)
+        assert tuning["fft_values_per_thread"] in (8, 16)
+        assert b.image([p["vis_re"] for p in d], [p["vis_im"] for p in d], [p["B"] for p in d],
+                       [p["V"] for p in d], [nb] * 3, res) == 1
+        torch.cuda.synchronize()
+    r64, _, _ = oracle.fipipe(small, "f64")
+    assert np.abs(res.cpu().numpy().reshape(u, u) - r64).max() <= 1e-4
+
+
+def test_batch_rejects_bad_arguments(cuda):
+    import torch
+    with pytest.raises(fip.FipError):
+        fip.Batch(100, 10, 1e-3, 10, 4)  # not a power of two
+    with pytest.raises(fip.FipError):
+        fip.Batch(64, 10, 1e-3, 16, 65)  # above the batch limit
+    z = torch.zeros(64, device=cuda)
+    with fip.Batch(64, 10, 1e-3, 16, 2) as b:
+        with pytest.raises(fip.FipError):
+            b.image([z] * 3, [z] * 3, [z] * 3, [z] * 3, [5] * 3, z)  # count > max_snapshots
+        with pytest.raises(fip.FipError):
+            b.image([z], [z], [z], [z], [11], z)  # nb > max_baselines
