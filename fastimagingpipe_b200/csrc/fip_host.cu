@@ -95,6 +95,23 @@ struct StageTimer {
 
 int fip_set_error(int code, const std::string& msg) { return fail(code, msg); }
 
+// Scratch of one snapshot in flight.  With the band-pruned transform an
+// imager has kLanes of them, so the snapshots of one call (or of a sequence)
+// image concurrently, each on its lane's stream.
+struct Lane {
+  float2* grid = nullptr;            // uv grid (band layout, or C2R in place)
+  FipBins bins{};
+  float2* colbuf = nullptr;          // column-pass output [G/2+1][N]
+  float* pre = nullptr;              // corrected pre-reprojection image [N*N]
+  float2* targets = nullptr;         // reference pixel mapping [N*N]
+  void* q_re = nullptr;              // reduced-precision visibility storage
+  void* q_im = nullptr;
+  float* q_scale = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_done = nullptr;
+};
+constexpr int kLanes = 3;
+
 struct fip_imager {
   fip_imager_config cfg{};
   FipGeom geo{};
@@ -111,20 +128,17 @@ struct fip_imager {
   fipfft::Plan fft{};
   int grid_ctas_per_sm = 0;          // persistent gridder CTAs per SM (0 = most that fit)
   float2* twiddles = nullptr;        // e^{+2 pi i k / G}, k < G
-  float2* colbuf = nullptr;          // column-pass output [G/2+1][N]
-  float* pre = nullptr;              // corrected pre-reprojection image [N*N]
-  float2* targets = nullptr;         // reference pixel mapping [N*N]
-  float2* grid = nullptr;            // uv grid (band layout, or C2R in place)
   float* taper = nullptr;            // N/2 + 1 taper values, N/2 + 1 reciprocals
-  FipBins bins{};
-  float* images[3] = {nullptr, nullptr, nullptr};
-  float* maxima = nullptr;           // [3] device floats (written as max bits)
+  Lane lane[kLanes];
+  int lanes = 1;                     // lanes in use (kLanes with the pruned transform)
+  int last_lane = 0;                 // lane of the last gridded snapshot
+  cudaEvent_t ev_start = nullptr;    // start of a multi-snapshot call (lanes wait on it)
+  cudaEvent_t ev_free[6] = {};       // sequence ring slot released by its last trigger
+  float* images[6] = {};             // 0..2: one call's snapshots; all: the sequence ring
+  int ring = 3;                      // images allocated (6 with lanes)
+  float* maxima = nullptr;           // [6] device floats (written as max bits)
   float* result = nullptr;           // U*U
   float* stats = nullptr;
-  // Reduced-precision visibility storage (precision form).
-  void* q_re = nullptr;
-  void* q_im = nullptr;
-  float* q_scale = nullptr;
   // Device and pinned staging of the host-buffer path, 3 snapshot slots.
   float* d_vr = nullptr;
   float* d_vi = nullptr;
@@ -189,13 +203,20 @@ static void imager_free(fip_imager* im) {
   if (im->copy_stream) cudaStreamSynchronize(im->copy_stream);
   if (im->side) cudaStreamSynchronize(im->side);
   if (im->plan_ok) cufftDestroy(im->plan);
-  void* dptrs[] = {im->grid, im->taper, im->bins.count, im->bins.offset, im->bins.cursor,
-                   im->bins.entries, im->bins.work, im->bins.nwork, im->bins.bbox,
-                   im->bins.multi, im->bins.nmulti, im->twiddles, im->colbuf, im->pre,
-                   im->targets,
-                   im->images[0], im->images[1], im->images[2], im->maxima, im->result,
-                   im->stats, im->q_re, im->q_im, im->q_scale, im->d_vr, im->d_vi, im->d_B,
-                   im->d_V};
+  for (Lane& L : im->lane) {
+    if (L.stream) cudaStreamSynchronize(L.stream);
+    void* lp[] = {L.grid, L.bins.count, L.bins.offset, L.bins.cursor, L.bins.entries,
+                  L.bins.work, L.bins.nwork, L.bins.bbox, L.bins.multi, L.bins.nmulti,
+                  L.colbuf, L.pre, L.targets, L.q_re, L.q_im, L.q_scale};
+    for (void* p : lp)
+      if (p) cudaFree(p);
+    if (L.ev_done) cudaEventDestroy(L.ev_done);
+    if (L.stream) cudaStreamDestroy(L.stream);
+  }
+  for (float* p : im->images)
+    if (p) cudaFree(p);
+  void* dptrs[] = {im->taper, im->twiddles, im->maxima, im->result, im->stats, im->d_vr,
+                   im->d_vi, im->d_B, im->d_V};
   for (void* p : dptrs)
     if (p) cudaFree(p);
   void* hptrs[] = {im->h_vr, im->h_vi, im->h_B, im->h_V, im->h_result};
@@ -211,6 +232,9 @@ static void imager_free(fip_imager* im) {
   if (im->ev_done) cudaEventDestroy(im->ev_done);
   if (im->ev_fork) cudaEventDestroy(im->ev_fork);
   if (im->ev_join) cudaEventDestroy(im->ev_join);
+  if (im->ev_start) cudaEventDestroy(im->ev_start);
+  for (cudaEvent_t e : im->ev_free)
+    if (e) cudaEventDestroy(e);
   if (im->stream) cudaStreamDestroy(im->stream);
   if (im->copy_stream) cudaStreamDestroy(im->copy_stream);
   if (im->side) cudaStreamDestroy(im->side);
@@ -299,6 +323,8 @@ int fip_imager_create(fip_imager** out, const fip_imager_config* cfg) {
   FIP_ALLOC(cudaStreamCreateWithFlags(&im->side, cudaStreamNonBlocking));
   FIP_ALLOC(cudaEventCreateWithFlags(&im->ev_fork, cudaEventDisableTiming));
   FIP_ALLOC(cudaEventCreateWithFlags(&im->ev_join, cudaEventDisableTiming));
+  FIP_ALLOC(cudaEventCreateWithFlags(&im->ev_start, cudaEventDisableTiming));
+  for (cudaEvent_t& e : im->ev_free) FIP_ALLOC(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   FIP_ALLOC(cudaEventCreateWithFlags(&im->ev_done, cudaEventDisableTiming));
   for (int k = 0; k < kMaxPending; ++k)
     for (int e = 0; e < 2; ++e) FIP_ALLOC(cudaEventCreate(&im->timer.ev[k][e]));
@@ -306,27 +332,39 @@ int fip_imager_create(fip_imager** out, const fip_imager_config* cfg) {
     FIP_ALLOC(cudaEventCreateWithFlags(&im->ev_copied[k], cudaEventDisableTiming));
     FIP_ALLOC(cudaEventCreateWithFlags(&im->ev_used[k], cudaEventDisableTiming));
   }
-  FIP_ALLOC(dalloc(&im->grid, (size_t)geo.g * geo.hp, tot));
   if (cfg->reproject != 0 && cfg->reproject != 1) return cleanup(fail(FIP_ERR_ARG, "unknown reproject mode"));
   if (cfg->reproject == 0 && !fip_gather_supported(geo, cfg->form == FIP_FORM_PRECISE))
     return cleanup(fail(FIP_ERR_ARG, "cell_size too small for the tile-gather reprojection; "
                                      "use reproject = 1"));
   FIP_ALLOC(dalloc(&im->taper, 2 * ((size_t)geo.n / 2 + 1), tot));
-  im->bins.cap = 12 * nb;
-  im->bins.wcap = ntiles + im->bins.cap / FIP_GCHUNK + 1;
-  FIP_ALLOC(dalloc(&im->bins.count, ntiles, tot));
-  FIP_ALLOC(dalloc(&im->bins.offset, ntiles + 1, tot));
-  FIP_ALLOC(dalloc(&im->bins.cursor, ntiles, tot));
-  FIP_ALLOC(dalloc(&im->bins.entries, im->bins.cap, tot));
-  FIP_ALLOC(dalloc(&im->bins.work, im->bins.wcap, tot));
-  FIP_ALLOC(dalloc(&im->bins.nwork, 1, tot));
-  FIP_ALLOC(dalloc(&im->bins.bbox, 4, tot));
-  FIP_ALLOC(dalloc(&im->bins.multi, ntiles, tot));
-  FIP_ALLOC(dalloc(&im->bins.nmulti, 1, tot));
-  FIP_ALLOC(dalloc(&im->pre, n2, tot));
-  if (cfg->form == FIP_FORM_PLAIN && cfg->reproject == 0) FIP_ALLOC(dalloc(&im->targets, n2, tot));
+  // The cuFFT fallback shares one plan (and its work area): one lane.
+  im->lanes = im->custom_fft ? kLanes : 1;
+  for (int l = 0; l < im->lanes; ++l) {
+    Lane& L = im->lane[l];
+    FIP_ALLOC(cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking));
+    FIP_ALLOC(cudaEventCreateWithFlags(&L.ev_done, cudaEventDisableTiming));
+    FIP_ALLOC(dalloc(&L.grid, (size_t)geo.g * geo.hp, tot));
+    L.bins.cap = 12 * nb;
+    L.bins.wcap = ntiles + L.bins.cap / FIP_GCHUNK + 1;
+    FIP_ALLOC(dalloc(&L.bins.count, ntiles, tot));
+    FIP_ALLOC(dalloc(&L.bins.offset, ntiles + 1, tot));
+    FIP_ALLOC(dalloc(&L.bins.cursor, ntiles, tot));
+    FIP_ALLOC(dalloc(&L.bins.entries, L.bins.cap, tot));
+    FIP_ALLOC(dalloc(&L.bins.work, L.bins.wcap, tot));
+    FIP_ALLOC(dalloc(&L.bins.nwork, 1, tot));
+    FIP_ALLOC(dalloc(&L.bins.bbox, 4, tot));
+    FIP_ALLOC(dalloc(&L.bins.multi, ntiles, tot));
+    FIP_ALLOC(dalloc(&L.bins.nmulti, 1, tot));
+    FIP_ALLOC(dalloc(&L.pre, n2, tot));
+    if (cfg->form == FIP_FORM_PLAIN && cfg->reproject == 0) FIP_ALLOC(dalloc(&L.targets, n2, tot));
+    if (im->custom_fft) FIP_ALLOC(dalloc(&L.colbuf, (size_t)geo.hp * geo.n, tot));
+    if (cfg->form == FIP_FORM_PRECISE && cfg->vis_storage != FIP_STORE_F32) {
+      FIP_ALLOC(dalloc((uint16_t**)&L.q_re, nb, tot));
+      FIP_ALLOC(dalloc((uint16_t**)&L.q_im, nb, tot));
+      FIP_ALLOC(dalloc(&L.q_scale, 1, tot));
+    }
+  }
   if (im->custom_fft) {
-    FIP_ALLOC(dalloc(&im->colbuf, (size_t)geo.hp * geo.n, tot));
     FIP_ALLOC(dalloc(&im->twiddles, (size_t)geo.g, tot));
     std::vector<float2> tw(geo.g);
     for (int k = 0; k < geo.g; ++k) {
@@ -336,14 +374,12 @@ int fip_imager_create(fip_imager** out, const fip_imager_config* cfg) {
     FIP_ALLOC(cudaMemcpy(im->twiddles, tw.data(), geo.g * sizeof(float2),
                          cudaMemcpyHostToDevice));
   }
-  for (int k = 0; k < 3; ++k) FIP_ALLOC(dalloc(&im->images[k], n2, tot));
-  FIP_ALLOC(dalloc(&im->maxima, 3, tot));
+  // With concurrent lanes a sequence keeps six images, so a lane can start a
+  // snapshot while the triggers of the previous ones still read theirs.
+  im->ring = im->lanes > 1 ? 6 : 3;
+  for (int k = 0; k < im->ring; ++k) FIP_ALLOC(dalloc(&im->images[k], n2, tot));
+  FIP_ALLOC(dalloc(&im->maxima, 6, tot));
   FIP_ALLOC(dalloc(&im->result, std::max<size_t>((size_t)geo.u * geo.u, 1), tot));
-  if (cfg->form == FIP_FORM_PRECISE && cfg->vis_storage != FIP_STORE_F32) {
-    FIP_ALLOC(dalloc((uint16_t**)&im->q_re, nb, tot));
-    FIP_ALLOC(dalloc((uint16_t**)&im->q_im, nb, tot));
-    FIP_ALLOC(dalloc(&im->q_scale, 1, tot));
-  }
   FIP_ALLOC(dalloc(&im->d_vr, 3 * nb, tot));
   FIP_ALLOC(dalloc(&im->d_vi, 3 * nb, tot));
   FIP_ALLOC(dalloc(&im->d_B, 3 * nb * 2, tot));
@@ -382,9 +418,13 @@ int fip_imager_destroy(fip_imager* im) {
 
 size_t fip_imager_device_bytes(const fip_imager* im) { return im ? im->device_bytes : 0; }
 
-static int image_snapshot_impl(fip_imager* im, const float* vr, const float* vi, const float* B,
-                               const float* V, size_t nb, float* image, float* image_max,
-                               cudaStream_t s) {
+// Images one snapshot with lane L's scratch on stream s.  fork_targets: run
+// the pixel mapping on the side stream beside gridding + FFT (single-snapshot
+// calls; calls that image several snapshots run them on concurrent lanes
+// instead).
+static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const float* vi,
+                               const float* B, const float* V, size_t nb, float* image,
+                               float* image_max, cudaStream_t s, bool fork_targets) {
   const FipGeom& geo = im->geo;
   if (nb > im->cfg.max_baselines) return fail(FIP_ERR_ARG, "nb exceeds the imager's capacity");
   if (nb == 0) return fail(FIP_ERR_ARG, "nb must be positive");
@@ -397,18 +437,18 @@ static int image_snapshot_impl(fip_imager* im, const float* vr, const float* vi,
   if (precise && im->cfg.vis_storage != FIP_STORE_F32) {
     vt = im->cfg.vis_storage == FIP_STORE_F16 ? FIP_VIS_F16 : FIP_VIS_BF16;
     k = stage_begin(im, ST_GRID, s);
-    FIP_CUDA(fip_launch_quantize(vr, vi, nb, vt, im->q_re, im->q_im, im->q_scale, s));
+    FIP_CUDA(fip_launch_quantize(vr, vi, nb, vt, L.q_re, L.q_im, L.q_scale, s));
     stage_end(im, k, s);
     im->launches += 3;
-    gvr = im->q_re;
-    gvi = im->q_im;
+    gvr = L.q_re;
+    gvi = L.q_im;
   }
   const bool gather = im->cfg.reproject == 0;
   const bool chain_targets = gather && !precise;
-  // The pixel mapping depends on V only: it runs beside gridding + FFT on
+  // The pixel mapping depends on V only: it may run beside gridding + FFT on
   // the side stream (serialised on s when profiling, so every stage's time
   // is its own).
-  const bool fork = chain_targets && !im->timer.on;
+  const bool fork = chain_targets && fork_targets && !im->timer.on;
   if (chain_targets) {
     cudaStream_t ts = fork ? im->side : s;
     if (fork) {
@@ -416,42 +456,41 @@ static int image_snapshot_impl(fip_imager* im, const float* vr, const float* vi,
       FIP_CUDA(cudaStreamWaitEvent(im->side, im->ev_fork, 0));
     }
     k = stage_begin(im, ST_TARGETS, ts);
-    FIP_CUDA(fip_launch_targets(geo, V, im->targets, ts));
+    FIP_CUDA(fip_launch_targets(geo, V, L.targets, ts));
     stage_end(im, k, ts);
     im->launches += 1;
     if (fork) FIP_CUDA(cudaEventRecord(im->ev_join, im->side));
   }
   k = stage_begin(im, ST_BIN, s);
-  FIP_CUDA(fip_launch_bin(geo, B, (int)nb, im->bins, s));
+  FIP_CUDA(fip_launch_bin(geo, B, (int)nb, L.bins, s));
   stage_end(im, k, s);
   k = stage_begin(im, ST_GRID, s);
-  FIP_CUDA(fip_launch_grid(geo, B, gvr, gvi, vt, im->q_scale, V, (int)nb, im->bins, im->grid,
+  FIP_CUDA(fip_launch_grid(geo, B, gvr, gvi, vt, L.q_scale, V, (int)nb, L.bins, L.grid,
                            precise ? 1 : 0, s, im->grid_ctas_per_sm));
   stage_end(im, k, s);
   im->launches += fip_bin_launches(geo) + 2;  // binning, zero tiles, grid
   if (im->custom_fft) {
     k = stage_begin(im, ST_FFT_COLS, s);
-    FIP_CUDA(fip_launch_fft_cols(geo, im->grid, im->bins.bbox, im->colbuf, im->twiddles,
-                                 im->fft, s));
+    FIP_CUDA(fip_launch_fft_cols(geo, L.grid, L.bins.bbox, L.colbuf, im->twiddles, im->fft, s));
     stage_end(im, k, s);
     k = stage_begin(im, ST_FFT_ROWS, s);
-    FIP_CUDA(fip_launch_fft_rows(geo, im->colbuf, im->bins.bbox, im->taper, im->twiddles,
-                                 im->fft, im->pre, s));
+    FIP_CUDA(fip_launch_fft_rows(geo, L.colbuf, L.bins.bbox, im->taper, im->twiddles, im->fft,
+                                 L.pre, s));
     im->launches += 2;
   } else {
     k = stage_begin(im, ST_FFT_ROWS, s);
     FIP_CUFFT(cufftSetStream(im->plan, s));
-    FIP_CUFFT(cufftExecC2R(im->plan, reinterpret_cast<cufftComplex*>(im->grid),
-                           reinterpret_cast<cufftReal*>(im->grid)));
-    FIP_CUDA(fip_launch_correct_c2r(geo, reinterpret_cast<const float*>(im->grid), im->taper,
-                                    im->pre, im->bins.bbox + 3, s));
+    FIP_CUFFT(cufftExecC2R(im->plan, reinterpret_cast<cufftComplex*>(L.grid),
+                           reinterpret_cast<cufftReal*>(L.grid)));
+    FIP_CUDA(fip_launch_correct_c2r(geo, reinterpret_cast<const float*>(L.grid), im->taper,
+                                    L.pre, L.bins.bbox + 3, s));
     im->launches += 1;
   }
   stage_end(im, k, s);
   if (image_max) FIP_CUDA(cudaMemsetAsync(image_max, 0, sizeof(float), s));
   if (!gather) {
     k = stage_begin(im, ST_REPROJECT, s);
-    FIP_CUDA(fip_launch_reproject_scatter(geo, im->pre, V, (int)nb, image, s));
+    FIP_CUDA(fip_launch_reproject_scatter(geo, L.pre, V, (int)nb, image, s));
     if (image_max)
       FIP_CUDA(fip_launch_image_max(image, (size_t)geo.n * geo.n,
                                     reinterpret_cast<unsigned*>(image_max), s));
@@ -460,13 +499,37 @@ static int image_snapshot_impl(fip_imager* im, const float* vr, const float* vi,
   } else {
     if (fork) FIP_CUDA(cudaStreamWaitEvent(s, im->ev_join, 0));
     k = stage_begin(im, ST_REPROJECT, s);
-    FIP_CUDA(fip_launch_reproject_gather(geo, im->pre, im->targets, V, (int)nb,
-                                         im->bins.bbox + 3, image,
-                                         reinterpret_cast<unsigned*>(image_max), precise ? 1 : 0,
-                                         s));
+    FIP_CUDA(fip_launch_reproject_gather(geo, L.pre, L.targets, V, (int)nb, L.bins.bbox + 3,
+                                         image, reinterpret_cast<unsigned*>(image_max),
+                                         precise ? 1 : 0, s));
     stage_end(im, k, s);
     im->launches += 1;
   }
+  return FIP_OK;
+}
+
+// Images snapshot k of a multi-snapshot call on lane k % lanes: the lane's
+// stream waits for `after`, images, and records the lane's ev_done, which
+// the caller's stream waits for (wait_lane).  When profiling, or with one
+// lane, everything runs on s in order.
+static int image_on_lane(fip_imager* im, int k, const float* vr, const float* vi,
+                         const float* B, const float* V, size_t nb, float* image,
+                         float* image_max, cudaStream_t s, cudaEvent_t after) {
+  if (im->lanes == 1 || im->timer.on) {
+    FIP_CUDA(cudaStreamWaitEvent(s, after, 0));
+    return image_snapshot_impl(im, im->lane[k % im->lanes], vr, vi, B, V, nb, image, image_max,
+                               s, true);
+  }
+  Lane& L = im->lane[k % im->lanes];
+  FIP_CUDA(cudaStreamWaitEvent(L.stream, after, 0));
+  FIP_TRY(image_snapshot_impl(im, L, vr, vi, B, V, nb, image, image_max, L.stream, false));
+  FIP_CUDA(cudaEventRecord(L.ev_done, L.stream));
+  return FIP_OK;
+}
+
+static int wait_lane(fip_imager* im, int k, cudaStream_t s) {
+  if (im->lanes == 1 || im->timer.on) return FIP_OK;
+  FIP_CUDA(cudaStreamWaitEvent(s, im->lane[k % im->lanes].ev_done, 0));
   return FIP_OK;
 }
 
@@ -476,7 +539,9 @@ int fip_image_snapshot(fip_imager* im, const float* vis_re, const float* vis_im,
   DeviceGuard g(im->cfg.device);
   cudaStream_t s = (cudaStream_t)stream;
   FIP_TRY(call_enter(im, s));
-  FIP_TRY(image_snapshot_impl(im, vis_re, vis_im, B, V, nb, image, image_max, s));
+  FIP_TRY(image_snapshot_impl(im, im->lane[0], vis_re, vis_im, B, V, nb, image, image_max, s,
+                              true));
+  im->last_lane = 0;
   return call_leave(im, s);
 }
 
@@ -496,17 +561,19 @@ int fip_grid_snapshot(fip_imager* im, const float* vis_re, const float* vis_im, 
   const void* gvr = vis_re;
   const void* gvi = vis_im;
   int vt = FIP_VIS_F32;
+  Lane& L = im->lane[0];
   if (precise && im->cfg.vis_storage != FIP_STORE_F32) {
     vt = im->cfg.vis_storage == FIP_STORE_F16 ? FIP_VIS_F16 : FIP_VIS_BF16;
-    FIP_CUDA(fip_launch_quantize(vis_re, vis_im, nb, vt, im->q_re, im->q_im, im->q_scale, s));
+    FIP_CUDA(fip_launch_quantize(vis_re, vis_im, nb, vt, L.q_re, L.q_im, L.q_scale, s));
     im->launches += 3;
-    gvr = im->q_re;
-    gvi = im->q_im;
+    gvr = L.q_re;
+    gvi = L.q_im;
   }
-  FIP_CUDA(fip_launch_bin(geo, B, (int)nb, im->bins, s));
-  FIP_CUDA(fip_launch_grid(geo, B, gvr, gvi, vt, im->q_scale, V, (int)nb, im->bins,
+  FIP_CUDA(fip_launch_bin(geo, B, (int)nb, L.bins, s));
+  FIP_CUDA(fip_launch_grid(geo, B, gvr, gvi, vt, L.q_scale, V, (int)nb, L.bins,
                            reinterpret_cast<float2*>(grid), precise ? 1 : 0, s,
                            im->grid_ctas_per_sm));
+  im->last_lane = 0;
   im->launches += fip_bin_launches(geo) + 2;
   return call_leave(im, s);
 }
@@ -534,10 +601,14 @@ int fip_pipe_device(fip_imager* im, const float* vr, const float* vi, const floa
   DeviceGuard g(im->cfg.device);
   cudaStream_t s = (cudaStream_t)stream;
   FIP_TRY(call_enter(im, s));
+  // The three snapshots image concurrently on the lanes; the trigger joins them.
+  FIP_CUDA(cudaEventRecord(im->ev_start, s));
   for (int k = 0; k < 3; ++k)
-    FIP_TRY(image_snapshot_impl(im, vr + (size_t)k * nb, vi + (size_t)k * nb,
-                                B + (size_t)k * nb * 2, V + (size_t)k * 9, nb, im->images[k],
-                                im->maxima + k, s));
+    FIP_TRY(image_on_lane(im, k, vr + (size_t)k * nb, vi + (size_t)k * nb,
+                          B + (size_t)k * nb * 2, V + (size_t)k * 9, nb, im->images[k],
+                          im->maxima + k, s, im->ev_start));
+  for (int k = 0; k < 3; ++k) FIP_TRY(wait_lane(im, k, s));
+  im->last_lane = 2 % im->lanes;
   if (im->geo.t > 0 && result) {
     const int k = stage_begin(im, ST_TRIGGER, s);
     FIP_CUDA(fip_launch_trigger(im->geo, im->images[0], im->images[1], im->images[2],
@@ -587,9 +658,11 @@ int fip_pipe_host(fip_imager* im, const float* vr, const float* vi, const float*
     FIP_CUDA(cudaMemcpyAsync(dB, hB, nb * 2 * sizeof(float), cudaMemcpyHostToDevice, cs));
     FIP_CUDA(cudaMemcpyAsync(dV, hV, 9 * sizeof(float), cudaMemcpyHostToDevice, cs));
     FIP_CUDA(cudaEventRecord(im->ev_copied[k], cs));
-    FIP_CUDA(cudaStreamWaitEvent(s, im->ev_copied[k], 0));
-    FIP_TRY(image_snapshot_impl(im, dvr, dvi, dB, dV, nb, im->images[k], im->maxima + k, s));
+    FIP_TRY(image_on_lane(im, k, dvr, dvi, dB, dV, nb, im->images[k], im->maxima + k, s,
+                          im->ev_copied[k]));
   }
+  for (int k = 0; k < 3; ++k) FIP_TRY(wait_lane(im, k, s));
+  im->last_lane = 2 % im->lanes;
   {
     const int k = stage_begin(im, ST_TRIGGER, s);
     FIP_CUDA(fip_launch_trigger(im->geo, im->images[0], im->images[1], im->images[2],
@@ -645,7 +718,7 @@ int fip_imager_band(fip_imager* im, unsigned* max_row, unsigned* max_col) {
   if (!im || !max_row || !max_col) return fail(FIP_ERR_ARG, "null argument");
   DeviceGuard g(im->cfg.device);
   unsigned b[4] = {0, 0, 0, 0};
-  FIP_CUDA(cudaMemcpy(b, im->bins.bbox, sizeof(b), cudaMemcpyDeviceToHost));
+  FIP_CUDA(cudaMemcpy(b, im->lane[im->last_lane].bins.bbox, sizeof(b), cudaMemcpyDeviceToHost));
   *max_row = b[0];
   *max_col = b[1];
   return FIP_OK;
@@ -679,7 +752,9 @@ int fip_imager_autotune(fip_imager* im, const float* vr, const float* vi, const 
   cudaStream_t s = (cudaStream_t)stream;
   FIP_TRY(call_enter(im, s));
   // One full snapshot leaves this snapshot's bins, band and grid in place.
-  FIP_TRY(image_snapshot_impl(im, vr, vi, B, V, nb, im->images[0], im->maxima, s));
+  Lane& L = im->lane[0];
+  FIP_TRY(image_snapshot_impl(im, L, vr, vi, B, V, nb, im->images[0], im->maxima, s, true));
+  im->last_lane = 0;
   const FipGeom& geo = im->geo;
   const bool precise = im->cfg.form == FIP_FORM_PRECISE;
   const void* gvr = vr;
@@ -687,8 +762,8 @@ int fip_imager_autotune(fip_imager* im, const float* vr, const float* vi, const 
   int vt = FIP_VIS_F32;
   if (precise && im->cfg.vis_storage != FIP_STORE_F32) {
     vt = im->cfg.vis_storage == FIP_STORE_F16 ? FIP_VIS_F16 : FIP_VIS_BF16;
-    gvr = im->q_re;
-    gvi = im->q_im;
+    gvr = L.q_re;
+    gvi = L.q_im;
   }
   EventPair ev;
   FIP_CUDA(cudaEventCreate(&ev.a));
@@ -716,11 +791,11 @@ int fip_imager_autotune(fip_imager* im, const float* vr, const float* vi, const 
       float ms = 0.f;
       FIP_TRY(timed(
           [&]() -> cudaError_t {
-            cudaError_t e = fip_launch_fft_cols(geo, im->grid, im->bins.bbox, im->colbuf,
+            cudaError_t e = fip_launch_fft_cols(geo, L.grid, L.bins.bbox, L.colbuf,
                                                 im->twiddles, p, s);
             if (e != cudaSuccess) return e;
-            return fip_launch_fft_rows(geo, im->colbuf, im->bins.bbox, im->taper, im->twiddles,
-                                       p, im->pre, s);
+            return fip_launch_fft_rows(geo, L.colbuf, L.bins.bbox, im->taper, im->twiddles,
+                                       p, L.pre, s);
           },
           ms));
       if (ms < best) {
@@ -737,8 +812,8 @@ int fip_imager_autotune(fip_imager* im, const float* vr, const float* vi, const 
       float ms = 0.f;
       FIP_TRY(timed(
           [&]() -> cudaError_t {
-            return fip_launch_grid(geo, B, gvr, gvi, vt, im->q_scale, V, (int)nb, im->bins,
-                                   im->grid, precise ? 1 : 0, s, c);
+            return fip_launch_grid(geo, B, gvr, gvi, vt, L.q_scale, V, (int)nb, L.bins,
+                                   L.grid, precise ? 1 : 0, s, c);
           },
           ms));
       if (ms < best) {
@@ -773,22 +848,32 @@ int fip_image_sequence(fip_imager* im, const float* vr, const float* vi, const f
   cudaStream_t s = (cudaStream_t)stream;
   const size_t uu = (size_t)im->geo.u * im->geo.u;
   FIP_TRY(call_enter(im, s));
+  // Snapshot k goes to ring slot k % R on lane k % lanes; trigger k (on s)
+  // waits for the lanes of snapshots k-2 .. k.  Slot k % R last held
+  // snapshot k - R, whose last reader is trigger k - R + 2: ev_free[slot],
+  // recorded on s after that trigger, releases it, so the lanes run up to
+  // R - 3 snapshots ahead of the triggers.
+  const int R = im->ring;
+  FIP_CUDA(cudaEventRecord(im->ev_start, s));
   for (size_t k = 0; k < nsnap; ++k) {
-    const int slot = (int)(k % 3);
-    FIP_TRY(image_snapshot_impl(im, vr + k * nb_stride, vi + k * nb_stride, B + k * nb_stride * 2,
-                                V + k * 9, nb[k], im->images[slot], im->maxima + slot, s));
+    const int slot = (int)(k % R);
+    FIP_TRY(image_on_lane(im, (int)k, vr + k * nb_stride, vi + k * nb_stride,
+                          B + k * nb_stride * 2, V + k * 9, nb[k], im->images[slot],
+                          im->maxima + slot, s, k < (size_t)R ? im->ev_start : im->ev_free[slot]));
     if (k >= 2) {
-      // Ring slots a, b, c hold snapshots k-2, k-1, k.  The combine uses the
-      // maximum of the three maxima only, so the maxima keep ring order.
-      const int a = (int)((k - 2) % 3), b = (int)((k - 1) % 3), c = slot;
+      for (int j = 0; j < 3; ++j) FIP_TRY(wait_lane(im, (int)(k - j), s));
+      const int a = (int)((k - 2) % R), b = (int)((k - 1) % R), c = slot;
       const int st = stage_begin(im, ST_TRIGGER, s);
-      FIP_CUDA(fip_launch_trigger(im->geo, im->images[a], im->images[b], im->images[c],
-                                  im->maxima, im->stats, results + (k - 2) * uu,
-                                  im->cfg.form == FIP_FORM_PRECISE ? 1 : 0, s));
+      FIP_CUDA(fip_launch_trigger3(im->geo, im->images[a], im->images[b], im->images[c],
+                                   im->maxima + a, im->maxima + b, im->maxima + c,
+                                   results + (k - 2) * uu,
+                                   im->cfg.form == FIP_FORM_PRECISE ? 1 : 0, s));
       stage_end(im, st, s);
       im->launches += 1;
+      FIP_CUDA(cudaEventRecord(im->ev_free[a], s));  // last reader of slot a
     }
   }
+  im->last_lane = (int)((nsnap - 1) % im->lanes);
   FIP_TRY(call_leave(im, s));
   if (im->timer.on) stage_collect(im);
   return FIP_OK;

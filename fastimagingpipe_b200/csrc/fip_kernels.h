@@ -94,6 +94,10 @@ cudaError_t fip_launch_image_max(const float* img, size_t count, unsigned* out, 
 cudaError_t fip_launch_trigger(const FipGeom& geo, const float* I1, const float* I2,
                                const float* I3, const float* max3, float* stats,
                                float* result, int precise, cudaStream_t s);
+// Same, the three maxima at separate addresses.
+cudaError_t fip_launch_trigger3(const FipGeom& geo, const float* I1, const float* I2,
+                                const float* I3, const float* m1, const float* m2,
+                                const float* m3, float* result, int precise, cudaStream_t s);
 // Batched trigger over a linear ring of images (stride N*N): triple k is
 // images k, k+1, k+2 with maxima[k .. k+2], result k at results + k * U*U.
 cudaError_t fip_launch_trigger_batch(const FipGeom& geo, const float* images, const float* maxima,

@@ -1271,16 +1271,18 @@ template <bool PRECISE>
 __global__ void __launch_bounds__(kThreads) k_trigger(const float* __restrict__ I1,
                                                       const float* __restrict__ I2,
                                                       const float* __restrict__ I3,
-                                                      const float* __restrict__ max3, int n,
+                                                      const float* __restrict__ m1,
+                                                      const float* __restrict__ m2,
+                                                      const float* __restrict__ m3, int n,
                                                       int t, int u, int vec,
                                                       float* __restrict__ result,
                                                       size_t img_stride, size_t res_stride) {
   // Batched launches: triple blockIdx.y is images y, y+1, y+2 of a linear ring
-  // (stride img_stride) with maxima max3[y .. y+2].
+  // (stride img_stride) with maxima m1[y], m2[y], m3[y].
   I1 += blockIdx.y * img_stride;
   I2 += blockIdx.y * img_stride;
   I3 += blockIdx.y * img_stride;
-  max3 += blockIdx.y;
+  const float max3[3] = {m1[blockIdx.y], m2[blockIdx.y], m3[blockIdx.y]};
   result += blockIdx.y * res_stride;
   const int lane = threadIdx.x & 31;
   const int b = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
@@ -1634,17 +1636,23 @@ cudaError_t fip_launch_trigger(const FipGeom& geo, const float* I1, const float*
                                const float* I3, const float* max3, float* stats, float* result,
                                int precise, cudaStream_t s) {
   (void)stats;
+  return fip_launch_trigger3(geo, I1, I2, I3, max3, max3 + 1, max3 + 2, result, precise, s);
+}
+
+cudaError_t fip_launch_trigger3(const FipGeom& geo, const float* I1, const float* I2,
+                                const float* I3, const float* m1, const float* m2,
+                                const float* m3, float* result, int precise, cudaStream_t s) {
   const int tiles = geo.u * geo.u;
   const int blocks = (tiles + kThreads / 32 - 1) / (kThreads / 32);
   if (tiles == 0) return cudaSuccess;
   const int vec = (geo.t % 4 == 0) && (geo.n % 4 == 0) &&
                   ((((uintptr_t)I1) | ((uintptr_t)I2) | ((uintptr_t)I3)) & 15) == 0;
   if (precise)
-    k_trigger<true><<<blocks, kThreads, 0, s>>>(I1, I2, I3, max3, geo.n, geo.t, geo.u, vec,
+    k_trigger<true><<<blocks, kThreads, 0, s>>>(I1, I2, I3, m1, m2, m3, geo.n, geo.t, geo.u, vec,
                                                 result, 0, 0);
   else
-    k_trigger<false><<<blocks, kThreads, 0, s>>>(I1, I2, I3, max3, geo.n, geo.t, geo.u, vec,
-                                                 result, 0, 0);
+    k_trigger<false><<<blocks, kThreads, 0, s>>>(I1, I2, I3, m1, m2, m3, geo.n, geo.t, geo.u,
+                                                 vec, result, 0, 0);
   return cudaGetLastError();
 }
 
@@ -1658,12 +1666,12 @@ cudaError_t fip_launch_trigger_batch(const FipGeom& geo, const float* images, co
   const int vec = (geo.t % 4 == 0) && (geo.n % 4 == 0) && ((uintptr_t)images & 15) == 0;
   if (precise)
     k_trigger<true><<<blocks, kThreads, 0, s>>>(images, images + n2, images + 2 * n2, maxima,
-                                                geo.n, geo.t, geo.u, vec, results, n2,
-                                                (size_t)tiles);
+                                                maxima + 1, maxima + 2, geo.n, geo.t, geo.u, vec,
+                                                results, n2, (size_t)tiles);
   else
     k_trigger<false><<<blocks, kThreads, 0, s>>>(images, images + n2, images + 2 * n2, maxima,
-                                                 geo.n, geo.t, geo.u, vec, results, n2,
-                                                 (size_t)tiles);
+                                                 maxima + 1, maxima + 2, geo.n, geo.t, geo.u,
+                                                 vec, results, n2, (size_t)tiles);
   return cudaGetLastError();
 }
 
