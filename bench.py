@@ -250,6 +250,44 @@ def run_batching(fip, synthetic, torch, dev, local, per_call=16, calls_per_size=
     return out
 
 
+def run_batching_reference_shape(fip, torch, d, snap, dev, local, plain_value, per_call=16,
+                                 calls=4):
+    """The batching form on the headline shape (4096^2, 130,816 baselines, tile 32, one
+    channel): the reference-shape snapshots cycled through calls of `per_call`
+    snapshots; snapshots/s over `calls` calls, and the ratio to the plain form's
+    device-resident value."""
+    out = {}
+    n, nb, t, cell = snap.image_size, snap.num_baselines, snap.unit_size, snap.cell_size
+    u = n // t
+    idx = [k % 3 for k in range(per_call)]
+    a = ([d["vis_re"][i * nb:(i + 1) * nb] for i in idx], [d["vis_im"][i * nb:(i + 1) * nb] for i in idx],
+         [d["B"][2 * i * nb:2 * (i + 1) * nb] for i in idx], [d["V"][9 * i:9 * (i + 1)] for i in idx],
+         [nb] * per_call)
+    res = torch.zeros((per_call, u * u), device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    for name, kw in (("batching_plain_reference_shape", {}),
+                     ("batching_precise_f16_reference_shape",
+                      dict(form=fip.FORM_PRECISE, vis_storage=fip.STORE_F16))):
+        with fip.Batch(n, nb, cell, t, per_call, device=local, **kw) as b:
+            tuning = b.autotune(*a)
+            with torch.cuda.stream(stream):
+                b.image(*a, res, stream=stream)  # instantiates the graph
+            torch.cuda.synchronize()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                ev0.record(stream)
+                for _ in range(calls):
+                    b.image(*a, res, stream=stream)
+                ev1.record(stream)
+            torch.cuda.synchronize()
+            v = per_call * calls / (ev0.elapsed_time(ev1) / 1e3)
+            out[name] = {"value": v, "unit": UNIT, "vs_plain_form": v / plain_value,
+                         "autotune": tuning,
+                         "config": f"4096^2, 130,816 baselines, tile 32, {per_call} snapshots "
+                                   f"per call, {calls} calls, CUDA graph per call"}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -466,6 +504,7 @@ def main():
     # half at 2048^2 and half at 4096^2 (fixed field of view), tile 32 ----
     if rank == 0 and not args.no_forms:
         forms.update(run_batching(fip, synthetic, torch, dev, local))
+        forms.update(run_batching_reference_shape(fip, torch, d, snap, dev, local, value))
 
     # ---- serving form: 4 beams, Poisson arrivals, HBM budget (rank 0) ----
     if rank == 0 and not args.no_forms:
