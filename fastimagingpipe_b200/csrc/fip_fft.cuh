@@ -198,17 +198,26 @@ __device__ __forceinline__ void load_smem(float2 (&v)[E], const float2* sm, int 
 
 // First-pass inputs of sub-transform s: element n is
 // y_s[n] = sum_{c = n + t M, lo <= c <= hi} z[c] w^{c s}.  WIDE: the band may
-// reach past +-M (t in -2..1); otherwise only t = -1, 0 can hit.
+// reach past +-M (t in -2..1); otherwise only t = -1, 0 can hit.  The thread's
+// elements are n = j + k M/R, so w^{c s} = w^{j s} w^{k s M/R} w^{t M s}: one
+// table read per butterfly (w^{j s}), R reads shared by every lane
+// (w^{k s M/R}) and the cube roots of unity w^{t M s} = e^{2 pi i t s / 3};
+// the first pass touches a few hundred table entries instead of the band's
+// thousands.
 template <int R, int E, int M, bool WIDE, class Load>
 __device__ __forceinline__ void first_load(float2 (&v)[E], int s, int lt, int lo, int hi,
                                            const float2* __restrict__ tw, Load& load) {
-  constexpr int G = 3 * M, TS = M / E;
+  constexpr int TS = M / E;
+  const float h3 = 0.86602540378443864676f;  // sqrt(3) / 2
 #pragma unroll
   for (int b = 0; b < E / R; ++b) {
     const int j = lt + b * TS;
+    const float2 wj = s ? __ldg(&tw[j * s]) : make_float2(1.f, 0.f);
 #pragma unroll
     for (int k = 0; k < R; ++k) {
       const int n = j + k * (M / R);
+      float2 wn = wj;
+      if (s != 0 && k != 0) wn = cmul(wj, __ldg(&tw[k * s * (M / R)]));
       float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
       for (int t = (WIDE ? -2 : -1); t <= (WIDE ? 1 : 0); ++t) {
@@ -216,10 +225,11 @@ __device__ __forceinline__ void first_load(float2 (&v)[E], int s, int lt, int lo
         if (c >= lo && c <= hi) {
           float2 z = load(c);
           if (s != 0) {
-            int e = c * s;
-            e += e < 0 ? G : 0;
-            e -= e >= G ? G : 0;
-            z = cmul(z, __ldg(&tw[e]));
+            float2 w = wn;
+            const int m = ((t * s) % 3 + 3) % 3;  // w^{t M s} = e^{2 pi i m / 3}
+            if (m == 1) w = cmul(wn, make_float2(-0.5f, h3));
+            if (m == 2) w = cmul(wn, make_float2(-0.5f, -h3));
+            z = cmul(z, w);
           }
           acc = cadd(acc, z);
         }

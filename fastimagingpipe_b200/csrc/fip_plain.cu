@@ -531,6 +531,7 @@ struct GridSmem {
   int col0[FIP_GCHUNK];   // half-plane column of the first kept tap column
   int meta[FIP_GCHUNK];   // nr | nc << 4 | mirrored << 8
   float k1[FIP_GCHUNK][9], k2[FIP_GCHUNK][9];  // stride 9: conflict-free both ways
+  float bound[kThreads / 32];
 };
 
 // One gridding work item (tile, entry range) of one snapshot.  Phase 1
@@ -557,6 +558,7 @@ __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_ci
     }
   }
   // Phase 1.
+  float bound = 0.f;  // sum over the item of max(|wr|, |wi|): bounds every cell sum
   for (int q = threadIdx.x; q < cnt; q += kThreads) {
     const unsigned ent = entries[item.y + q];
     const int v = (int)(ent >> 1), mir = (int)(ent & 1);
@@ -576,6 +578,7 @@ __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_ci
     }
     S.wr[q] = 0.5f * wr;
     S.wi[q] = mir ? -0.5f * wi : 0.5f * wi;
+    bound += 0.5f * fmaxf(fabsf(wr), fabsf(wi));
     const int nr = f.a1 - f.a0 + 1, nc = c1 - c0 + 1;
     S.row0[q] = mir ? -f.a0 : f.a0;
     S.col0[q] = c0;
@@ -593,7 +596,27 @@ __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_ci
         S.k2[q][b] = fipref::es((static_cast<float>(r2) - f.p2) * ihs);
       }
   }
+  // Plain form: the tile sums are fixed point, q = round(tap * 2^30 / bound),
+  // so every cell (|sum| <= bound) stays within int32 and the shared-memory
+  // sums are native integer atomics (exact, order-independent); resolution
+  // 2^-30 of the item's summed weights.  Precision form: Neumaier-compensated
+  // FP32.
+  float fx = 0.f, fx_inv = 0.f;
+  if (!COMP) {
+    for (int o = 16; o > 0; o >>= 1) bound += __shfl_xor_sync(0xffffffffu, bound, o);
+    if (lane == 0) S.bound[warp] = bound;
+  }
   __syncthreads();
+  if (!COMP) {
+    float tot = 0.f;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) tot += S.bound[w];
+    tot *= 1.0001f;  // margin for the rounding of the weights and their sum
+    fx = tot > 0.f ? 1073741824.0f / tot : 0.f;
+    fx_inv = tot * (1.0f / 1073741824.0f);
+  }
+  int* s_qre = reinterpret_cast<int*>(S.re);
+  int* s_qim = reinterpret_cast<int*>(S.im);
   // Phase 2.
   for (int q = warp; q < cnt; q += kThreads / 32) {
     const int meta = S.meta[q];
@@ -614,8 +637,9 @@ __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_ci
       const float cr = wr * kval, ci = wi * kval;
       const int cell = lr * kTS + lc;
       if (!COMP) {
-        atomicAdd(&S.re[cell], cr);
-        atomicAdd(&S.im[cell], ci);
+        const int qr = __float2int_rn(cr * fx), qi = __float2int_rn(ci * fx);
+        if (qr) atomicAdd(&s_qre[cell], qr);
+        if (qi) atomicAdd(&s_qim[cell], qi);
       } else {
         float o = atomicAdd(&S.re[cell], cr);
         float sm = o + cr;
@@ -636,10 +660,13 @@ __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_ci
     const int lc = layout ? k / FIP_GTILE : k % FIP_GTILE;
     const int row = trow0 + lr, col = tcol0 + lc;
     if (row < g && col < hp) {
-      float2 val = make_float2(S.re[lr * kTS + lc], S.im[lr * kTS + lc]);
+      float2 val;
       if (COMP) {
-        val.x += s_cre[lr * kTS + lc];
-        val.y += s_cim[lr * kTS + lc];
+        val = make_float2(S.re[lr * kTS + lc] + s_cre[lr * kTS + lc],
+                          S.im[lr * kTS + lc] + s_cim[lr * kTS + lc]);
+      } else {
+        val = make_float2((float)s_qre[lr * kTS + lc] * fx_inv,
+                          (float)s_qim[lr * kTS + lc] * fx_inv);
       }
       float2* dst = &grid[cell_index(row, col, g, hp, layout)];
       if (single) {
@@ -977,20 +1004,22 @@ __device__ __forceinline__ void exact_inverse(const ExactMap<T>& m, T LL, T MM, 
 // the tile is stored once and its maximum folded into *img_max.
 // EXACT: targets from the closed form in FP64 (precision form) instead of
 // the precomputed reference-chain targets.
-// Physical shared-memory column of destination pixel (row, col) in a tile:
-// an XOR swizzle of 4-column groups by the row, so the lanes of a warp
-// (neighbouring sources, mapped along an arbitrary direction) spread over the
-// banks while 4-column groups stay contiguous for 128-bit stores.
-__device__ __forceinline__ int tile_slot(int row, int col) {
-  return row * kDT + (col ^ ((row & 7) << 2));
-}
+// The shared tile carries an apron of kAp pixels on every side, so the four
+// pixels of any candidate's splat land inside it without per-pixel checks
+// (apron pixels belong to the neighbouring tiles, which splat them
+// themselves, and are dropped at the commit).  Its row stride is odd, so the
+// lanes of a warp (neighbouring sources, mapped along an arbitrary
+// direction) fall on distinct banks down a column as well as along a row.
+constexpr int kAp = 4;
+constexpr int kTW = kDT + 2 * kAp;  // tile side with the apron
+constexpr int kTR = kTW + 1;        // row stride
 
 template <bool EXACT>
 __global__ void __launch_bounds__(kThreads) k_reproject_gather(
     const float* __restrict__ pre, const float2* __restrict__ tg, const float* __restrict__ V,
     int n, int nb, float cell, float delta, const unsigned* __restrict__ pre_max,
     float* __restrict__ dst, unsigned* img_max) {
-  __shared__ __align__(16) unsigned s_tile[kDT * kDT];
+  __shared__ __align__(16) unsigned s_tile[kTW * kTR];
   __shared__ int s_ilo[kMaxRows];
   __shared__ int s_off[kMaxRows + 1];
   __shared__ int s_wsum[kThreads / 32];
@@ -1003,7 +1032,7 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
   const int h = n / 2;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
-  for (int k = threadIdx.x; k < kDT * kDT; k += kThreads) s_tile[k] = 0u;
+  for (int k = threadIdx.x; k < kTW * kTR; k += kThreads) s_tile[k] = 0u;
   if (threadIdx.x < 4) {
     const ExactMap<float> mf = make_map<float>(V, cell);
     const float Llo = (float)(c0 - h) - 1.0f - delta, Lhi = (float)(c0 + kDT - h) + delta;
@@ -1104,10 +1133,6 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
     off1 = (float)(P1 - (double)(c0 - h));
     off2 = (float)(P2 - (double)(r0 - h));
   }
-  auto add = [&](int row, int col, float w) {
-    const unsigned q = __float2uint_rn(w);
-    if (q) atomicAdd(&s_tile[tile_slot(row, col)], q);
-  };
   auto splat = [&](int i, int j, float vq, float2 t) {
     int fl, fm;
     float wl1, wm1, wl0, wm0;
@@ -1135,16 +1160,18 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
       wl1 = Lr - flr; wm1 = Mr - fmr;
       wl0 = 1.0f - wl1; wm0 = 1.0f - wm1;
     }
-    // Local destination pixels (fm|fm+1, fl|fl+1) of this tile.
-    const int lc = fl + 1, mc = fm + 1;
-    if ((unsigned)fm < (unsigned)kDT) {
-      if ((unsigned)fl < (unsigned)kDT) add(fm, fl, wl0 * wm0 * vq);
-      if ((unsigned)lc < (unsigned)kDT) add(fm, lc, wl1 * wm0 * vq);
-    }
-    if ((unsigned)mc < (unsigned)kDT) {
-      if ((unsigned)fl < (unsigned)kDT) add(mc, fl, wl0 * wm1 * vq);
-      if ((unsigned)lc < (unsigned)kDT) add(mc, lc, wl1 * wm1 * vq);
-    }
+    // Pixels (fm|fm+1, fl|fl+1), local to the tile with its apron.  A splat
+    // that reaches the tile lies inside the apron (fl, fm >= -1); one that
+    // does not touches no pixel of the tile and is skipped.
+    fl += kAp;
+    fm += kAp;
+    if ((unsigned)fl > (unsigned)(kTW - 2) || (unsigned)fm > (unsigned)(kTW - 2)) return;
+    const float a = wl0 * vq, b = wl1 * vq;
+    unsigned* px = &s_tile[fm * kTR + fl];
+    atomicAdd(px, __float2uint_rn(a * wm0));
+    atomicAdd(px + 1, __float2uint_rn(b * wm0));
+    atomicAdd(px + kTR, __float2uint_rn(a * wm1));
+    atomicAdd(px + kTR + 1, __float2uint_rn(b * wm1));
   };
   // Warp step: candidates f0 + lane and f0 + 32 + lane, loads issued first.
   int ra = 0, rb = 0;
@@ -1176,7 +1203,8 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
   for (int k = threadIdx.x; k < kDT * kDT / 4; k += kThreads) {
     const int lr = (4 * k) / kDT, g4 = ((4 * k) % kDT) >> 2;
     const int rr = r0 + lr, cc = c0 + 4 * g4;
-    const uint4 q = *reinterpret_cast<const uint4*>(&s_tile[tile_slot(lr, 4 * g4)]);
+    const unsigned* src = &s_tile[(lr + kAp) * kTR + kAp + 4 * g4];
+    const uint4 q = make_uint4(src[0], src[1], src[2], src[3]);
     const float4 val = make_float4((float)q.x * deq, (float)q.y * deq, (float)q.z * deq,
                                    (float)q.w * deq);
     if (rr < n) {
