@@ -31,6 +31,7 @@ struct Plan {
   int le;  // log2 of the complex values per thread (3 or 4)
   int e;   // values per thread
   int nt;  // threads = 3 M / e
+  int split;  // 1: one CTA per sub-transform (grid.y = s), 0: one CTA per transform
 };
 
 // Padded shared-memory index.
@@ -38,13 +39,13 @@ __device__ __forceinline__ int sidx(int i) { return i + (i >> 4); }
 // Distance between the three sub-transform buffers: the padded length plus 6
 // elements, so that outputs read across the buffers (fetch) start on
 // different banks.
-__host__ __device__ __forceinline__ int sub_stride(int m) { return m + m / 16 + 6; }
+__host__ __device__ constexpr int sub_stride(int m) { return m + m / 16 + 6; }
 // Shared memory: two buffers of three sub-transforms (passes alternate
 // between them, so a pass's stores never wait for the previous pass's loads);
 // the input band is staged in the second (stage_offset), which the first
 // pass does not write.
-__host__ __device__ __forceinline__ int stage_offset(int g) { return 3 * sub_stride(g / 3); }
-__host__ __device__ __forceinline__ int smem_elems(int g) { return 6 * sub_stride(g / 3) + 16; }
+__host__ __device__ constexpr int stage_offset(int g) { return 3 * sub_stride(g / 3); }
+__host__ __device__ constexpr int smem_elems(int g) { return 6 * sub_stride(g / 3) + 16; }
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -249,21 +250,21 @@ __host__ __device__ constexpr int pass_count() {
   return (LM + LE - 1) / LE;
 }
 
-// Pass Q of the Stockham transform: butterflies, stores into buffer Q & 1,
-// and the loads of pass Q + 1 from it.
-template <int LM, int LE, int Q>
-__device__ __forceinline__ void passes(float2 (&v)[1 << LE], float2* sm, int s,
+// Pass Q of the Stockham transform: butterflies, stores into buffer Q & 1
+// (base + (Q & 1) * BUF), and the loads of pass Q + 1 from it.
+template <int LM, int LE, int Q, int BUF>
+__device__ __forceinline__ void passes(float2 (&v)[1 << LE], float2* base,
                                        const float2* __restrict__ tw, int lt) {
   constexpr int E = 1 << LE, M = 1 << LM, TS = M / E, NP = pass_count<LM, LE>();
   if constexpr (Q < NP) {
     constexpr int LNS = Q * LE, R = 1 << pass_lr<LM, LE>(Q);
-    float2* sub = sm + (Q & 1) * stage_offset(3 * M) + s * sub_stride(M);
+    float2* sub = base + (Q & 1) * BUF;
     butterflies<R, E>(v, tw, LM, LNS, lt, TS);
     store_smem<R, E>(v, sub, LNS, lt, TS);
     __syncthreads();
     if constexpr (Q + 1 < NP) {
       load_smem<(1 << pass_lr<LM, LE>(Q + 1)), E>(v, sub, M, lt, TS);
-      passes<LM, LE, Q + 1>(v, sm, s, tw, lt);
+      passes<LM, LE, Q + 1, BUF>(v, base, tw, lt);
     }
   }
 }
@@ -287,7 +288,7 @@ __device__ __forceinline__ void run(float2* sm, const float2* __restrict__ tw, i
     first_load<R0, E, M, true>(v, s, lt, lo, hi, tw, load);
   else
     first_load<R0, E, M, false>(v, s, lt, lo, hi, tw, load);
-  passes<LM, LE, 0>(v, sm, s, tw, lt);
+  passes<LM, LE, 0, stage_offset(3 * M)>(v, sm + s * sub_stride(M), tw, lt);
 }
 
 // Output o in [0, 2M) after run(): X[p] with p = o - M, i.e. Y_s[q] for
@@ -300,6 +301,33 @@ __device__ __forceinline__ float2 fetch(const float2* sm, int o) {
   if (pp < 0) pp += 3 * M;
   const int q = pp / 3, s = pp - 3 * q;
   return sm[last * stage_offset(3 * M) + s * sub_stride(M) + sidx(q)];
+}
+
+// Split form: one CTA of M / E threads computes the single sub-transform
+// Y_s (s given) into two buffers of sub_stride(M) elements at sm (staging, if
+// any, is read by load() before the first barrier and may sit in the second
+// buffer).  Ends with a barrier; Y_s[q] is then at single_out<LM, LE>(sm, q).
+template <int LM, int LE, class Load>
+__device__ __forceinline__ void run_single(float2* sm, int s, const float2* __restrict__ tw,
+                                           int lo, int hi, Load& load) {
+  constexpr int E = 1 << LE, M = 1 << LM;
+  constexpr int R0 = 1 << pass_lr<LM, LE>(0);
+  float2 v[E];
+  if (hi >= M || lo < -M)
+    first_load<R0, E, M, true>(v, s, threadIdx.x, lo, hi, tw, load);
+  else
+    first_load<R0, E, M, false>(v, s, threadIdx.x, lo, hi, tw, load);
+  // The first pass writes buffer 0 while the staging in buffer 1 is still
+  // being read by other threads: passes' barriers come after each store, so
+  // buffer 1 is only written (pass 1) after every thread passed barrier 0.
+  passes<LM, LE, 0, sub_stride(M)>(v, sm, tw, threadIdx.x);
+}
+
+template <int LM, int LE>
+__device__ __forceinline__ float2 single_out(const float2* sm, int q) {
+  constexpr int M = 1 << LM;
+  constexpr int last = (pass_count<LM, LE>() - 1) & 1;
+  return sm[last * sub_stride(M) + sidx(q)];
 }
 
 }  // namespace fipfft

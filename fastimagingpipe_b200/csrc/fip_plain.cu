@@ -871,6 +871,110 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), fft_min_blocks<LM, LE>(
   block_max_to(vmax, &bbox[3]);
 }
 
+// Split forms of the two passes: one CTA of M / E threads per (column or row
+// pair, sub-transform s), grid.y = s, grid.z = snapshot of a batch.  Three
+// times the CTAs of a quarter of the size: each CTA's barriers hold four
+// warps instead of twelve, and CTAs at different phases share an SM.  Each
+// CTA stages the band itself (in its second buffer when it fits, else reads
+// it from global memory) and writes its outputs X[3 q + s] directly.
+template <int LM, int LE>
+__host__ __device__ constexpr int split_threads() { return 1 << (LM - LE); }
+
+template <int LM, int LE>
+__global__ void __launch_bounds__(split_threads<LM, LE>(), (LE == 4 ? 6 : 4))
+    k_fft_cols_split(const float2* __restrict__ H, const unsigned* __restrict__ bbox,
+                     float2* __restrict__ P, const float2* __restrict__ tw, size_t grid_stride,
+                     size_t col_stride) {
+  constexpr int M = 1 << LM, g = 3 * M, half = g / 2, n = 2 * M, NT = split_threads<LM, LE>();
+  constexpr int kCap = fipfft::sub_stride(M);  // staging capacity (the second buffer)
+  extern __shared__ float2 s_fft[];
+  H += blockIdx.z * grid_stride;
+  P += blockIdx.z * col_stride;
+  bbox += 4 * blockIdx.z;
+  const int c = blockIdx.x, s = blockIdx.y;
+  const int k2 = (int)bbox[1];
+  if (c > k2) return;
+  const int k1 = min((int)bbox[0], half);
+  const int lo = (k1 == half) ? 1 - k1 : -k1, hi = k1;
+  const float2* col = H + (size_t)c * g;
+  float2* st = s_fft + kCap;
+  const bool staged = hi - lo + 1 <= kCap;
+  if (staged)
+    for (int i = threadIdx.x; i <= hi - lo; i += NT) {
+      const int r = i + lo;
+      st[i] = col[r < 0 ? r + g : r];
+    }
+  __syncthreads();
+  auto load = [&](int r) -> float2 { return staged ? st[r - lo] : col[r < 0 ? r + g : r]; };
+  fipfft::run_single<LM, LE>(s_fft, s, tw, lo, hi, load);
+  float2* out = P + (size_t)c * n;
+  for (int q = threadIdx.x; q < M; q += NT) {
+    const int pp = 3 * q + s;  // output p = pp (mod G), kept when |p| <= M
+    const int o = pp < M ? pp + M : (pp >= 2 * M ? pp - 2 * M : -1);
+    if (o >= 0) out[o] = fipfft::single_out<LM, LE>(s_fft, q);
+  }
+}
+
+template <int LM, int LE>
+__global__ void __launch_bounds__(split_threads<LM, LE>(), (LE == 4 ? 6 : 4))
+    k_fft_rows_split(const float2* __restrict__ P, unsigned* bbox, const float* __restrict__ rck,
+                     float* __restrict__ pre, const float2* __restrict__ tw, size_t col_stride,
+                     size_t pre_stride) {
+  constexpr int M = 1 << LM, g = 3 * M, half = g / 2, n = 2 * M, h = M;
+  constexpr int NT = split_threads<LM, LE>(), kCap = fipfft::sub_stride(M);
+  extern __shared__ float2 s_fft[];
+  P += blockIdx.z * col_stride;
+  pre += blockIdx.z * pre_stride;
+  bbox += 4 * blockIdx.z;
+  const int yy1 = 2 * blockIdx.x, s = blockIdx.y;
+  const int k2 = min((int)bbox[1], half);
+  const int lo = (k2 == half) ? 1 - k2 : -k2, hi = k2;
+  // Z[c] = X1[c] + i X2[c], X(-c) = conj X(c), from the column-pass output.
+  auto zval = [&](int c) -> float2 {
+    const int a = c < 0 ? -c : c;
+    const float4 ab = *reinterpret_cast<const float4*>(P + (size_t)a * n + yy1);
+    float ay = ab.y, by = ab.w;
+    if (a == 0 || a == half) {  // self-conjugate bins are real
+      ay = 0.f;
+      by = 0.f;
+    }
+    return c >= 0 ? make_float2(ab.x - by, ay + ab.z) : make_float2(ab.x + by, ab.z - ay);
+  };
+  float2* st = s_fft + kCap;
+  const bool staged = hi - lo + 1 <= kCap;
+  if (staged)
+    for (int c = threadIdx.x; c <= k2; c += NT) {
+      const float4 ab = *reinterpret_cast<const float4*>(P + (size_t)c * n + yy1);
+      float ay = ab.y, by = ab.w;
+      if (c == 0 || c == half) {
+        ay = 0.f;
+        by = 0.f;
+      }
+      st[c - lo] = make_float2(ab.x - by, ay + ab.z);
+      if (c > 0 && -c >= lo) st[-c - lo] = make_float2(ab.x + by, ab.z - ay);
+    }
+  __syncthreads();
+  auto load = [&](int c) -> float2 { return staged ? st[c - lo] : zval(c); };
+  fipfft::run_single<LM, LE>(s_fft, s, tw, lo, hi, load);
+  const float ry1 = rck[abs(yy1 - h)], ry2 = rck[abs(yy1 + 1 - h)];
+  float* row1 = pre + (size_t)yy1 * n;
+  float* row2 = row1 + n;
+  float vmax = 0.f;
+  for (int q = threadIdx.x; q < M; q += NT) {
+    const int pp = 3 * q + s;
+    const int o = pp < M ? pp + M : (pp >= 2 * M ? pp - 2 * M : -1);
+    if (o >= 0) {
+      const float2 v = fipfft::single_out<LM, LE>(s_fft, q);
+      const float rx = rck[abs(o - h)];
+      const float a = fabsf(v.x * (rx * ry1)), b = fabsf(v.y * (rx * ry2));
+      row1[o] = a;
+      row2[o] = b;
+      vmax = fmaxf(vmax, fmaxf(a, b));
+    }
+  }
+  block_max_to(vmax, &bbox[3]);
+}
+
 // Crop + correction of the cuFFT C2R output (images whose grid side is not
 // 3 * 2^k): row (y mod G), column (x mod G), row stride G + 2 floats.
 __global__ void k_correct_c2r(const float* __restrict__ fft_out, const float* __restrict__ ck,
@@ -1397,6 +1501,7 @@ bool fip_fft_plan(int g, fipfft::Plan& p, int values_per_thread) {
   p.le = le;
   p.e = 1 << le;
   p.nt = 3 * (m >> le);
+  p.split = 0;
   return true;
 }
 
@@ -1541,9 +1646,18 @@ static cudaError_t fft_smem_attr(const void* fn, int g, size_t& smem) {
 template <int LM, int LE>
 static cudaError_t launch_cols(const FipGeom& geo, const float2* grid, const unsigned* bbox,
                                float2* colbuf, const float2* tw, cudaStream_t s, int batch,
-                               size_t grid_stride, size_t col_stride) {
+                               size_t grid_stride, size_t col_stride, int split) {
   size_t smem;
-  cudaError_t e = fft_smem_attr((const void*)k_fft_cols<LM, LE>, geo.g, smem);
+  cudaError_t e;
+  if (split) {
+    if ((e = fft_smem_attr((const void*)k_fft_cols_split<LM, LE>, geo.g, smem)) != cudaSuccess)
+      return e;
+    smem = 2 * (size_t)fipfft::sub_stride(1 << LM) * sizeof(float2);
+    k_fft_cols_split<LM, LE><<<dim3(geo.hp, 3, batch), split_threads<LM, LE>(), smem, s>>>(
+        grid, bbox, colbuf, tw, grid_stride, col_stride);
+    return cudaGetLastError();
+  }
+  e = fft_smem_attr((const void*)k_fft_cols<LM, LE>, geo.g, smem);
   if (e != cudaSuccess) return e;
   k_fft_cols<LM, LE><<<dim3(geo.hp, batch), fft_threads<LM, LE>(), smem, s>>>(
       grid, bbox, colbuf, tw, grid_stride, col_stride);
@@ -1554,9 +1668,18 @@ template <int LM, int LE>
 static cudaError_t launch_rows(const FipGeom& geo, const float2* colbuf, unsigned* bbox,
                                const float* taper, const float2* tw, float* pre,
                                cudaStream_t s, int batch, size_t col_stride,
-                               size_t pre_stride) {
+                               size_t pre_stride, int split) {
   size_t smem;
-  cudaError_t e = fft_smem_attr((const void*)k_fft_rows<LM, LE>, geo.g, smem);
+  cudaError_t e;
+  if (split) {
+    if ((e = fft_smem_attr((const void*)k_fft_rows_split<LM, LE>, geo.g, smem)) != cudaSuccess)
+      return e;
+    smem = 2 * (size_t)fipfft::sub_stride(1 << LM) * sizeof(float2);
+    k_fft_rows_split<LM, LE><<<dim3(geo.n / 2, 3, batch), split_threads<LM, LE>(), smem, s>>>(
+        colbuf, bbox, taper + geo.n / 2 + 1, pre, tw, col_stride, pre_stride);
+    return cudaGetLastError();
+  }
+  e = fft_smem_attr((const void*)k_fft_rows<LM, LE>, geo.g, smem);
   if (e != cudaSuccess) return e;
   k_fft_rows<LM, LE><<<dim3(geo.n / 2, batch), fft_threads<LM, LE>(), smem, s>>>(
       colbuf, bbox, taper + geo.n / 2 + 1, pre, tw, col_stride, pre_stride);
@@ -1594,7 +1717,7 @@ cudaError_t fip_launch_fft_cols(const FipGeom& geo, const float2* grid, const un
                                 size_t col_stride) {
   if (plan.g != geo.g || batch < 1 || batch > 65535) return cudaErrorInvalidValue;
   FIP_FFT_SWITCH(plan, (launch_cols<LM_, LE_>(geo, grid, bbox, colbuf, twiddles, s, batch,
-                                              grid_stride, col_stride)));
+                                              grid_stride, col_stride, plan.split)));
 }
 
 cudaError_t fip_launch_fft_rows(const FipGeom& geo, const float2* colbuf, unsigned* bbox,
@@ -1603,7 +1726,7 @@ cudaError_t fip_launch_fft_rows(const FipGeom& geo, const float2* colbuf, unsign
                                 size_t col_stride, size_t pre_stride) {
   if (plan.g != geo.g || batch < 1 || batch > 65535) return cudaErrorInvalidValue;
   FIP_FFT_SWITCH(plan, (launch_rows<LM_, LE_>(geo, colbuf, bbox, taper, twiddles, pre, s, batch,
-                                              col_stride, pre_stride)));
+                                              col_stride, pre_stride, plan.split)));
 }
 
 cudaError_t fip_launch_correct_c2r(const FipGeom& geo, const float* fft_out, const float* taper,
