@@ -10,11 +10,14 @@
 #include <cufft.h>
 
 #include <algorithm>
+#include <atomic>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/fip.h"
@@ -94,6 +97,96 @@ struct StageTimer {
 }  // namespace
 
 int fip_set_error(int code, const std::string& msg) { return fail(code, msg); }
+
+namespace {
+// Host copies into the pinned staging of the host-buffer path.  One thread
+// copies a few GB/s from pageable memory, so a 2 MB snapshot would keep the
+// first snapshot's upload (which the GPU waits for) on the critical path; a
+// small pool of persistent workers splits each large copy.
+class CopyPool {
+ public:
+  static CopyPool& get() {
+    static CopyPool pool;
+    return pool;
+  }
+  // Copies `bytes` from src to dst, split over the workers and the caller.
+  void copy(void* dst, const void* src, size_t bytes) {
+    const size_t parts = std::min<size_t>(kWorkers + 1, bytes / kMinPart);
+    if (parts <= 1 || workers_.empty()) {
+      std::memcpy(dst, src, bytes);
+      return;
+    }
+    std::unique_lock<std::mutex> call(call_mu_);  // one split copy at a time
+    const size_t step = (bytes / parts + 63) & ~size_t(63);
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      dst_ = static_cast<char*>(dst);
+      src_ = static_cast<const char*>(src);
+      bytes_ = bytes;
+      step_ = step;
+      next_ = 1;  // part 0 is the caller's
+      parts_ = parts;
+      pending_ = parts - 1;
+      ++epoch_;
+    }
+    cv_.notify_all();
+    std::memcpy(dst, src, std::min(step, bytes));
+    std::unique_lock<std::mutex> lk(mu_);
+    done_.wait(lk, [&] { return pending_ == 0; });
+  }
+
+ private:
+  static constexpr size_t kWorkers = 3;
+  static constexpr size_t kMinPart = 256 * 1024;
+
+  CopyPool() {
+    for (size_t k = 0; k < kWorkers; ++k) {
+      try {
+        workers_.emplace_back([this] { run(); });
+      } catch (...) {
+        break;  // fewer workers (or none: plain copies)
+      }
+    }
+  }
+  ~CopyPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (std::thread& t : workers_) t.join();
+  }
+  void run() {
+    unsigned long long seen = 0;
+    std::unique_lock<std::mutex> lk(mu_);
+    for (;;) {
+      cv_.wait(lk, [&] { return stop_ || (epoch_ != seen && next_ < parts_); });
+      if (stop_) return;
+      seen = epoch_;
+      while (next_ < parts_) {
+        const size_t part = next_++;
+        const size_t off = part * step_;
+        const size_t len = off < bytes_ ? std::min(step_, bytes_ - off) : 0;
+        char* d = dst_ + off;
+        const char* sp = src_ + off;
+        lk.unlock();
+        if (len) std::memcpy(d, sp, len);
+        lk.lock();
+        if (--pending_ == 0) done_.notify_one();
+      }
+    }
+  }
+
+  std::vector<std::thread> workers_;
+  std::mutex call_mu_, mu_;
+  std::condition_variable cv_, done_;
+  char* dst_ = nullptr;
+  const char* src_ = nullptr;
+  size_t bytes_ = 0, step_ = 0, next_ = 0, parts_ = 0, pending_ = 0;
+  unsigned long long epoch_ = 0;
+  bool stop_ = false;
+};
+}  // namespace
 
 // Scratch of one snapshot in flight.  With the band-pruned transform an
 // imager has kLanes of them, so the snapshots of one call (or of a sequence)
@@ -424,7 +517,8 @@ size_t fip_imager_device_bytes(const fip_imager* im) { return im ? im->device_by
 // instead).
 static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const float* vi,
                                const float* B, const float* V, size_t nb, float* image,
-                               float* image_max, cudaStream_t s, bool fork_targets) {
+                               float* image_max, cudaStream_t s, bool fork_targets,
+                               bool targets_ready = false) {
   const FipGeom& geo = im->geo;
   if (nb > im->cfg.max_baselines) return fail(FIP_ERR_ARG, "nb exceeds the imager's capacity");
   if (nb == 0) return fail(FIP_ERR_ARG, "nb must be positive");
@@ -449,7 +543,7 @@ static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const f
   // the side stream (serialised on s when profiling, so every stage's time
   // is its own).
   const bool fork = chain_targets && fork_targets && !im->timer.on;
-  if (chain_targets) {
+  if (chain_targets && !targets_ready) {
     cudaStream_t ts = fork ? im->side : s;
     if (fork) {
       FIP_CUDA(cudaEventRecord(im->ev_fork, s));
@@ -514,7 +608,8 @@ static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const f
 // lane, everything runs on s in order.
 static int image_on_lane(fip_imager* im, int k, const float* vr, const float* vi,
                          const float* B, const float* V, size_t nb, float* image,
-                         float* image_max, cudaStream_t s, cudaEvent_t after) {
+                         float* image_max, cudaStream_t s, cudaEvent_t after,
+                         bool targets_ready = false) {
   if (im->lanes == 1 || im->timer.on) {
     FIP_CUDA(cudaStreamWaitEvent(s, after, 0));
     return image_snapshot_impl(im, im->lane[k % im->lanes], vr, vi, B, V, nb, image, image_max,
@@ -522,7 +617,8 @@ static int image_on_lane(fip_imager* im, int k, const float* vr, const float* vi
   }
   Lane& L = im->lane[k % im->lanes];
   FIP_CUDA(cudaStreamWaitEvent(L.stream, after, 0));
-  FIP_TRY(image_snapshot_impl(im, L, vr, vi, B, V, nb, image, image_max, L.stream, false));
+  FIP_TRY(image_snapshot_impl(im, L, vr, vi, B, V, nb, image, image_max, L.stream, false,
+                              targets_ready));
   FIP_CUDA(cudaEventRecord(L.ev_done, L.stream));
   return FIP_OK;
 }
@@ -638,17 +734,32 @@ int fip_pipe_host(fip_imager* im, const float* vr, const float* vi, const float*
   cudaStream_t s = im->stream, cs = im->copy_stream;
   FIP_TRY(call_enter(im, s));
   FIP_TRY(call_enter(im, cs));
+  // The three bases V first: the pixel mapping (the longest kernel) needs
+  // only V, so with concurrent lanes it starts on every lane while the host
+  // still stages the visibilities.
+  std::memcpy(im->h_V, V, 27 * sizeof(float));
+  FIP_CUDA(cudaMemcpyAsync(im->d_V, im->h_V, 27 * sizeof(float), cudaMemcpyHostToDevice, cs));
+  const bool early = im->lanes > 1 && !im->timer.on && im->cfg.reproject == 0 &&
+                     im->cfg.form == FIP_FORM_PLAIN;
+  if (early) {
+    FIP_CUDA(cudaEventRecord(im->ev_start, cs));
+    for (int k = 0; k < 3; ++k) {
+      Lane& L = im->lane[k % im->lanes];
+      FIP_CUDA(cudaStreamWaitEvent(L.stream, im->ev_start, 0));
+      FIP_CUDA(fip_launch_targets(im->geo, im->d_V + (size_t)k * 9, L.targets, L.stream));
+      im->launches += 1;
+    }
+  }
   // Per snapshot: host copy into pinned slot k (CPU), async H2D on the copy
-  // stream, then the compute stream images it while the CPU stages k+1.
+  // stream, then the snapshot's lane images it while the CPU stages k+1.
   for (int k = 0; k < 3; ++k) {
     float* hvr = im->h_vr + (size_t)k * nb;
     float* hvi = im->h_vi + (size_t)k * nb;
     float* hB = im->h_B + (size_t)k * nb * 2;
-    float* hV = im->h_V + (size_t)k * 9;
-    std::memcpy(hvr, vr + (size_t)k * nb, nb * sizeof(float));
-    std::memcpy(hvi, vi + (size_t)k * nb, nb * sizeof(float));
-    std::memcpy(hB, B + (size_t)k * nb * 2, nb * 2 * sizeof(float));
-    std::memcpy(hV, V + (size_t)k * 9, 9 * sizeof(float));
+    CopyPool& pool = CopyPool::get();
+    pool.copy(hB, B + (size_t)k * nb * 2, nb * 2 * sizeof(float));
+    pool.copy(hvr, vr + (size_t)k * nb, nb * sizeof(float));
+    pool.copy(hvi, vi + (size_t)k * nb, nb * sizeof(float));
     float* dvr = im->d_vr + (size_t)k * nb;
     float* dvi = im->d_vi + (size_t)k * nb;
     float* dB = im->d_B + (size_t)k * nb * 2;
@@ -656,10 +767,9 @@ int fip_pipe_host(fip_imager* im, const float* vr, const float* vi, const float*
     FIP_CUDA(cudaMemcpyAsync(dvr, hvr, nb * sizeof(float), cudaMemcpyHostToDevice, cs));
     FIP_CUDA(cudaMemcpyAsync(dvi, hvi, nb * sizeof(float), cudaMemcpyHostToDevice, cs));
     FIP_CUDA(cudaMemcpyAsync(dB, hB, nb * 2 * sizeof(float), cudaMemcpyHostToDevice, cs));
-    FIP_CUDA(cudaMemcpyAsync(dV, hV, 9 * sizeof(float), cudaMemcpyHostToDevice, cs));
     FIP_CUDA(cudaEventRecord(im->ev_copied[k], cs));
     FIP_TRY(image_on_lane(im, k, dvr, dvi, dB, dV, nb, im->images[k], im->maxima + k, s,
-                          im->ev_copied[k]));
+                          im->ev_copied[k], early));
   }
   for (int k = 0; k < 3; ++k) FIP_TRY(wait_lane(im, k, s));
   im->last_lane = 2 % im->lanes;
