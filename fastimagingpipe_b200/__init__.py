@@ -96,9 +96,9 @@ def lib() -> ctypes.CDLL:
         L.fip_batch_reset.argtypes = [vp]
         L.fip_batch_image.argtypes = [vp, vp, vp, vp, vp, vp, sz, vp, ctypes.POINTER(sz), vp]
         L.fip_batch_autotune.argtypes = [vp, vp, vp, vp, vp, vp, sz, vp]
-        L.fip_batch_tuning.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int)] * 3
-        L.fip_imager_tuning.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int)] * 3
-        L.fip_imager_set_tuning.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.fip_batch_tuning.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int)] * 4
+        L.fip_imager_tuning.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int)] * 4
+        L.fip_imager_set_tuning.argtypes = [vp] + [ctypes.c_int] * 4
         L.fip_grid_snapshot.argtypes = [vp, vp, vp, vp, vp, sz, vp, vp]
         L.fip_grid_snapshot_noalloc.argtypes = [vp, vp, vp, vp, sz, sz, fp, vp, vp]
         L.fip_server_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, sz, ctypes.c_int, sz]
@@ -229,15 +229,16 @@ class Imager:
         return self.tuning()
 
     def set_tuning(self, fft_values_per_thread: int = 0, fft_split: int = 0,
-                   grid_ctas_per_sm: int = 0):
+                   grid_ctas_per_sm: int = 0, fft_direct: int = 0):
         _check(lib().fip_imager_set_tuning(self._h, fft_values_per_thread, fft_split,
-                                           grid_ctas_per_sm))
+                                           fft_direct, grid_ctas_per_sm))
 
     def tuning(self) -> dict:
-        e, sp, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        _check(lib().fip_imager_tuning(self._h, ctypes.byref(e), ctypes.byref(sp), ctypes.byref(c)))
+        e, sp, dr, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().fip_imager_tuning(self._h, ctypes.byref(e), ctypes.byref(sp),
+                                       ctypes.byref(dr), ctypes.byref(c)))
         return {"fft_values_per_thread": int(e.value), "fft_split": int(sp.value),
-                "grid_ctas_per_sm": int(c.value)}
+                "fft_direct": int(dr.value), "grid_ctas_per_sm": int(c.value)}
 
     def band(self):
         """(max |r1|, max half-plane column) of the last gridded snapshot."""
@@ -327,10 +328,11 @@ class Batch:
         return self.tuning()
 
     def tuning(self) -> dict:
-        e, sp, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        _check(lib().fip_batch_tuning(self._h, ctypes.byref(e), ctypes.byref(sp), ctypes.byref(c)))
+        e, sp, dr, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().fip_batch_tuning(self._h, ctypes.byref(e), ctypes.byref(sp),
+                                      ctypes.byref(dr), ctypes.byref(c)))
         return {"fft_values_per_thread": int(e.value), "fft_split": int(sp.value),
-                "grid_ctas_per_sm": int(c.value)}
+                "fft_direct": int(dr.value), "grid_ctas_per_sm": int(c.value)}
 
     def reset(self):
         _check(lib().fip_batch_reset(self._h))

@@ -32,6 +32,7 @@ struct Plan {
   int e;   // values per thread
   int nt;  // threads = 3 M / e
   int split;  // 1: one CTA per sub-transform (grid.y = s), 0: one CTA per transform
+  int direct;  // 1: the first pass reads the band from global memory (no staging)
 };
 
 // Padded shared-memory index.
@@ -252,19 +253,32 @@ __host__ __device__ constexpr int pass_count() {
 
 // Pass Q of the Stockham transform: butterflies, stores into buffer Q & 1
 // (base + (Q & 1) * BUF), and the loads of pass Q + 1 from it.
-template <int LM, int LE, int Q, int BUF>
+// GROUP: the barriers between passes hold only the sub-transform's own
+// threads (named barrier 1 + s; the group is a whole number of warps), the
+// last pass ends with a CTA barrier.  Only valid when nothing else lives in
+// the buffers (no staged band).
+template <int LM, int LE, int Q, int BUF, bool GROUP = false>
 __device__ __forceinline__ void passes(float2 (&v)[1 << LE], float2* base,
-                                       const float2* __restrict__ tw, int lt) {
+                                       const float2* __restrict__ tw, int lt, int s = 0) {
   constexpr int E = 1 << LE, M = 1 << LM, TS = M / E, NP = pass_count<LM, LE>();
   if constexpr (Q < NP) {
     constexpr int LNS = Q * LE, R = 1 << pass_lr<LM, LE>(Q);
     float2* sub = base + (Q & 1) * BUF;
     butterflies<R, E>(v, tw, LM, LNS, lt, TS);
     store_smem<R, E>(v, sub, LNS, lt, TS);
-    __syncthreads();
+    if constexpr (GROUP && Q + 1 < NP && TS % 32 == 0) {
+      if (s == 0)
+        asm volatile("bar.sync 1, %0;" ::"n"(TS) : "memory");
+      else if (s == 1)
+        asm volatile("bar.sync 2, %0;" ::"n"(TS) : "memory");
+      else
+        asm volatile("bar.sync 3, %0;" ::"n"(TS) : "memory");
+    } else {
+      __syncthreads();
+    }
     if constexpr (Q + 1 < NP) {
       load_smem<(1 << pass_lr<LM, LE>(Q + 1)), E>(v, sub, M, lt, TS);
-      passes<LM, LE, Q + 1, BUF>(v, base, tw, lt);
+      passes<LM, LE, Q + 1, BUF, GROUP>(v, base, tw, lt, s);
     }
   }
 }
@@ -275,7 +289,9 @@ __device__ __forceinline__ void passes(float2 (&v)[1 << LE], float2* base,
 // sm + stage_offset(G) (written before a barrier).  All threads of the CTA
 // must call it; sm holds smem_elems(G) float2.  Ends with a barrier: sm is
 // then ready for fetch().
-template <int LM, int LE, class Load>
+// DIRECT: load() reads global memory (no staged band), so the passes may
+// use group barriers.
+template <int LM, int LE, bool DIRECT = false, class Load>
 __device__ __forceinline__ void run(float2* sm, const float2* __restrict__ tw, int lo, int hi,
                                     Load& load) {
   constexpr int E = 1 << LE, M = 1 << LM, TS = M / E;
@@ -288,7 +304,7 @@ __device__ __forceinline__ void run(float2* sm, const float2* __restrict__ tw, i
     first_load<R0, E, M, true>(v, s, lt, lo, hi, tw, load);
   else
     first_load<R0, E, M, false>(v, s, lt, lo, hi, tw, load);
-  passes<LM, LE, 0, stage_offset(3 * M)>(v, sm + s * sub_stride(M), tw, lt);
+  passes<LM, LE, 0, stage_offset(3 * M), DIRECT>(v, sm + s * sub_stride(M), tw, lt, s);
 }
 
 // Output o in [0, 2M) after run(): X[p] with p = o - M, i.e. Y_s[q] for

@@ -895,10 +895,12 @@ int fip_imager_autotune(fip_imager* im, const float* vr, const float* vi, const 
   if (im->custom_fft) {
     float best = 1e30f;
     fipfft::Plan chosen = im->fft;
-    for (int shape = 0; shape < 4; ++shape) {
+    // Values per thread 8 or 16 x {joint, split, joint with a direct first pass}.
+    for (int shape = 0; shape < 6; ++shape) {
       fipfft::Plan p{};
       if (!fip_fft_plan(geo.g, p, shape & 1 ? 16 : 8)) continue;
-      p.split = shape >> 1;
+      p.split = (shape >> 1) == 1;
+      p.direct = (shape >> 1) == 2;
       float ms = 0.f;
       FIP_TRY(timed(
           [&]() -> cudaError_t {
@@ -940,7 +942,7 @@ int fip_imager_autotune(fip_imager* im, const float* vr, const float* vi, const 
 }
 
 int fip_imager_set_tuning(fip_imager* im, int fft_values_per_thread, int fft_split,
-                          int grid_ctas_per_sm) {
+                          int fft_direct, int grid_ctas_per_sm) {
   if (!im) return fail(FIP_ERR_ARG, "null imager");
   if (grid_ctas_per_sm < 0 || grid_ctas_per_sm > 8)
     return fail(FIP_ERR_ARG, "grid_ctas_per_sm must be in [0, 8]");
@@ -949,6 +951,7 @@ int fip_imager_set_tuning(fip_imager* im, int fft_values_per_thread, int fft_spl
     if (!fip_fft_plan(im->geo.g, p, fft_values_per_thread))
       return fail(FIP_ERR_ARG, "no transform with these values per thread for this size");
     p.split = fft_split ? 1 : 0;
+    p.direct = fft_direct && !fft_split ? 1 : 0;
     im->fft = p;
   }
   im->grid_ctas_per_sm = grid_ctas_per_sm;
@@ -956,10 +959,11 @@ int fip_imager_set_tuning(fip_imager* im, int fft_values_per_thread, int fft_spl
 }
 
 int fip_imager_tuning(const fip_imager* im, int* fft_values_per_thread, int* fft_split,
-                      int* grid_ctas_per_sm) {
+                      int* fft_direct, int* grid_ctas_per_sm) {
   if (!im) return fail(FIP_ERR_ARG, "null imager");
   if (fft_values_per_thread) *fft_values_per_thread = im->custom_fft ? im->fft.e : 0;
   if (fft_split) *fft_split = im->custom_fft ? im->fft.split : 0;
+  if (fft_direct) *fft_direct = im->custom_fft ? im->fft.direct : 0;
   if (grid_ctas_per_sm)
     *grid_ctas_per_sm = im->grid_ctas_per_sm > 0
                             ? im->grid_ctas_per_sm
@@ -1503,10 +1507,12 @@ int fip_batch_autotune(fip_batch* b, const float* const* vis_re, const float* co
   {
     float best = 1e30f;
     fipfft::Plan chosen = b->fft;
-    for (int shape = 0; shape < 4; ++shape) {
+    // Values per thread 8 or 16 x {joint, split, joint with a direct first pass}.
+    for (int shape = 0; shape < 6; ++shape) {
       fipfft::Plan p{};
       if (!fip_fft_plan(geo.g, p, shape & 1 ? 16 : 8)) continue;
-      p.split = shape >> 1;
+      p.split = (shape >> 1) == 1;
+      p.direct = (shape >> 1) == 2;
       float ms = 0.f;
       FIP_TRY(timed(
           [&]() -> cudaError_t {
@@ -1553,10 +1559,11 @@ int fip_batch_autotune(fip_batch* b, const float* const* vis_re, const float* co
 }
 
 int fip_batch_tuning(const fip_batch* b, int* fft_values_per_thread, int* fft_split,
-                     int* grid_ctas_per_sm) {
+                     int* fft_direct, int* grid_ctas_per_sm) {
   if (!b) return fail(FIP_ERR_ARG, "null batch");
   if (fft_values_per_thread) *fft_values_per_thread = b->fft.e;
   if (fft_split) *fft_split = b->fft.split;
+  if (fft_direct) *fft_direct = b->fft.direct;
   if (grid_ctas_per_sm)
     *grid_ctas_per_sm = b->grid_ctas_per_sm > 0
                             ? b->grid_ctas_per_sm

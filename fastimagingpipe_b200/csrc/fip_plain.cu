@@ -774,7 +774,7 @@ __host__ __device__ constexpr int fft_min_blocks() {
   return fft_threads<LM, LE>() >= 768 && LE == 4 ? 1 : 2;
 }
 
-template <int LM, int LE>
+template <int LM, int LE, bool DIRECT>
 __global__ void __launch_bounds__(fft_threads<LM, LE>(), fft_min_blocks<LM, LE>())
     k_fft_cols(const float2* __restrict__ H, const unsigned* __restrict__ bbox,
                float2* __restrict__ P, const float2* __restrict__ tw, size_t grid_stride,
@@ -792,15 +792,18 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), fft_min_blocks<LM, LE>(
   // Row band [lo, hi]; row -G/2 is row +G/2 (counted once).
   const int lo = (k1 == half) ? 1 - k1 : -k1, hi = k1;
   const float2* col = H + (size_t)c * g;
-  // Stage the band densely (coalesced): st[r - lo] = H[c][r mod G].
+  // Stage the band densely (coalesced): st[r - lo] = H[c][r mod G]; or
+  // (DIRECT) read it from global memory in the first pass.
   float2* st = s_fft + fipfft::stage_offset(g);
-  for (int i = threadIdx.x; i <= hi - lo; i += NT) {
-    const int r = i + lo;
-    st[i] = col[r < 0 ? r + g : r];
+  if (!DIRECT) {
+    for (int i = threadIdx.x; i <= hi - lo; i += NT) {
+      const int r = i + lo;
+      st[i] = col[r < 0 ? r + g : r];
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  auto load = [&](int r) -> float2 { return st[r - lo]; };
-  fipfft::run<LM, LE>(s_fft, tw, lo, hi, load);
+  auto load = [&](int r) -> float2 { return DIRECT ? col[r < 0 ? r + g : r] : st[r - lo]; };
+  fipfft::run<LM, LE, DIRECT>(s_fft, tw, lo, hi, load);
   float4* out = reinterpret_cast<float4*>(P + (size_t)c * n);
   for (int o2 = threadIdx.x; o2 < n / 2; o2 += NT) {
     const float2 a = fipfft::fetch<LM, LE>(s_fft, 2 * o2);
@@ -816,7 +819,7 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), fft_min_blocks<LM, LE>(
 // is |out| / (taper|x| taper|y| norm^2) (the checkerboard signs cancel
 // against the centred grid origin), applied as a product of the reciprocal
 // table rck[t] = 1 / (taper[t] norm).
-template <int LM, int LE>
+template <int LM, int LE, bool DIRECT>
 __global__ void __launch_bounds__(fft_threads<LM, LE>(), fft_min_blocks<LM, LE>())
     k_fft_rows(const float2* __restrict__ P, unsigned* bbox,
                const float* __restrict__ rck, float* __restrict__ pre,
@@ -835,19 +838,32 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), fft_min_blocks<LM, LE>(
   // one 16-byte load per occupied column c (the column pass stores
   // P[c][yy]), written at c and -c.
   float2* st = s_fft + fipfft::stage_offset(g);
-  for (int c = threadIdx.x; c <= k2; c += NT) {
-    const float4 ab = *reinterpret_cast<const float4*>(P + (size_t)c * n + yy1);
+  if (!DIRECT) {
+    for (int c = threadIdx.x; c <= k2; c += NT) {
+      const float4 ab = *reinterpret_cast<const float4*>(P + (size_t)c * n + yy1);
+      float ay = ab.y, by = ab.w;
+      if (c == 0 || c == half) {  // self-conjugate bins are real
+        ay = 0.f;
+        by = 0.f;
+      }
+      st[c - lo] = make_float2(ab.x - by, ay + ab.z);
+      if (c > 0 && -c >= lo) st[-c - lo] = make_float2(ab.x + by, ab.z - ay);  // conj X1 + i conj X2
+    }
+    __syncthreads();
+  }
+  // DIRECT: Z[c] straight from the column-pass output (L2-resident).
+  auto zval = [&](int c) -> float2 {
+    const int a = c < 0 ? -c : c;
+    const float4 ab = *reinterpret_cast<const float4*>(P + (size_t)a * n + yy1);
     float ay = ab.y, by = ab.w;
-    if (c == 0 || c == half) {  // self-conjugate bins are real
+    if (a == 0 || a == half) {
       ay = 0.f;
       by = 0.f;
     }
-    st[c - lo] = make_float2(ab.x - by, ay + ab.z);
-    if (c > 0 && -c >= lo) st[-c - lo] = make_float2(ab.x + by, ab.z - ay);  // conj X1 + i conj X2
-  }
-  __syncthreads();
-  auto load = [&](int c) -> float2 { return st[c - lo]; };
-  fipfft::run<LM, LE>(s_fft, tw, lo, hi, load);
+    return c >= 0 ? make_float2(ab.x - by, ay + ab.z) : make_float2(ab.x + by, ab.z - ay);
+  };
+  auto load = [&](int c) -> float2 { return DIRECT ? zval(c) : st[c - lo]; };
+  fipfft::run<LM, LE, DIRECT>(s_fft, tw, lo, hi, load);
   const float ry1 = rck[abs(yy1 - h)], ry2 = rck[abs(yy1 + 1 - h)];
   float4* row1 = reinterpret_cast<float4*>(pre + (size_t)yy1 * n);
   float4* row2 = reinterpret_cast<float4*>(pre + (size_t)(yy1 + 1) * n);
@@ -1502,6 +1518,7 @@ bool fip_fft_plan(int g, fipfft::Plan& p, int values_per_thread) {
   p.e = 1 << le;
   p.nt = 3 * (m >> le);
   p.split = 0;
+  p.direct = 0;
   return true;
 }
 
@@ -1646,7 +1663,7 @@ static cudaError_t fft_smem_attr(const void* fn, int g, size_t& smem) {
 template <int LM, int LE>
 static cudaError_t launch_cols(const FipGeom& geo, const float2* grid, const unsigned* bbox,
                                float2* colbuf, const float2* tw, cudaStream_t s, int batch,
-                               size_t grid_stride, size_t col_stride, int split) {
+                               size_t grid_stride, size_t col_stride, int split, int direct) {
   size_t smem;
   cudaError_t e;
   if (split) {
@@ -1657,9 +1674,16 @@ static cudaError_t launch_cols(const FipGeom& geo, const float2* grid, const uns
         grid, bbox, colbuf, tw, grid_stride, col_stride);
     return cudaGetLastError();
   }
-  e = fft_smem_attr((const void*)k_fft_cols<LM, LE>, geo.g, smem);
+  if (direct) {
+    e = fft_smem_attr((const void*)k_fft_cols<LM, LE, true>, geo.g, smem);
+    if (e != cudaSuccess) return e;
+    k_fft_cols<LM, LE, true><<<dim3(geo.hp, batch), fft_threads<LM, LE>(), smem, s>>>(
+        grid, bbox, colbuf, tw, grid_stride, col_stride);
+    return cudaGetLastError();
+  }
+  e = fft_smem_attr((const void*)k_fft_cols<LM, LE, false>, geo.g, smem);
   if (e != cudaSuccess) return e;
-  k_fft_cols<LM, LE><<<dim3(geo.hp, batch), fft_threads<LM, LE>(), smem, s>>>(
+  k_fft_cols<LM, LE, false><<<dim3(geo.hp, batch), fft_threads<LM, LE>(), smem, s>>>(
       grid, bbox, colbuf, tw, grid_stride, col_stride);
   return cudaGetLastError();
 }
@@ -1668,7 +1692,7 @@ template <int LM, int LE>
 static cudaError_t launch_rows(const FipGeom& geo, const float2* colbuf, unsigned* bbox,
                                const float* taper, const float2* tw, float* pre,
                                cudaStream_t s, int batch, size_t col_stride,
-                               size_t pre_stride, int split) {
+                               size_t pre_stride, int split, int direct) {
   size_t smem;
   cudaError_t e;
   if (split) {
@@ -1679,9 +1703,16 @@ static cudaError_t launch_rows(const FipGeom& geo, const float2* colbuf, unsigne
         colbuf, bbox, taper + geo.n / 2 + 1, pre, tw, col_stride, pre_stride);
     return cudaGetLastError();
   }
-  e = fft_smem_attr((const void*)k_fft_rows<LM, LE>, geo.g, smem);
+  if (direct) {
+    e = fft_smem_attr((const void*)k_fft_rows<LM, LE, true>, geo.g, smem);
+    if (e != cudaSuccess) return e;
+    k_fft_rows<LM, LE, true><<<dim3(geo.n / 2, batch), fft_threads<LM, LE>(), smem, s>>>(
+        colbuf, bbox, taper + geo.n / 2 + 1, pre, tw, col_stride, pre_stride);
+    return cudaGetLastError();
+  }
+  e = fft_smem_attr((const void*)k_fft_rows<LM, LE, false>, geo.g, smem);
   if (e != cudaSuccess) return e;
-  k_fft_rows<LM, LE><<<dim3(geo.n / 2, batch), fft_threads<LM, LE>(), smem, s>>>(
+  k_fft_rows<LM, LE, false><<<dim3(geo.n / 2, batch), fft_threads<LM, LE>(), smem, s>>>(
       colbuf, bbox, taper + geo.n / 2 + 1, pre, tw, col_stride, pre_stride);
   return cudaGetLastError();
 }
@@ -1717,7 +1748,8 @@ cudaError_t fip_launch_fft_cols(const FipGeom& geo, const float2* grid, const un
                                 size_t col_stride) {
   if (plan.g != geo.g || batch < 1 || batch > 65535) return cudaErrorInvalidValue;
   FIP_FFT_SWITCH(plan, (launch_cols<LM_, LE_>(geo, grid, bbox, colbuf, twiddles, s, batch,
-                                              grid_stride, col_stride, plan.split)));
+                                              grid_stride, col_stride, plan.split,
+                                              plan.direct)));
 }
 
 cudaError_t fip_launch_fft_rows(const FipGeom& geo, const float2* colbuf, unsigned* bbox,
@@ -1726,7 +1758,8 @@ cudaError_t fip_launch_fft_rows(const FipGeom& geo, const float2* colbuf, unsign
                                 size_t col_stride, size_t pre_stride) {
   if (plan.g != geo.g || batch < 1 || batch > 65535) return cudaErrorInvalidValue;
   FIP_FFT_SWITCH(plan, (launch_rows<LM_, LE_>(geo, colbuf, bbox, taper, twiddles, pre, s, batch,
-                                              col_stride, pre_stride, plan.split)));
+                                              col_stride, pre_stride, plan.split,
+                                              plan.direct)));
 }
 
 cudaError_t fip_launch_correct_c2r(const FipGeom& geo, const float* fft_out, const float* taper,

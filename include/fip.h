@@ -182,18 +182,20 @@ int fip_imager_grid_side(const fip_imager* im);
  * once (device buffers, as fip_image_snapshot), then times the launch shapes
  * that do not change the arithmetic beyond rounding -- the transform's complex
  * values per thread (8 or 16), one CTA per transform or one per sub-transform
- * (fft_split), and the persistent gridder's CTAs per SM -- on
+ * (fft_split), the first pass reading a staged band or global memory
+ * (fft_direct), and the persistent gridder's CTAs per SM -- on
  * that snapshot's band and bins, and keeps the fastest for later calls.
  * Synchronous; overwrites the imager's trigger ring, so call it before a run
  * of snapshots, not inside one.  fip_imager_tuning reports the choice. */
 int fip_imager_autotune(fip_imager* im, const float* vis_re, const float* vis_im,
                         const float* B, const float* V, size_t nb, void* stream);
 int fip_imager_tuning(const fip_imager* im, int* fft_values_per_thread, int* fft_split,
-                      int* grid_ctas_per_sm);
+                      int* fft_direct, int* grid_ctas_per_sm);
 /* Pins the launch shapes instead (values per thread 8 or 16, or 0 for the
- * default; split 0 or 1; gridder CTAs per SM, 0 for the most that fit). */
+ * default; split 0 or 1; direct first pass 0 or 1 (joint form only); gridder
+ * CTAs per SM, 0 for the most that fit). */
 int fip_imager_set_tuning(fip_imager* im, int fft_values_per_thread, int fft_split,
-                          int grid_ctas_per_sm);
+                          int fft_direct, int grid_ctas_per_sm);
 
 /* ---- Batching form (no counterpart in the reference) ----------------------
  * Many snapshots of one image size per call: one persistent gridding launch
@@ -225,7 +227,7 @@ int fip_batch_autotune(fip_batch* b, const float* const* vis_re, const float* co
                        const float* const* B, const float* const* V, const size_t* nb,
                        size_t count, void* stream);
 int fip_batch_tuning(const fip_batch* b, int* fft_values_per_thread, int* fft_split,
-                     int* grid_ctas_per_sm);
+                     int* fft_direct, int* grid_ctas_per_sm);
 
 /* Per-pixel targets (LL, MM) of the reprojection, [N*N][2] (device), for
  * tests: exact = 0 the plain form's FP32 chain, 1 the exact closed form. */

@@ -329,8 +329,9 @@ def test_profiling_and_launch_count(cuda, tiny):
             assert st[k][1] >= 1 and st[k][0] > 0
 
 
-@pytest.mark.parametrize("vpt,split,ctas", [(8, 0, 3), (16, 0, 2), (8, 1, 1), (16, 1, 3)])
-def test_every_launch_shape_gives_the_same_results(cuda, small, vpt, split, ctas):
+@pytest.mark.parametrize("vpt,split,direct,ctas", [(8, 0, 0, 3), (16, 0, 0, 2), (8, 1, 0, 1),
+                                                   (16, 1, 0, 3), (8, 0, 1, 2), (16, 0, 1, 3)])
+def test_every_launch_shape_gives_the_same_results(cuda, small, vpt, split, direct, ctas):
     """Transform values per thread, split/joint transform and gridder CTAs per SM
     change rounding only."""
     import torch
@@ -340,9 +341,9 @@ def test_every_launch_shape_gives_the_same_results(cuda, small, vpt, split, ctas
     ref, got = torch.zeros(u * u, device=cuda), torch.zeros(u * u, device=cuda)
     with fip.Imager(n, nb, small.cell_size, t) as im:
         im.pipe_device(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, ref)
-        im.set_tuning(vpt, split, ctas)
+        im.set_tuning(vpt, split, ctas, direct)
         assert im.tuning() == {"fft_values_per_thread": vpt, "fft_split": split,
-                               "grid_ctas_per_sm": ctas}
+                               "fft_direct": direct, "grid_ctas_per_sm": ctas}
         im.pipe_device(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, got)
         torch.cuda.synchronize()
     assert np.abs(got.cpu().numpy() - ref.cpu().numpy()).max() <= 1e-5
