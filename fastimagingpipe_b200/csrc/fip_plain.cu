@@ -538,7 +538,8 @@ struct GridSmem {
 // loads the item's visibilities and their separable kernel values into
 // shared memory (all loads in flight at once); phase 2 lets each warp spread
 // one visibility's taps over its lanes into the shared tile; phase 3 commits.
-// COMP: Neumaier-compensated tile sums (precision form).
+// COMP: compensated tile sums of the precision form (exact two-limb fixed
+// point, below).
 template <int VT, bool COMP>
 __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_cim,
                                           const float* __restrict__ B, const void* vr,
@@ -596,27 +597,46 @@ __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_ci
         S.k2[q][b] = fipref::es((static_cast<float>(r2) - f.p2) * ihs);
       }
   }
-  // Plain form: the tile sums are fixed point, q = round(tap * 2^30 / bound),
-  // so every cell (|sum| <= bound) stays within int32 and the shared-memory
-  // sums are native integer atomics (exact, order-independent); resolution
-  // 2^-30 of the item's summed weights.  Precision form: Neumaier-compensated
-  // FP32.
+  // The tile sums are fixed point, so the shared-memory sums are native
+  // integer atomics: exact and independent of their order.  `bound` (the
+  // item's summed weights) bounds every cell sum.
+  // Plain form: q = round(tap * 2^30 / bound) in one int32; resolution 2^-30
+  // of the bound.
+  // Precision form (compensated sums): t = tap * 2^e, 2^e = the power of two
+  // with bound * 2^e < 2^45, is exact in FP32 and is split exactly into
+  // hi * 2^23 + lo (hi < 2^22 in magnitude, 0 <= lo <= 2^23), two int32 limbs
+  // summed separately (at most 256 taps per cell per item: no overflow), so a
+  // cell holds the exact sum of its FP32 taps to 2^-45 of the bound and is
+  // rounded once at the commit.
+  for (int o = 16; o > 0; o >>= 1) bound += __shfl_xor_sync(0xffffffffu, bound, o);
+  if (lane == 0) S.bound[warp] = bound;
+  __syncthreads();
+  float tot = 0.f;
+#pragma unroll
+  for (int w = 0; w < kThreads / 32; ++w) tot += S.bound[w];
+  tot *= 1.0001f;  // margin for the rounding of the weights and their sum
   float fx = 0.f, fx_inv = 0.f;
   if (!COMP) {
-    for (int o = 16; o > 0; o >>= 1) bound += __shfl_xor_sync(0xffffffffu, bound, o);
-    if (lane == 0) S.bound[warp] = bound;
-  }
-  __syncthreads();
-  if (!COMP) {
-    float tot = 0.f;
-#pragma unroll
-    for (int w = 0; w < kThreads / 32; ++w) tot += S.bound[w];
-    tot *= 1.0001f;  // margin for the rounding of the weights and their sum
     fx = tot > 0.f ? 1073741824.0f / tot : 0.f;
     fx_inv = tot * (1.0f / 1073741824.0f);
+  } else if (tot > 0.f) {
+    int ex = 0;
+    frexpf(tot, &ex);  // tot < 2^ex
+    fx = ldexpf(1.0f, 45 - ex);
+    fx_inv = ldexpf(1.0f, ex - 45);
   }
   int* s_qre = reinterpret_cast<int*>(S.re);
   int* s_qim = reinterpret_cast<int*>(S.im);
+  unsigned* s_lre = reinterpret_cast<unsigned*>(s_cre);
+  unsigned* s_lim = reinterpret_cast<unsigned*>(s_cim);
+  // Exact limbs of t = x * 2^e (see above).
+  auto limbs = [&](float x, int& hi, unsigned& lo) {
+    const float t = x * fx;
+    const float hf = floorf(t * (1.0f / 8388608.0f));
+    const float lf = fmaf(hf, -8388608.0f, t);  // exact: t - hi 2^23 in [0, 2^23]
+    hi = __float_as_int(hf + 12582912.0f) - 0x4B400000;  // |hf| < 2^22: exact
+    lo = __float_as_uint(lf + 8388608.0f) - 0x4B000000u;  // round to integer
+  };
   // Phase 2.
   for (int q = warp; q < cnt; q += kThreads / 32) {
     const int meta = S.meta[q];
@@ -641,14 +661,14 @@ __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_ci
         if (qr) atomicAdd(&s_qre[cell], qr);
         if (qi) atomicAdd(&s_qim[cell], qi);
       } else {
-        float o = atomicAdd(&S.re[cell], cr);
-        float sm = o + cr;
-        float err = (fabsf(o) >= fabsf(cr)) ? (o - sm) + cr : (cr - sm) + o;
-        atomicAdd(&s_cre[cell], err);
-        o = atomicAdd(&S.im[cell], ci);
-        sm = o + ci;
-        err = (fabsf(o) >= fabsf(ci)) ? (o - sm) + ci : (ci - sm) + o;
-        atomicAdd(&s_cim[cell], err);
+        int hr, hi;
+        unsigned lr2, li2;
+        limbs(cr, hr, lr2);
+        limbs(ci, hi, li2);
+        if (hr) atomicAdd(&s_qre[cell], hr);
+        if (lr2) atomicAdd(&s_lre[cell], lr2);
+        if (hi) atomicAdd(&s_qim[cell], hi);
+        if (li2) atomicAdd(&s_lim[cell], li2);
       }
     }
   }
@@ -662,8 +682,9 @@ __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_ci
     if (row < g && col < hp) {
       float2 val;
       if (COMP) {
-        val = make_float2(S.re[lr * kTS + lc] + s_cre[lr * kTS + lc],
-                          S.im[lr * kTS + lc] + s_cim[lr * kTS + lc]);
+        const int at = lr * kTS + lc;
+        val = make_float2((float)(((double)s_qre[at] * 8388608.0 + (double)s_lre[at]) * fx_inv),
+                          (float)(((double)s_qim[at] * 8388608.0 + (double)s_lim[at]) * fx_inv));
       } else {
         val = make_float2((float)s_qre[lr * kTS + lc] * fx_inv,
                           (float)s_qim[lr * kTS + lc] * fx_inv);
