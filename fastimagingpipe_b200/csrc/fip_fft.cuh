@@ -47,6 +47,8 @@ __host__ __device__ constexpr int sub_stride(int m) { return m + m / 16 + 6; }
 // pass does not write.
 __host__ __device__ constexpr int stage_offset(int g) { return 3 * sub_stride(g / 3); }
 __host__ __device__ constexpr int smem_elems(int g) { return 6 * sub_stride(g / 3) + 16; }
+// The direct form (no staging) keeps one buffer.
+__host__ __device__ constexpr int direct_smem_elems(int g) { return 3 * sub_stride(g / 3) + 16; }
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -278,6 +280,18 @@ __device__ __forceinline__ void passes(float2 (&v)[1 << LE], float2* base,
     }
     if constexpr (Q + 1 < NP) {
       load_smem<(1 << pass_lr<LM, LE>(Q + 1)), E>(v, sub, M, lt, TS);
+      if constexpr (BUF == 0) {  // one buffer: the next stores wait for these loads
+        if constexpr (GROUP && TS % 32 == 0) {
+          if (s == 0)
+            asm volatile("bar.sync 1, %0;" ::"n"(TS) : "memory");
+          else if (s == 1)
+            asm volatile("bar.sync 2, %0;" ::"n"(TS) : "memory");
+          else
+            asm volatile("bar.sync 3, %0;" ::"n"(TS) : "memory");
+        } else {
+          __syncthreads();
+        }
+      }
       passes<LM, LE, Q + 1, BUF, GROUP>(v, base, tw, lt, s);
     }
   }
@@ -290,7 +304,8 @@ __device__ __forceinline__ void passes(float2 (&v)[1 << LE], float2* base,
 // must call it; sm holds smem_elems(G) float2.  Ends with a barrier: sm is
 // then ready for fetch().
 // DIRECT: load() reads global memory (no staged band), so the passes may
-// use group barriers.
+// use group barriers, and one buffer (sm holds direct_smem_elems(G)) serves
+// all passes.
 template <int LM, int LE, bool DIRECT = false, class Load>
 __device__ __forceinline__ void run(float2* sm, const float2* __restrict__ tw, int lo, int hi,
                                     Load& load) {
@@ -304,15 +319,16 @@ __device__ __forceinline__ void run(float2* sm, const float2* __restrict__ tw, i
     first_load<R0, E, M, true>(v, s, lt, lo, hi, tw, load);
   else
     first_load<R0, E, M, false>(v, s, lt, lo, hi, tw, load);
-  passes<LM, LE, 0, stage_offset(3 * M), DIRECT>(v, sm + s * sub_stride(M), tw, lt, s);
+  passes<LM, LE, 0, DIRECT ? 0 : stage_offset(3 * M), DIRECT>(v, sm + s * sub_stride(M), tw,
+                                                                 lt, s);
 }
 
 // Output o in [0, 2M) after run(): X[p] with p = o - M, i.e. Y_s[q] for
 // (p mod G) = 3 q + s, in the buffer of the last pass.
-template <int LM, int LE>
+template <int LM, int LE, bool DIRECT = false>
 __device__ __forceinline__ float2 fetch(const float2* sm, int o) {
   constexpr int M = 1 << LM;
-  constexpr int last = (pass_count<LM, LE>() - 1) & 1;
+  constexpr int last = DIRECT ? 0 : (pass_count<LM, LE>() - 1) & 1;
   int pp = o - M;
   if (pp < 0) pp += 3 * M;
   const int q = pp / 3, s = pp - 3 * q;

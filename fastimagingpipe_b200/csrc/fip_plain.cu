@@ -790,13 +790,16 @@ __device__ __forceinline__ void block_max_to(float v, unsigned* out) {
 // ---------------------------------------------------------------------------
 template <int LM, int LE>
 __host__ __device__ constexpr int fft_threads() { return 3 << (LM - LE); }
-template <int LM, int LE>
+// CTAs per SM the register budget allows: the staged forms hold two
+// buffers of shared memory (two CTAs of 768 or 384 threads); the direct form
+// holds one, so three CTAs of 384 threads fit.
+template <int LM, int LE, bool DIRECT>
 __host__ __device__ constexpr int fft_min_blocks() {
-  return fft_threads<LM, LE>() >= 768 && LE == 4 ? 1 : 2;
+  return fft_threads<LM, LE>() >= 768 && LE == 4 ? 1 : (DIRECT && LE == 4 ? 3 : 2);
 }
 
 template <int LM, int LE, bool DIRECT>
-__global__ void __launch_bounds__(fft_threads<LM, LE>(), fft_min_blocks<LM, LE>())
+__global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE, DIRECT>()))
     k_fft_cols(const float2* __restrict__ H, const unsigned* __restrict__ bbox,
                float2* __restrict__ P, const float2* __restrict__ tw, size_t grid_stride,
                size_t col_stride) {
@@ -827,8 +830,8 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), fft_min_blocks<LM, LE>(
   fipfft::run<LM, LE, DIRECT>(s_fft, tw, lo, hi, load);
   float4* out = reinterpret_cast<float4*>(P + (size_t)c * n);
   for (int o2 = threadIdx.x; o2 < n / 2; o2 += NT) {
-    const float2 a = fipfft::fetch<LM, LE>(s_fft, 2 * o2);
-    const float2 b = fipfft::fetch<LM, LE>(s_fft, 2 * o2 + 1);
+    const float2 a = fipfft::fetch<LM, LE, DIRECT>(s_fft, 2 * o2);
+    const float2 b = fipfft::fetch<LM, LE, DIRECT>(s_fft, 2 * o2 + 1);
     out[o2] = make_float4(a.x, a.y, b.x, b.y);
   }
 }
@@ -841,7 +844,7 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), fft_min_blocks<LM, LE>(
 // against the centred grid origin), applied as a product of the reciprocal
 // table rck[t] = 1 / (taper[t] norm).
 template <int LM, int LE, bool DIRECT>
-__global__ void __launch_bounds__(fft_threads<LM, LE>(), fft_min_blocks<LM, LE>())
+__global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE, DIRECT>()))
     k_fft_rows(const float2* __restrict__ P, unsigned* bbox,
                const float* __restrict__ rck, float* __restrict__ pre,
                const float2* __restrict__ tw, size_t col_stride, size_t pre_stride) {
@@ -894,7 +897,7 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), fft_min_blocks<LM, LE>(
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       const int o = 4 * o4 + e;
-      const float2 v = fipfft::fetch<LM, LE>(s_fft, o);
+      const float2 v = fipfft::fetch<LM, LE, DIRECT>(s_fft, o);
       const float rx = rck[abs(o - h)];
       a[e] = fabsf(v.x * (rx * ry1));
       b[e] = fabsf(v.y * (rx * ry2));
@@ -1698,6 +1701,7 @@ static cudaError_t launch_cols(const FipGeom& geo, const float2* grid, const uns
   if (direct) {
     e = fft_smem_attr((const void*)k_fft_cols<LM, LE, true>, geo.g, smem);
     if (e != cudaSuccess) return e;
+    smem = (size_t)fipfft::direct_smem_elems(geo.g) * sizeof(float2);
     k_fft_cols<LM, LE, true><<<dim3(geo.hp, batch), fft_threads<LM, LE>(), smem, s>>>(
         grid, bbox, colbuf, tw, grid_stride, col_stride);
     return cudaGetLastError();
@@ -1727,6 +1731,7 @@ static cudaError_t launch_rows(const FipGeom& geo, const float2* colbuf, unsigne
   if (direct) {
     e = fft_smem_attr((const void*)k_fft_rows<LM, LE, true>, geo.g, smem);
     if (e != cudaSuccess) return e;
+    smem = (size_t)fipfft::direct_smem_elems(geo.g) * sizeof(float2);
     k_fft_rows<LM, LE, true><<<dim3(geo.n / 2, batch), fft_threads<LM, LE>(), smem, s>>>(
         colbuf, bbox, taper + geo.n / 2 + 1, pre, tw, col_stride, pre_stride);
     return cudaGetLastError();
