@@ -240,6 +240,33 @@ def test_host_and_device_entry_points_agree(cuda, tiny):
     assert np.abs(out.cpu().numpy().reshape(u, u) - res).max() <= 1e-6
 
 
+@pytest.mark.parametrize("kw", [{}, dict(form=fip.FORM_PRECISE, vis_storage=fip.STORE_F16)])
+def test_concurrent_lanes_match_single_snapshot_calls(cuda, small, kw):
+    """pipe_device / pipe_host image the three snapshots on concurrent lanes;
+    back-to-back calls with different inputs must each give the result of the
+    one-snapshot-at-a-time path."""
+    import torch
+    other = synthetic.config_small(transient_snapshot=1, seed=7)
+    n, nb, t = small.image_size, small.num_baselines, small.unit_size
+    u = n // t
+    ref_a, _, _ = run(small, cuda, **kw)
+    ref_b, _, _ = run(other, cuda, **kw)
+    da, db = to_dev(small, cuda), to_dev(other, cuda)
+    ra, rb = torch.zeros(u * u, device=cuda), torch.zeros(u * u, device=cuda)
+    with fip.Imager(n, nb, small.cell_size, t, **kw) as im:
+        for _ in range(2):
+            im.pipe_device(da["vis_re"], da["vis_im"], da["B"], da["V"], nb, ra)
+            im.pipe_device(db["vis_re"], db["vis_im"], db["B"], db["V"], nb, rb)
+        hb = im.pipe_host(other.vis_re, other.vis_im, other.B, other.V, nb)
+        ha = im.pipe_host(small.vis_re, small.vis_im, small.B, small.V, nb)
+        torch.cuda.synchronize()
+    tol = 1e-5
+    assert np.abs(ra.cpu().numpy().reshape(u, u) - ref_a).max() <= tol
+    assert np.abs(rb.cpu().numpy().reshape(u, u) - ref_b).max() <= tol
+    assert np.abs(ha - ref_a).max() <= tol
+    assert np.abs(hb - ref_b).max() <= tol
+
+
 def test_sequence_matches_triples(cuda):
     import torch
     snap = synthetic.config_tiny(n_snap=5, transient_snapshot=3)
