@@ -323,6 +323,50 @@ __device__ __forceinline__ void run(float2* sm, const float2* __restrict__ tw, i
                                                                  lt, s);
 }
 
+// Pre-twiddled staging, for bands no wider than M (each n then receives one
+// c at most): the staging loop writes y_s[n] = z[c] w^{c s} (n = c mod M) for
+// s = 0, 1, 2 at pre + s * sub_stride(M) + sidx(n), pre = sm + stage_offset(G),
+// and zeros where no c lands (zero_pre); the first pass is then a plain
+// shared-memory read.
+template <int M>
+__device__ __forceinline__ void stage_pre(float2* pre, int c, float2 z,
+                                          const float2* __restrict__ tw) {
+  constexpr int G = 3 * M;
+  const int nn = c < 0 ? c + M : c;
+  const float2 w1 = __ldg(&tw[c < 0 ? c + G : c]);
+  const int c2 = 2 * c;
+  const float2 w2 = __ldg(&tw[c2 < 0 ? c2 + G : c2]);
+  pre[sidx(nn)] = z;
+  pre[sub_stride(M) + sidx(nn)] = cmul(z, w1);
+  pre[2 * sub_stride(M) + sidx(nn)] = cmul(z, w2);
+}
+template <int M>
+__device__ __forceinline__ void zero_pre(float2* pre, int lo, int hi, int tid, int nt) {
+  for (int nn = hi + 1 + tid; nn < M + lo; nn += nt) {
+    pre[sidx(nn)] = make_float2(0.f, 0.f);
+    pre[sub_stride(M) + sidx(nn)] = make_float2(0.f, 0.f);
+    pre[2 * sub_stride(M) + sidx(nn)] = make_float2(0.f, 0.f);
+  }
+}
+
+template <int LM, int LE>
+__device__ __forceinline__ void run_pre(float2* sm, const float2* __restrict__ tw) {
+  constexpr int E = 1 << LE, M = 1 << LM, TS = M / E;
+  constexpr int R0 = 1 << pass_lr<LM, LE>(0);
+  const int tid = threadIdx.x;
+  const int s = tid >= 2 * TS ? 2 : (tid >= TS ? 1 : 0);
+  const int lt = tid - s * TS;
+  const float2* pre = sm + stage_offset(3 * M) + s * sub_stride(M);
+  float2 v[E];
+#pragma unroll
+  for (int b = 0; b < E / R0; ++b) {
+    const int j = lt + b * TS;
+#pragma unroll
+    for (int k = 0; k < R0; ++k) v[b * R0 + k] = pre[sidx(j + k * (M / R0))];
+  }
+  passes<LM, LE, 0, stage_offset(3 * M), false>(v, sm + s * sub_stride(M), tw, lt, s);
+}
+
 // Output o in [0, 2M) after run(): X[p] with p = o - M, i.e. Y_s[q] for
 // (p mod G) = 3 q + s, in the buffer of the last pass.
 template <int LM, int LE, bool DIRECT = false>

@@ -818,16 +818,29 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
   const float2* col = H + (size_t)c * g;
   // Stage the band densely (coalesced): st[r - lo] = H[c][r mod G]; or
   // (DIRECT) read it from global memory in the first pass.
+  // A band no wider than M is staged pre-twiddled for the three
+  // sub-transforms (fipfft::stage_pre).
   float2* st = s_fft + fipfft::stage_offset(g);
-  if (!DIRECT) {
+  const bool fold = !DIRECT && hi - lo + 1 <= M;
+  if (fold) {
     for (int i = threadIdx.x; i <= hi - lo; i += NT) {
       const int r = i + lo;
-      st[i] = col[r < 0 ? r + g : r];
+      fipfft::stage_pre<M>(st, r, col[r < 0 ? r + g : r], tw);
     }
+    fipfft::zero_pre<M>(st, lo, hi, threadIdx.x, NT);
     __syncthreads();
+    fipfft::run_pre<LM, LE>(s_fft, tw);
+  } else {
+    if (!DIRECT) {
+      for (int i = threadIdx.x; i <= hi - lo; i += NT) {
+        const int r = i + lo;
+        st[i] = col[r < 0 ? r + g : r];
+      }
+      __syncthreads();
+    }
+    auto load = [&](int r) -> float2 { return DIRECT ? col[r < 0 ? r + g : r] : st[r - lo]; };
+    fipfft::run<LM, LE, DIRECT>(s_fft, tw, lo, hi, load);
   }
-  auto load = [&](int r) -> float2 { return DIRECT ? col[r < 0 ? r + g : r] : st[r - lo]; };
-  fipfft::run<LM, LE, DIRECT>(s_fft, tw, lo, hi, load);
   float4* out = reinterpret_cast<float4*>(P + (size_t)c * n);
   for (int o2 = threadIdx.x; o2 < n / 2; o2 += NT) {
     const float2 a = fipfft::fetch<LM, LE, DIRECT>(s_fft, 2 * o2);
@@ -862,6 +875,8 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
   // one 16-byte load per occupied column c (the column pass stores
   // P[c][yy]), written at c and -c.
   float2* st = s_fft + fipfft::stage_offset(g);
+  // A band no wider than M is staged pre-twiddled (fipfft::stage_pre).
+  const bool fold = !DIRECT && hi - lo + 1 <= M;
   if (!DIRECT) {
     for (int c = threadIdx.x; c <= k2; c += NT) {
       const float4 ab = *reinterpret_cast<const float4*>(P + (size_t)c * n + yy1);
@@ -870,9 +885,17 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
         ay = 0.f;
         by = 0.f;
       }
-      st[c - lo] = make_float2(ab.x - by, ay + ab.z);
-      if (c > 0 && -c >= lo) st[-c - lo] = make_float2(ab.x + by, ab.z - ay);  // conj X1 + i conj X2
+      const float2 zp = make_float2(ab.x - by, ay + ab.z);
+      const float2 zm = make_float2(ab.x + by, ab.z - ay);  // conj X1 + i conj X2
+      if (fold) {
+        fipfft::stage_pre<M>(st, c, zp, tw);
+        if (c > 0 && -c >= lo) fipfft::stage_pre<M>(st, -c, zm, tw);
+      } else {
+        st[c - lo] = zp;
+        if (c > 0 && -c >= lo) st[-c - lo] = zm;
+      }
     }
+    if (fold) fipfft::zero_pre<M>(st, lo, hi, threadIdx.x, NT);
     __syncthreads();
   }
   // DIRECT: Z[c] straight from the column-pass output (L2-resident).
@@ -887,7 +910,10 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
     return c >= 0 ? make_float2(ab.x - by, ay + ab.z) : make_float2(ab.x + by, ab.z - ay);
   };
   auto load = [&](int c) -> float2 { return DIRECT ? zval(c) : st[c - lo]; };
-  fipfft::run<LM, LE, DIRECT>(s_fft, tw, lo, hi, load);
+  if (fold)
+    fipfft::run_pre<LM, LE>(s_fft, tw);
+  else
+    fipfft::run<LM, LE, DIRECT>(s_fft, tw, lo, hi, load);
   const float ry1 = rck[abs(yy1 - h)], ry2 = rck[abs(yy1 + 1 - h)];
   float4* row1 = reinterpret_cast<float4*>(pre + (size_t)yy1 * n);
   float4* row2 = reinterpret_cast<float4*>(pre + (size_t)(yy1 + 1) * n);
