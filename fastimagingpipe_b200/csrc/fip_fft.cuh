@@ -176,27 +176,43 @@ __device__ __forceinline__ void butterflies(float2 (&v)[E], const float2* __rest
   }
 }
 
-template <int R, int E>
-__device__ __forceinline__ void store_smem(const float2 (&v)[E], float2* sm, int lns, int lt,
-                                           int ts) {
-  const int ns = 1 << lns;
+// Stockham store of pass outputs: butterfly j's output q goes to
+// d + q ns, d = (j / ns) ns R + (j mod ns).  When ns is a multiple of 16 the
+// padded index of d + q ns is sidx(d) + q ns 17/16 (no per-element shift).
+template <int R, int E, int LNS>
+__device__ __forceinline__ void store_smem(const float2 (&v)[E], float2* sm, int lt, int ts) {
+  constexpr int ns = 1 << LNS;
 #pragma unroll
   for (int b = 0; b < E / R; ++b) {
     const int j = lt + b * ts;
-    const int d = ((j >> lns) << (lns + log2c<R>())) + (j & (ns - 1));
+    const int d = ((j >> LNS) << (LNS + log2c<R>())) + (j & (ns - 1));
+    if constexpr (ns % 16 == 0) {
+      float2* base = sm + sidx(d);
 #pragma unroll
-    for (int q = 0; q < R; ++q) sm[sidx(d + q * ns)] = v[b * R + q];
+      for (int q = 0; q < R; ++q) base[q * (ns + ns / 16)] = v[b * R + q];
+    } else {
+#pragma unroll
+      for (int q = 0; q < R; ++q) sm[sidx(d + q * ns)] = v[b * R + q];
+    }
   }
 }
 
-template <int R, int E>
-__device__ __forceinline__ void load_smem(float2 (&v)[E], const float2* sm, int m, int lt,
-                                          int ts) {
+// Loads of the next pass: butterfly j reads j + k M/R (M/R >= 16, so the
+// padded index is sidx(j) + k (M/R) 17/16).
+template <int R, int E, int M>
+__device__ __forceinline__ void load_smem(float2 (&v)[E], const float2* sm, int lt, int ts) {
+  constexpr int step = M / R;
 #pragma unroll
   for (int b = 0; b < E / R; ++b) {
     const int j = lt + b * ts;
+    if constexpr (step % 16 == 0) {
+      const float2* base = sm + sidx(j);
 #pragma unroll
-    for (int k = 0; k < R; ++k) v[b * R + k] = sm[sidx(j + k * (m / R))];
+      for (int k = 0; k < R; ++k) v[b * R + k] = base[k * (step + step / 16)];
+    } else {
+#pragma unroll
+      for (int k = 0; k < R; ++k) v[b * R + k] = sm[sidx(j + k * step)];
+    }
   }
 }
 
@@ -267,7 +283,7 @@ __device__ __forceinline__ void passes(float2 (&v)[1 << LE], float2* base,
     constexpr int LNS = Q * LE, R = 1 << pass_lr<LM, LE>(Q);
     float2* sub = base + (Q & 1) * BUF;
     butterflies<R, E>(v, tw, LM, LNS, lt, TS);
-    store_smem<R, E>(v, sub, LNS, lt, TS);
+    store_smem<R, E, LNS>(v, sub, lt, TS);
     if constexpr (GROUP && Q + 1 < NP && TS % 32 == 0) {
       if (s == 0)
         asm volatile("bar.sync 1, %0;" ::"n"(TS) : "memory");
@@ -279,7 +295,7 @@ __device__ __forceinline__ void passes(float2 (&v)[1 << LE], float2* base,
       __syncthreads();
     }
     if constexpr (Q + 1 < NP) {
-      load_smem<(1 << pass_lr<LM, LE>(Q + 1)), E>(v, sub, M, lt, TS);
+      load_smem<(1 << pass_lr<LM, LE>(Q + 1)), E, M>(v, sub, lt, TS);
       if constexpr (BUF == 0) {  // one buffer: the next stores wait for these loads
         if constexpr (GROUP && TS % 32 == 0) {
           if (s == 0)
@@ -377,6 +393,27 @@ __device__ __forceinline__ float2 fetch(const float2* sm, int o) {
   if (pp < 0) pp += 3 * M;
   const int q = pp / 3, s = pp - 3 * q;
   return sm[last * stage_offset(3 * M) + s * sub_stride(M) + sidx(q)];
+}
+
+// Outputs o, o + 1, ..., o + K - 1 (o a multiple of K, K | M) after run():
+// one division by 3 for the group, then (q, s) steps through the
+// interleaved sub-transforms.
+template <int LM, int LE, int K, bool DIRECT = false>
+__device__ __forceinline__ void fetch_run(const float2* sm, int o, float2 (&out)[K]) {
+  constexpr int M = 1 << LM;
+  constexpr int last = DIRECT ? 0 : (pass_count<LM, LE>() - 1) & 1;
+  const float2* buf = sm + last * stage_offset(3 * M);
+  int pp = o - M;
+  if (pp < 0) pp += 3 * M;  // the K outputs do not straddle o = M (K | M)
+  int q = pp / 3, s = pp - 3 * q;
+#pragma unroll
+  for (int e = 0; e < K; ++e) {
+    out[e] = buf[s * sub_stride(M) + sidx(q)];
+    if (++s == 3) {
+      s = 0;
+      ++q;
+    }
+  }
 }
 
 // Split form: one CTA of M / E threads computes the single sub-transform

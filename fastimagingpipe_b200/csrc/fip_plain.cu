@@ -843,9 +843,9 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
   }
   float4* out = reinterpret_cast<float4*>(P + (size_t)c * n);
   for (int o2 = threadIdx.x; o2 < n / 2; o2 += NT) {
-    const float2 a = fipfft::fetch<LM, LE, DIRECT>(s_fft, 2 * o2);
-    const float2 b = fipfft::fetch<LM, LE, DIRECT>(s_fft, 2 * o2 + 1);
-    out[o2] = make_float4(a.x, a.y, b.x, b.y);
+    float2 ab[2];
+    fipfft::fetch_run<LM, LE, 2, DIRECT>(s_fft, 2 * o2, ab);
+    out[o2] = make_float4(ab[0].x, ab[0].y, ab[1].x, ab[1].y);
   }
 }
 
@@ -920,13 +920,14 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
   float vmax = 0.f;
   for (int o4 = threadIdx.x; o4 < n / 4; o4 += NT) {
     float a[4], b[4];
+    float2 v[4];
+    fipfft::fetch_run<LM, LE, 4, DIRECT>(s_fft, 4 * o4, v);
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       const int o = 4 * o4 + e;
-      const float2 v = fipfft::fetch<LM, LE, DIRECT>(s_fft, o);
       const float rx = rck[abs(o - h)];
-      a[e] = fabsf(v.x * (rx * ry1));
-      b[e] = fabsf(v.y * (rx * ry2));
+      a[e] = fabsf(v[e].x * (rx * ry1));
+      b[e] = fabsf(v[e].y * (rx * ry2));
       vmax = fmaxf(vmax, fmaxf(a[e], b[e]));
     }
     row1[o4] = make_float4(a[0], a[1], a[2], a[3]);
