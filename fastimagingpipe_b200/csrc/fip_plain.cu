@@ -534,6 +534,17 @@ struct GridSmem {
   float bound[kThreads / 32];
 };
 
+// Lane -> (tap row, tap column) of a warp step for nc tap columns, without a
+// division per visibility: s_lane_map[nc][lane] = (lane / nc) | (lane % nc)
+// << 8 | (32 / nc) << 16, filled once per CTA (init_lane_map + a barrier).
+__shared__ int s_lane_map[10][32];
+__device__ __forceinline__ void init_lane_map() {
+  for (int t = threadIdx.x; t < 10 * 32; t += blockDim.x) {
+    const int nc = t >> 5, l = t & 31;
+    s_lane_map[nc][l] = nc ? (l / nc) | ((l % nc) << 8) | ((32 / nc) << 16) : 0;
+  }
+}
+
 // One gridding work item (tile, entry range) of one snapshot.  Phase 1
 // loads the item's visibilities and their separable kernel values into
 // shared memory (all loads in flight at once); phase 2 lets each warp spread
@@ -641,8 +652,8 @@ __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_ci
   for (int q = warp; q < cnt; q += kThreads / 32) {
     const int meta = S.meta[q];
     const int nr = meta & 15, nc = (meta >> 4) & 15, mir = (meta >> 8) & 1;
-    const int per = 32 / nc;  // tap rows per warp step
-    const int ia0 = lane / nc, ib = lane - ia0 * nc;
+    const int map = s_lane_map[nc][lane];  // (lane / nc) | (lane % nc) << 8 | (32 / nc) << 16
+    const int ia0 = map & 255, ib = (map >> 8) & 255, per = map >> 16;  // tap rows per warp step
     if (ia0 >= per) continue;
     const float wr = S.wr[q], wi = S.wi[q];
     const int rbase = S.row0[q], col = S.col0[q] + ib;
@@ -722,6 +733,8 @@ __global__ void __launch_bounds__(kThreads) k_grid(const float* __restrict__ B, 
   const float inten = plane_intensity(V);
   const float vis_scale = vis_scale_p ? *vis_scale_p : 1.0f;
   const unsigned nw = *nwork;
+  init_lane_map();
+  __syncthreads();
   for (unsigned w = blockIdx.x; w < nw; w += gridDim.x)
     grid_item<VT, COMP>(S, s_cre, s_cim, B, vr, vi, vis_scale, inten, scale, g, hp, tiles_c,
                         layout, entries, work[w], grid);
@@ -753,6 +766,7 @@ __global__ void __launch_bounds__(kThreads) k_grid_batch(const FipGridBatch in, 
     }
     s_first[in.count] = acc;
   }
+  init_lane_map();
   __syncthreads();
   const unsigned total = s_first[in.count];
   int k = 0;
