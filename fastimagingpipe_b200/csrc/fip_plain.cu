@@ -1091,7 +1091,7 @@ __global__ void k_targets(const float* __restrict__ V, int n, float dc, float2* 
     const int i = (blockIdx.x * kTargetsPerThread + q) * blockDim.x + threadIdx.x;
     if (i < n) {
       float LL, MM;
-      fipref::pixel_target(fr, (size_t)i, (size_t)j, (size_t)n, LL, MM);
+      fipref::pixel_target(fr, i, j, n, LL, MM);
       tg[(size_t)j * n + i] = make_float2(LL, MM);
     }
   }
@@ -1108,7 +1108,7 @@ __global__ void k_reproject_scatter(const float* __restrict__ pre, const float* 
   const float inv_nb = 1.0f / static_cast<float>(nb);
   const float value = pre[(size_t)j * n + i] * inv_nb;
   float LL, MM;
-  fipref::pixel_target(fr, (size_t)i, (size_t)j, (size_t)n, LL, MM);
+  fipref::pixel_target(fr, i, j, n, LL, MM);
   const size_t half = n / 2;
   const long c = (long)(half * n + half);
   if (fabs(LL) < half - 1 && fabs(MM) < half - 1) {
@@ -1373,12 +1373,14 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
     float pa = 0.f, pb = 0.f;
     float2 ta = make_float2(0.f, 0.f), tb = make_float2(0.f, 0.f);
     if (va) {
-      pa = pre[(size_t)ja * n + ia];
-      if (!EXACT) ta = tg[(size_t)ja * n + ia];
+      const int at = ja * n + ia;  // < N^2 <= 2^30 (image_size <= 32768)
+      pa = pre[at];
+      if (!EXACT) ta = tg[at];
     }
     if (vb) {
-      pb = pre[(size_t)jb * n + ib];
-      if (!EXACT) tb = tg[(size_t)jb * n + ib];
+      const int at = jb * n + ib;
+      pb = pre[at];
+      if (!EXACT) tb = tg[at];
     }
     if (va) splat(ia, ja, pa * qk, ta);
     if (vb) splat(ib, jb, pb * qk, tb);
@@ -1424,7 +1426,7 @@ __global__ void k_pixel_targets(const float* __restrict__ V, int n, float dc, fl
   float LL, MM;
   if (!exact) {
     fipref::Frame fr{V[0], V[1], V[3], V[4], V[8], V[6], V[7], dc};
-    fipref::pixel_target(fr, (size_t)i, (size_t)j, (size_t)n, LL, MM);
+    fipref::pixel_target(fr, i, j, n, LL, MM);
   } else {
     const ExactMap<double> m = make_map<double>(V, cell);
     double Ld, Md;

@@ -162,9 +162,11 @@ struct Frame {
 // centre: the plane-pixel coordinates of FIPkernels.cu:296-297 followed by
 // the SIN -> slant-SIN step of FIPkernels.cu:307-374 and the centring of
 // :385-386.  di = N.
-__device__ __forceinline__ void pixel_target(const Frame& f, size_t i, size_t j, size_t di,
+__device__ __forceinline__ void pixel_target(const Frame& f, int i, int j, int di,
                                              float& LL, float& MM) {
-  const size_t half = di / 2;
+  // Integer-to-float conversions are exact below 2^24, whatever the integer
+  // type, so 32-bit indices give the reference's values.
+  const int half = di / 2;
   float p1 = (-f.v0 * (static_cast<float>(i) - static_cast<float>(half)) +
               f.v3 * (static_cast<float>(j) - static_cast<float>(half))) /
                  fabsf(f.v8) +
