@@ -296,6 +296,10 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the extra forms")
+    ap.add_argument("--tuning", default=None,
+                    help="pin the launch shapes VPT,SPLIT,DIRECT,CTAS instead of autotuning "
+                         "(profiling runs: the autotuner's timings are not meaningful under a "
+                         "profiler)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -332,7 +336,12 @@ def main():
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.Stream(device=dev)
     im = fip.Imager(n, nb, cell, t, device=local)
-    tuning = im.autotune(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, stream=stream)
+    if args.tuning:
+        vpt, split, direct, ctas = (int(x) for x in args.tuning.split(","))
+        im.set_tuning(vpt, split, ctas, direct)
+        tuning = im.tuning()
+    else:
+        tuning = im.autotune(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, stream=stream)
 
     def step():
         im.pipe_device(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, result, stream=stream)
