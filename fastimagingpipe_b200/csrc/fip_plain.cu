@@ -1205,7 +1205,7 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
     int n, int nb, float cell, float delta, const unsigned* __restrict__ pre_max,
     float* __restrict__ dst, unsigned* img_max) {
   __shared__ __align__(16) unsigned s_tile[kTW * kTR];
-  __shared__ int s_ilo[kMaxRows];
+  __shared__ int s_base[kMaxRows];  // pixel index of row r's first candidate minus its number
   __shared__ int s_off[kMaxRows + 1];
   __shared__ int s_wsum[kThreads / 32];
   __shared__ float s_q[4][2];
@@ -1244,7 +1244,7 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
   // intersected with the row), one row per thread, and the exclusive prefix
   // of the interval lengths: candidates are then numbered 0 .. total-1 row by
   // row, so every warp step splats 32 candidates whatever the row lengths.
-  int cnt = 0;
+  int cnt = 0, ilo = 0;
   {
     const int r = threadIdx.x;
     if (r < nrows) {
@@ -1265,12 +1265,11 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
           }
         }
       }
-      int ilo = 0, ihi = -1;
+      int ihi = -1;
       if (alo <= ahi) {
         ilo = (int)fmaxf(0.f, ceilf(fmaxf(alo + h - 1e-3f, -1.f)));
         ihi = (int)fminf((float)(n - 1), floorf(fminf(ahi + h + 1e-3f, (float)n)));
       }
-      s_ilo[r] = ilo;
       cnt = ihi >= ilo ? ihi - ilo + 1 : 0;
     }
     int inc = cnt;
@@ -1282,7 +1281,12 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
     __syncthreads();
     int wbase = 0;
     for (int w = 0; w < warp; ++w) wbase += s_wsum[w];
-    if (r < kMaxRows) s_off[r] = wbase + inc - cnt;
+    if (r < kMaxRows) {
+      s_off[r] = wbase + inc - cnt;
+      // Candidate f of row r is pixel (jlo + r) n + ilo + (f - off): s_base + f
+      // (< N^2 <= 2^30 for image_size <= 32768).
+      s_base[r] = (jlo + r) * n + ilo - (wbase + inc - cnt);
+    }
     if (r == kThreads - 1) s_off[kMaxRows] = wbase + inc;
   }
   __syncthreads();
@@ -1358,32 +1362,32 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
     atomicAdd(px + kTR, __float2uint_rn(a * wm1));
     atomicAdd(px + kTR + 1, __float2uint_rn(b * wm1));
   };
-  // Warp step: candidates f0 + lane and f0 + 32 + lane, loads issued first.
-  int ra = 0, rb = 0;
-  for (int f0 = warp * 64; f0 < total; f0 += kThreads * 2) {
-    const int fa = f0 + lane, fb = fa + 32;
-    const bool va = fa < total, vb = fb < total;
-    if (va)
-      while (s_off[ra + 1] <= fa) ++ra;
-    if (rb < ra) rb = ra;
-    if (vb)
-      while (s_off[rb + 1] <= fb) ++rb;
-    const int ja = jlo + ra, ia = s_ilo[ra] + (fa - s_off[ra]);
-    const int jb = jlo + rb, ib = s_ilo[rb] + (fb - s_off[rb]);
-    float pa = 0.f, pb = 0.f;
-    float2 ta = make_float2(0.f, 0.f), tb = make_float2(0.f, 0.f);
-    if (va) {
-      const int at = ja * n + ia;  // < N^2 <= 2^30 (image_size <= 32768)
-      pa = pre[at];
-      if (!EXACT) ta = tg[at];
+  // Warp step: candidates f0 + lane + 32 e, e < 4, all loads issued first.
+  // The lane's row cursor only moves forward (its candidates increase).
+  constexpr int kPer = 4;
+  int row = 0;
+  for (int f0 = warp * 32 * kPer; f0 < total; f0 += kThreads * kPer) {
+    int at[kPer], rw[kPer];
+    float p[kPer];
+    float2 tt[kPer];
+#pragma unroll
+    for (int e = 0; e < kPer; ++e) {
+      const int f = f0 + lane + 32 * e;
+      rw[e] = -1;
+      if (f < total) {
+        while (s_off[row + 1] <= f) ++row;
+        rw[e] = row;
+        at[e] = s_base[row] + f;
+        p[e] = pre[at[e]];
+        if (!EXACT) tt[e] = tg[at[e]];
+      }
     }
-    if (vb) {
-      const int at = jb * n + ib;
-      pb = pre[at];
-      if (!EXACT) tb = tg[at];
+#pragma unroll
+    for (int e = 0; e < kPer; ++e) {
+      if (rw[e] < 0) continue;
+      const int j = jlo + rw[e];
+      splat(at[e] - j * n, j, p[e] * qk, EXACT ? make_float2(0.f, 0.f) : tt[e]);
     }
-    if (va) splat(ia, ja, pa * qk, ta);
-    if (vb) splat(ib, jb, pb * qk, tb);
   }
   __syncthreads();
   float vmax = 0.f;
