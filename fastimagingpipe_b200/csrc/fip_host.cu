@@ -202,6 +202,7 @@ struct Lane {
   float* q_scale = nullptr;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev_done = nullptr;
+  cudaEvent_t ev_targets = nullptr;  // pixel mapping of the lane's snapshot written
 };
 constexpr int kLanes = 3;
 
@@ -213,7 +214,10 @@ struct fip_imager {
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_copied[3] = {nullptr, nullptr, nullptr};
   cudaEvent_t ev_used[3] = {nullptr, nullptr, nullptr};
-  cudaStream_t side = nullptr;       // pixel-mapping stream (overlaps gridding + FFT)
+  // Pixel-mapping stream (overlaps gridding + FFT), at the lowest priority:
+  // the lanes' latency-bound stages take SM slots first and the
+  // issue-bound mapping fills what they leave.
+  cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cufftHandle plan = 0;              // cuFFT C2R fallback (grid side not 3 * 2^k)
   bool plan_ok = false;
@@ -304,6 +308,7 @@ static void imager_free(fip_imager* im) {
     for (void* p : lp)
       if (p) cudaFree(p);
     if (L.ev_done) cudaEventDestroy(L.ev_done);
+    if (L.ev_targets) cudaEventDestroy(L.ev_targets);
     if (L.stream) cudaStreamDestroy(L.stream);
   }
   for (float* p : im->images)
@@ -413,7 +418,9 @@ int fip_imager_create(fip_imager** out, const fip_imager_config* cfg) {
 
   FIP_ALLOC(cudaStreamCreateWithFlags(&im->stream, cudaStreamNonBlocking));
   FIP_ALLOC(cudaStreamCreateWithFlags(&im->copy_stream, cudaStreamNonBlocking));
-  FIP_ALLOC(cudaStreamCreateWithFlags(&im->side, cudaStreamNonBlocking));
+  int prio_least = 0, prio_greatest = 0;
+  FIP_ALLOC(cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest));
+  FIP_ALLOC(cudaStreamCreateWithPriority(&im->side, cudaStreamNonBlocking, prio_least));
   FIP_ALLOC(cudaEventCreateWithFlags(&im->ev_fork, cudaEventDisableTiming));
   FIP_ALLOC(cudaEventCreateWithFlags(&im->ev_join, cudaEventDisableTiming));
   FIP_ALLOC(cudaEventCreateWithFlags(&im->ev_start, cudaEventDisableTiming));
@@ -434,8 +441,9 @@ int fip_imager_create(fip_imager** out, const fip_imager_config* cfg) {
   im->lanes = im->custom_fft ? kLanes : 1;
   for (int l = 0; l < im->lanes; ++l) {
     Lane& L = im->lane[l];
-    FIP_ALLOC(cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking));
+    FIP_ALLOC(cudaStreamCreateWithPriority(&L.stream, cudaStreamNonBlocking, prio_greatest));
     FIP_ALLOC(cudaEventCreateWithFlags(&L.ev_done, cudaEventDisableTiming));
+    FIP_ALLOC(cudaEventCreateWithFlags(&L.ev_targets, cudaEventDisableTiming));
     FIP_ALLOC(dalloc(&L.grid, (size_t)geo.g * geo.hp, tot));
     L.bins.cap = 12 * nb;
     L.bins.wcap = ntiles + L.bins.cap / FIP_GCHUNK + 1;
@@ -518,7 +526,7 @@ size_t fip_imager_device_bytes(const fip_imager* im) { return im ? im->device_by
 static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const float* vi,
                                const float* B, const float* V, size_t nb, float* image,
                                float* image_max, cudaStream_t s, bool fork_targets,
-                               bool targets_ready = false) {
+                               bool targets_ready = false, cudaEvent_t targets_ev = nullptr) {
   const FipGeom& geo = im->geo;
   if (nb > im->cfg.max_baselines) return fail(FIP_ERR_ARG, "nb exceeds the imager's capacity");
   if (nb == 0) return fail(FIP_ERR_ARG, "nb must be positive");
@@ -592,6 +600,7 @@ static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const f
     im->launches += image_max ? 2 : 1;
   } else {
     if (fork) FIP_CUDA(cudaStreamWaitEvent(s, im->ev_join, 0));
+    if (targets_ready && targets_ev) FIP_CUDA(cudaStreamWaitEvent(s, targets_ev, 0));
     k = stage_begin(im, ST_REPROJECT, s);
     FIP_CUDA(fip_launch_reproject_gather(geo, L.pre, L.targets, V, (int)nb, L.bins.bbox + 3,
                                          image, reinterpret_cast<unsigned*>(image_max),
@@ -618,8 +627,30 @@ static int image_on_lane(fip_imager* im, int k, const float* vr, const float* vi
   Lane& L = im->lane[k % im->lanes];
   FIP_CUDA(cudaStreamWaitEvent(L.stream, after, 0));
   FIP_TRY(image_snapshot_impl(im, L, vr, vi, B, V, nb, image, image_max, L.stream, false,
-                              targets_ready));
+                              targets_ready, targets_ready ? L.ev_targets : nullptr));
   FIP_CUDA(cudaEventRecord(L.ev_done, L.stream));
+  return FIP_OK;
+}
+
+// Whether a three-snapshot call maps its pixels ahead on the side stream:
+// concurrent lanes, the gather reprojection of the plain form (the precision
+// form evaluates the exact map inside the gather).
+static bool targets_ahead(const fip_imager* im) {
+  return im->lanes > 1 && !im->timer.on && im->cfg.reproject == 0 &&
+         im->cfg.form == FIP_FORM_PLAIN;
+}
+
+// The pixel mappings of a call's three snapshots (bases V + 9 k), on the
+// low-priority side stream after `after`; lane k's gather waits on its
+// ev_targets.
+static int launch_targets_ahead(fip_imager* im, const float* V, cudaEvent_t after) {
+  FIP_CUDA(cudaStreamWaitEvent(im->side, after, 0));
+  for (int k = 0; k < 3; ++k) {
+    Lane& L = im->lane[k % im->lanes];
+    FIP_CUDA(fip_launch_targets(im->geo, V + (size_t)k * 9, L.targets, im->side));
+    FIP_CUDA(cudaEventRecord(L.ev_targets, im->side));
+    im->launches += 1;
+  }
   return FIP_OK;
 }
 
@@ -699,10 +730,12 @@ int fip_pipe_device(fip_imager* im, const float* vr, const float* vi, const floa
   FIP_TRY(call_enter(im, s));
   // The three snapshots image concurrently on the lanes; the trigger joins them.
   FIP_CUDA(cudaEventRecord(im->ev_start, s));
+  const bool ahead = targets_ahead(im);
+  if (ahead) FIP_TRY(launch_targets_ahead(im, V, im->ev_start));
   for (int k = 0; k < 3; ++k)
     FIP_TRY(image_on_lane(im, k, vr + (size_t)k * nb, vi + (size_t)k * nb,
                           B + (size_t)k * nb * 2, V + (size_t)k * 9, nb, im->images[k],
-                          im->maxima + k, s, im->ev_start));
+                          im->maxima + k, s, im->ev_start, ahead));
   for (int k = 0; k < 3; ++k) FIP_TRY(wait_lane(im, k, s));
   im->last_lane = 2 % im->lanes;
   if (im->geo.t > 0 && result) {
@@ -739,16 +772,10 @@ int fip_pipe_host(fip_imager* im, const float* vr, const float* vi, const float*
   // still stages the visibilities.
   std::memcpy(im->h_V, V, 27 * sizeof(float));
   FIP_CUDA(cudaMemcpyAsync(im->d_V, im->h_V, 27 * sizeof(float), cudaMemcpyHostToDevice, cs));
-  const bool early = im->lanes > 1 && !im->timer.on && im->cfg.reproject == 0 &&
-                     im->cfg.form == FIP_FORM_PLAIN;
+  const bool early = targets_ahead(im);
   if (early) {
     FIP_CUDA(cudaEventRecord(im->ev_start, cs));
-    for (int k = 0; k < 3; ++k) {
-      Lane& L = im->lane[k % im->lanes];
-      FIP_CUDA(cudaStreamWaitEvent(L.stream, im->ev_start, 0));
-      FIP_CUDA(fip_launch_targets(im->geo, im->d_V + (size_t)k * 9, L.targets, L.stream));
-      im->launches += 1;
-    }
+    FIP_TRY(launch_targets_ahead(im, im->d_V, im->ev_start));
   }
   // Per snapshot: host copy into pinned slot k (CPU), async H2D on the copy
   // stream, then the snapshot's lane images it while the CPU stages k+1.
