@@ -12,7 +12,12 @@
 // length-M transform runs on M / E threads that keep E (8 or 16) complex
 // values in registers: radix-E (or smaller for the last factor) Stockham
 // passes with table twiddles, exchanging values through shared memory padded
-// by one element every 16 (conflict-free 64-bit accesses).  The first pass
+// by one element every 16 (conflict-free 64-bit accesses).  Twiddle tables:
+// tw[k] = w^k for k < G, followed by the half table tw[G + m] = W^m,
+// W = e^{+2 pi i / M}, m < M / 2, which is all the passes read.  A thread's
+// pass twiddles depend on its lane only, so with 16 values per thread they
+// are loaded into registers before the band is staged (PassTw) and their
+// latency hides behind the staging loads.  The first pass
 // reads the band through a caller functor and applies w^{c s}; the last pass
 // leaves Y_s in shared memory in natural order, read back per output by
 // fetch().
@@ -49,6 +54,8 @@ __host__ __device__ constexpr int stage_offset(int g) { return 3 * sub_stride(g 
 __host__ __device__ constexpr int smem_elems(int g) { return 6 * sub_stride(g / 3) + 16; }
 // The direct form (no staging) keeps one buffer.
 __host__ __device__ constexpr int direct_smem_elems(int g) { return 3 * sub_stride(g / 3) + 16; }
+// Entries of the passes' half table (M / 2), stored after the G entries.
+__host__ __device__ constexpr int half_table_elems(int g) { return g / 6; }
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -131,16 +138,16 @@ __device__ __forceinline__ void dft<16>(float2* x) {
 template <int R>
 __host__ __device__ constexpr int log2c() { return R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : 4; }
 
-// w[k] = W^k for k < R, W = tw[step]: the power-of-two powers come from the
-// table (exact to rounding), the rest as products of at most three of them
-// (a few ulps), so one butterfly reads log2(R) table entries instead of R - 1.
+// w[k] = W^k for k < R from the power-of-two powers p[l] = W^{2^l}
+// (table entries, exact to rounding): the rest as products of at most three
+// of them (a few ulps), so one butterfly reads log2(R) table entries instead
+// of R - 1.
 template <int R>
-__device__ __forceinline__ void twiddle_powers(float2 (&w)[R], const float2* __restrict__ tw,
-                                               int step) {
-  w[1] = __ldg(&tw[step]);
-  if (R > 2) w[2] = __ldg(&tw[2 * step]);
-  if (R > 4) w[4] = __ldg(&tw[4 * step]);
-  if (R > 8) w[8] = __ldg(&tw[8 * step]);
+__device__ __forceinline__ void twiddle_powers(float2 (&w)[R], const float2* p) {
+  w[1] = p[0];
+  if (R > 2) w[2] = p[1];
+  if (R > 4) w[4] = p[2];
+  if (R > 8) w[8] = p[3];
   if (R > 2) w[3] = cmul(w[1], w[2]);
   if (R > 4) {
     w[5] = cmul(w[1], w[4]);
@@ -153,22 +160,25 @@ __device__ __forceinline__ void twiddle_powers(float2 (&w)[R], const float2* __r
   }
 }
 
+// Pass-twiddle step of butterfly j in a pass of radix 2^lr after ns = 2^lns
+// outputs: its twiddles are W^{step 2^l}, l < lr, with (R / 2) step < M / 2.
+__device__ __forceinline__ int pass_step(int j, int lm, int lns, int lr) {
+  return (j & ((1 << lns) - 1)) << (lm - lns - lr);
+}
+
 // Radix-R pass on a length-M sub-transform: butterfly j = lt + b * ts,
-// inputs at j + k M/R, twiddle e^{+2 pi i (j mod ns) k / (ns R)} read from
-// the length-G table (index 3 * ...), outputs at (j/ns) ns R + (j mod ns) +
-// m ns (Stockham, self-sorting).  ns and M are powers of two:
-// lns = log2 ns, lm = log2 M.
-template <int R, int E>
-__device__ __forceinline__ void butterflies(float2 (&v)[E], const float2* __restrict__ tw, int lm,
-                                            int lns, int lt, int ts) {
+// inputs at j + k M/R, twiddle e^{+2 pi i (j mod ns) k / (ns R)} = W^{step k}
+// (pass_step; p[b * log2 R + l] = W^{step 2^l}; none in the first pass,
+// ns = 1), outputs at (j/ns) ns R + (j mod ns) + m ns (Stockham,
+// self-sorting).
+template <int R, int E, bool TWIDDLED>
+__device__ __forceinline__ void butterflies(float2 (&v)[E], const float2* p) {
 #pragma unroll
   for (int b = 0; b < E / R; ++b) {
     float2* x = &v[b * R];
-    if (lns > 0) {
-      const int j = lt + b * ts;
-      const int step = 3 * ((j & ((1 << lns) - 1)) << (lm - lns - log2c<R>()));
+    if constexpr (TWIDDLED) {
       float2 w[R];
-      twiddle_powers<R>(w, tw, step);
+      twiddle_powers<R>(w, p + b * log2c<R>());
 #pragma unroll
       for (int k = 1; k < R; ++k) x[k] = cmul(x[k], w[k]);
     }
@@ -268,6 +278,70 @@ template <int LM, int LE>
 __host__ __device__ constexpr int pass_count() {
   return (LM + LE - 1) / LE;
 }
+// Table entries a thread reads in passes 1 .. Q - 1 ((E / R) butterflies of
+// log2 R entries each; pass 0 has no twiddles).
+template <int LM, int LE>
+__host__ __device__ constexpr int pass_tw_offset(int Q) {
+  int n = 0;
+  for (int q = 1; q < Q; ++q) n += ((1 << LE) >> pass_lr<LM, LE>(q)) * pass_lr<LM, LE>(q);
+  return n;
+}
+
+// A thread's pass twiddles.  With 16 values per thread they are loaded up
+// front (load()) into registers; with 8 (launches of up to 768 threads,
+// tighter register budgets) each pass loads its own from the table.
+template <int LM, int LE>
+struct PassTw {
+  static constexpr bool kAhead = LE == 4;
+  static constexpr int kCount = pass_tw_offset<LM, LE>(pass_count<LM, LE>());
+  float2 w[kAhead && kCount > 0 ? kCount : 1];
+  const float2* half;  // the half table (global memory)
+  int lt;              // thread index within its sub-transform
+
+  __device__ __forceinline__ void load(const float2* __restrict__ tw_half, int lane) {
+    half = tw_half;
+    lt = lane;
+    if constexpr (kAhead) fill<1>();
+  }
+  template <int Q>
+  __device__ __forceinline__ void fill() {
+    if constexpr (Q < pass_count<LM, LE>()) {
+      constexpr int L = pass_lr<LM, LE>(Q), E = 1 << LE, TS = (1 << LM) / E;
+#pragma unroll
+      for (int b = 0; b < (E >> L); ++b) {
+        const int step = pass_step(lt + b * TS, LM, Q * LE, L);
+#pragma unroll
+        for (int l = 0; l < L; ++l)
+          w[pass_tw_offset<LM, LE>(Q) + b * L + l] = __ldg(&half[step << l]);
+      }
+      fill<Q + 1>();
+    }
+  }
+  // Pass Q's entries (log2 R per butterfly) into p.
+  template <int Q, int N>
+  __device__ __forceinline__ void get(float2 (&p)[N]) const {
+    constexpr int L = pass_lr<LM, LE>(Q), E = 1 << LE, TS = (1 << LM) / E;
+    static_assert(N == (E >> L) * L, "one pass's entries");
+    if constexpr (kAhead) {
+#pragma unroll
+      for (int k = 0; k < N; ++k) p[k] = w[pass_tw_offset<LM, LE>(Q) + k];
+    } else {
+#pragma unroll
+      for (int b = 0; b < (E >> L); ++b) {
+        const int step = pass_step(lt + b * TS, LM, Q * LE, L);
+#pragma unroll
+        for (int l = 0; l < L; ++l) p[b * L + l] = __ldg(&half[step << l]);
+      }
+    }
+  }
+};
+
+// Thread index within its sub-transform of the joint forms (3 M / E threads).
+template <int LM, int LE>
+__device__ __forceinline__ int sub_lane(int tid) {
+  constexpr int TS = (1 << LM) >> LE;
+  return tid >= 2 * TS ? tid - 2 * TS : (tid >= TS ? tid - TS : tid);
+}
 
 // Pass Q of the Stockham transform: butterflies, stores into buffer Q & 1
 // (base + (Q & 1) * BUF), and the loads of pass Q + 1 from it.
@@ -277,12 +351,18 @@ __host__ __device__ constexpr int pass_count() {
 // the buffers (no staged band).
 template <int LM, int LE, int Q, int BUF, bool GROUP = false>
 __device__ __forceinline__ void passes(float2 (&v)[1 << LE], float2* base,
-                                       const float2* __restrict__ tw, int lt, int s = 0) {
+                                       const PassTw<LM, LE>& pt, int lt, int s = 0) {
   constexpr int E = 1 << LE, M = 1 << LM, TS = M / E, NP = pass_count<LM, LE>();
   if constexpr (Q < NP) {
     constexpr int LNS = Q * LE, R = 1 << pass_lr<LM, LE>(Q);
     float2* sub = base + (Q & 1) * BUF;
-    butterflies<R, E>(v, tw, LM, LNS, lt, TS);
+    if constexpr (Q > 0) {
+      float2 p[(E / R) * log2c<R>()];
+      pt.template get<Q>(p);
+      butterflies<R, E, true>(v, p);
+    } else {
+      butterflies<R, E, false>(v, nullptr);
+    }
     store_smem<R, E, LNS>(v, sub, lt, TS);
     if constexpr (GROUP && Q + 1 < NP && TS % 32 == 0) {
       if (s == 0)
@@ -308,7 +388,7 @@ __device__ __forceinline__ void passes(float2 (&v)[1 << LE], float2* base,
           __syncthreads();
         }
       }
-      passes<LM, LE, Q + 1, BUF, GROUP>(v, base, tw, lt, s);
+      passes<LM, LE, Q + 1, BUF, GROUP>(v, base, pt, lt, s);
     }
   }
 }
@@ -321,10 +401,11 @@ __device__ __forceinline__ void passes(float2 (&v)[1 << LE], float2* base,
 // then ready for fetch().
 // DIRECT: load() reads global memory (no staged band), so the passes may
 // use group barriers, and one buffer (sm holds direct_smem_elems(G)) serves
-// all passes.
+// all passes.  pt: the thread's pass twiddles (loaded for lane
+// sub_lane(threadIdx.x)).
 template <int LM, int LE, bool DIRECT = false, class Load>
-__device__ __forceinline__ void run(float2* sm, const float2* __restrict__ tw, int lo, int hi,
-                                    Load& load) {
+__device__ __forceinline__ void run(float2* sm, const float2* __restrict__ tw,
+                                    const PassTw<LM, LE>& pt, int lo, int hi, Load& load) {
   constexpr int E = 1 << LE, M = 1 << LM, TS = M / E;
   constexpr int R0 = 1 << pass_lr<LM, LE>(0);
   const int tid = threadIdx.x;
@@ -335,7 +416,7 @@ __device__ __forceinline__ void run(float2* sm, const float2* __restrict__ tw, i
     first_load<R0, E, M, true>(v, s, lt, lo, hi, tw, load);
   else
     first_load<R0, E, M, false>(v, s, lt, lo, hi, tw, load);
-  passes<LM, LE, 0, DIRECT ? 0 : stage_offset(3 * M), DIRECT>(v, sm + s * sub_stride(M), tw,
+  passes<LM, LE, 0, DIRECT ? 0 : stage_offset(3 * M), DIRECT>(v, sm + s * sub_stride(M), pt,
                                                                  lt, s);
 }
 
@@ -366,7 +447,7 @@ __device__ __forceinline__ void zero_pre(float2* pre, int lo, int hi, int tid, i
 }
 
 template <int LM, int LE>
-__device__ __forceinline__ void run_pre(float2* sm, const float2* __restrict__ tw) {
+__device__ __forceinline__ void run_pre(float2* sm, const PassTw<LM, LE>& pt) {
   constexpr int E = 1 << LE, M = 1 << LM, TS = M / E;
   constexpr int R0 = 1 << pass_lr<LM, LE>(0);
   const int tid = threadIdx.x;
@@ -380,7 +461,7 @@ __device__ __forceinline__ void run_pre(float2* sm, const float2* __restrict__ t
 #pragma unroll
     for (int k = 0; k < R0; ++k) v[b * R0 + k] = pre[sidx(j + k * (M / R0))];
   }
-  passes<LM, LE, 0, stage_offset(3 * M), false>(v, sm + s * sub_stride(M), tw, lt, s);
+  passes<LM, LE, 0, stage_offset(3 * M), false>(v, sm + s * sub_stride(M), pt, lt, s);
 }
 
 // Output o in [0, 2M) after run(): X[p] with p = o - M, i.e. Y_s[q] for
@@ -422,7 +503,7 @@ __device__ __forceinline__ void fetch_run(const float2* sm, int o, float2 (&out)
 // buffer).  Ends with a barrier; Y_s[q] is then at single_out<LM, LE>(sm, q).
 template <int LM, int LE, class Load>
 __device__ __forceinline__ void run_single(float2* sm, int s, const float2* __restrict__ tw,
-                                           int lo, int hi, Load& load) {
+                                           const PassTw<LM, LE>& pt, int lo, int hi, Load& load) {
   constexpr int E = 1 << LE, M = 1 << LM;
   constexpr int R0 = 1 << pass_lr<LM, LE>(0);
   float2 v[E];
@@ -433,7 +514,7 @@ __device__ __forceinline__ void run_single(float2* sm, int s, const float2* __re
   // The first pass writes buffer 0 while the staging in buffer 1 is still
   // being read by other threads: passes' barriers come after each store, so
   // buffer 1 is only written (pass 1) after every thread passed barrier 0.
-  passes<LM, LE, 0, sub_stride(M)>(v, sm, tw, threadIdx.x);
+  passes<LM, LE, 0, sub_stride(M)>(v, sm, pt, threadIdx.x);
 }
 
 template <int LM, int LE>

@@ -188,6 +188,19 @@ class CopyPool {
 };
 }  // namespace
 
+// Twiddle tables of the band-pruned transform of length g = 3 M: w^k,
+// w = e^{+2 pi i / g}, for k < g, then the passes' half table W^m = w^{3 m},
+// W = e^{+2 pi i / M}, for m < M / 2 (fipfft).
+static std::vector<float2> fft_twiddles(int g) {
+  std::vector<float2> tw((size_t)g + g / 6);
+  for (int k = 0; k < g; ++k) {
+    const double a = 2.0 * FIP_M_PI * (double)k / (double)g;
+    tw[k] = make_float2((float)cos(a), (float)sin(a));
+  }
+  for (int m = 0; m < g / 6; ++m) tw[(size_t)g + m] = tw[(size_t)3 * m];
+  return tw;
+}
+
 // Scratch of one snapshot in flight.  With the band-pruned transform an
 // imager has kLanes of them, so the snapshots of one call (or of a sequence)
 // image concurrently, each on its lane's stream.
@@ -466,13 +479,9 @@ int fip_imager_create(fip_imager** out, const fip_imager_config* cfg) {
     }
   }
   if (im->custom_fft) {
-    FIP_ALLOC(dalloc(&im->twiddles, (size_t)geo.g, tot));
-    std::vector<float2> tw(geo.g);
-    for (int k = 0; k < geo.g; ++k) {
-      const double a = 2.0 * FIP_M_PI * (double)k / (double)geo.g;
-      tw[k] = make_float2((float)cos(a), (float)sin(a));
-    }
-    FIP_ALLOC(cudaMemcpy(im->twiddles, tw.data(), geo.g * sizeof(float2),
+    const std::vector<float2> tw = fft_twiddles(geo.g);
+    FIP_ALLOC(dalloc(&im->twiddles, tw.size(), tot));
+    FIP_ALLOC(cudaMemcpy(im->twiddles, tw.data(), tw.size() * sizeof(float2),
                          cudaMemcpyHostToDevice));
   }
   // With concurrent lanes a sequence keeps six images, so a lane can start a
@@ -1379,14 +1388,10 @@ int fip_batch_create(fip_batch** out, const fip_imager_config* cfg, size_t max_s
   FIP_BALLOC(dalloc(&b->images, (S + 2) * b->n2, tot));
   FIP_BALLOC(dalloc(&b->maxima, S + 2, tot));
   FIP_BALLOC(dalloc(&b->taper, 2 * ((size_t)geo.n / 2 + 1), tot));
-  FIP_BALLOC(dalloc(&b->twiddles, (size_t)geo.g, tot));
   {
-    std::vector<float2> tw(geo.g);
-    for (int k = 0; k < geo.g; ++k) {
-      const double a = 2.0 * FIP_M_PI * (double)k / (double)geo.g;
-      tw[k] = make_float2((float)cos(a), (float)sin(a));
-    }
-    FIP_BALLOC(cudaMemcpy(b->twiddles, tw.data(), geo.g * sizeof(float2),
+    const std::vector<float2> tw = fft_twiddles(geo.g);
+    FIP_BALLOC(dalloc(&b->twiddles, tw.size(), tot));
+    FIP_BALLOC(cudaMemcpy(b->twiddles, tw.data(), tw.size() * sizeof(float2),
                           cudaMemcpyHostToDevice));
   }
   for (int k = 0; k < kBranches; ++k) {

@@ -830,6 +830,11 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
   // Row band [lo, hi]; row -G/2 is row +G/2 (counted once).
   const int lo = (k1 == half) ? 1 - k1 : -k1, hi = k1;
   const float2* col = H + (size_t)c * g;
+  // Pass twiddles (registers): loaded after the staging loop, so their
+  // latency overlaps the staging barrier without holding registers through
+  // the loop (measured faster here than loading them up front).
+  fipfft::PassTw<LM, LE> pt;
+  if (DIRECT) pt.load(tw + g, fipfft::sub_lane<LM, LE>(threadIdx.x));
   // Stage the band densely (coalesced): st[r - lo] = H[c][r mod G]; or
   // (DIRECT) read it from global memory in the first pass.
   // A band no wider than M is staged pre-twiddled for the three
@@ -841,19 +846,21 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
       const int r = i + lo;
       fipfft::stage_pre<M>(st, r, col[r < 0 ? r + g : r], tw);
     }
+    pt.load(tw + g, fipfft::sub_lane<LM, LE>(threadIdx.x));
     fipfft::zero_pre<M>(st, lo, hi, threadIdx.x, NT);
     __syncthreads();
-    fipfft::run_pre<LM, LE>(s_fft, tw);
+    fipfft::run_pre<LM, LE>(s_fft, pt);
   } else {
     if (!DIRECT) {
       for (int i = threadIdx.x; i <= hi - lo; i += NT) {
         const int r = i + lo;
         st[i] = col[r < 0 ? r + g : r];
       }
+      pt.load(tw + g, fipfft::sub_lane<LM, LE>(threadIdx.x));
       __syncthreads();
     }
     auto load = [&](int r) -> float2 { return DIRECT ? col[r < 0 ? r + g : r] : st[r - lo]; };
-    fipfft::run<LM, LE, DIRECT>(s_fft, tw, lo, hi, load);
+    fipfft::run<LM, LE, DIRECT>(s_fft, tw, pt, lo, hi, load);
   }
   float4* out = reinterpret_cast<float4*>(P + (size_t)c * n);
   for (int o2 = threadIdx.x; o2 < n / 2; o2 += NT) {
@@ -889,6 +896,9 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
   // one 16-byte load per occupied column c (the column pass stores
   // P[c][yy]), written at c and -c.
   float2* st = s_fft + fipfft::stage_offset(g);
+  // Pass twiddles first: their loads overlap the staging loads.
+  fipfft::PassTw<LM, LE> pt;
+  pt.load(tw + g, fipfft::sub_lane<LM, LE>(threadIdx.x));
   // A band no wider than M is staged pre-twiddled (fipfft::stage_pre).
   const bool fold = !DIRECT && hi - lo + 1 <= M;
   if (!DIRECT) {
@@ -925,9 +935,9 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
   };
   auto load = [&](int c) -> float2 { return DIRECT ? zval(c) : st[c - lo]; };
   if (fold)
-    fipfft::run_pre<LM, LE>(s_fft, tw);
+    fipfft::run_pre<LM, LE>(s_fft, pt);
   else
-    fipfft::run<LM, LE, DIRECT>(s_fft, tw, lo, hi, load);
+    fipfft::run<LM, LE, DIRECT>(s_fft, tw, pt, lo, hi, load);
   const float ry1 = rck[abs(yy1 - h)], ry2 = rck[abs(yy1 + 1 - h)];
   float4* row1 = reinterpret_cast<float4*>(pre + (size_t)yy1 * n);
   float4* row2 = reinterpret_cast<float4*>(pre + (size_t)(yy1 + 1) * n);
@@ -987,7 +997,9 @@ __global__ void __launch_bounds__(split_threads<LM, LE>(), (LE == 4 ? 6 : 4))
     }
   __syncthreads();
   auto load = [&](int r) -> float2 { return staged ? st[r - lo] : col[r < 0 ? r + g : r]; };
-  fipfft::run_single<LM, LE>(s_fft, s, tw, lo, hi, load);
+  fipfft::PassTw<LM, LE> pt;
+  pt.load(tw + g, threadIdx.x);
+  fipfft::run_single<LM, LE>(s_fft, s, tw, pt, lo, hi, load);
   float2* out = P + (size_t)c * n;
   for (int q = threadIdx.x; q < M; q += NT) {
     const int pp = 3 * q + s;  // output p = pp (mod G), kept when |p| <= M
@@ -1036,7 +1048,9 @@ __global__ void __launch_bounds__(split_threads<LM, LE>(), (LE == 4 ? 6 : 4))
     }
   __syncthreads();
   auto load = [&](int c) -> float2 { return staged ? st[c - lo] : zval(c); };
-  fipfft::run_single<LM, LE>(s_fft, s, tw, lo, hi, load);
+  fipfft::PassTw<LM, LE> pt;
+  pt.load(tw + g, threadIdx.x);
+  fipfft::run_single<LM, LE>(s_fft, s, tw, pt, lo, hi, load);
   const float ry1 = rck[abs(yy1 - h)], ry2 = rck[abs(yy1 + 1 - h)];
   float* row1 = pre + (size_t)yy1 * n;
   float* row2 = row1 + n;
@@ -1716,8 +1730,7 @@ cudaError_t fip_launch_grid_batch(const FipGeom& geo, const FipGridBatch& in, in
 // shared memory, the same value for every caller, so imagers of different
 // sizes launching from concurrent host threads never lower it under one
 // another's launch.
-static cudaError_t fft_smem_attr(const void* fn, int g, size_t& smem) {
-  smem = (size_t)fipfft::smem_elems(g) * sizeof(float2);
+static cudaError_t fft_smem_attr(const void* fn, size_t smem) {
   int dev = 0, optin = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess)
@@ -1738,22 +1751,23 @@ static cudaError_t launch_cols(const FipGeom& geo, const float2* grid, const uns
   size_t smem;
   cudaError_t e;
   if (split) {
-    if ((e = fft_smem_attr((const void*)k_fft_cols_split<LM, LE>, geo.g, smem)) != cudaSuccess)
-      return e;
     smem = 2 * (size_t)fipfft::sub_stride(1 << LM) * sizeof(float2);
+    if ((e = fft_smem_attr((const void*)k_fft_cols_split<LM, LE>, smem)) != cudaSuccess)
+      return e;
     k_fft_cols_split<LM, LE><<<dim3(geo.hp, 3, batch), split_threads<LM, LE>(), smem, s>>>(
         grid, bbox, colbuf, tw, grid_stride, col_stride);
     return cudaGetLastError();
   }
   if (direct) {
-    e = fft_smem_attr((const void*)k_fft_cols<LM, LE, true>, geo.g, smem);
-    if (e != cudaSuccess) return e;
     smem = (size_t)fipfft::direct_smem_elems(geo.g) * sizeof(float2);
+    e = fft_smem_attr((const void*)k_fft_cols<LM, LE, true>, smem);
+    if (e != cudaSuccess) return e;
     k_fft_cols<LM, LE, true><<<dim3(geo.hp, batch), fft_threads<LM, LE>(), smem, s>>>(
         grid, bbox, colbuf, tw, grid_stride, col_stride);
     return cudaGetLastError();
   }
-  e = fft_smem_attr((const void*)k_fft_cols<LM, LE, false>, geo.g, smem);
+  smem = (size_t)fipfft::smem_elems(geo.g) * sizeof(float2);
+  e = fft_smem_attr((const void*)k_fft_cols<LM, LE, false>, smem);
   if (e != cudaSuccess) return e;
   k_fft_cols<LM, LE, false><<<dim3(geo.hp, batch), fft_threads<LM, LE>(), smem, s>>>(
       grid, bbox, colbuf, tw, grid_stride, col_stride);
@@ -1768,22 +1782,23 @@ static cudaError_t launch_rows(const FipGeom& geo, const float2* colbuf, unsigne
   size_t smem;
   cudaError_t e;
   if (split) {
-    if ((e = fft_smem_attr((const void*)k_fft_rows_split<LM, LE>, geo.g, smem)) != cudaSuccess)
-      return e;
     smem = 2 * (size_t)fipfft::sub_stride(1 << LM) * sizeof(float2);
+    if ((e = fft_smem_attr((const void*)k_fft_rows_split<LM, LE>, smem)) != cudaSuccess)
+      return e;
     k_fft_rows_split<LM, LE><<<dim3(geo.n / 2, 3, batch), split_threads<LM, LE>(), smem, s>>>(
         colbuf, bbox, taper + geo.n / 2 + 1, pre, tw, col_stride, pre_stride);
     return cudaGetLastError();
   }
   if (direct) {
-    e = fft_smem_attr((const void*)k_fft_rows<LM, LE, true>, geo.g, smem);
-    if (e != cudaSuccess) return e;
     smem = (size_t)fipfft::direct_smem_elems(geo.g) * sizeof(float2);
+    e = fft_smem_attr((const void*)k_fft_rows<LM, LE, true>, smem);
+    if (e != cudaSuccess) return e;
     k_fft_rows<LM, LE, true><<<dim3(geo.n / 2, batch), fft_threads<LM, LE>(), smem, s>>>(
         colbuf, bbox, taper + geo.n / 2 + 1, pre, tw, col_stride, pre_stride);
     return cudaGetLastError();
   }
-  e = fft_smem_attr((const void*)k_fft_rows<LM, LE, false>, geo.g, smem);
+  smem = (size_t)fipfft::smem_elems(geo.g) * sizeof(float2);
+  e = fft_smem_attr((const void*)k_fft_rows<LM, LE, false>, smem);
   if (e != cudaSuccess) return e;
   k_fft_rows<LM, LE, false><<<dim3(geo.n / 2, batch), fft_threads<LM, LE>(), smem, s>>>(
       colbuf, bbox, taper + geo.n / 2 + 1, pre, tw, col_stride, pre_stride);
