@@ -426,17 +426,33 @@ __device__ __forceinline__ void run(float2* sm, const float2* __restrict__ tw,
 // and zeros where no c lands (zero_pre); the first pass is then a plain
 // shared-memory read.
 template <int M>
-__device__ __forceinline__ void stage_pre(float2* pre, int c, float2 z,
-                                          const float2* __restrict__ tw) {
-  constexpr int G = 3 * M;
+__device__ __forceinline__ void stage_pre(float2* pre, int c, float2 z, float2 w1, float2 w2) {
   const int nn = c < 0 ? c + M : c;
-  const float2 w1 = __ldg(&tw[c < 0 ? c + G : c]);
-  const int c2 = 2 * c;
-  const float2 w2 = __ldg(&tw[c2 < 0 ? c2 + G : c2]);
   pre[sidx(nn)] = z;
   pre[sub_stride(M) + sidx(nn)] = cmul(z, w1);
   pre[2 * sub_stride(M) + sidx(nn)] = cmul(z, w2);
 }
+
+// w^c and w^{2 c} for c = c0, c0 + d, c0 + 2 d, ... (a staging loop's
+// sequence): two table reads at the start, then one product per step with
+// w^d and w^{2 d} (the error grows by about an ulp per step; a staging loop
+// takes at most G / (2 d) steps).
+struct StageTw {
+  float2 w1, w2, d1, d2;
+  __device__ __forceinline__ StageTw(const float2* __restrict__ tw, int g, int c0, int d) {
+    const int a = c0 < 0 ? c0 + g : c0;
+    int b = 2 * c0;
+    b = b < 0 ? b + g : (b >= g ? b - g : b);
+    w1 = __ldg(&tw[a]);
+    w2 = __ldg(&tw[b]);
+    d1 = __ldg(&tw[d]);
+    d2 = __ldg(&tw[2 * d]);
+  }
+  __device__ __forceinline__ void next() {
+    w1 = cmul(w1, d1);
+    w2 = cmul(w2, d2);
+  }
+};
 template <int M>
 __device__ __forceinline__ void zero_pre(float2* pre, int lo, int hi, int tid, int nt) {
   for (int nn = hi + 1 + tid; nn < M + lo; nn += nt) {

@@ -842,9 +842,10 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
   float2* st = s_fft + fipfft::stage_offset(g);
   const bool fold = !DIRECT && hi - lo + 1 <= M;
   if (fold) {
-    for (int i = threadIdx.x; i <= hi - lo; i += NT) {
+    fipfft::StageTw w(tw, g, lo + (int)threadIdx.x, NT);
+    for (int i = threadIdx.x; i <= hi - lo; i += NT, w.next()) {
       const int r = i + lo;
-      fipfft::stage_pre<M>(st, r, col[r < 0 ? r + g : r], tw);
+      fipfft::stage_pre<M>(st, r, col[r < 0 ? r + g : r], w.w1, w.w2);
     }
     pt.load(tw + g, fipfft::sub_lane<LM, LE>(threadIdx.x));
     fipfft::zero_pre<M>(st, lo, hi, threadIdx.x, NT);
@@ -902,7 +903,8 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
   // A band no wider than M is staged pre-twiddled (fipfft::stage_pre).
   const bool fold = !DIRECT && hi - lo + 1 <= M;
   if (!DIRECT) {
-    for (int c = threadIdx.x; c <= k2; c += NT) {
+    fipfft::StageTw w(tw, g, threadIdx.x, NT);
+    for (int c = threadIdx.x; c <= k2; c += NT, w.next()) {
       const float4 ab = *reinterpret_cast<const float4*>(P + (size_t)c * n + yy1);
       float ay = ab.y, by = ab.w;
       if (c == 0 || c == half) {  // self-conjugate bins are real
@@ -912,8 +914,11 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
       const float2 zp = make_float2(ab.x - by, ay + ab.z);
       const float2 zm = make_float2(ab.x + by, ab.z - ay);  // conj X1 + i conj X2
       if (fold) {
-        fipfft::stage_pre<M>(st, c, zp, tw);
-        if (c > 0 && -c >= lo) fipfft::stage_pre<M>(st, -c, zm, tw);
+        // w^{-c} = conj w^c
+        fipfft::stage_pre<M>(st, c, zp, w.w1, w.w2);
+        if (c > 0 && -c >= lo)
+          fipfft::stage_pre<M>(st, -c, zm, make_float2(w.w1.x, -w.w1.y),
+                               make_float2(w.w2.x, -w.w2.y));
       } else {
         st[c - lo] = zp;
         if (c > 0 && -c >= lo) st[-c - lo] = zm;
