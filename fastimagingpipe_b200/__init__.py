@@ -274,8 +274,12 @@ class Imager:
                                    out.ctypes.data))
         return out
 
-    def pixel_targets(self, V, out, exact: bool = False, stream=None):
-        _check(lib().fip_pixel_targets(self._h, _ptr(V), _ptr(out), int(exact), _stream(stream)))
+    def pixel_targets(self, V, out, exact: bool = False, stream=None, evaluated: bool = False):
+        """Targets (LL, MM) of every pixel into out [N*N*2]: the plain form's
+        FP32 chain as imaged (evaluated=True: step by step, without the
+        theta-terms table; the same bits), or the exact closed form."""
+        mode = 1 if exact else (2 if evaluated else 0)
+        _check(lib().fip_pixel_targets(self._h, _ptr(V), _ptr(out), mode, _stream(stream)))
 
     def image_sequence(self, vis_re, vis_im, B, V, nb_per_snapshot, nb_stride: int, results,
                        stream=None):

@@ -238,6 +238,7 @@ struct fip_imager {
   fipfft::Plan fft{};
   int grid_ctas_per_sm = 0;          // persistent gridder CTAs per SM (0 = most that fit)
   float2* twiddles = nullptr;        // e^{+2 pi i k / G}, k < G
+  float2* theta_tab = nullptr;       // theta terms of the pixel mapping (plain form)
   float* taper = nullptr;            // N/2 + 1 taper values, N/2 + 1 reciprocals
   Lane lane[kLanes];
   int lanes = 1;                     // lanes in use (kLanes with the pruned transform)
@@ -326,8 +327,8 @@ static void imager_free(fip_imager* im) {
   }
   for (float* p : im->images)
     if (p) cudaFree(p);
-  void* dptrs[] = {im->taper, im->twiddles, im->maxima, im->result, im->stats, im->d_vr,
-                   im->d_vi, im->d_B, im->d_V};
+  void* dptrs[] = {im->taper, im->twiddles, im->theta_tab, im->maxima, im->result, im->stats,
+                   im->d_vr, im->d_vi, im->d_B, im->d_V};
   for (void* p : dptrs)
     if (p) cudaFree(p);
   void* hptrs[] = {im->h_vr, im->h_vi, im->h_B, im->h_V, im->h_result};
@@ -450,6 +451,10 @@ int fip_imager_create(fip_imager** out, const fip_imager_config* cfg) {
     return cleanup(fail(FIP_ERR_ARG, "cell_size too small for the tile-gather reprojection; "
                                      "use reproject = 1"));
   FIP_ALLOC(dalloc(&im->taper, 2 * ((size_t)geo.n / 2 + 1), tot));
+  if (cfg->form == FIP_FORM_PLAIN) {
+    FIP_ALLOC(dalloc(&im->theta_tab, fip_theta_table_elems(), tot));
+    FIP_ALLOC(fip_launch_theta_table(im->theta_tab, im->stream));
+  }
   // The cuFFT fallback shares one plan (and its work area): one lane.
   im->lanes = im->custom_fft ? kLanes : 1;
   for (int l = 0; l < im->lanes; ++l) {
@@ -567,7 +572,7 @@ static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const f
       FIP_CUDA(cudaStreamWaitEvent(im->side, im->ev_fork, 0));
     }
     k = stage_begin(im, ST_TARGETS, ts);
-    FIP_CUDA(fip_launch_targets(geo, V, L.targets, ts));
+    FIP_CUDA(fip_launch_targets(geo, V, im->theta_tab, L.targets, ts));
     stage_end(im, k, ts);
     im->launches += 1;
     if (fork) FIP_CUDA(cudaEventRecord(im->ev_join, im->side));
@@ -656,7 +661,7 @@ static int launch_targets_ahead(fip_imager* im, const float* V, cudaEvent_t afte
   FIP_CUDA(cudaStreamWaitEvent(im->side, after, 0));
   for (int k = 0; k < 3; ++k) {
     Lane& L = im->lane[k % im->lanes];
-    FIP_CUDA(fip_launch_targets(im->geo, V + (size_t)k * 9, L.targets, im->side));
+    FIP_CUDA(fip_launch_targets(im->geo, V + (size_t)k * 9, im->theta_tab, L.targets, im->side));
     FIP_CUDA(cudaEventRecord(L.ev_targets, im->side));
     im->launches += 1;
   }
@@ -875,7 +880,8 @@ int fip_imager_grid_side(const fip_imager* im) { return im ? im->geo.g : 0; }
 int fip_pixel_targets(fip_imager* im, const float* V, float* out, int exact, void* stream) {
   if (!im || !V || !out) return fail(FIP_ERR_ARG, "null argument");
   DeviceGuard g(im->cfg.device);
-  FIP_CUDA(fip_launch_pixel_targets(im->geo, V, out, exact, (cudaStream_t)stream));
+  if (exact < 0 || exact > 2) return fail(FIP_ERR_ARG, "exact must be 0, 1 or 2");
+  FIP_CUDA(fip_launch_pixel_targets(im->geo, V, out, exact, im->theta_tab, (cudaStream_t)stream));
   im->launches += 1;
   return FIP_OK;
 }
@@ -1152,6 +1158,7 @@ struct fip_batch {
   fipfft::Plan fft{};
   int grid_ctas_per_sm = 0;
   float2* twiddles = nullptr;
+  float2* theta_tab = nullptr;  // theta terms of the pixel mapping (plain form)
   float* taper = nullptr;
   // Per-snapshot scratch, snapshot k at base + k * stride.
   size_t ntiles = 0, cap = 0, wcap = 0, n2 = 0, grid_elems = 0, col_elems = 0;
@@ -1204,7 +1211,7 @@ void batch_free(fip_batch* b) {
   if (!b) return;
   DeviceGuard g(b->cfg.device);
   if (b->exec) cudaGraphExecDestroy(b->exec);
-  void* ptrs[] = {b->twiddles, b->taper, b->count, b->offset, b->cursor, b->entries, b->work,
+  void* ptrs[] = {b->twiddles, b->theta_tab, b->taper, b->count, b->offset, b->cursor, b->entries, b->work,
                   b->nwork, b->bbox, b->multi, b->nmulti, b->grid, b->colbuf, b->pre,
                   b->targets, b->q_re, b->q_im, b->q_scale, b->images, b->maxima};
   for (void* p : ptrs)
@@ -1253,7 +1260,7 @@ int batch_record(fip_batch* b, const float* const* vr, const float* const* vi,
     FIP_CUDA(fip_launch_bin(geo, B[k], (int)nb[k], bins, bs));
     launches += fip_bin_launches(geo);
     if (!precise) {
-      FIP_CUDA(fip_launch_targets(geo, V[k], b->targets + k * b->n2, bs));
+      FIP_CUDA(fip_launch_targets(geo, V[k], b->theta_tab, b->targets + k * b->n2, bs));
       launches += 1;
     }
   }
@@ -1379,7 +1386,10 @@ int fip_batch_create(fip_batch** out, const fip_imager_config* cfg, size_t max_s
   FIP_BALLOC(dalloc(&b->grid, S * b->grid_elems, tot));
   FIP_BALLOC(dalloc(&b->colbuf, S * b->col_elems, tot));
   FIP_BALLOC(dalloc(&b->pre, S * b->n2, tot));
-  if (cfg->form == FIP_FORM_PLAIN) FIP_BALLOC(dalloc(&b->targets, S * b->n2, tot));
+  if (cfg->form == FIP_FORM_PLAIN) {
+    FIP_BALLOC(dalloc(&b->targets, S * b->n2, tot));
+    FIP_BALLOC(dalloc(&b->theta_tab, fip_theta_table_elems(), tot));
+  }
   if (cfg->form == FIP_FORM_PRECISE && cfg->vis_storage != FIP_STORE_F32) {
     FIP_BALLOC(dalloc((uint16_t**)&b->q_re, S * nb, tot));
     FIP_BALLOC(dalloc((uint16_t**)&b->q_im, S * nb, tot));
@@ -1400,6 +1410,7 @@ int fip_batch_create(fip_batch** out, const fip_imager_config* cfg, size_t max_s
   }
   FIP_BALLOC(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
   FIP_BALLOC(fip_launch_taper(b->taper, geo, b->branch[0]));
+  if (b->theta_tab) FIP_BALLOC(fip_launch_theta_table(b->theta_tab, b->branch[0]));
   FIP_BALLOC(cudaStreamSynchronize(b->branch[0]));
 #undef FIP_BALLOC
   *out = b;

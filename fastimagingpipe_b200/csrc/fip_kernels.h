@@ -74,8 +74,13 @@ cudaError_t fip_launch_fft_rows(const FipGeom& geo, const float2* colbuf, unsign
 cudaError_t fip_launch_correct_c2r(const FipGeom& geo, const float* fft_out, const float* taper,
                                    float* pre, unsigned* pre_max, cudaStream_t s);
 // The reference's pixel mapping of every source pixel -> targets [N*N].
-cudaError_t fip_launch_targets(const FipGeom& geo, const float* V, float2* targets,
-                               cudaStream_t s);
+// theta_tab: the table fip_launch_theta_table fills (bit-identical results,
+// fewer instructions), or null.
+cudaError_t fip_launch_targets(const FipGeom& geo, const float* V, const float2* theta_tab,
+                               float2* targets, cudaStream_t s);
+// Entries of the theta-terms table of the pixel mapping, and its fill.
+size_t fip_theta_table_elems();
+cudaError_t fip_launch_theta_table(float2* tab, cudaStream_t s);
 // Source-major reprojection: one thread per source pixel, atomics into a
 // zeroed destination (the reference's scheme).
 cudaError_t fip_launch_reproject_scatter(const FipGeom& geo, const float* pre, const float* V,
@@ -102,8 +107,10 @@ cudaError_t fip_launch_trigger3(const FipGeom& geo, const float* I1, const float
 // images k, k+1, k+2 with maxima[k .. k+2], result k at results + k * U*U.
 cudaError_t fip_launch_trigger_batch(const FipGeom& geo, const float* images, const float* maxima,
                                      int count, float* results, int precise, cudaStream_t s);
+// mode 0: the FP32 chain (theta_tab as in fip_launch_targets), 1: the exact
+// closed form, 2: the FP32 chain evaluated without the table.
 cudaError_t fip_launch_pixel_targets(const FipGeom& geo, const float* V, float* out,
-                                     int exact_targets, cudaStream_t s);
+                                     int mode, const float2* theta_tab, cudaStream_t s);
 
 // ---- plane projection (fip_precise.cu) ----
 cudaError_t fip_launch_plane_project(const float* uvw, const float* freqs, size_t rows,

@@ -1102,7 +1102,9 @@ __global__ void k_correct_c2r(const float* __restrict__ fft_out, const float* __
 // (LL, MM) of source column i, row j.  Compute-bound; overlapped with the
 // gridding and the FFT on a side stream.
 constexpr int kTargetsPerThread = 4;
-__global__ void k_targets(const float* __restrict__ V, int n, float dc, float2* __restrict__ tg) {
+// ttab: the theta-terms table (fipref::kThetaTabSize entries) or null.
+__global__ void k_targets(const float* __restrict__ V, int n, float dc,
+                          const float2* __restrict__ ttab, float2* __restrict__ tg) {
   const int j = blockIdx.y;
   const fipref::Frame fr{V[0], V[1], V[3], V[4], V[8], V[6], V[7], dc};
 #pragma unroll
@@ -1110,10 +1112,18 @@ __global__ void k_targets(const float* __restrict__ V, int n, float dc, float2* 
     const int i = (blockIdx.x * kTargetsPerThread + q) * blockDim.x + threadIdx.x;
     if (i < n) {
       float LL, MM;
-      fipref::pixel_target(fr, i, j, n, LL, MM);
+      fipref::pixel_target(fr, i, j, n, LL, MM, ttab);
       tg[(size_t)j * n + i] = make_float2(LL, MM);
     }
   }
+}
+
+__global__ void k_theta_table(float2* __restrict__ tab) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= fipref::kThetaTabSize) return;
+  float r, zr0;
+  fipref::theta_terms(__uint_as_float(fipref::kThetaTabLo + (unsigned)k), r, zr0);
+  tab[k] = make_float2(r, zr0);
 }
 
 // Source-major reprojection, the reference's own scheme (FIPkernels.cu:378-413):
@@ -1381,11 +1391,17 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
     atomicAdd(px + kTR, __float2uint_rn(a * wm1));
     atomicAdd(px + kTR + 1, __float2uint_rn(b * wm1));
   };
-  // Warp step: candidates f0 + lane + 32 e, e < 4, all loads issued first.
-  // The lane's row cursor only moves forward (its candidates increase).
-  constexpr int kPer = 4;
+  // Each warp takes a contiguous eighth of the candidates, so a lane's row
+  // cursor moves about half a row per candidate; its start is found by
+  // bisection of the row offsets.  Warp step: candidates f0 + lane + 32 e,
+  // e < 4, all loads issued first; the cursor only moves forward.
+  constexpr int kPer = 4, kWarps = kThreads / 32;
+  const int per = (total + kWarps - 1) / kWarps;
+  const int wb = min(total, warp * per), we = min(total, wb + per);
   int row = 0;
-  for (int f0 = warp * 32 * kPer; f0 < total; f0 += kThreads * kPer) {
+  for (int step = kMaxRows / 2; step > 0; step >>= 1)
+    if (s_off[row + step] <= wb) row += step;  // last row whose offset is <= wb
+  for (int f0 = wb; f0 < we; f0 += 32 * kPer) {
     int at[kPer], rw[kPer];
     float p[kPer];
     float2 tt[kPer];
@@ -1393,7 +1409,7 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
     for (int e = 0; e < kPer; ++e) {
       const int f = f0 + lane + 32 * e;
       rw[e] = -1;
-      if (f < total) {
+      if (f < we) {
         while (s_off[row + 1] <= f) ++row;
         rw[e] = row;
         at[e] = s_base[row] + f;
@@ -1441,15 +1457,18 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
   }
 }
 
+// mode 0: the FP32 chain with the theta table (null: evaluated), 2: the
+// chain evaluated, 1: the exact closed form.
 __global__ void k_pixel_targets(const float* __restrict__ V, int n, float dc, float cell,
-                                int exact, float* __restrict__ out) {
+                                int mode, const float2* __restrict__ ttab,
+                                float* __restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   if (i >= n) return;
   float LL, MM;
-  if (!exact) {
+  if (mode != 1) {
     fipref::Frame fr{V[0], V[1], V[3], V[4], V[8], V[6], V[7], dc};
-    fipref::pixel_target(fr, i, j, n, LL, MM);
+    fipref::pixel_target(fr, i, j, n, LL, MM, mode == 0 ? ttab : nullptr);
   } else {
     const ExactMap<double> m = make_map<double>(V, cell);
     double Ld, Md;
@@ -1862,11 +1881,11 @@ cudaError_t fip_launch_correct_c2r(const FipGeom& geo, const float* fft_out, con
   return cudaGetLastError();
 }
 
-cudaError_t fip_launch_targets(const FipGeom& geo, const float* V, float2* targets,
-                               cudaStream_t s) {
+cudaError_t fip_launch_targets(const FipGeom& geo, const float* V, const float2* theta_tab,
+                               float2* targets, cudaStream_t s) {
   const int per = kThreads * kTargetsPerThread;
   dim3 bl((geo.n + per - 1) / per, geo.n);
-  k_targets<<<bl, kThreads, 0, s>>>(V, geo.n, cell_degrees(geo.cell), targets);
+  k_targets<<<bl, kThreads, 0, s>>>(V, geo.n, cell_degrees(geo.cell), theta_tab, targets);
   return cudaGetLastError();
 }
 
@@ -1953,9 +1972,17 @@ cudaError_t fip_launch_trigger_batch(const FipGeom& geo, const float* images, co
 }
 
 cudaError_t fip_launch_pixel_targets(const FipGeom& geo, const float* V, float* out,
-                                     int exact_targets, cudaStream_t s) {
+                                     int mode, const float2* theta_tab, cudaStream_t s) {
+  if (mode < 0 || mode > 2) return cudaErrorInvalidValue;
   dim3 bl((geo.n + kThreads - 1) / kThreads, geo.n);
-  k_pixel_targets<<<bl, kThreads, 0, s>>>(V, geo.n, cell_degrees(geo.cell), geo.cell,
-                                          exact_targets, out);
+  k_pixel_targets<<<bl, kThreads, 0, s>>>(V, geo.n, cell_degrees(geo.cell), geo.cell, mode,
+                                          theta_tab, out);
+  return cudaGetLastError();
+}
+
+size_t fip_theta_table_elems() { return (size_t)fipref::kThetaTabSize; }
+
+cudaError_t fip_launch_theta_table(float2* tab, cudaStream_t s) {
+  k_theta_table<<<(fipref::kThetaTabSize + kThreads - 1) / kThreads, kThreads, 0, s>>>(tab);
   return cudaGetLastError();
 }

@@ -158,12 +158,48 @@ struct Frame {
   float dc;                  // cell in degrees: (float)((double)cell / pi * 180)
 };
 
+// The slant-step terms of the chain that depend on theta alone
+// (FIPkernels.cu:344-359, 366): r = r0 cos(theta) and z r0 with
+// z = 1 - sin(theta) (small-angle forms below 1e-5 rad), in the chain's
+// FP32 steps.
+__device__ __forceinline__ void theta_terms(float theta, float& r, float& zr0) {
+  float t = (90.0f - fabsf(theta)) / 180.0f * FIP_M_PI;
+  float z, costhe;
+  if (t < 1.0e-5f) {
+    if (theta > 0.0f) {
+      z = t * t / 2.0f;
+    } else {
+      z = 2.0f - t * t / 2.0f;
+    }
+    costhe = t;
+  } else {
+    z = 1.0f - sin_deg(theta);
+    costhe = cos_deg(theta);
+  }
+  const float r0 = 180.0f / FIP_M_PI;
+  r = r0 * costhe;
+  zr0 = z * r0;
+}
+
+// theta_terms tabulated over theta in [80, 90] degrees, indexed by the bit
+// pattern of theta (every FP32 value in the range, 1,310,721 entries): the
+// values are the chain's own FP32 results, so a lookup returns the same bits
+// as the evaluation (two trigonometric calls, two FP64 conversions) at a
+// fraction of the instructions.  Fields within 10 degrees of the phase
+// centre (r < cos 80 deg) map every pixel through the table; the rest
+// evaluate.
+constexpr unsigned kThetaTabLo = 0x42A00000u;  // 80.0f
+constexpr unsigned kThetaTabHi = 0x42B40000u;  // 90.0f
+constexpr int kThetaTabSize = (int)(kThetaTabHi - kThetaTabLo) + 1;
+
 // Target (LL, MM) of source pixel (column i, row j), relative to the image
 // centre: the plane-pixel coordinates of FIPkernels.cu:296-297 followed by
 // the SIN -> slant-SIN step of FIPkernels.cu:307-374 and the centring of
 // :385-386.  di = N.
+// ttab: the theta_terms table, or null to evaluate them.
 __device__ __forceinline__ void pixel_target(const Frame& f, int i, int j, int di,
-                                             float& LL, float& MM) {
+                                             float& LL, float& MM,
+                                             const float2* __restrict__ ttab = nullptr) {
   // Integer-to-float conversions are exact below 2^24, whatever the integer
   // type, so 32-bit indices give the reference's values.
   const int half = di / 2;
@@ -206,29 +242,22 @@ __device__ __forceinline__ void pixel_target(const Frame& f, int i, int j, int d
     sincos_deg(phi, sinphi, cosphi);
     x = sinphi;
     y = cosphi;
-    float t = (90.0f - fabsf(theta)) / 180.0f * FIP_M_PI;
-    float z, costhe;
-    if (t < 1.0e-5f) {
-      if (theta > 0.0f) {
-        z = t * t / 2.0f;
-      } else {
-        z = 2.0f - t * t / 2.0f;
-      }
-      costhe = t;
+    float r, zr0;
+    const unsigned tb = __float_as_uint(theta) - kThetaTabLo;
+    if (ttab && tb < (unsigned)kThetaTabSize) {
+      const float2 q = __ldg(&ttab[tb]);
+      r = q.x;
+      zr0 = q.y;
     } else {
-      z = 1.0f - sin_deg(theta);
-      costhe = cos_deg(theta);
+      theta_terms(theta, r, zr0);
     }
-    r0 = 180.0f / FIP_M_PI;
-    float r = r0 * costhe;
     float w = xi * xi + eta * eta;
     if (w == 0.0f) {
       x = r * x;
       y = -r * y;
     } else {
-      z = z * r0;
-      float z1 = xi * z;
-      float z2 = eta * z;
+      float z1 = xi * zr0;
+      float z2 = eta * zr0;
       x = r * x + z1;
       y = -r * y + z2;
     }

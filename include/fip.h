@@ -230,7 +230,9 @@ int fip_batch_tuning(const fip_batch* b, int* fft_values_per_thread, int* fft_sp
                      int* fft_direct, int* grid_ctas_per_sm);
 
 /* Per-pixel targets (LL, MM) of the reprojection, [N*N][2] (device), for
- * tests: exact = 0 the plain form's FP32 chain, 1 the exact closed form. */
+ * tests: exact = 0 the plain form's FP32 chain as the imager evaluates it
+ * (its theta-terms table where the field allows), 1 the exact closed form,
+ * 2 the FP32 chain evaluated step by step (no table; the same bits as 0). */
 int fip_pixel_targets(fip_imager* im, const float* V, float* out, int exact, void* stream);
 
 /* ------------------------------------------------------------------------ */

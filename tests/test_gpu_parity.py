@@ -166,6 +166,28 @@ def test_precision_form_vs_fp64(cuda, small, storage, img_tol):
     assert np.abs(res - r64).max() <= 1e-4
 
 
+@pytest.mark.parametrize("cfg", ["reference", "wide"])
+def test_theta_table_targets_identical_to_evaluated_chain(cuda, cfg):
+    """The plain form maps pixels through a table of the chain's theta terms;
+    every target must carry the same bits as the chain evaluated step by step.
+    "reference": the 4096^2 shape (every theta inside the table); "wide": a
+    29-degree field, whose outer pixels fall below the table's 80 degrees and
+    evaluate."""
+    import torch
+    snap = (synthetic.config_reference() if cfg == "reference" else
+            synthetic.config_tiny(image_size=512, cell_size=1e-3))
+    n = snap.image_size
+    a = torch.empty(n * n * 2, device=cuda)
+    b = torch.empty_like(a)
+    with fip.Imager(n, snap.num_baselines, snap.cell_size, snap.unit_size) as im:
+        for k in range(3):
+            V = torch.tensor(snap.V[9 * k:9 * k + 9], device=cuda)
+            im.pixel_targets(V, a)
+            im.pixel_targets(V, b, evaluated=True)
+            torch.cuda.synchronize()
+            assert torch.equal(a.view(torch.int32), b.view(torch.int32))
+
+
 def test_exact_targets_vs_oracle(cuda, small):
     tg = targets(small, cuda, exact=True)
     o = oracle.pixel_targets(small.V[:9], small.image_size, small.cell_size, "f64")
