@@ -946,21 +946,34 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
   const float ry1 = rck[abs(yy1 - h)], ry2 = rck[abs(yy1 + 1 - h)];
   float4* row1 = reinterpret_cast<float4*>(pre + (size_t)yy1 * n);
   float4* row2 = reinterpret_cast<float4*>(pre + (size_t)(yy1 + 1) * n);
-  float vmax = 0.f;
-  for (int o4 = threadIdx.x; o4 < n / 4; o4 += NT) {
-    float a[4], b[4];
-    float2 v[4];
-    fipfft::fetch_run<LM, LE, 4, DIRECT>(s_fft, 4 * o4, v);
+  // The epilogue's correction factors, all loads issued before the first
+  // output is formed.
+  constexpr int KQ = (n / 4 + NT - 1) / NT;
+  float rxs[KQ][4];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const int o = 4 * o4 + e;
-      const float rx = rck[abs(o - h)];
-      a[e] = fabsf(v[e].x * (rx * ry1));
-      b[e] = fabsf(v[e].y * (rx * ry2));
-      vmax = fmaxf(vmax, fmaxf(a[e], b[e]));
+  for (int q = 0; q < KQ; ++q) {
+    const int o4 = threadIdx.x + q * NT;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) rxs[q][e] = o4 < n / 4 ? __ldg(&rck[abs(4 * o4 + e - h)]) : 0.f;
+  }
+  float vmax = 0.f;
+#pragma unroll
+  for (int q = 0; q < KQ; ++q) {
+    const int o4 = threadIdx.x + q * NT;
+    if (o4 < n / 4) {
+      float a[4], b[4];
+      float2 v[4];
+      fipfft::fetch_run<LM, LE, 4, DIRECT>(s_fft, 4 * o4, v);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float rx = rxs[q][e];
+        a[e] = fabsf(v[e].x * (rx * ry1));
+        b[e] = fabsf(v[e].y * (rx * ry2));
+        vmax = fmaxf(vmax, fmaxf(a[e], b[e]));
+      }
+      row1[o4] = make_float4(a[0], a[1], a[2], a[3]);
+      row2[o4] = make_float4(b[0], b[1], b[2], b[3]);
     }
-    row1[o4] = make_float4(a[0], a[1], a[2], a[3]);
-    row2[o4] = make_float4(b[0], b[1], b[2], b[3]);
   }
   // Image maximum (bbox[3], float bits; zeroed by the binning), which
   // scales the reprojection's fixed-point sums.
