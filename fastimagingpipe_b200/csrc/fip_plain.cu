@@ -1259,7 +1259,9 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
   const int h = n / 2;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
-  for (int k = threadIdx.x; k < kTW * kTR; k += kThreads) s_tile[k] = 0u;
+  static_assert((kTW * kTR) % 4 == 0, "the tile is zeroed in 16-byte stores");
+  for (int k = threadIdx.x; k < kTW * kTR / 4; k += kThreads)
+    reinterpret_cast<uint4*>(s_tile)[k] = make_uint4(0u, 0u, 0u, 0u);
   if (threadIdx.x < 4) {
     const ExactMap<float> mf = make_map<float>(V, cell);
     const float Llo = (float)(c0 - h) - 1.0f - delta, Lhi = (float)(c0 + kDT - h) + delta;
