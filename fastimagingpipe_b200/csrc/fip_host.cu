@@ -11,6 +11,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <cstdint>
 #include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
@@ -102,42 +104,64 @@ namespace {
 // Host copies into the pinned staging of the host-buffer path.  One thread
 // copies a few GB/s from pageable memory, so a 2 MB snapshot would keep the
 // first snapshot's upload (which the GPU waits for) on the critical path; a
-// small pool of persistent workers splits each large copy.
+// small pool of persistent workers shares each copy job.  A job is a list of
+// segments cut into chunks that the workers and the caller claim from one
+// atomic word (job epoch << 32 | next chunk, claimed by compare-and-swap, so a
+// worker still finishing an earlier job never takes a chunk of the next).
+// Between jobs the workers poll for a short while (a call issues one job per
+// snapshot, back to back) before they block.
 class CopyPool {
  public:
+  struct Seg {
+    void* dst;
+    const void* src;
+    size_t bytes;
+  };
   static CopyPool& get() {
     static CopyPool pool;
     return pool;
   }
-  // Copies `bytes` from src to dst, split over the workers and the caller.
-  void copy(void* dst, const void* src, size_t bytes) {
-    const size_t parts = std::min<size_t>(kWorkers + 1, bytes / kMinPart);
-    if (parts <= 1 || workers_.empty()) {
-      std::memcpy(dst, src, bytes);
+  void copy(const Seg* segs, int nseg) {
+    size_t total = 0;
+    for (int k = 0; k < nseg; ++k) total += segs[k].bytes;
+    if (workers_.empty() || total < 2 * kChunk) {
+      for (int k = 0; k < nseg; ++k) std::memcpy(segs[k].dst, segs[k].src, segs[k].bytes);
       return;
     }
-    std::unique_lock<std::mutex> call(call_mu_);  // one split copy at a time
-    const size_t step = (bytes / parts + 63) & ~size_t(63);
+    std::lock_guard<std::mutex> call(call_mu_);  // one job at a time
+    uint32_t n = 0;
+    for (int k = 0; k < nseg; ++k)
+      for (size_t off = 0; off < segs[k].bytes; off += kChunk) {
+        if (n == kMaxChunks) {  // too many chunks for one job: the rest inline
+          std::memcpy(static_cast<char*>(segs[k].dst) + off,
+                      static_cast<const char*>(segs[k].src) + off, segs[k].bytes - off);
+          break;
+        }
+        chunks_[n++] = Chunk{static_cast<char*>(segs[k].dst) + off,
+                             static_cast<const char*>(segs[k].src) + off,
+                             std::min(kChunk, segs[k].bytes - off)};
+      }
+    count_.store(n, std::memory_order_relaxed);
+    remaining_.store(n, std::memory_order_relaxed);
+    const uint64_t epoch = (word_.load(std::memory_order_relaxed) >> 32) + 1;
     {
       std::lock_guard<std::mutex> lk(mu_);
-      dst_ = static_cast<char*>(dst);
-      src_ = static_cast<const char*>(src);
-      bytes_ = bytes;
-      step_ = step;
-      next_ = 1;  // part 0 is the caller's
-      parts_ = parts;
-      pending_ = parts - 1;
-      ++epoch_;
+      word_.store(epoch << 32, std::memory_order_release);  // publishes chunks_, count_
     }
     cv_.notify_all();
-    std::memcpy(dst, src, std::min(step, bytes));
-    std::unique_lock<std::mutex> lk(mu_);
-    done_.wait(lk, [&] { return pending_ == 0; });
+    work(epoch);
+    while (remaining_.load(std::memory_order_acquire) != 0) std::this_thread::yield();
   }
 
  private:
+  struct Chunk {
+    char* dst;
+    const char* src;
+    size_t bytes;
+  };
   static constexpr size_t kWorkers = 3;
-  static constexpr size_t kMinPart = 256 * 1024;
+  static constexpr size_t kChunk = 256 * 1024;
+  static constexpr uint32_t kMaxChunks = 256;
 
   CopyPool() {
     for (size_t k = 0; k < kWorkers; ++k) {
@@ -151,40 +175,50 @@ class CopyPool {
   ~CopyPool() {
     {
       std::lock_guard<std::mutex> lk(mu_);
-      stop_ = true;
+      stop_.store(true);
     }
     cv_.notify_all();
     for (std::thread& t : workers_) t.join();
   }
-  void run() {
-    unsigned long long seen = 0;
-    std::unique_lock<std::mutex> lk(mu_);
+  // Claims and copies chunks of job `epoch` until none is left.
+  void work(uint64_t epoch) {
+    uint64_t w = word_.load(std::memory_order_acquire);
     for (;;) {
-      cv_.wait(lk, [&] { return stop_ || (epoch_ != seen && next_ < parts_); });
-      if (stop_) return;
-      seen = epoch_;
-      while (next_ < parts_) {
-        const size_t part = next_++;
-        const size_t off = part * step_;
-        const size_t len = off < bytes_ ? std::min(step_, bytes_ - off) : 0;
-        char* d = dst_ + off;
-        const char* sp = src_ + off;
-        lk.unlock();
-        if (len) std::memcpy(d, sp, len);
-        lk.lock();
-        if (--pending_ == 0) done_.notify_one();
+      if ((w >> 32) != epoch || (uint32_t)w >= count_.load(std::memory_order_relaxed)) return;
+      if (!word_.compare_exchange_weak(w, w + 1, std::memory_order_acq_rel)) continue;
+      const Chunk& c = chunks_[(uint32_t)w];
+      std::memcpy(c.dst, c.src, c.bytes);
+      remaining_.fetch_sub(1, std::memory_order_release);
+      w = word_.load(std::memory_order_acquire);
+    }
+  }
+  void run() {
+    uint64_t seen = 0;
+    for (;;) {
+      const auto t0 = std::chrono::steady_clock::now();
+      uint64_t e;
+      while ((e = word_.load(std::memory_order_acquire) >> 32) == seen && !stop_.load()) {
+        if (std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(300)) {
+          std::unique_lock<std::mutex> lk(mu_);
+          cv_.wait(lk, [&] { return stop_.load() || (word_.load() >> 32) != seen; });
+        } else {
+          std::this_thread::yield();
+        }
       }
+      if (stop_.load()) return;
+      seen = e;
+      work(e);
     }
   }
 
   std::vector<std::thread> workers_;
   std::mutex call_mu_, mu_;
-  std::condition_variable cv_, done_;
-  char* dst_ = nullptr;
-  const char* src_ = nullptr;
-  size_t bytes_ = 0, step_ = 0, next_ = 0, parts_ = 0, pending_ = 0;
-  unsigned long long epoch_ = 0;
-  bool stop_ = false;
+  std::condition_variable cv_;
+  Chunk chunks_[kMaxChunks];
+  std::atomic<uint32_t> count_{0};
+  std::atomic<uint64_t> word_{0};
+  std::atomic<uint32_t> remaining_{0};
+  std::atomic<bool> stop_{false};
 };
 }  // namespace
 
@@ -797,10 +831,10 @@ int fip_pipe_host(fip_imager* im, const float* vr, const float* vi, const float*
     float* hvr = im->h_vr + (size_t)k * nb;
     float* hvi = im->h_vi + (size_t)k * nb;
     float* hB = im->h_B + (size_t)k * nb * 2;
-    CopyPool& pool = CopyPool::get();
-    pool.copy(hB, B + (size_t)k * nb * 2, nb * 2 * sizeof(float));
-    pool.copy(hvr, vr + (size_t)k * nb, nb * sizeof(float));
-    pool.copy(hvi, vi + (size_t)k * nb, nb * sizeof(float));
+    const CopyPool::Seg segs[3] = {{hB, B + (size_t)k * nb * 2, nb * 2 * sizeof(float)},
+                                   {hvr, vr + (size_t)k * nb, nb * sizeof(float)},
+                                   {hvi, vi + (size_t)k * nb, nb * sizeof(float)}};
+    CopyPool::get().copy(segs, 3);
     float* dvr = im->d_vr + (size_t)k * nb;
     float* dvi = im->d_vi + (size_t)k * nb;
     float* dB = im->d_B + (size_t)k * nb * 2;

@@ -1193,6 +1193,27 @@ __device__ __forceinline__ ExactMap<T> make_map(const float* V, float cell) {
   return m;
 }
 
+// The same map in FP32 arithmetic throughout (no FP64 divisions): for the
+// gather's candidate bounds, whose margins (a quarter pixel at least) dwarf
+// its rounding (~1e-4 pixel at 4096^2).
+__device__ __forceinline__ ExactMap<float> make_map_f32(const float* V, float cell) {
+  ExactMap<float> m;
+  const float a22 = fabsf(V[8]);
+  m.m00 = -V[0] / a22;
+  m.m01 = V[3] / a22;
+  m.m10 = -V[1] / a22;
+  m.m11 = V[4] / a22;
+  const float det = m.m00 * m.m11 - m.m01 * m.m10;
+  m.i00 = m.m11 / det;
+  m.i01 = -m.m01 / det;
+  m.i10 = -m.m10 / det;
+  m.i11 = m.m00 / det;
+  m.xi = V[6] / V[8];
+  m.eta = V[7] / V[8];
+  m.cell = cell;
+  return m;
+}
+
 template <typename T>
 __device__ __forceinline__ T slant_over_cell(const ExactMap<T>& m, T P1, T P2) {
   const T rho = m.cell * m.cell * ((P1 - 1) * (P1 - 1) + (P2 - 1) * (P2 - 1));
@@ -1263,7 +1284,7 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
   for (int k = threadIdx.x; k < kTW * kTR / 4; k += kThreads)
     reinterpret_cast<uint4*>(s_tile)[k] = make_uint4(0u, 0u, 0u, 0u);
   if (threadIdx.x < 4) {
-    const ExactMap<float> mf = make_map<float>(V, cell);
+    const ExactMap<float> mf = make_map_f32(V, cell);
     const float Llo = (float)(c0 - h) - 1.0f - delta, Lhi = (float)(c0 + kDT - h) + delta;
     const float Mlo = (float)(r0 - h) - 1.0f - delta, Mhi = (float)(r0 + kDT - h) + delta;
     const float L = (threadIdx.x == 0 || threadIdx.x == 3) ? Llo : Lhi;
