@@ -823,51 +823,64 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
   H += blockIdx.y * grid_stride;
   P += blockIdx.y * col_stride;
   bbox += 4 * blockIdx.y;
-  const int c = blockIdx.x;
   const int k2 = (int)bbox[1];
-  if (c > k2) return;
   const int k1 = min((int)bbox[0], half);
   // Row band [lo, hi]; row -G/2 is row +G/2 (counted once).
   const int lo = (k1 == half) ? 1 - k1 : -k1, hi = k1;
-  const float2* col = H + (size_t)c * g;
-  // Pass twiddles (registers): loaded after the staging loop, so their
-  // latency overlaps the staging barrier without holding registers through
-  // the loop (measured faster here than loading them up front).
-  fipfft::PassTw<LM, LE> pt;
-  if (DIRECT) pt.load(tw + g, fipfft::sub_lane<LM, LE>(threadIdx.x));
   // Stage the band densely (coalesced): st[r - lo] = H[c][r mod G]; or
   // (DIRECT) read it from global memory in the first pass.
   // A band no wider than M is staged pre-twiddled for the three
   // sub-transforms (fipfft::stage_pre).
   float2* st = s_fft + fipfft::stage_offset(g);
   const bool fold = !DIRECT && hi - lo + 1 <= M;
-  if (fold) {
-    fipfft::StageTw w(tw, g, lo + (int)threadIdx.x, NT);
-    for (int i = threadIdx.x; i <= hi - lo; i += NT, w.next()) {
-      const int r = i + lo;
-      fipfft::stage_pre<M>(st, r, col[r < 0 ? r + g : r], w.w1, w.w2);
-    }
-    pt.load(tw + g, fipfft::sub_lane<LM, LE>(threadIdx.x));
-    fipfft::zero_pre<M>(st, lo, hi, threadIdx.x, NT);
-    __syncthreads();
-    fipfft::run_pre<LM, LE>(s_fft, pt);
-  } else {
-    if (!DIRECT) {
-      for (int i = threadIdx.x; i <= hi - lo; i += NT) {
+  auto band = [&](int c, int r) -> float2 { return H[(size_t)c * g + (r < 0 ? r + g : r)]; };
+  // The staged form is persistent over columns (blockIdx.x + k gridDim.x):
+  // a thread's first staged element of the next column is loaded while the
+  // current column is transformed.
+  const int r0 = lo + (int)threadIdx.x;
+  float2 pf = make_float2(0.f, 0.f);
+  if (!DIRECT && (int)blockIdx.x <= k2 && r0 <= hi) pf = band(blockIdx.x, r0);
+  for (int c = blockIdx.x; c <= k2; c += gridDim.x) {
+    // Pass twiddles (registers): loaded after the staging loop, so their
+    // latency overlaps the staging barrier without holding registers through
+    // the loop (measured faster here than loading them up front).
+    fipfft::PassTw<LM, LE> pt;
+    if (DIRECT) pt.load(tw + g, fipfft::sub_lane<LM, LE>(threadIdx.x));
+    if (fold) {
+      fipfft::StageTw w(tw, g, r0, NT);
+      if (r0 <= hi) fipfft::stage_pre<M>(st, r0, pf, w.w1, w.w2);
+      w.next();
+      for (int i = threadIdx.x + NT; i <= hi - lo; i += NT, w.next()) {
         const int r = i + lo;
-        st[i] = col[r < 0 ? r + g : r];
+        fipfft::stage_pre<M>(st, r, band(c, r), w.w1, w.w2);
       }
-      pt.load(tw + g, fipfft::sub_lane<LM, LE>(threadIdx.x));
-      __syncthreads();
+    } else if (!DIRECT) {
+      if (r0 <= hi) st[threadIdx.x] = pf;
+      for (int i = threadIdx.x + NT; i <= hi - lo; i += NT) st[i] = band(c, i + lo);
     }
-    auto load = [&](int r) -> float2 { return DIRECT ? col[r < 0 ? r + g : r] : st[r - lo]; };
-    fipfft::run<LM, LE, DIRECT>(s_fft, tw, pt, lo, hi, load);
-  }
-  float4* out = reinterpret_cast<float4*>(P + (size_t)c * n);
-  for (int o2 = threadIdx.x; o2 < n / 2; o2 += NT) {
-    float2 ab[2];
-    fipfft::fetch_run<LM, LE, 2, DIRECT>(s_fft, 2 * o2, ab);
-    out[o2] = make_float4(ab[0].x, ab[0].y, ab[1].x, ab[1].y);
+    if (!DIRECT) {
+      pt.load(tw + g, fipfft::sub_lane<LM, LE>(threadIdx.x));
+      if (fold) fipfft::zero_pre<M>(st, lo, hi, threadIdx.x, NT);
+      __syncthreads();
+      // The next column's first element, in flight during this transform.
+      const int nx = c + gridDim.x;
+      if (nx <= k2 && r0 <= hi) pf = band(nx, r0);
+    }
+    if (fold) {
+      fipfft::run_pre<LM, LE>(s_fft, pt);
+    } else {
+      auto load = [&](int r) -> float2 { return DIRECT ? band(c, r) : st[r - lo]; };
+      fipfft::run<LM, LE, DIRECT>(s_fft, tw, pt, lo, hi, load);
+    }
+    float4* out = reinterpret_cast<float4*>(P + (size_t)c * n);
+    for (int o2 = threadIdx.x; o2 < n / 2; o2 += NT) {
+      float2 ab[2];
+      fipfft::fetch_run<LM, LE, 2, DIRECT>(s_fft, 2 * o2, ab);
+      out[o2] = make_float4(ab[0].x, ab[0].y, ab[1].x, ab[1].y);
+    }
+    // The next staging writes the second buffer: when the last pass left
+    // its outputs there, every thread must be done reading them.
+    if constexpr (!DIRECT && ((fipfft::pass_count<LM, LE>() - 1) & 1)) __syncthreads();
   }
 }
 
@@ -889,7 +902,6 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
   P += blockIdx.y * col_stride;
   pre += blockIdx.y * pre_stride;
   bbox += 4 * blockIdx.y;
-  const int yy1 = 2 * blockIdx.x;
   const int k2 = min((int)bbox[1], half);
   // Column band [lo, hi]; column -G/2 is column +G/2 (counted once).
   const int lo = (k2 == half) ? 1 - k2 : -k2, hi = k2;
@@ -902,78 +914,111 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
   pt.load(tw + g, fipfft::sub_lane<LM, LE>(threadIdx.x));
   // A band no wider than M is staged pre-twiddled (fipfft::stage_pre).
   const bool fold = !DIRECT && hi - lo + 1 <= M;
-  if (!DIRECT) {
-    fipfft::StageTw w(tw, g, threadIdx.x, NT);
-    for (int c = threadIdx.x; c <= k2; c += NT, w.next()) {
-      const float4 ab = *reinterpret_cast<const float4*>(P + (size_t)c * n + yy1);
+  // The staged form is persistent over row pairs (blockIdx.x + k gridDim.x):
+  // a thread's first staged column of the next row pair is loaded into
+  // registers while the current pair is transformed, so its latency leaves
+  // the staging step (two columns measured slower: more spills).
+  constexpr int kPf = 1;
+  float4 pf[kPf];
+  auto col_load = [&](int c, int yy) -> float4 {
+    return *reinterpret_cast<const float4*>(P + (size_t)c * n + yy);
+  };
+#pragma unroll
+  for (int m = 0; m < kPf; ++m) {
+    const int c = threadIdx.x + m * NT;
+    if (!DIRECT && c <= k2) pf[m] = col_load(c, 2 * blockIdx.x);
+  }
+  float vmax = 0.f;
+  for (int rp = blockIdx.x; rp < n / 2; rp += gridDim.x) {
+    const int yy1 = 2 * rp;
+    if (!DIRECT) {
+      fipfft::StageTw w(tw, g, threadIdx.x, NT);
+      auto stage = [&](int c, const float4& ab) {
+        float ay = ab.y, by = ab.w;
+        if (c == 0 || c == half) {  // self-conjugate bins are real
+          ay = 0.f;
+          by = 0.f;
+        }
+        const float2 zp = make_float2(ab.x - by, ay + ab.z);
+        const float2 zm = make_float2(ab.x + by, ab.z - ay);  // conj X1 + i conj X2
+        if (fold) {
+          // w^{-c} = conj w^c
+          fipfft::stage_pre<M>(st, c, zp, w.w1, w.w2);
+          if (c > 0 && -c >= lo)
+            fipfft::stage_pre<M>(st, -c, zm, make_float2(w.w1.x, -w.w1.y),
+                                 make_float2(w.w2.x, -w.w2.y));
+        } else {
+          st[c - lo] = zp;
+          if (c > 0 && -c >= lo) st[-c - lo] = zm;
+        }
+      };
+#pragma unroll
+      for (int m = 0; m < kPf; ++m, w.next()) {
+        const int c = threadIdx.x + m * NT;
+        if (c <= k2) stage(c, pf[m]);
+      }
+      for (int c = threadIdx.x + kPf * NT; c <= k2; c += NT, w.next()) stage(c, col_load(c, yy1));
+      if (fold) fipfft::zero_pre<M>(st, lo, hi, threadIdx.x, NT);
+      __syncthreads();
+      // The next row pair's first columns, in flight during this transform.
+      const int nx = rp + gridDim.x;
+#pragma unroll
+      for (int m = 0; m < kPf; ++m) {
+        const int c = threadIdx.x + m * NT;
+        if (nx < n / 2 && c <= k2) pf[m] = col_load(c, 2 * nx);
+      }
+    }
+    // DIRECT: Z[c] straight from the column-pass output (L2-resident).
+    auto zval = [&](int c) -> float2 {
+      const int a = c < 0 ? -c : c;
+      const float4 ab = col_load(a, yy1);
       float ay = ab.y, by = ab.w;
-      if (c == 0 || c == half) {  // self-conjugate bins are real
+      if (a == 0 || a == half) {
         ay = 0.f;
         by = 0.f;
       }
-      const float2 zp = make_float2(ab.x - by, ay + ab.z);
-      const float2 zm = make_float2(ab.x + by, ab.z - ay);  // conj X1 + i conj X2
-      if (fold) {
-        // w^{-c} = conj w^c
-        fipfft::stage_pre<M>(st, c, zp, w.w1, w.w2);
-        if (c > 0 && -c >= lo)
-          fipfft::stage_pre<M>(st, -c, zm, make_float2(w.w1.x, -w.w1.y),
-                               make_float2(w.w2.x, -w.w2.y));
-      } else {
-        st[c - lo] = zp;
-        if (c > 0 && -c >= lo) st[-c - lo] = zm;
+      return c >= 0 ? make_float2(ab.x - by, ay + ab.z) : make_float2(ab.x + by, ab.z - ay);
+    };
+    auto load = [&](int c) -> float2 { return DIRECT ? zval(c) : st[c - lo]; };
+    if (fold)
+      fipfft::run_pre<LM, LE>(s_fft, pt);
+    else
+      fipfft::run<LM, LE, DIRECT>(s_fft, tw, pt, lo, hi, load);
+    const float ry1 = rck[abs(yy1 - h)], ry2 = rck[abs(yy1 + 1 - h)];
+    float4* row1 = reinterpret_cast<float4*>(pre + (size_t)yy1 * n);
+    float4* row2 = reinterpret_cast<float4*>(pre + (size_t)(yy1 + 1) * n);
+    // The epilogue's correction factors, all loads issued before the first
+    // output is formed.
+    constexpr int KQ = (n / 4 + NT - 1) / NT;
+    float rxs[KQ][4];
+#pragma unroll
+    for (int q = 0; q < KQ; ++q) {
+      const int o4 = threadIdx.x + q * NT;
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        rxs[q][e] = o4 < n / 4 ? __ldg(&rck[abs(4 * o4 + e - h)]) : 0.f;
+    }
+#pragma unroll
+    for (int q = 0; q < KQ; ++q) {
+      const int o4 = threadIdx.x + q * NT;
+      if (o4 < n / 4) {
+        float a[4], b[4];
+        float2 v[4];
+        fipfft::fetch_run<LM, LE, 4, DIRECT>(s_fft, 4 * o4, v);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const float rx = rxs[q][e];
+          a[e] = fabsf(v[e].x * (rx * ry1));
+          b[e] = fabsf(v[e].y * (rx * ry2));
+          vmax = fmaxf(vmax, fmaxf(a[e], b[e]));
+        }
+        row1[o4] = make_float4(a[0], a[1], a[2], a[3]);
+        row2[o4] = make_float4(b[0], b[1], b[2], b[3]);
       }
     }
-    if (fold) fipfft::zero_pre<M>(st, lo, hi, threadIdx.x, NT);
-    __syncthreads();
-  }
-  // DIRECT: Z[c] straight from the column-pass output (L2-resident).
-  auto zval = [&](int c) -> float2 {
-    const int a = c < 0 ? -c : c;
-    const float4 ab = *reinterpret_cast<const float4*>(P + (size_t)a * n + yy1);
-    float ay = ab.y, by = ab.w;
-    if (a == 0 || a == half) {
-      ay = 0.f;
-      by = 0.f;
-    }
-    return c >= 0 ? make_float2(ab.x - by, ay + ab.z) : make_float2(ab.x + by, ab.z - ay);
-  };
-  auto load = [&](int c) -> float2 { return DIRECT ? zval(c) : st[c - lo]; };
-  if (fold)
-    fipfft::run_pre<LM, LE>(s_fft, pt);
-  else
-    fipfft::run<LM, LE, DIRECT>(s_fft, tw, pt, lo, hi, load);
-  const float ry1 = rck[abs(yy1 - h)], ry2 = rck[abs(yy1 + 1 - h)];
-  float4* row1 = reinterpret_cast<float4*>(pre + (size_t)yy1 * n);
-  float4* row2 = reinterpret_cast<float4*>(pre + (size_t)(yy1 + 1) * n);
-  // The epilogue's correction factors, all loads issued before the first
-  // output is formed.
-  constexpr int KQ = (n / 4 + NT - 1) / NT;
-  float rxs[KQ][4];
-#pragma unroll
-  for (int q = 0; q < KQ; ++q) {
-    const int o4 = threadIdx.x + q * NT;
-#pragma unroll
-    for (int e = 0; e < 4; ++e) rxs[q][e] = o4 < n / 4 ? __ldg(&rck[abs(4 * o4 + e - h)]) : 0.f;
-  }
-  float vmax = 0.f;
-#pragma unroll
-  for (int q = 0; q < KQ; ++q) {
-    const int o4 = threadIdx.x + q * NT;
-    if (o4 < n / 4) {
-      float a[4], b[4];
-      float2 v[4];
-      fipfft::fetch_run<LM, LE, 4, DIRECT>(s_fft, 4 * o4, v);
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const float rx = rxs[q][e];
-        a[e] = fabsf(v[e].x * (rx * ry1));
-        b[e] = fabsf(v[e].y * (rx * ry2));
-        vmax = fmaxf(vmax, fmaxf(a[e], b[e]));
-      }
-      row1[o4] = make_float4(a[0], a[1], a[2], a[3]);
-      row2[o4] = make_float4(b[0], b[1], b[2], b[3]);
-    }
+    // The next staging writes the second buffer: when the last pass left
+    // its outputs there, every thread must be done reading them.
+    if constexpr (!DIRECT && ((fipfft::pass_count<LM, LE>() - 1) & 1)) __syncthreads();
   }
   // Image maximum (bbox[3], float bits; zeroed by the binning), which
   // scales the reprojection's fixed-point sums.
@@ -1283,6 +1328,10 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
   static_assert((kTW * kTR) % 4 == 0, "the tile is zeroed in 16-byte stores");
   for (int k = threadIdx.x; k < kTW * kTR / 4; k += kThreads)
     reinterpret_cast<uint4*>(s_tile)[k] = make_uint4(0u, 0u, 0u, 0u);
+  // Precision form: the FP64 map, formed once per CTA (thread 4) beside the
+  // corners and read by every thread after the barrier.
+  __shared__ ExactMap<double> s_md;
+  if (EXACT && threadIdx.x == 4) s_md = make_map<double>(V, cell);
   if (threadIdx.x < 4) {
     const ExactMap<float> mf = make_map_f32(V, cell);
     const float Llo = (float)(c0 - h) - 1.0f - delta, Lhi = (float)(c0 + kDT - h) + delta;
@@ -1377,8 +1426,12 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
   float p10 = 0.f, p20 = 0.f, off1 = 0.f, off2 = 0.f;
   int a0 = 0, b0 = 0;
   if (EXACT) {
-    const ExactMap<double> md = make_map<double>(V, cell);
-    mf = make_map<float>(V, cell);
+    const ExactMap<double> md = s_md;
+    // make_map<float>: the FP64 map's coefficients rounded to FP32.
+    mf.m00 = (float)md.m00; mf.m01 = (float)md.m01; mf.m10 = (float)md.m10;
+    mf.m11 = (float)md.m11; mf.i00 = (float)md.i00; mf.i01 = (float)md.i01;
+    mf.i10 = (float)md.i10; mf.i11 = (float)md.i11; mf.xi = (float)md.xi;
+    mf.eta = (float)md.eta; mf.cell = (float)md.cell;
     a0 = (int)rintf(0.25f * (s_q[0][0] + s_q[1][0] + s_q[2][0] + s_q[3][0]));
     b0 = (int)rintf(0.25f * (s_q[0][1] + s_q[1][1] + s_q[2][1] + s_q[3][1]));
     const double P1 = md.m00 * a0 + md.m01 * b0, P2 = md.m10 * a0 + md.m11 * b0;
@@ -1829,7 +1882,13 @@ static cudaError_t launch_cols(const FipGeom& geo, const float2* grid, const uns
   smem = (size_t)fipfft::smem_elems(geo.g) * sizeof(float2);
   e = fft_smem_attr((const void*)k_fft_cols<LM, LE, false>, smem);
   if (e != cudaSuccess) return e;
-  k_fft_cols<LM, LE, false><<<dim3(geo.hp, batch), fft_threads<LM, LE>(), smem, s>>>(
+  // Persistent over columns: the CTAs that fit at once.
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fft_cols<LM, LE, false>,
+                                                    fft_threads<LM, LE>(), smem);
+  if (e != cudaSuccess) return e;
+  const int ctas = std::max(1, std::min(geo.hp, per_sm * sm_count()));
+  k_fft_cols<LM, LE, false><<<dim3(ctas, batch), fft_threads<LM, LE>(), smem, s>>>(
       grid, bbox, colbuf, tw, grid_stride, col_stride);
   return cudaGetLastError();
 }
@@ -1860,7 +1919,13 @@ static cudaError_t launch_rows(const FipGeom& geo, const float2* colbuf, unsigne
   smem = (size_t)fipfft::smem_elems(geo.g) * sizeof(float2);
   e = fft_smem_attr((const void*)k_fft_rows<LM, LE, false>, smem);
   if (e != cudaSuccess) return e;
-  k_fft_rows<LM, LE, false><<<dim3(geo.n / 2, batch), fft_threads<LM, LE>(), smem, s>>>(
+  // Persistent over row pairs: the CTAs that fit at once.
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fft_rows<LM, LE, false>,
+                                                    fft_threads<LM, LE>(), smem);
+  if (e != cudaSuccess) return e;
+  const int ctas = std::max(1, std::min(geo.n / 2, per_sm * sm_count()));
+  k_fft_rows<LM, LE, false><<<dim3(ctas, batch), fft_threads<LM, LE>(), smem, s>>>(
       colbuf, bbox, taper + geo.n / 2 + 1, pre, tw, col_stride, pre_stride);
   return cudaGetLastError();
 }
