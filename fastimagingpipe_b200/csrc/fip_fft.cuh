@@ -16,8 +16,8 @@
 // tw[k] = w^k for k < G, followed by the half table tw[G + m] = W^m,
 // W = e^{+2 pi i / M}, m < M / 2, which is all the passes read.  A thread's
 // pass twiddles depend on its lane only, so with 16 values per thread they
-// are loaded into registers before the band is staged (PassTw) and their
-// latency hides behind the staging loads.  The first pass
+// are loaded into registers once per transform (PassTw), beside the band's
+// staging loads, so their latency leaves the passes.  The first pass
 // reads the band through a caller functor and applies w^{c s}; the last pass
 // leaves Y_s in shared memory in natural order, read back per output by
 // fetch().

@@ -1883,10 +1883,14 @@ static cudaError_t launch_cols(const FipGeom& geo, const float2* grid, const uns
   e = fft_smem_attr((const void*)k_fft_cols<LM, LE, false>, smem);
   if (e != cudaSuccess) return e;
   // Persistent over columns: the CTAs that fit at once.
-  int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fft_cols<LM, LE, false>,
-                                                    fft_threads<LM, LE>(), smem);
-  if (e != cudaSuccess) return e;
+  // (Queried once per instantiation: the shape and shared memory are fixed by it.)
+  static const int per_sm = [&] {
+    int v = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_fft_cols<LM, LE, false>,
+                                                      fft_threads<LM, LE>(), smem) != cudaSuccess)
+      v = 1;
+    return std::max(v, 1);
+  }();
   const int ctas = std::max(1, std::min(geo.hp, per_sm * sm_count()));
   k_fft_cols<LM, LE, false><<<dim3(ctas, batch), fft_threads<LM, LE>(), smem, s>>>(
       grid, bbox, colbuf, tw, grid_stride, col_stride);
@@ -1920,10 +1924,14 @@ static cudaError_t launch_rows(const FipGeom& geo, const float2* colbuf, unsigne
   e = fft_smem_attr((const void*)k_fft_rows<LM, LE, false>, smem);
   if (e != cudaSuccess) return e;
   // Persistent over row pairs: the CTAs that fit at once.
-  int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fft_rows<LM, LE, false>,
-                                                    fft_threads<LM, LE>(), smem);
-  if (e != cudaSuccess) return e;
+  // (Queried once per instantiation: the shape and shared memory are fixed by it.)
+  static const int per_sm = [&] {
+    int v = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_fft_rows<LM, LE, false>,
+                                                      fft_threads<LM, LE>(), smem) != cudaSuccess)
+      v = 1;
+    return std::max(v, 1);
+  }();
   const int ctas = std::max(1, std::min(geo.n / 2, per_sm * sm_count()));
   k_fft_rows<LM, LE, false><<<dim3(ctas, batch), fft_threads<LM, LE>(), smem, s>>>(
       colbuf, bbox, taper + geo.n / 2 + 1, pre, tw, col_stride, pre_stride);
