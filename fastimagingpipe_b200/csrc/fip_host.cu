@@ -226,12 +226,12 @@ class CopyPool {
 // w = e^{+2 pi i / g}, for k < g, then the passes' half table W^m = w^{3 m},
 // W = e^{+2 pi i / M}, for m < M / 2 (fipfft).
 static std::vector<float2> fft_twiddles(int g) {
-  std::vector<float2> tw((size_t)g + g / 6);
+  std::vector<float2> tw((size_t)g + fipfft::half_table_elems(g));
   for (int k = 0; k < g; ++k) {
     const double a = 2.0 * FIP_M_PI * (double)k / (double)g;
     tw[k] = make_float2((float)cos(a), (float)sin(a));
   }
-  for (int m = 0; m < g / 6; ++m) tw[(size_t)g + m] = tw[(size_t)3 * m];
+  for (int m = 0; m < fipfft::half_table_elems(g); ++m) tw[(size_t)g + m] = tw[(size_t)3 * m];
   return tw;
 }
 
