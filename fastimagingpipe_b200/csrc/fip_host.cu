@@ -108,8 +108,8 @@ namespace {
 // segments cut into chunks that the workers and the caller claim from one
 // atomic word (job epoch << 32 | next chunk, claimed by compare-and-swap, so a
 // worker still finishing an earlier job never takes a chunk of the next).
-// Between jobs the workers poll for a short while (a call issues one job per
-// snapshot, back to back) before they block.
+// Between jobs the workers poll for a while (a call issues one job per
+// snapshot, and calls often follow one another) before they block.
 class CopyPool {
  public:
   struct Seg {
@@ -162,6 +162,9 @@ class CopyPool {
   static constexpr size_t kWorkers = 3;
   static constexpr size_t kChunk = 256 * 1024;
   static constexpr uint32_t kMaxChunks = 256;
+  // Poll window between jobs: longer than one call, so back-to-back calls
+  // find the workers awake.
+  static constexpr int kPollUs = 2000;
 
   CopyPool() {
     for (size_t k = 0; k < kWorkers; ++k) {
@@ -198,7 +201,7 @@ class CopyPool {
       const auto t0 = std::chrono::steady_clock::now();
       uint64_t e;
       while ((e = word_.load(std::memory_order_acquire) >> 32) == seen && !stop_.load()) {
-        if (std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(300)) {
+        if (std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(kPollUs)) {
           std::unique_lock<std::mutex> lk(mu_);
           cv_.wait(lk, [&] { return stop_.load() || (word_.load() >> 32) != seen; });
         } else {
@@ -285,13 +288,11 @@ struct fip_imager {
   float* result = nullptr;           // U*U
   float* stats = nullptr;
   // Device and pinned staging of the host-buffer path, 3 snapshot slots.
-  float* d_vr = nullptr;
-  float* d_vi = nullptr;
-  float* d_B = nullptr;
+  // Per snapshot k, one block of 4 nb floats at k * 4 nb: B [2 nb], vis
+  // real [nb], vis imaginary [nb], so each snapshot crosses PCIe in one copy.
+  float* d_snap = nullptr;
   float* d_V = nullptr;
-  float* h_vr = nullptr;
-  float* h_vi = nullptr;
-  float* h_B = nullptr;
+  float* h_snap = nullptr;
   float* h_V = nullptr;
   float* h_result = nullptr;
   StageTimer timer;
@@ -362,10 +363,10 @@ static void imager_free(fip_imager* im) {
   for (float* p : im->images)
     if (p) cudaFree(p);
   void* dptrs[] = {im->taper, im->twiddles, im->theta_tab, im->maxima, im->result, im->stats,
-                   im->d_vr, im->d_vi, im->d_B, im->d_V};
+                   im->d_snap, im->d_V};
   for (void* p : dptrs)
     if (p) cudaFree(p);
-  void* hptrs[] = {im->h_vr, im->h_vi, im->h_B, im->h_V, im->h_result};
+  void* hptrs[] = {im->h_snap, im->h_V, im->h_result};
   for (void* p : hptrs)
     if (p) cudaFreeHost(p);
   for (int k = 0; k < 3; ++k) {
@@ -529,13 +530,9 @@ int fip_imager_create(fip_imager** out, const fip_imager_config* cfg) {
   for (int k = 0; k < im->ring; ++k) FIP_ALLOC(dalloc(&im->images[k], n2, tot));
   FIP_ALLOC(dalloc(&im->maxima, 6, tot));
   FIP_ALLOC(dalloc(&im->result, std::max<size_t>((size_t)geo.u * geo.u, 1), tot));
-  FIP_ALLOC(dalloc(&im->d_vr, 3 * nb, tot));
-  FIP_ALLOC(dalloc(&im->d_vi, 3 * nb, tot));
-  FIP_ALLOC(dalloc(&im->d_B, 3 * nb * 2, tot));
+  FIP_ALLOC(dalloc(&im->d_snap, 3 * 4 * nb, tot));
   FIP_ALLOC(dalloc(&im->d_V, 27, tot));
-  FIP_ALLOC(cudaMallocHost((void**)&im->h_vr, 3 * nb * sizeof(float)));
-  FIP_ALLOC(cudaMallocHost((void**)&im->h_vi, 3 * nb * sizeof(float)));
-  FIP_ALLOC(cudaMallocHost((void**)&im->h_B, 3 * nb * 2 * sizeof(float)));
+  FIP_ALLOC(cudaMallocHost((void**)&im->h_snap, 3 * 4 * nb * sizeof(float)));
   FIP_ALLOC(cudaMallocHost((void**)&im->h_V, 27 * sizeof(float)));
   FIP_ALLOC(cudaMallocHost((void**)&im->h_result,
                            std::max<size_t>((size_t)geo.u * geo.u, 1) * sizeof(float)));
@@ -828,20 +825,17 @@ int fip_pipe_host(fip_imager* im, const float* vr, const float* vi, const float*
   // Per snapshot: host copy into pinned slot k (CPU), async H2D on the copy
   // stream, then the snapshot's lane images it while the CPU stages k+1.
   for (int k = 0; k < 3; ++k) {
-    float* hvr = im->h_vr + (size_t)k * nb;
-    float* hvi = im->h_vi + (size_t)k * nb;
-    float* hB = im->h_B + (size_t)k * nb * 2;
-    const CopyPool::Seg segs[3] = {{hB, B + (size_t)k * nb * 2, nb * 2 * sizeof(float)},
-                                   {hvr, vr + (size_t)k * nb, nb * sizeof(float)},
-                                   {hvi, vi + (size_t)k * nb, nb * sizeof(float)}};
+    float* hs = im->h_snap + (size_t)k * 4 * nb;
+    float* ds = im->d_snap + (size_t)k * 4 * nb;
+    const CopyPool::Seg segs[3] = {{hs, B + (size_t)k * nb * 2, nb * 2 * sizeof(float)},
+                                   {hs + 2 * nb, vr + (size_t)k * nb, nb * sizeof(float)},
+                                   {hs + 3 * nb, vi + (size_t)k * nb, nb * sizeof(float)}};
     CopyPool::get().copy(segs, 3);
-    float* dvr = im->d_vr + (size_t)k * nb;
-    float* dvi = im->d_vi + (size_t)k * nb;
-    float* dB = im->d_B + (size_t)k * nb * 2;
+    float* dB = ds;
+    float* dvr = ds + 2 * nb;
+    float* dvi = ds + 3 * nb;
     float* dV = im->d_V + (size_t)k * 9;
-    FIP_CUDA(cudaMemcpyAsync(dvr, hvr, nb * sizeof(float), cudaMemcpyHostToDevice, cs));
-    FIP_CUDA(cudaMemcpyAsync(dvi, hvi, nb * sizeof(float), cudaMemcpyHostToDevice, cs));
-    FIP_CUDA(cudaMemcpyAsync(dB, hB, nb * 2 * sizeof(float), cudaMemcpyHostToDevice, cs));
+    FIP_CUDA(cudaMemcpyAsync(ds, hs, 4 * nb * sizeof(float), cudaMemcpyHostToDevice, cs));
     FIP_CUDA(cudaEventRecord(im->ev_copied[k], cs));
     FIP_TRY(image_on_lane(im, k, dvr, dvi, dB, dV, nb, im->images[k], im->maxima + k, s,
                           im->ev_copied[k], early));
