@@ -144,6 +144,40 @@ def algorithmic_bytes(stage, n, nb, band, t):
     return None
 
 
+def _peak():
+    peaks_path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        with open(peaks_path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _profile_counters():
+    """Per-stage DRAM traffic and issue counters from the committed ncu summary."""
+    path = os.path.join(REPO, "profiles", "stage_counters.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return {}
+
+
+def roofline_of(stage, ms, n, nb, band, t):
+    """HBM roofline of one launch of a stage: algorithmic bytes / launch time
+    against the measured copy bandwidth."""
+    peak, src = _peak()
+    alg = algorithmic_bytes(stage, n, nb, band, t)
+    achieved = alg / (ms * 1e-3) / 1e9 if alg and ms > 0 else None
+    prof = _profile_counters().get(stage, {})
+    out = {"kernel": stage, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+           "frac": (achieved / peak) if achieved else None,
+           "traffic": prof.get("dram_bytes"), "peak_source": src,
+           "algorithmic_bytes_per_launch": alg, "avg_launch_ms": ms}
+    for k in ("issue_active_pct", "warp_instructions", "instructions_per_unit", "unit"):
+        if k in prof:
+            out["ncu_" + k] = prof[k]
+    return out
+
+
 def run_reference(args, rank):
     line = {"impl": "reference", "metric": METRIC, "unit": UNIT, "higher_is_better": True}
     if rank != 0:
@@ -412,32 +446,19 @@ def main():
 
     line = None
     if rank == 0:
-        # Dominant HBM-bound kernel and its roofline (the reference-chain
-        # pixel mapping, k_targets, is bound by the SFU/conversion pipe, not
-        # by memory; it is reported beside it).
+        # The dominant kernel (largest share of the serialised stage time) and
+        # its HBM roofline: algorithmic bytes per launch over the measured
+        # launch time.  Its issue-side figures (from the committed ncu summary)
+        # ride along, since a kernel far below the HBM roof is bound elsewhere.
         per_launch = {k: (ms / c if c else 0.0, c) for k, (ms, c) in stages.items()}
-        hbm_stages = [k for k in per_launch if per_launch[k][1] > 0 and k != "targets"]
-        dom = max(hbm_stages, key=lambda k: per_launch[k][0] * per_launch[k][1])
-        dom_ms = per_launch[dom][0]
-        alg = algorithmic_bytes(dom, n, nb, band, t)
-        peaks_path = os.path.join(REPO, "MEASURED_PEAKS.json")
-        peak, peak_src = 6650.0, "fallback"
-        if os.path.exists(peaks_path):
-            with open(peaks_path) as f:
-                peak, peak_src = float(json.load(f)["hbm_gbs"]), "measured"
-        achieved = alg / (dom_ms * 1e-3) / 1e9 if alg and dom_ms > 0 else None
-        traffic = None
-        tpath = os.path.join(REPO, "profiles", "dram_traffic.json")
-        if os.path.exists(tpath):
-            with open(tpath) as f:
-                traffic = json.load(f).get(dom)
-        roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
-                    "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                    "traffic": traffic, "peak_source": peak_src,
-                    "algorithmic_bytes_per_launch": alg, "avg_launch_ms": dom_ms,
-                    "compute_bound_kernel": {
-                        "kernel": "targets", "bound": "sfu/conversion pipe",
-                        "avg_launch_ms": per_launch.get("targets", (None,))[0]}}
+        shares = {k: per_launch[k][0] * per_launch[k][1] for k in per_launch
+                  if per_launch[k][1] > 0}
+        total_stage_ms = sum(shares.values())
+        dom = max(shares, key=shares.get)
+        roofline = roofline_of(dom, per_launch[dom][0], n, nb, band, t)
+        roofline["time_share"] = shares[dom] / total_stage_ms if total_stage_ms else None
+        roofline["others"] = {k: roofline_of(k, per_launch[k][0], n, nb, band, t)["frac"]
+                              for k in shares if k != dom}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,

@@ -71,6 +71,8 @@ def lib() -> ctypes.CDLL:
         L.fip_pipe_device.argtypes = [vp, vp, vp, vp, vp, sz, vp, vp]
         L.fip_imager_image.argtypes = [vp, ctypes.c_int]
         L.fip_imager_image.restype = vp
+        L.fip_imager_check.argtypes = [vp, vp]
+        L.fip_batch_check.argtypes = [vp, vp]
         L.fip_pipe_host.argtypes = [vp, vp, vp, vp, vp, sz, sz, vp]
         L.fip_pixel_targets.argtypes = [vp, vp, vp, ctypes.c_int, vp]
         L.fip_plane_project.argtypes = [vp, vp, sz, sz, vp, vp, vp]
@@ -263,6 +265,11 @@ class Imager:
         _check(lib().fip_pipe_device(self._h, _ptr(vis_re), _ptr(vis_im), _ptr(B), _ptr(V), nb,
                                      _ptr(result), _stream(stream)))
 
+    def check(self, stream=None):
+        """Raises FipError if a gather reprojection since the last check had a
+        tile outside its domain (a folding wide-field geometry)."""
+        _check(lib().fip_imager_check(self._h, _stream(stream)))
+
     def image_ptr(self, k: int) -> int:
         return int(lib().fip_imager_image(self._h, k) or 0)
 
@@ -340,6 +347,11 @@ class Batch:
 
     def reset(self):
         _check(lib().fip_batch_reset(self._h))
+
+    def check(self, stream=None):
+        """Raises FipError if a gather reprojection since the last check had a
+        tile outside its domain (a folding wide-field geometry)."""
+        _check(lib().fip_batch_check(self._h, _stream(stream)))
 
     @property
     def device_bytes(self) -> int:

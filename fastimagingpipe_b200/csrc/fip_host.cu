@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -163,8 +164,18 @@ class CopyPool {
   static constexpr size_t kChunk = 256 * 1024;
   static constexpr uint32_t kMaxChunks = 256;
   // Poll window between jobs: longer than one call, so back-to-back calls
-  // find the workers awake.
-  static constexpr int kPollUs = 2000;
+  // find the workers awake.  Each worker spins (yielding) for this long after
+  // every job, about 3 x 2 ms of CPU per call at the default; the
+  // FIP_COPY_POLL_US environment variable sets it (0: block at once).
+  static int poll_us() {
+    static const int us = [] {
+      const char* e = std::getenv("FIP_COPY_POLL_US");
+      if (!e || !*e) return 2000;
+      const long v = std::strtol(e, nullptr, 10);
+      return (int)std::max(0L, std::min(v, 1000000L));
+    }();
+    return us;
+  }
 
   CopyPool() {
     for (size_t k = 0; k < kWorkers; ++k) {
@@ -201,7 +212,7 @@ class CopyPool {
       const auto t0 = std::chrono::steady_clock::now();
       uint64_t e;
       while ((e = word_.load(std::memory_order_acquire) >> 32) == seen && !stop_.load()) {
-        if (std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(kPollUs)) {
+        if (std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(poll_us())) {
           std::unique_lock<std::mutex> lk(mu_);
           cv_.wait(lk, [&] { return stop_.load() || (word_.load() >> 32) != seen; });
         } else {
@@ -287,6 +298,11 @@ struct fip_imager {
   float* maxima = nullptr;           // [6] device floats (written as max bits)
   float* result = nullptr;           // U*U
   float* stats = nullptr;
+  // Set by a gather launch whose tile lay outside the gather's domain
+  // (fip_gather_domain_ok), read and cleared by fip_imager_check and the
+  // host-buffer path; h_err is its pinned copy.
+  unsigned* gather_err = nullptr;
+  unsigned* h_err = nullptr;
   // Device and pinned staging of the host-buffer path, 3 snapshot slots.
   // Per snapshot k, one block of 4 nb floats at k * 4 nb: B [2 nb], vis
   // real [nb], vis imaginary [nb], so each snapshot crosses PCIe in one copy.
@@ -363,10 +379,10 @@ static void imager_free(fip_imager* im) {
   for (float* p : im->images)
     if (p) cudaFree(p);
   void* dptrs[] = {im->taper, im->twiddles, im->theta_tab, im->maxima, im->result, im->stats,
-                   im->d_snap, im->d_V};
+                   im->d_snap, im->d_V, im->gather_err};
   for (void* p : dptrs)
     if (p) cudaFree(p);
-  void* hptrs[] = {im->h_snap, im->h_V, im->h_result};
+  void* hptrs[] = {im->h_snap, im->h_V, im->h_result, im->h_err};
   for (void* p : hptrs)
     if (p) cudaFreeHost(p);
   for (int k = 0; k < 3; ++k) {
@@ -536,6 +552,10 @@ int fip_imager_create(fip_imager** out, const fip_imager_config* cfg) {
   FIP_ALLOC(cudaMallocHost((void**)&im->h_V, 27 * sizeof(float)));
   FIP_ALLOC(cudaMallocHost((void**)&im->h_result,
                            std::max<size_t>((size_t)geo.u * geo.u, 1) * sizeof(float)));
+  FIP_ALLOC(dalloc(&im->gather_err, 1, tot));
+  FIP_ALLOC(cudaMemset(im->gather_err, 0, sizeof(unsigned)));
+  FIP_ALLOC(cudaMallocHost((void**)&im->h_err, sizeof(unsigned)));
+  *im->h_err = 0;
 
   if (!im->custom_fft) {
     cufftResult r = cufftCreate(&im->plan);
@@ -571,7 +591,8 @@ size_t fip_imager_device_bytes(const fip_imager* im) { return im ? im->device_by
 static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const float* vi,
                                const float* B, const float* V, size_t nb, float* image,
                                float* image_max, cudaStream_t s, bool fork_targets,
-                               bool targets_ready = false, cudaEvent_t targets_ev = nullptr) {
+                               bool targets_ready = false, cudaEvent_t targets_ev = nullptr,
+                               bool force_scatter = false) {
   const FipGeom& geo = im->geo;
   if (nb > im->cfg.max_baselines) return fail(FIP_ERR_ARG, "nb exceeds the imager's capacity");
   if (nb == 0) return fail(FIP_ERR_ARG, "nb must be positive");
@@ -590,7 +611,9 @@ static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const f
     gvr = L.q_re;
     gvi = L.q_im;
   }
-  const bool gather = im->cfg.reproject == 0;
+  // force_scatter: the snapshot's geometry lies outside the gather's domain
+  // (checked on the host where V is a host array): the reference's scheme.
+  const bool gather = im->cfg.reproject == 0 && !force_scatter;
   const bool chain_targets = gather && !precise;
   // The pixel mapping depends on V only: it may run beside gridding + FFT on
   // the side stream (serialised on s when profiling, so every stage's time
@@ -649,7 +672,7 @@ static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const f
     k = stage_begin(im, ST_REPROJECT, s);
     FIP_CUDA(fip_launch_reproject_gather(geo, L.pre, L.targets, V, (int)nb, L.bins.bbox + 3,
                                          image, reinterpret_cast<unsigned*>(image_max),
-                                         precise ? 1 : 0, s));
+                                         precise ? 1 : 0, s, im->gather_err));
     stage_end(im, k, s);
     im->launches += 1;
   }
@@ -663,16 +686,17 @@ static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const f
 static int image_on_lane(fip_imager* im, int k, const float* vr, const float* vi,
                          const float* B, const float* V, size_t nb, float* image,
                          float* image_max, cudaStream_t s, cudaEvent_t after,
-                         bool targets_ready = false) {
+                         bool targets_ready = false, bool force_scatter = false) {
   if (im->lanes == 1 || im->timer.on) {
     FIP_CUDA(cudaStreamWaitEvent(s, after, 0));
     return image_snapshot_impl(im, im->lane[k % im->lanes], vr, vi, B, V, nb, image, image_max,
-                               s, true);
+                               s, true, false, nullptr, force_scatter);
   }
   Lane& L = im->lane[k % im->lanes];
   FIP_CUDA(cudaStreamWaitEvent(L.stream, after, 0));
   FIP_TRY(image_snapshot_impl(im, L, vr, vi, B, V, nb, image, image_max, L.stream, false,
-                              targets_ready, targets_ready ? L.ev_targets : nullptr));
+                              targets_ready, targets_ready ? L.ev_targets : nullptr,
+                              force_scatter));
   FIP_CUDA(cudaEventRecord(L.ev_done, L.stream));
   return FIP_OK;
 }
@@ -801,12 +825,37 @@ const float* fip_imager_image(const fip_imager* im, int k) {
   return im->images[k];
 }
 
+static const char* gather_domain_message() {
+  return "a reprojection tile lay outside the tile gather's domain (the plane-to-sky map "
+         "folds or nears the horizon there: a very wide field with a strongly tilted "
+         "plane); its image is not reliable; image such snapshots with reproject = 1 "
+         "(the reference's scatter)";
+}
+
+int fip_imager_check(fip_imager* im, void* stream) {
+  if (!im) return fail(FIP_ERR_ARG, "null imager");
+  DeviceGuard g(im->cfg.device);
+  cudaStream_t s = (cudaStream_t)stream;
+  FIP_TRY(call_enter(im, s));
+  FIP_CUDA(cudaMemcpyAsync(im->h_err, im->gather_err, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                           s));
+  FIP_CUDA(cudaMemsetAsync(im->gather_err, 0, sizeof(unsigned), s));
+  FIP_TRY(call_leave(im, s));
+  FIP_CUDA(cudaStreamSynchronize(s));
+  if (*im->h_err) return fail(FIP_ERR_STATE, gather_domain_message());
+  return FIP_OK;
+}
+
 int fip_pipe_host(fip_imager* im, const float* vr, const float* vi, const float* B,
                   const float* V, size_t nb, size_t nsnap, float* result) {
   if (!im) return fail(FIP_ERR_ARG, "null imager");
   if (!vr || !vi || !B || !V || !result) return fail(FIP_ERR_ARG, "null host pointer");
   if (nsnap < 3)
     return fail(FIP_ERR_ARG, "num_snapshots must be >= 3 (the pipeline images three snapshots)");
+  // The pinned staging block and the device upload buffer hold three
+  // snapshots of max_baselines each: check before any copy into them.
+  if (nb == 0 || nb > im->cfg.max_baselines)
+    return fail(FIP_ERR_ARG, "nb must be in [1, the imager's max_baselines]");
   if (im->geo.t <= 0) return fail(FIP_ERR_ARG, "imager has no trigger tile (unit_size 0)");
   DeviceGuard g(im->cfg.device);
   cudaStream_t s = im->stream, cs = im->copy_stream;
@@ -816,6 +865,12 @@ int fip_pipe_host(fip_imager* im, const float* vr, const float* vi, const float*
   // only V, so with concurrent lanes it starts on every lane while the host
   // still stages the visibilities.
   std::memcpy(im->h_V, V, 27 * sizeof(float));
+  // Snapshots whose plane-to-sky map leaves the gather's domain (very wide,
+  // strongly tilted fields) reproject with the reference's scatter instead.
+  bool scatter[3] = {false, false, false};
+  if (im->cfg.reproject == 0)
+    for (int k = 0; k < 3; ++k)
+      scatter[k] = !fip_gather_domain_ok(V + 9 * k, im->geo.n, im->cfg.cell_size);
   FIP_CUDA(cudaMemcpyAsync(im->d_V, im->h_V, 27 * sizeof(float), cudaMemcpyHostToDevice, cs));
   const bool early = targets_ahead(im);
   if (early) {
@@ -838,7 +893,7 @@ int fip_pipe_host(fip_imager* im, const float* vr, const float* vi, const float*
     FIP_CUDA(cudaMemcpyAsync(ds, hs, 4 * nb * sizeof(float), cudaMemcpyHostToDevice, cs));
     FIP_CUDA(cudaEventRecord(im->ev_copied[k], cs));
     FIP_TRY(image_on_lane(im, k, dvr, dvi, dB, dV, nb, im->images[k], im->maxima + k, s,
-                          im->ev_copied[k], early));
+                          im->ev_copied[k], early, scatter[k]));
   }
   for (int k = 0; k < 3; ++k) FIP_TRY(wait_lane(im, k, s));
   im->last_lane = 2 % im->lanes;
@@ -853,9 +908,13 @@ int fip_pipe_host(fip_imager* im, const float* vr, const float* vi, const float*
   const size_t uu = (size_t)im->geo.u * im->geo.u;
   FIP_CUDA(cudaMemcpyAsync(im->h_result, im->result, uu * sizeof(float), cudaMemcpyDeviceToHost,
                            s));
+  FIP_CUDA(cudaMemcpyAsync(im->h_err, im->gather_err, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                           s));
+  FIP_CUDA(cudaMemsetAsync(im->gather_err, 0, sizeof(unsigned), s));
   FIP_TRY(call_leave(im, s));
   FIP_CUDA(cudaStreamSynchronize(s));
   std::memcpy(result, im->h_result, uu * sizeof(float));
+  if (*im->h_err) return fail(FIP_ERR_STATE, gather_domain_message());
   if (im->timer.on) stage_collect(im);
   return FIP_OK;
 }
@@ -1107,15 +1166,26 @@ int fip_collapse_visibilities(const float* v0r, const float* v0i, const float* v
 // ---------------------------------------------------------------------------
 
 namespace {
+// One cached imager.  Its mutex is held for the whole call that uses it, so
+// concurrent callers serialise only when they share an imager; the cache's
+// own mutex covers the lookup.  An entry evicted while a call still uses it
+// is freed when that call drops its reference.
+struct CachedImager {
+  fip_imager* im = nullptr;
+  std::mutex mu;
+  ~CachedImager() { imager_free(im); }
+};
 struct CacheEntry {
   int device;
   size_t n, nb, t;
   float cell;
-  fip_imager* im;
+  std::shared_ptr<CachedImager> box;
   unsigned long long last_use;
 };
 std::mutex g_cache_mu;
-std::vector<CacheEntry> g_cache;
+// Never destroyed: imagers still cached at exit are left to the driver's
+// teardown rather than freed after the CUDA runtime has unloaded.
+std::vector<CacheEntry>& g_cache = *new std::vector<CacheEntry>;
 unsigned long long g_tick = 0;
 constexpr size_t kCacheMax = 2;
 }  // namespace
@@ -1131,37 +1201,45 @@ int fip_pipe(const float* vis_re, const float* vis_im, const float* B, const flo
     return fail(FIP_ERR_ARG, "num_snapshots must be >= 3 (three snapshots are imaged)");
   int dev = 0;
   FIP_CUDA(cudaGetDevice(&dev));
-  std::lock_guard<std::mutex> lock(g_cache_mu);
-  fip_imager* im = nullptr;
-  for (auto& e : g_cache)
-    if (e.device == dev && e.n == image_size && e.nb == num_baselines && e.t == unit_size &&
-        e.cell == cell_size) {
-      im = e.im;
-      e.last_use = ++g_tick;
+  std::shared_ptr<CachedImager> box;
+  {
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    // Any imager of this geometry with room for num_baselines serves the call
+    // (nb is a per-call argument below its capacity), the smallest first, so
+    // a change in the flagged count does not re-create an imager.
+    CacheEntry* best = nullptr;
+    for (auto& e : g_cache)
+      if (e.device == dev && e.n == image_size && e.nb >= num_baselines && e.t == unit_size &&
+          e.cell == cell_size && (!best || e.nb < best->nb))
+        best = &e;
+    if (best) {
+      best->last_use = ++g_tick;
+      box = best->box;
+    } else {
+      if (g_cache.size() >= kCacheMax) {
+        auto it = std::min_element(g_cache.begin(), g_cache.end(),
+                                   [](const CacheEntry& a, const CacheEntry& b) {
+                                     return a.last_use < b.last_use;
+                                   });
+        g_cache.erase(it);
+      }
+      fip_imager_config cfg{};
+      cfg.image_size = image_size;
+      cfg.max_baselines = num_baselines;
+      cfg.unit_size = unit_size;
+      cfg.cell_size = cell_size;
+      cfg.form = FIP_FORM_PLAIN;
+      cfg.vis_storage = FIP_STORE_F32;
+      cfg.device = dev;
+      cfg.reproject = 0;
+      box = std::make_shared<CachedImager>();
+      FIP_TRY(fip_imager_create(&box->im, &cfg));
+      g_cache.push_back(CacheEntry{dev, image_size, num_baselines, unit_size, cell_size, box,
+                                   ++g_tick});
     }
-  if (!im) {
-    if (g_cache.size() >= kCacheMax) {
-      auto it = std::min_element(g_cache.begin(), g_cache.end(),
-                                 [](const CacheEntry& a, const CacheEntry& b) {
-                                   return a.last_use < b.last_use;
-                                 });
-      imager_free(it->im);
-      g_cache.erase(it);
-    }
-    fip_imager_config cfg{};
-    cfg.image_size = image_size;
-    cfg.max_baselines = num_baselines;
-    cfg.unit_size = unit_size;
-    cfg.cell_size = cell_size;
-    cfg.form = FIP_FORM_PLAIN;
-    cfg.vis_storage = FIP_STORE_F32;
-    cfg.device = dev;
-    cfg.reproject = 0;
-    FIP_TRY(fip_imager_create(&im, &cfg));
-    g_cache.push_back(CacheEntry{dev, image_size, num_baselines, unit_size, cell_size, im,
-                                 ++g_tick});
   }
-  return fip_pipe_host(im, vis_re, vis_im, B, V, num_baselines, num_snapshots, result);
+  std::lock_guard<std::mutex> lock(box->mu);
+  return fip_pipe_host(box->im, vis_re, vis_im, B, V, num_baselines, num_snapshots, result);
 }
 
 }  // extern "C"
@@ -1210,6 +1288,7 @@ struct fip_batch {
   // snapshots go to slots 2 .. count + 1.
   float* images = nullptr;            // [smax + 2][N N]
   float* maxima = nullptr;            // [smax + 2]
+  unsigned* gather_err = nullptr;     // [1] set by a gather tile outside its domain
   int carried = 0;
   cudaStream_t branch[kBranches] = {};
   cudaEvent_t fork = nullptr;
@@ -1241,7 +1320,8 @@ void batch_free(fip_batch* b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   void* ptrs[] = {b->twiddles, b->theta_tab, b->taper, b->count, b->offset, b->cursor, b->entries, b->work,
                   b->nwork, b->bbox, b->multi, b->nmulti, b->grid, b->colbuf, b->pre,
-                  b->targets, b->q_re, b->q_im, b->q_scale, b->images, b->maxima};
+                  b->targets, b->q_re, b->q_im, b->q_scale, b->images, b->maxima,
+                  b->gather_err};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int k = 0; k < kBranches; ++k) {
@@ -1314,7 +1394,7 @@ int batch_record(fip_batch* b, const float* const* vr, const float* const* vi,
     FIP_CUDA(fip_launch_reproject_gather(
         geo, b->pre + k * b->n2, precise ? nullptr : b->targets + k * b->n2, V[k], (int)nb[k],
         b->bbox + 4 * k + 3, b->images + (k + 2) * b->n2,
-        reinterpret_cast<unsigned*>(b->maxima + k + 2), precise ? 1 : 0, bs));
+        reinterpret_cast<unsigned*>(b->maxima + k + 2), precise ? 1 : 0, bs, b->gather_err));
     launches += 1;
   }
   for (int i = 0; i < kBranches; ++i) {
@@ -1425,6 +1505,8 @@ int fip_batch_create(fip_batch** out, const fip_imager_config* cfg, size_t max_s
   }
   FIP_BALLOC(dalloc(&b->images, (S + 2) * b->n2, tot));
   FIP_BALLOC(dalloc(&b->maxima, S + 2, tot));
+  FIP_BALLOC(dalloc(&b->gather_err, 1, tot));
+  FIP_BALLOC(cudaMemset(b->gather_err, 0, sizeof(unsigned)));
   FIP_BALLOC(dalloc(&b->taper, 2 * ((size_t)geo.n / 2 + 1), tot));
   {
     const std::vector<float2> tw = fft_twiddles(geo.g);
@@ -1457,6 +1539,18 @@ unsigned long long fip_batch_kernel_launches(const fip_batch* b) { return b ? b-
 int fip_batch_reset(fip_batch* b) {
   if (!b) return fail(FIP_ERR_ARG, "null batch");
   b->carried = 0;
+  return FIP_OK;
+}
+
+int fip_batch_check(fip_batch* b, void* stream) {
+  if (!b) return fail(FIP_ERR_ARG, "null batch");
+  DeviceGuard g(b->cfg.device);
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned flag = 0;
+  FIP_CUDA(cudaMemcpyAsync(&flag, b->gather_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  FIP_CUDA(cudaMemsetAsync(b->gather_err, 0, sizeof(unsigned), s));
+  FIP_CUDA(cudaStreamSynchronize(s));
+  if (flag) return fail(FIP_ERR_STATE, gather_domain_message());
   return FIP_OK;
 }
 

@@ -90,10 +90,16 @@ cudaError_t fip_launch_reproject_scatter(const FipGeom& geo, const float* pre, c
 // records the image maximum into *img_max (atomic max, caller zeroes it).
 bool fip_gather_supported(const FipGeom& geo, int exact_targets);
 // pre_max: maximum of pre (float bits), from the transform's epilogue.
+// err (or null): set to nonzero when a tile lies outside the gather's domain
+// (fip_gather_domain_ok); its image is then not to be trusted.
 cudaError_t fip_launch_reproject_gather(const FipGeom& geo, const float* pre,
                                         const float2* targets, const float* V, int nb,
                                         const unsigned* pre_max, float* dst, unsigned* img_max,
-                                        int exact_targets, cudaStream_t s);
+                                        int exact_targets, cudaStream_t s, unsigned* err);
+// Whether the plane-to-sky map of basis V (host, row-major 3 x 3) stays in
+// the tile gather's domain over an N x N image: well inside the horizon and
+// without folds.  Outside it only the source scatter reprojects correctly.
+bool fip_gather_domain_ok(const float* V, int n, float cell);
 cudaError_t fip_launch_image_max(const float* img, size_t count, unsigned* out, cudaStream_t s);
 // Trigger: per-tile statistics of (I1, I2, I3) and the tLISI combine.
 cudaError_t fip_launch_trigger(const FipGeom& geo, const float* I1, const float* I2,

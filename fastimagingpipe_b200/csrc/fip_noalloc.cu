@@ -57,15 +57,22 @@ std::mutex g_addr_mu;
 void* g_addr[kMaxDevices] = {};
 
 // Device address of g_grid_scratch on the current device.  Host code only
-// sees a host-side stand-in for the symbol, so the address is looked up once
-// per device, with that device current, and cached.
-int scratch_address(Scratch** out) {
+// sees a host-side stand-in for the symbol, so the address is looked up with
+// the device current.  Outside stream capture the lookup runs on every call
+// (it allocates nothing), so a caller that reset the device and got a new
+// context gets the array's new address; while `stream` is capturing, the
+// address recorded by the last call outside capture is used, so that the
+// first call on a device has to come before any capture.
+int scratch_address(cudaStream_t stream, Scratch** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fip_set_error(FIP_ERR_CUDA, cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) return fip_set_error(FIP_ERR_ARG, "device ordinal too large");
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(stream, &cap);
+  if (e != cudaSuccess) return fip_set_error(FIP_ERR_CUDA, cudaGetErrorString(e));
   std::lock_guard<std::mutex> lock(g_addr_mu);
-  if (!g_addr[dev]) {
+  if (cap == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_grid_scratch);
     if (e != cudaSuccess || p == nullptr)
@@ -73,6 +80,10 @@ int scratch_address(Scratch** out) {
                            std::string("cudaGetSymbolAddress(grid scratch): ") +
                                cudaGetErrorString(e));
     g_addr[dev] = p;
+  } else if (!g_addr[dev]) {
+    return fip_set_error(FIP_ERR_STATE,
+                         "fip_grid_snapshot_noalloc: the first call on a device must come "
+                         "before any stream capture");
   }
   *out = static_cast<Scratch*>(g_addr[dev]);
   return FIP_OK;
@@ -95,8 +106,9 @@ extern "C" int fip_grid_snapshot_noalloc(const float* vis_re, const float* vis_i
                          "[8, 4096] (fixed scratch size)");
   if (!(cell_size > 0.f) || !(cell_size < 1.f))
     return fip_set_error(FIP_ERR_ARG, "cell_size must be in (0, 1) rad");
+  cudaStream_t s = (cudaStream_t)stream;
   Scratch* sc = nullptr;
-  const int st = scratch_address(&sc);
+  const int st = scratch_address(s, &sc);
   if (st != FIP_OK) return st;
 
   FipGeom geo{};
@@ -121,7 +133,6 @@ extern "C" int fip_grid_snapshot_noalloc(const float* vis_re, const float* vis_i
   bins.cap = kMaxEntries;
   bins.wcap = kMaxWork;
 
-  cudaStream_t s = (cudaStream_t)stream;
   cudaError_t e = fip_launch_bin(geo, B, (int)nb, bins, s);
   if (e == cudaSuccess)
     e = fip_launch_grid(geo, B, vis_re, vis_im, FIP_VIS_F32, nullptr, V, (int)nb, bins,

@@ -1274,19 +1274,26 @@ __device__ __forceinline__ void exact_forward(const ExactMap<T>& m, T a, T b, T&
 }
 
 // Source (a, b), relative to the centre, of an exact target (LL, MM):
-// fixed-point iteration on the slant term, a contraction for any field
-// smaller than a radian.
+// fixed-point iteration on the slant term, a contraction wherever the map
+// does not fold (the slant part's Jacobian determinant stays positive); it
+// runs until the step is below 1e-3 pixel (or 64 steps).  Returns how far
+// the forward map of the result lands from (LL, MM), in pixels.
 template <typename T>
-__device__ __forceinline__ void exact_inverse(const ExactMap<T>& m, T LL, T MM, T& a, T& b) {
+__device__ __forceinline__ T exact_inverse(const ExactMap<T>& m, T LL, T MM, T& a, T& b) {
   T P1 = LL, P2 = MM;
-#pragma unroll
-  for (int it = 0; it < 6; ++it) {
+  for (int it = 0; it < 64; ++it) {
     const T zc = slant_over_cell(m, P1, P2);
-    P1 = LL + m.xi * zc;
-    P2 = MM - m.eta * zc;
+    const T q1 = LL + m.xi * zc, q2 = MM - m.eta * zc;
+    const T step = fmax(fabs(q1 - P1), fabs(q2 - P2));
+    P1 = q1;
+    P2 = q2;
+    if (step <= (T)1e-3) break;
   }
   a = m.i00 * P1 + m.i01 * P2;
   b = m.i10 * P1 + m.i11 * P2;
+  T L2, M2;
+  exact_forward(m, a, b, L2, M2);
+  return fmax(fabs(L2 - LL), fabs(M2 - MM));
 }
 
 // Destination-tile-major reprojection.  The candidate source pixels of a
@@ -1311,7 +1318,7 @@ template <bool EXACT>
 __global__ void __launch_bounds__(kThreads) k_reproject_gather(
     const float* __restrict__ pre, const float2* __restrict__ tg, const float* __restrict__ V,
     int n, int nb, float cell, float delta, const unsigned* __restrict__ pre_max,
-    float* __restrict__ dst, unsigned* img_max) {
+    float* __restrict__ dst, unsigned* img_max, unsigned* err) {
   __shared__ __align__(16) unsigned s_tile[kTW * kTR];
   __shared__ int s_base[kMaxRows];  // pixel index of row r's first candidate minus its number
   __shared__ int s_off[kMaxRows + 1];
@@ -1332,16 +1339,48 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
   // corners and read by every thread after the barrier.
   __shared__ ExactMap<double> s_md;
   if (EXACT && threadIdx.x == 4) s_md = make_map<double>(V, cell);
-  if (threadIdx.x < 4) {
+  // Preimage corners of the tile widened by the splat reach and delta (lanes
+  // 0-3 of warp 0), the tile's domain check and its curvature margin.
+  __shared__ float s_sag;
+  if (warp == 0) {
     const ExactMap<float> mf = make_map_f32(V, cell);
     const float Llo = (float)(c0 - h) - 1.0f - delta, Lhi = (float)(c0 + kDT - h) + delta;
     const float Mlo = (float)(r0 - h) - 1.0f - delta, Mhi = (float)(r0 + kDT - h) + delta;
-    const float L = (threadIdx.x == 0 || threadIdx.x == 3) ? Llo : Lhi;
-    const float M = (threadIdx.x < 2) ? Mlo : Mhi;
-    float a, b;
-    exact_inverse(mf, L, M, a, b);
-    s_q[threadIdx.x][0] = a;
-    s_q[threadIdx.x][1] = b;
+    float a = 0.f, b = 0.f, res = 0.f, r2 = 0.f, det = 1.f;
+    if (lane < 4) {
+      const float L = (lane == 0 || lane == 3) ? Llo : Lhi;
+      const float M = (lane < 2) ? Mlo : Mhi;
+      res = exact_inverse(mf, L, M, a, b);
+      s_q[lane][0] = a;
+      s_q[lane][1] = b;
+      // Sky offset (X, Y) of the source point in radians, the slant part's
+      // Jacobian determinant there: 1 - xi X / n + eta Y / n, n = sqrt(1 - r2).
+      const float X = cell * (mf.m00 * a + mf.m01 * b - 1.0f);
+      const float Y = cell * (mf.m10 * a + mf.m11 * b - 1.0f);
+      r2 = X * X + Y * Y;
+      const float nn = sqrtf(fmaxf(1.0f - r2, 1e-6f));
+      det = 1.0f - mf.xi * X / nn + mf.eta * Y / nn;
+    }
+#pragma unroll
+    for (int o = 1; o < 4; o <<= 1) {
+      res = fmaxf(res, __shfl_xor_sync(0xffffffffu, res, o));
+      r2 = fmaxf(r2, __shfl_xor_sync(0xffffffffu, r2, o));
+      det = fminf(det, __shfl_xor_sync(0xffffffffu, det, o));
+    }
+    if (lane == 0) {
+      // The candidate bounds hold while the inverse converged, the tile lies
+      // well inside the horizon (r2 < 0.98) and the map does not fold
+      // (det > 1/4); a tile outside that domain is reported, not skipped.
+      if (err && !(res < 0.05f && r2 < 0.98f && det > 0.25f)) atomicOr(err, 1u);
+      // The preimage's edges bow away from the chords between its corners
+      // by at most ell^2 / 8 times the slant term's second derivative
+      // (|(xi, eta)| cell / n^3, divided by det for the inverse): widen the
+      // candidate intervals by that (with a 20 % allowance).
+      const float nn = sqrtf(fmaxf(1.0f - r2, 0.02f));
+      const float ell = (float)kDT + 2.0f + 2.0f * delta;
+      s_sag = 0.15f * hypotf(mf.xi, mf.eta) * cell * ell * ell /
+              (nn * nn * nn * fmaxf(det, 0.25f));
+    }
   }
   __syncthreads();
   float bmin = s_q[0][1], bmax = s_q[0][1];
@@ -1350,75 +1389,32 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
     bmin = fminf(bmin, s_q[k][1]);
     bmax = fmaxf(bmax, s_q[k][1]);
   }
-  const int jlo = (int)fmaxf(0.f, ceilf(fmaxf(bmin + h - 1e-3f, -1.f)));
-  int jhi = (int)fminf((float)(n - 1), floorf(fminf(bmax + h + 1e-3f, (float)n)));
-  jhi = min(jhi, jlo + kMaxRows - 1);
-  const int nrows = max(0, jhi - jlo + 1);
-  // Column interval of every candidate row (the preimage quadrilateral
-  // intersected with the row), one row per thread, and the exclusive prefix
-  // of the interval lengths: candidates are then numbered 0 .. total-1 row by
-  // row, so every warp step splats 32 candidates whatever the row lengths.
-  int cnt = 0, ilo = 0;
-  {
-    const int r = threadIdx.x;
-    if (r < nrows) {
-      const float b = (float)(jlo + r - h);
-      float alo = 3e38f, ahi = -3e38f;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const float ax = s_q[k][0], bx = s_q[k][1];
-        const float ay = s_q[(k + 1) & 3][0], by = s_q[(k + 1) & 3][1];
-        if ((bx <= b && b <= by) || (by <= b && b <= bx)) {
-          if (by == bx) {
-            alo = fminf(alo, fminf(ax, ay));
-            ahi = fmaxf(ahi, fmaxf(ax, ay));
-          } else {
-            const float a = ax + (ay - ax) * ((b - bx) / (by - bx));
-            alo = fminf(alo, a);
-            ahi = fmaxf(ahi, a);
-          }
-        }
-      }
-      int ihi = -1;
-      if (alo <= ahi) {
-        ilo = (int)fmaxf(0.f, ceilf(fmaxf(alo + h - 1e-3f, -1.f)));
-        ihi = (int)fminf((float)(n - 1), floorf(fminf(ahi + h + 1e-3f, (float)n)));
-      }
-      cnt = ihi >= ilo ? ihi - ilo + 1 : 0;
-    }
-    int inc = cnt;
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, inc, o);
-      if (lane >= o) inc += y;
-    }
-    if (lane == 31) s_wsum[warp] = inc;
-    __syncthreads();
-    int wbase = 0;
-    for (int w = 0; w < warp; ++w) wbase += s_wsum[w];
-    if (r < kMaxRows) {
-      s_off[r] = wbase + inc - cnt;
-      // Candidate f of row r is pixel (jlo + r) n + ilo + (f - off): s_base + f
-      // (< N^2 <= 2^30 for image_size <= 32768).
-      s_base[r] = (jlo + r) * n + ilo - (wbase + inc - cnt);
-    }
-    if (r == kThreads - 1) s_off[kMaxRows] = wbase + inc;
-  }
-  __syncthreads();
-  const int total = s_off[kMaxRows];
-  // Rows past nrows have no candidates: their offsets equal total.
-
+  const float sag = s_sag + 1e-3f;
+  const int jlo = (int)fmaxf(0.f, ceilf(fmaxf(bmin + h - sag, -1.f)));
+  const int jhi = (int)fminf((float)(n - 1), floorf(fminf(bmax + h + sag, (float)n)));
   const float inv_nb = 1.0f / static_cast<float>(nb);
   const size_t half = n / 2;
   const float lim = half - 1;  // the reference compares |LL| with size_t (N/2 - 1)
   // Fixed-point tile sums: a source's splat value v / nb is carried as
-  // v * 2^28 / max(pre).  Every contribution is <= 2^28 and the bilinear
-  // weights landing on one pixel sum to a few units at most (the map never
-  // contracts), far below 2^32, so the shared-memory sums are native integer
-  // atomics, exact and independent of their order; the tile is converted
-  // back once.  Resolution 2^-28 of the image maximum.
+  // v * 2^(28 - sh) / max(pre).  Every contribution is <= 2^(28 - sh), and
+  // the bilinear weights landing on one pixel sum to about the density of
+  // sources per destination pixel (four times it at most), so the sums stay
+  // below 2^32 while that density is <= 2^(2 + sh): the shared-memory sums
+  // are native integer atomics, exact and independent of their order, and
+  // the tile is converted back once.  sh is 0 (resolution 2^-28 of the image
+  // maximum) unless the preimage of the tile, with its margins, covers more
+  // than twice the tile's area -- a map that contracts, which only very wide
+  // fields with a tilted plane reach -- and then grows by one per doubling.
+  float parea = 0.f;  // preimage quadrilateral's area (shoelace)
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    parea += s_q[k][0] * s_q[(k + 1) & 3][1] - s_q[(k + 1) & 3][0] * s_q[k][1];
+  parea = fabsf(0.5f * parea);
+  int sh = 0;
+  while (sh < 12 && parea > (float)(2 * kDT * kDT) * (float)(1 << sh)) ++sh;
   const float pmax = __uint_as_float(*pre_max);
-  const float qk = pmax > 0.f ? 268435456.0f / pmax : 0.f;
-  const float deq = pmax * inv_nb * (1.0f / 268435456.0f);
+  const float qk = pmax > 0.f ? 268435456.0f / (pmax * (float)(1 << sh)) : 0.f;
+  const float deq = pmax * inv_nb * ((float)(1 << sh) / 268435456.0f);
   // Precision form: exact targets in FP32 around a per-tile origin (a0, b0),
   // so offsets stay small; P at the origin and the destination-tile offset
   // come from FP64.
@@ -1480,40 +1476,99 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
     atomicAdd(px + kTR, __float2uint_rn(a * wm1));
     atomicAdd(px + kTR + 1, __float2uint_rn(b * wm1));
   };
-  // Each warp takes a contiguous eighth of the candidates, so a lane's row
-  // cursor moves about half a row per candidate; its start is found by
-  // bisection of the row offsets.  Warp step: candidates f0 + lane + 32 e,
-  // e < 4, all loads issued first; the cursor only moves forward.
-  constexpr int kPer = 4, kWarps = kThreads / 32;
-  const int per = (total + kWarps - 1) / kWarps;
-  const int wb = min(total, warp * per), we = min(total, wb + per);
-  int row = 0;
-  for (int step = kMaxRows / 2; step > 0; step >>= 1)
-    if (s_off[row + step] <= wb) row += step;  // last row whose offset is <= wb
-  for (int f0 = wb; f0 < we; f0 += 32 * kPer) {
-    int at[kPer], rw[kPer];
-    float p[kPer];
-    float2 tt[kPer];
+  // Candidate rows in chunks of kMaxRows (one row per thread): a single
+  // chunk unless the preimage spans more than kMaxRows source rows.
+  for (int cj = jlo; cj <= jhi; cj += kMaxRows) {
+    const int nrows = min(kMaxRows, jhi - cj + 1);
+    // Column interval of every candidate row (the preimage quadrilateral
+    // intersected with the row), one row per thread, and the exclusive prefix
+    // of the interval lengths: candidates are then numbered 0 .. total-1 row by
+    // row, so every warp step splats 32 candidates whatever the row lengths.
+    int cnt = 0, ilo = 0;
+    {
+      const int r = threadIdx.x;
+      if (r < nrows) {
+        // Rows in the margin beyond the quadrilateral's extreme corners take
+        // the interval at that corner (then widened like every interval).
+        const float b = fminf(fmaxf((float)(cj + r - h), bmin), bmax);
+        float alo = 3e38f, ahi = -3e38f;
 #pragma unroll
-    for (int e = 0; e < kPer; ++e) {
-      const int f = f0 + lane + 32 * e;
-      rw[e] = -1;
-      if (f < we) {
-        while (s_off[row + 1] <= f) ++row;
-        rw[e] = row;
-        at[e] = s_base[row] + f;
-        p[e] = pre[at[e]];
-        if (!EXACT) tt[e] = tg[at[e]];
+        for (int k = 0; k < 4; ++k) {
+          const float ax = s_q[k][0], bx = s_q[k][1];
+          const float ay = s_q[(k + 1) & 3][0], by = s_q[(k + 1) & 3][1];
+          if ((bx <= b && b <= by) || (by <= b && b <= bx)) {
+            if (by == bx) {
+              alo = fminf(alo, fminf(ax, ay));
+              ahi = fmaxf(ahi, fmaxf(ax, ay));
+            } else {
+              const float a = ax + (ay - ax) * ((b - bx) / (by - bx));
+              alo = fminf(alo, a);
+              ahi = fmaxf(ahi, a);
+            }
+          }
+        }
+        int ihi = -1;
+        if (alo <= ahi) {
+          ilo = (int)fmaxf(0.f, ceilf(fmaxf(alo + h - sag, -1.f)));
+          ihi = (int)fminf((float)(n - 1), floorf(fminf(ahi + h + sag, (float)n)));
+        }
+        cnt = ihi >= ilo ? ihi - ilo + 1 : 0;
+      }
+      int inc = cnt;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+      }
+      if (lane == 31) s_wsum[warp] = inc;
+      __syncthreads();
+      int wbase = 0;
+      for (int w = 0; w < warp; ++w) wbase += s_wsum[w];
+      if (r < kMaxRows) {
+        s_off[r] = wbase + inc - cnt;
+        // Candidate f of row r is pixel (cj + r) n + ilo + (f - off): s_base + f
+        // (< N^2 <= 2^30 for image_size <= 32768).
+        s_base[r] = (cj + r) * n + ilo - (wbase + inc - cnt);
+      }
+      if (r == kThreads - 1) s_off[kMaxRows] = wbase + inc;
+    }
+    __syncthreads();
+    const int total = s_off[kMaxRows];
+    // Rows past nrows have no candidates: their offsets equal total.
+    // Each warp takes a contiguous eighth of the candidates, so a lane's row
+    // cursor moves about half a row per candidate; its start is found by
+    // bisection of the row offsets.  Warp step: candidates f0 + lane + 32 e,
+    // e < 4, all loads issued first; the cursor only moves forward.
+    constexpr int kPer = 4, kWarps = kThreads / 32;
+    const int per = (total + kWarps - 1) / kWarps;
+    const int wb = min(total, warp * per), we = min(total, wb + per);
+    int row = 0;
+    for (int step = kMaxRows / 2; step > 0; step >>= 1)
+      if (s_off[row + step] <= wb) row += step;  // last row whose offset is <= wb
+    for (int f0 = wb; f0 < we; f0 += 32 * kPer) {
+      int at[kPer], rw[kPer];
+      float p[kPer];
+      float2 tt[kPer];
+#pragma unroll
+      for (int e = 0; e < kPer; ++e) {
+        const int f = f0 + lane + 32 * e;
+        rw[e] = -1;
+        if (f < we) {
+          while (s_off[row + 1] <= f) ++row;
+          rw[e] = row;
+          at[e] = s_base[row] + f;
+          p[e] = pre[at[e]];
+          if (!EXACT) tt[e] = tg[at[e]];
+        }
+      }
+#pragma unroll
+      for (int e = 0; e < kPer; ++e) {
+        if (rw[e] < 0) continue;
+        const int j = cj + rw[e];
+        splat(at[e] - j * n, j, p[e] * qk, EXACT ? make_float2(0.f, 0.f) : tt[e]);
       }
     }
-#pragma unroll
-    for (int e = 0; e < kPer; ++e) {
-      if (rw[e] < 0) continue;
-      const int j = jlo + rw[e];
-      splat(at[e] - j * n, j, p[e] * qk, EXACT ? make_float2(0.f, 0.f) : tt[e]);
-    }
+    __syncthreads();  // the next chunk rewrites the row offsets
   }
-  __syncthreads();
   float vmax = 0.f;
   for (int k = threadIdx.x; k < kDT * kDT / 4; k += kThreads) {
     const int lr = (4 * k) / kDT, g4 = ((4 * k) % kDT) >> 2;
@@ -2019,17 +2074,40 @@ bool fip_gather_supported(const FipGeom& geo, int exact_targets) {
 cudaError_t fip_launch_reproject_gather(const FipGeom& geo, const float* pre,
                                         const float2* targets, const float* V, int nb,
                                         const unsigned* pre_max, float* dst, unsigned* img_max,
-                                        int exact_targets, cudaStream_t s) {
+                                        int exact_targets, cudaStream_t s, unsigned* err) {
   const int tiles = (geo.n + kDT - 1) / kDT;
   const float delta = exact_targets ? 0.25f : chain_delta(geo.cell);
   if (!fip_gather_supported(geo, exact_targets)) return cudaErrorInvalidValue;
   if (exact_targets)
     k_reproject_gather<true><<<tiles * tiles, kThreads, 0, s>>>(
-        pre, nullptr, V, geo.n, nb, geo.cell, delta, pre_max, dst, img_max);
+        pre, nullptr, V, geo.n, nb, geo.cell, delta, pre_max, dst, img_max, err);
   else
     k_reproject_gather<false><<<tiles * tiles, kThreads, 0, s>>>(
-        pre, targets, V, geo.n, nb, geo.cell, delta, pre_max, dst, img_max);
+        pre, targets, V, geo.n, nb, geo.cell, delta, pre_max, dst, img_max, err);
   return cudaGetLastError();
+}
+
+bool fip_gather_domain_ok(const float* V, int n, float cell) {
+  // The exact map on a 65 x 65 lattice over the source image (and one pixel
+  // beyond): inside the horizon with room (r2 < 0.98) and no fold of the
+  // slant part (its Jacobian determinant above 1/4), the conditions the
+  // gather checks per tile.  V is row-major 3 x 3 on the host.
+  const double a22 = fabs((double)V[8]);
+  if (!(a22 > 0.0)) return false;
+  const double m00 = -(double)V[0] / a22, m01 = (double)V[3] / a22;
+  const double m10 = -(double)V[1] / a22, m11 = (double)V[4] / a22;
+  const double xi = (double)V[6] / (double)V[8], eta = (double)V[7] / (double)V[8];
+  const double h = n / 2, lo = -h - 2.0, span = (double)n + 4.0;
+  for (int q = 0; q <= 64; ++q)
+    for (int p = 0; p <= 64; ++p) {
+      const double a = lo + span * p / 64.0, b = lo + span * q / 64.0;
+      const double X = cell * (m00 * a + m01 * b - 1.0), Y = cell * (m10 * a + m11 * b - 1.0);
+      const double r2 = X * X + Y * Y;
+      if (!(r2 < 0.98)) return false;
+      const double nn = sqrt(1.0 - r2);
+      if (!(1.0 - xi * X / nn + eta * Y / nn > 0.25)) return false;
+    }
+  return true;
 }
 
 cudaError_t fip_launch_image_max(const float* img, size_t count, unsigned* out, cudaStream_t s) {

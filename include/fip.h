@@ -124,10 +124,13 @@ int fip_grid_snapshot(fip_imager* im, const float* vis_re, const float* vis_im, 
  * binning scratch is a fixed ~6.5 MB device array inside the library, held
  * on every GPU that loads it until the process exits.  Limits: nb <= 131072
  * and image_size <= 4096 (multiple of 4); larger requests return
- * FIP_ERR_ARG.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress, with that device current); make that first
- * call before any stream capture.  All calls share the array: calls whose
- * work overlaps on the GPU race, so serialise them (one stream, or events).
+ * FIP_ERR_ARG.  Every call made outside stream capture looks up the array's
+ * device address (cudaGetSymbolAddress, with the device current), so a
+ * device reset between calls is followed; a call on a capturing stream uses
+ * the address of the last call outside capture, so make the first call on a
+ * device before any stream capture (FIP_ERR_STATE otherwise).  All calls
+ * share the array: calls whose work overlaps on the GPU race, so serialise
+ * them (one stream, or events).
  */
 int fip_grid_snapshot_noalloc(const float* vis_re, const float* vis_im, const float* B,
                               const float* V, size_t nb, size_t image_size, float cell_size,
@@ -151,6 +154,21 @@ int fip_pipe_device(fip_imager* im, const float* vis_re, const float* vis_im, co
                     const float* V, size_t nb, float* result, void* stream);
 /* Device pointer to image k (0..2) of the last fip_pipe_device call. */
 const float* fip_imager_image(const fip_imager* im, int k);
+
+/*
+ * Reprojection domain check (no counterpart in the reference, whose scatter
+ * has no domain limit).  The tile gather reprojection is exact while the
+ * plane-to-sky map is invertible tile by tile: well inside the horizon and
+ * without folds, which every field up to tens of degrees satisfies unless
+ * its plane is strongly tilted.  Each gather tile checks this for itself and
+ * flags a tile outside it.  fip_imager_check waits (on `stream`, after the
+ * imager's earlier calls) and returns FIP_ERR_STATE if any gather since the
+ * last check flagged a tile -- those images are not reliable; image such
+ * snapshots with reproject = 1 -- then clears the flag.  fip_pipe_host (and
+ * so FIpipe), whose bases V are host arrays, checks each snapshot's geometry
+ * before imaging and reprojects an out-of-domain snapshot with the scatter.
+ */
+int fip_imager_check(fip_imager* im, void* stream);
 
 /*
  * FIpipe through an imager with host buffers (pinned staging owned by the
@@ -228,6 +246,10 @@ int fip_batch_autotune(fip_batch* b, const float* const* vis_re, const float* co
                        size_t count, void* stream);
 int fip_batch_tuning(const fip_batch* b, int* fft_values_per_thread, int* fft_split,
                      int* fft_direct, int* grid_ctas_per_sm);
+/* The batch's reprojection domain check, as fip_imager_check: waits for the
+ * work enqueued on `stream`, returns FIP_ERR_STATE if a gather tile lay
+ * outside the gather's domain since the last check, and clears the flag. */
+int fip_batch_check(fip_batch* b, void* stream);
 
 /* Per-pixel targets (LL, MM) of the reprojection, [N*N][2] (device), for
  * tests: exact = 0 the plain form's FP32 chain as the imager evaluates it

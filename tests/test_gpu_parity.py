@@ -56,6 +56,7 @@ def run(snap, dev, **kw):
                               d["V"][9 * k:], nb, imgs[k], mx[k:])
         im.trigger(imgs[0], imgs[1], imgs[2], mx, res)
         torch.cuda.synchronize()
+        im.check()  # no gather tile outside its domain
     return (res.cpu().numpy().reshape(u, u), imgs.cpu().numpy().reshape(3, n, n),
             mx.cpu().numpy())
 
@@ -186,6 +187,55 @@ def test_theta_table_targets_identical_to_evaluated_chain(cuda, cfg):
             im.pixel_targets(V, b, evaluated=True)
             torch.cuda.synchronize()
             assert torch.equal(a.view(torch.int32), b.view(torch.int32))
+
+
+@pytest.mark.parametrize("ha", [1.5, 4.0])
+def test_wide_field_gather_matches_scatter_and_reference(cuda, ha):
+    """29-degree fields (512^2, cell 1e-3 rad).  At hour angle 4 h the plane is
+    tilted by ~50 degrees (xi = 1.27): the slant term bows every tile's
+    preimage by most of a pixel and the map contracts by up to 2, so the
+    gather's candidate bounds (curvature margin, row chunks, per-tile
+    fixed-point scale) are exercised at image level, against the reference's
+    own scatter (the source-major path and the reference build) and, for the
+    precision form, against FP64."""
+    snap = synthetic.config_tiny(image_size=512, cell_size=1e-3, hour_angle0_h=ha,
+                                 transient_snapshot=2)
+    n, nb = snap.image_size, snap.num_baselines
+    res_g, img_g, mx_g = run(snap, cuda)
+    res_s, img_s, mx_s = run(snap, cuda, reproject=fip.REPROJECT_SCATTER)
+    for k in range(3):
+        assert relrms(img_g[k], img_s[k]) <= 1e-6
+    assert np.allclose(mx_g, mx_s, rtol=1e-6)
+    assert np.abs(res_g - res_s).max() <= 1e-5
+    if ref.available():
+        for k in range(3):
+            vr, vi, B, V = snap.snapshot(k)
+            rimg, _, _ = ref.image_snapshot(vr, vi, B, V, nb, n, snap.cell_size)
+            assert relrms(img_g[k], rimg) <= 1e-5
+        assert np.abs(res_g - ref.fipipe(snap)).max() <= 1e-4
+    res_p, img_p, _ = run(snap, cuda, form=fip.FORM_PRECISE)
+    r64, i64, _ = oracle.fipipe(snap, "f64", want_images=True)
+    for k in range(3):
+        assert relrms(img_p[k], i64[k]) <= 3e-5
+    assert np.abs(res_p - r64).max() <= 1e-4
+
+
+def test_geometry_outside_the_gather_domain(cuda):
+    """A 37-degree field with the plane tilted by ~65 degrees: corners of the
+    source image lie beyond the horizon of the slant projection, where the
+    map is not invertible tile by tile.  The gather flags it (no silent
+    image), and FIpipe, whose bases are host arrays, reprojects such snapshots
+    with the reference's scatter."""
+    snap = synthetic.config_tiny(image_size=256, cell_size=2.5e-3, hour_angle0_h=5.0,
+                                 transient_snapshot=2)
+    with pytest.raises(fip.FipError, match="domain"):
+        run(snap, cuda)
+    want, _, _ = run(snap, cuda, reproject=fip.REPROJECT_SCATTER)
+    got = fip.FIpipe(snap.vis_re, snap.vis_im, snap.B, snap.V, snap.num_baselines,
+                     snap.image_size, 3, snap.cell_size, snap.unit_size)
+    assert np.allclose(got, want, atol=1e-6, equal_nan=True)
+    if ref.available():
+        assert np.allclose(got, ref.fipipe(snap), atol=1e-4, equal_nan=True)
 
 
 def test_exact_targets_vs_oracle(cuda, small):
