@@ -48,6 +48,24 @@ class ImagerConfig(ctypes.Structure):
                 ("device", ctypes.c_int), ("reproject", ctypes.c_int)]
 
 
+class Location(ctypes.Structure):
+    """fip_location: one transient location (see locate_transients)."""
+    _fields_ = [("tile_row", ctypes.c_int32), ("tile_col", ctypes.c_int32),
+                ("tlisi", ctypes.c_float), ("row", ctypes.c_float), ("col", ctypes.c_float),
+                ("x", ctypes.c_float), ("y", ctypes.c_float)]
+
+
+LOCATION_DTYPE = np.dtype([("tile_row", "<i4"), ("tile_col", "<i4"), ("tlisi", "<f4"),
+                           ("row", "<f4"), ("col", "<f4"), ("x", "<f4"), ("y", "<f4")])
+
+
+class RawVis(ctypes.Structure):
+    """fip_raw_vis: device pointers of one snapshot's raw polarisations 0 and 3,
+    their flags (uint8, nonzero = flagged) and weights."""
+    _fields_ = [(k, ctypes.c_void_p) for k in ("v0_re", "v0_im", "v3_re", "v3_im", "flag0",
+                                              "flag3", "weight0", "weight3")]
+
+
 def lib() -> ctypes.CDLL:
     """Loads libfip_b200.so; raises if it has not been built."""
     global _lib
@@ -72,6 +90,9 @@ def lib() -> ctypes.CDLL:
         L.fip_imager_image.argtypes = [vp, ctypes.c_int]
         L.fip_imager_image.restype = vp
         L.fip_imager_check.argtypes = [vp, vp]
+        L.fip_locate_transients.argtypes = [vp, sz, sz, fp, fp, vp, sz,
+                                             ctypes.POINTER(sz), vp]
+        L.fip_image_snapshot_raw.argtypes = [vp, ctypes.POINTER(RawVis), vp, vp, sz, vp, vp, vp]
         L.fip_batch_check.argtypes = [vp, vp]
         L.fip_pipe_host.argtypes = [vp, vp, vp, vp, vp, sz, sz, vp]
         L.fip_pixel_targets.argtypes = [vp, vp, vp, ctypes.c_int, vp]
@@ -252,6 +273,16 @@ class Imager:
         _check(lib().fip_image_snapshot(self._h, _ptr(vis_re), _ptr(vis_im), _ptr(B), _ptr(V), nb,
                                         _ptr(image), _ptr(image_max), _stream(stream)))
 
+    def image_snapshot_raw(self, v0_re, v0_im, v3_re, v3_im, flag0, flag3, weight0, weight3, B,
+                           V, nb: int, image, image_max=None, stream=None):
+        """image_snapshot from raw polarisations 0 and 3 with flags and weights
+        (device arrays of nb samples): the Stokes-I collapse runs inside the
+        gridder's load."""
+        raw = RawVis(*(_ptr(x) for x in (v0_re, v0_im, v3_re, v3_im, flag0, flag3, weight0,
+                                          weight3)))
+        _check(lib().fip_image_snapshot_raw(self._h, ctypes.byref(raw), _ptr(B), _ptr(V), nb,
+                                            _ptr(image), _ptr(image_max), _stream(stream)))
+
     def grid_snapshot(self, vis_re, vis_im, B, V, nb: int, grid, stream=None):
         """Gridding stage only: grid [G][G/2+1] complex (2 floats each)."""
         _check(lib().fip_grid_snapshot(self._h, _ptr(vis_re), _ptr(vis_im), _ptr(B), _ptr(V),
@@ -387,6 +418,21 @@ def grid_snapshot_noalloc(vis_re, vis_im, B, V, nb: int, image_size: int, cell_s
     _check(lib().fip_grid_snapshot_noalloc(_ptr(vis_re), _ptr(vis_im), _ptr(B), _ptr(V), nb,
                                            image_size, float(cell_size), _ptr(grid),
                                            _stream(stream)))
+
+
+def locate_transients(tlisi, image_size: int, unit_size: int, cell_size: float,
+                      threshold: float = 0.99, max_out: int = 256, stream=None):
+    """Transient locations from a device tLISI matrix (U*U floats): tiles below
+    `threshold` that are the strict minimum of their 3 x 3 neighbourhood,
+    refined to the neighbourhood's centroid of 1 - tLISI.  Returns
+    (records, found): a LOCATION_DTYPE array of up to max_out locations,
+    deepest first, and the number found."""
+    out = np.zeros(max(int(max_out), 0), LOCATION_DTYPE)
+    found = ctypes.c_size_t()
+    _check(lib().fip_locate_transients(_ptr(tlisi), image_size, unit_size, float(cell_size),
+                                       float(threshold), out.ctypes.data if out.size else None,
+                                       out.size, ctypes.byref(found), _stream(stream)))
+    return out[:min(found.value, out.size)], int(found.value)
 
 
 def plane_project(uvw, freqs, rows: int, chans: int, B, V, stream=None):

@@ -31,6 +31,7 @@ UNITS = {
     "fip_host.cu": [],
     "fip_noalloc.cu": [],
     "fip_server.cu": [],
+    "fip_locate.cu": [],
 }
 HOST_CXX = ["fits_io.cpp"]
 
@@ -79,7 +80,8 @@ def build(verbose_ptxas: bool = False) -> str:
              ["-L" + os.path.join(CUDA_HOME, "lib64"), "-lcufft",
               "-Xlinker", "-rpath", "-Xlinker", os.path.join(CUDA_HOME, "lib64")])
     cli_src = os.path.join(CSRC, "sharedlibrary_gpu.cpp")
-    if os.path.exists(cli_src) and _stale(CLI, [cli_src, LIB] + hdrs):
+    cli_deps = [cli_src, LIB, os.path.join(CSRC, "fits_io.cpp")] + hdrs
+    if os.path.exists(cli_src) and _stale(CLI, cli_deps):
         _run([NVCC, cli_src, "-o", CLI, "-O2", "-std=c++17", "-Wno-deprecated-gpu-targets", "-I" + os.path.join(REPO, "include"),
               "-I" + CSRC, "-L" + HERE, "-lfip_b200", "-Xlinker", "-rpath", "-Xlinker",
               "$ORIGIN/..", "-Xlinker", "-rpath", "-Xlinker",

@@ -33,6 +33,38 @@ struct FipGeom {
                // 0 = full half plane, row-major (cuFFT C2R fallback)
 };
 
+// Raw two-polarisation visibilities of one snapshot (device arrays of nb
+// samples in the preprocessing's sample order): polarisations 0 and 3 (XX,
+// YY), their flags (nonzero = flagged) and weights.
+struct FipRawVis {
+  const float* v0r;
+  const float* v0i;
+  const float* v3r;
+  const float* v3i;
+  const unsigned char* f0;
+  const unsigned char* f3;
+  const float* w0;
+  const float* w3;
+};
+
+// Stokes-I collapse of sample s (SVDPreprocessKernels.cu:208-237, SVD_MFS.py
+// :77-95): the weighted mean of polarisations 0 and 3 over their unflagged
+// weights, 0 when both vanish.  The roundings are spelled out so that every
+// translation unit (fast-math or not) gives the same bits.
+__device__ __forceinline__ void fip_collapse_sample(const FipRawVis& r, size_t s, float& re,
+                                                    float& im) {
+  const float a = r.f0[s] ? 0.0f : r.w0[s];
+  const float b = r.f3[s] ? 0.0f : r.w3[s];
+  const float ws = __fadd_rn(a, b);
+  if (ws > 0.0f) {
+    re = __fdiv_rn(__fmaf_rn(r.v0r[s], a, __fmul_rn(r.v3r[s], b)), ws);
+    im = __fdiv_rn(__fmaf_rn(r.v0i[s], a, __fmul_rn(r.v3i[s], b)), ws);
+  } else {
+    re = 0.0f;
+    im = 0.0f;
+  }
+}
+
 // Batched launches: at most FIP_MAX_BATCH snapshots of one image size.
 #define FIP_MAX_BATCH 64
 

@@ -592,20 +592,26 @@ static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const f
                                const float* B, const float* V, size_t nb, float* image,
                                float* image_max, cudaStream_t s, bool fork_targets,
                                bool targets_ready = false, cudaEvent_t targets_ev = nullptr,
-                               bool force_scatter = false) {
+                               bool force_scatter = false, const FipRawVis* raw = nullptr) {
   const FipGeom& geo = im->geo;
   if (nb > im->cfg.max_baselines) return fail(FIP_ERR_ARG, "nb exceeds the imager's capacity");
   if (nb == 0) return fail(FIP_ERR_ARG, "nb must be positive");
-  if (!vr || !vi || !B || !V || !image) return fail(FIP_ERR_ARG, "null device pointer");
+  if ((!raw && (!vr || !vi)) || !B || !V || !image)
+    return fail(FIP_ERR_ARG, "null device pointer");
   const bool precise = im->cfg.form == FIP_FORM_PRECISE;
   const void* gvr = vr;
   const void* gvi = vi;
-  int vt = FIP_VIS_F32;
+  // raw: two-polarisation samples, collapsed to Stokes I inside the gridder's
+  // load (or inside the reduced-storage conversion).
+  int vt = raw ? FIP_VIS_RAW : FIP_VIS_F32;
   int k;
   if (precise && im->cfg.vis_storage != FIP_STORE_F32) {
     vt = im->cfg.vis_storage == FIP_STORE_F16 ? FIP_VIS_F16 : FIP_VIS_BF16;
     k = stage_begin(im, ST_GRID, s);
-    FIP_CUDA(fip_launch_quantize(vr, vi, nb, vt, L.q_re, L.q_im, L.q_scale, s));
+    if (raw)
+      FIP_CUDA(fip_launch_quantize_raw(*raw, nb, vt, L.q_re, L.q_im, L.q_scale, s));
+    else
+      FIP_CUDA(fip_launch_quantize(vr, vi, nb, vt, L.q_re, L.q_im, L.q_scale, s));
     stage_end(im, k, s);
     im->launches += 3;
     gvr = L.q_re;
@@ -636,7 +642,7 @@ static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const f
   stage_end(im, k, s);
   k = stage_begin(im, ST_GRID, s);
   FIP_CUDA(fip_launch_grid(geo, B, gvr, gvi, vt, L.q_scale, V, (int)nb, L.bins, L.grid,
-                           precise ? 1 : 0, s, im->grid_ctas_per_sm));
+                           precise ? 1 : 0, s, im->grid_ctas_per_sm, raw));
   stage_end(im, k, s);
   im->launches += fip_bin_launches(geo) + 2;  // binning, zero tiles, grid
   if (im->custom_fft) {
@@ -737,6 +743,24 @@ int fip_image_snapshot(fip_imager* im, const float* vis_re, const float* vis_im,
   FIP_TRY(call_enter(im, s));
   FIP_TRY(image_snapshot_impl(im, im->lane[0], vis_re, vis_im, B, V, nb, image, image_max, s,
                               true));
+  im->last_lane = 0;
+  return call_leave(im, s);
+}
+
+int fip_image_snapshot_raw(fip_imager* im, const fip_raw_vis* raw, const float* B,
+                           const float* V, size_t nb, float* image, float* image_max,
+                           void* stream) {
+  if (!im) return fail(FIP_ERR_ARG, "null imager");
+  if (!raw || !raw->v0_re || !raw->v0_im || !raw->v3_re || !raw->v3_im || !raw->flag0 ||
+      !raw->flag3 || !raw->weight0 || !raw->weight3)
+    return fail(FIP_ERR_ARG, "null raw visibility array");
+  const FipRawVis rv{raw->v0_re, raw->v0_im, raw->v3_re, raw->v3_im,
+                     raw->flag0, raw->flag3, raw->weight0, raw->weight3};
+  DeviceGuard g(im->cfg.device);
+  cudaStream_t s = (cudaStream_t)stream;
+  FIP_TRY(call_enter(im, s));
+  FIP_TRY(image_snapshot_impl(im, im->lane[0], nullptr, nullptr, B, V, nb, image, image_max, s,
+                              true, false, nullptr, false, &rv));
   im->last_lane = 0;
   return call_leave(im, s);
 }

@@ -30,7 +30,9 @@ struct FipBins {
   size_t wcap;        // capacity of work
 };
 
-enum FipVisType { FIP_VIS_F32 = 0, FIP_VIS_F16 = 1, FIP_VIS_BF16 = 2 };
+// FIP_VIS_RAW: FP32 two-polarisation samples (FipRawVis), collapsed to
+// Stokes I as the gridder loads them.
+enum FipVisType { FIP_VIS_F32 = 0, FIP_VIS_F16 = 1, FIP_VIS_BF16 = 2, FIP_VIS_RAW = 3 };
 
 // ---- plain FP32 form (reference-faithful arithmetic, fip_plain.cu) ----
 cudaError_t fip_launch_taper(float* taper, const FipGeom& geo, cudaStream_t s);
@@ -40,10 +42,11 @@ cudaError_t fip_launch_bin(const FipGeom& geo, const float* B, int nb, FipBins& 
 int fip_bin_launches(const FipGeom& geo);
 // ctas_per_sm: persistent gridder CTAs per SM (0 = the most that fit,
 // fip_grid_max_ctas_per_sm).
+// vis_type FIP_VIS_RAW: vr, vi unused, the samples are *raw.
 cudaError_t fip_launch_grid(const FipGeom& geo, const float* B, const void* vr, const void* vi,
                             int vis_type, const float* vis_scale, const float* V, int nb,
                             const FipBins& bins, float2* grid, int compensated, cudaStream_t s,
-                            int ctas_per_sm = 0);
+                            int ctas_per_sm = 0, const FipRawVis* raw = nullptr);
 int fip_grid_max_ctas_per_sm(int compensated);
 // One persistent gridding launch over a batch of snapshots (plus the zeroing
 // of their split tiles): snapshot k's inputs in in.*[k], its bins and grid at
@@ -128,3 +131,6 @@ cudaError_t fip_launch_collapse(const float* v0r, const float* v0i, const float*
                                 float* out_re, float* out_im, size_t ns, cudaStream_t s);
 cudaError_t fip_launch_quantize(const float* vr, const float* vi, size_t nb, int vis_type,
                                 void* out_re, void* out_im, float* scale_out, cudaStream_t s);
+// The same from raw two-polarisation samples, collapsed to Stokes I on load.
+cudaError_t fip_launch_quantize_raw(const FipRawVis& raw, size_t nb, int vis_type, void* out_re,
+                                    void* out_im, float* scale_out, cudaStream_t s);

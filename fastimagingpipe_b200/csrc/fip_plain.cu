@@ -557,7 +557,8 @@ __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_ci
                                           const void* vi, float vis_scale, float inten,
                                           float scale, int g, int hp, int tiles_c, int layout,
                                           const unsigned* __restrict__ entries, int4 item,
-                                          float2* __restrict__ grid) {
+                                          float2* __restrict__ grid,
+                                          const FipRawVis& raw = FipRawVis{}) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int tile = item.x, cnt = item.z - item.y;
   const int trow0 = (tile / tiles_c) * FIP_GTILE, tcol0 = (tile % tiles_c) * FIP_GTILE;
@@ -581,7 +582,13 @@ __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_ci
     // Visibility weighting (FIPkernels.cu:188-195), halved for the
     // Hermitian split, conjugated for the mirrored copy.
     float wr, wi;
-    if (VT == FIP_VIS_F32) {
+    if constexpr (VT == FIP_VIS_RAW) {
+      // Stokes-I collapse fused into the load: no collapsed copy in memory.
+      float cr, ci;
+      fip_collapse_sample(raw, (size_t)v, cr, ci);
+      wr = cr / inten;
+      wi = ci / inten;
+    } else if constexpr (VT == FIP_VIS_F32) {
       wr = load_vis<VT>(vr, v) / inten;
       wi = load_vis<VT>(vi, v) / inten;
     } else {
@@ -725,7 +732,8 @@ __global__ void __launch_bounds__(kThreads) k_grid(const float* __restrict__ B, 
                                                    const unsigned* __restrict__ entries,
                                                    const int4* __restrict__ work,
                                                    const unsigned* __restrict__ nwork,
-                                                   float2* __restrict__ grid) {
+                                                   float2* __restrict__ grid,
+                                                   const FipRawVis raw) {
   extern __shared__ float4 s_raw[];
   GridSmem& S = *reinterpret_cast<GridSmem*>(s_raw);
   float* s_cre = reinterpret_cast<float*>(reinterpret_cast<char*>(s_raw) + sizeof(GridSmem));
@@ -737,7 +745,7 @@ __global__ void __launch_bounds__(kThreads) k_grid(const float* __restrict__ B, 
   __syncthreads();
   for (unsigned w = blockIdx.x; w < nw; w += gridDim.x)
     grid_item<VT, COMP>(S, s_cre, s_cim, B, vr, vi, vis_scale, inten, scale, g, hp, tiles_c,
-                        layout, entries, work[w], grid);
+                        layout, entries, work[w], grid, raw);
 }
 
 // Persistent gridder over the work items of a batch of snapshots (one launch
@@ -1170,7 +1178,10 @@ __global__ void k_targets(const float* __restrict__ V, int n, float dc,
     const int i = (blockIdx.x * kTargetsPerThread + q) * blockDim.x + threadIdx.x;
     if (i < n) {
       float LL, MM;
-      fipref::pixel_target(fr, i, j, n, LL, MM, ttab);
+      if (ttab)
+        fipref::pixel_target_fast(fr, i, j, n, LL, MM, ttab);
+      else
+        fipref::pixel_target(fr, i, j, n, LL, MM);
       tg[(size_t)j * n + i] = make_float2(LL, MM);
     }
   }
@@ -1612,7 +1623,10 @@ __global__ void k_pixel_targets(const float* __restrict__ V, int n, float dc, fl
   float LL, MM;
   if (mode != 1) {
     fipref::Frame fr{V[0], V[1], V[3], V[4], V[8], V[6], V[7], dc};
-    fipref::pixel_target(fr, i, j, n, LL, MM, mode == 0 ? ttab : nullptr);
+    if (mode == 0 && ttab)
+      fipref::pixel_target_fast(fr, i, j, n, LL, MM, ttab);  // as k_targets maps
+    else
+      fipref::pixel_target(fr, i, j, n, LL, MM);
   } else {
     const ExactMap<double> m = make_map<double>(V, cell);
     double Ld, Md;
@@ -1831,7 +1845,9 @@ int fip_grid_max_ctas_per_sm(int compensated) { return compensated ? 2 : 3; }
 cudaError_t fip_launch_grid(const FipGeom& geo, const float* B, const void* vr, const void* vi,
                             int vis_type, const float* vis_scale, const float* V, int nb,
                             const FipBins& bins, float2* grid, int compensated, cudaStream_t s,
-                            int ctas_per_sm) {
+                            int ctas_per_sm, const FipRawVis* raw) {
+  if (vis_type == FIP_VIS_RAW && !raw) return cudaErrorInvalidValue;
+  const FipRawVis rv = raw ? *raw : FipRawVis{};
   const float scale = geo.cell * (float)(size_t)geo.g;
   const int sms = sm_count();
   k_zero_tiles<<<sms, kThreads, 0, s>>>(bins.multi, bins.nmulti, geo.tiles_c, geo.g, geo.hp,
@@ -1845,9 +1861,11 @@ cudaError_t fip_launch_grid(const FipGeom& geo, const float* B, const void* vr, 
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);         \
     kern<<<blocks, kThreads, smem, s>>>(B, vr, vi, vis_scale, V, scale, geo.g, geo.hp,          \
                                         geo.tiles_c, geo.layout, bins.entries, bins.work,       \
-                                        bins.nwork, grid);                                      \
+                                        bins.nwork, grid, rv);                                  \
   } while (0)
-  if (vis_type == FIP_VIS_F32) {
+  if (vis_type == FIP_VIS_RAW) {
+    if (compensated) FIP_GRID_CASE(FIP_VIS_RAW, true); else FIP_GRID_CASE(FIP_VIS_RAW, false);
+  } else if (vis_type == FIP_VIS_F32) {
     if (compensated) FIP_GRID_CASE(FIP_VIS_F32, true); else FIP_GRID_CASE(FIP_VIS_F32, false);
   } else if (vis_type == FIP_VIS_F16) {
     if (compensated) FIP_GRID_CASE(FIP_VIS_F16, true); else FIP_GRID_CASE(FIP_VIS_F16, false);

@@ -158,47 +158,60 @@ __global__ void k_plane_projectB(const float* uvw, const float* freqs, size_t ro
 __global__ void k_collapse(const float* v0r, const float* v0i, const float* v3r, const float* v3i,
                            const unsigned char* f0, const unsigned char* f3, const float* w0,
                            const float* w3, float* out_re, float* out_im, size_t ns) {
+  const FipRawVis r{v0r, v0i, v3r, v3i, f0, f3, w0, w3};
   for (size_t s = blockIdx.x * (size_t)kThreads + threadIdx.x; s < ns;
-       s += (size_t)gridDim.x * kThreads) {
-    const float a = f0[s] ? 0.0f : w0[s];
-    const float b = f3[s] ? 0.0f : w3[s];
-    const float ws = a + b;
-    if (ws > 0.0f) {
-      out_re[s] = (v0r[s] * a + v3r[s] * b) / ws;
-      out_im[s] = (v0i[s] * a + v3i[s] * b) / ws;
-    } else {
-      out_re[s] = 0.0f;
-      out_im[s] = 0.0f;
-    }
-  }
+       s += (size_t)gridDim.x * kThreads)
+    fip_collapse_sample(r, s, out_re[s], out_im[s]);
 }
 
+// Sample k of the visibilities: FP32 arrays, or raw polarisations collapsed
+// to Stokes I on load.
+struct F32Vis {
+  const float* vr;
+  const float* vi;
+  __device__ __forceinline__ void operator()(size_t k, float& re, float& im) const {
+    re = vr[k];
+    im = vi[k];
+  }
+};
+struct RawVis {
+  FipRawVis r;
+  __device__ __forceinline__ void operator()(size_t k, float& re, float& im) const {
+    fip_collapse_sample(r, k, re, im);
+  }
+};
+
 // Per-snapshot max-abs of the visibilities (as float bits, values >= 0).
-__global__ void k_maxabs(const float* vr, const float* vi, size_t nb, unsigned* out) {
+template <class L>
+__global__ void k_maxabs(const L load, size_t nb, unsigned* out) {
   float m = 0.f;
   for (size_t k = blockIdx.x * (size_t)kThreads + threadIdx.x; k < nb;
-       k += (size_t)gridDim.x * kThreads)
-    m = fmaxf(m, fmaxf(fabsf(vr[k]), fabsf(vi[k])));
+       k += (size_t)gridDim.x * kThreads) {
+    float re, im;
+    load(k, re, im);
+    m = fmaxf(m, fmaxf(fabsf(re), fabsf(im)));
+  }
   for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
 }
 
 // Scaled storage: the maximum maps to 2^14 (FP16 keeps 2^-24..65504), the
 // stored value is v / scale and the gridder multiplies by scale.
-template <int VT>
-__global__ void k_quantize(const float* vr, const float* vi, size_t nb, void* qr, void* qi,
-                           float* scale_io) {
+template <int VT, class L>
+__global__ void k_quantize(const L load, size_t nb, void* qr, void* qi, float* scale_io) {
   const float mx = scale_io[0];  // max-abs bits written by k_maxabs
   const float scale = mx > 0.f ? mx / 16384.0f : 1.0f;
   const float inv = 1.0f / scale;
   for (size_t k = blockIdx.x * (size_t)kThreads + threadIdx.x; k < nb;
        k += (size_t)gridDim.x * kThreads) {
+    float re, im;
+    load(k, re, im);
     if (VT == FIP_VIS_F16) {
-      reinterpret_cast<__half*>(qr)[k] = __float2half_rn(vr[k] * inv);
-      reinterpret_cast<__half*>(qi)[k] = __float2half_rn(vi[k] * inv);
+      reinterpret_cast<__half*>(qr)[k] = __float2half_rn(re * inv);
+      reinterpret_cast<__half*>(qi)[k] = __float2half_rn(im * inv);
     } else {
-      reinterpret_cast<__nv_bfloat16*>(qr)[k] = __float2bfloat16_rn(vr[k] * inv);
-      reinterpret_cast<__nv_bfloat16*>(qi)[k] = __float2bfloat16_rn(vi[k] * inv);
+      reinterpret_cast<__nv_bfloat16*>(qr)[k] = __float2bfloat16_rn(re * inv);
+      reinterpret_cast<__nv_bfloat16*>(qi)[k] = __float2bfloat16_rn(im * inv);
     }
   }
 }
@@ -250,16 +263,27 @@ cudaError_t fip_launch_collapse(const float* v0r, const float* v0i, const float*
   return cudaGetLastError();
 }
 
-cudaError_t fip_launch_quantize(const float* vr, const float* vi, size_t nb, int vis_type,
-                                void* out_re, void* out_im, float* scale_out, cudaStream_t s) {
+template <class L>
+static cudaError_t launch_quantize(const L& load, size_t nb, int vis_type, void* out_re,
+                                  void* out_im, float* scale_out, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(scale_out, 0, sizeof(float), s);
   if (e != cudaSuccess) return e;
   const int blocks = (int)std::min<size_t>(4 * 148, (nb + kThreads - 1) / kThreads + 1);
-  k_maxabs<<<blocks, kThreads, 0, s>>>(vr, vi, nb, reinterpret_cast<unsigned*>(scale_out));
+  k_maxabs<<<blocks, kThreads, 0, s>>>(load, nb, reinterpret_cast<unsigned*>(scale_out));
   if (vis_type == FIP_VIS_F16)
-    k_quantize<FIP_VIS_F16><<<blocks, kThreads, 0, s>>>(vr, vi, nb, out_re, out_im, scale_out);
+    k_quantize<FIP_VIS_F16><<<blocks, kThreads, 0, s>>>(load, nb, out_re, out_im, scale_out);
   else
-    k_quantize<FIP_VIS_BF16><<<blocks, kThreads, 0, s>>>(vr, vi, nb, out_re, out_im, scale_out);
+    k_quantize<FIP_VIS_BF16><<<blocks, kThreads, 0, s>>>(load, nb, out_re, out_im, scale_out);
   k_store_scale<<<1, 1, 0, s>>>(scale_out);
   return cudaGetLastError();
+}
+
+cudaError_t fip_launch_quantize(const float* vr, const float* vi, size_t nb, int vis_type,
+                                void* out_re, void* out_im, float* scale_out, cudaStream_t s) {
+  return launch_quantize(F32Vis{vr, vi}, nb, vis_type, out_re, out_im, scale_out, s);
+}
+
+cudaError_t fip_launch_quantize_raw(const FipRawVis& raw, size_t nb, int vis_type, void* out_re,
+                                    void* out_im, float* scale_out, cudaStream_t s) {
+  return launch_quantize(RawVis{raw}, nb, vis_type, out_re, out_im, scale_out, s);
 }

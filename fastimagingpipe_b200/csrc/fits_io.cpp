@@ -45,6 +45,27 @@ T be_load(const unsigned char* p) {
   return v;
 }
 
+// A string-valued card: the quoted value starts in column 11, padded to at
+// least 8 characters inside the quotes.
+void put_str_card(std::string& h, const std::string& key, const std::string& value) {
+  std::string v = value;
+  if (v.size() < 8) v.resize(8, ' ');
+  std::string c = key;
+  c.resize(8, ' ');
+  c += "= '" + v + "'";
+  c.resize(kCard, ' ');
+  h += c;
+}
+
+void be_store32(unsigned char* d, const void* src) {
+  unsigned char b[4];
+  std::memcpy(b, src, 4);
+  d[0] = b[3];
+  d[1] = b[2];
+  d[2] = b[1];
+  d[3] = b[0];
+}
+
 void put_card(std::string& h, const std::string& key, const std::string& value) {
   char buf[kCard + 1];
   if (value.empty())
@@ -196,6 +217,90 @@ bool fits_write_image(const std::string& path, const float* data, const std::vec
   if (!f) {
     err = "write failed for " + path;
     return false;
+  }
+  return true;
+}
+
+bool fits_write_table(const std::string& path, const std::vector<FitsColumn>& cols, size_t nrows,
+                      const std::string& extname, std::string& err) {
+  for (const FitsColumn& c : cols)
+    if (c.form != 'J' && c.form != 'E') {
+      err = "unsupported column form for " + c.name;
+      return false;
+    }
+  std::string h;
+  put_card(h, "SIMPLE", "T");
+  put_card(h, "BITPIX", "8");
+  put_card(h, "NAXIS", "0");
+  put_card(h, "EXTEND", "T");
+  put_card(h, "END", "");
+  h.resize(((h.size() + kBlock - 1) / kBlock) * kBlock, ' ');
+  const size_t row_bytes = 4 * cols.size();
+  std::string x;
+  put_str_card(x, "XTENSION", "BINTABLE");
+  put_card(x, "BITPIX", "8");
+  put_card(x, "NAXIS", "2");
+  put_card(x, "NAXIS1", std::to_string(row_bytes));
+  put_card(x, "NAXIS2", std::to_string(nrows));
+  put_card(x, "PCOUNT", "0");
+  put_card(x, "GCOUNT", "1");
+  put_card(x, "TFIELDS", std::to_string(cols.size()));
+  for (size_t k = 0; k < cols.size(); ++k) {
+    put_str_card(x, "TTYPE" + std::to_string(k + 1), cols[k].name);
+    put_str_card(x, "TFORM" + std::to_string(k + 1), std::string("1") + cols[k].form);
+  }
+  put_str_card(x, "EXTNAME", extname);
+  put_card(x, "END", "");
+  x.resize(((x.size() + kBlock - 1) / kBlock) * kBlock, ' ');
+  std::vector<unsigned char> d(((row_bytes * nrows + kBlock - 1) / kBlock) * kBlock, 0);
+  for (size_t r = 0; r < nrows; ++r)
+    for (size_t k = 0; k < cols.size(); ++k)
+      be_store32(&d[r * row_bytes + 4 * k], static_cast<const char*>(cols[k].data) + 4 * r);
+  std::ofstream f(path, std::ios::binary | std::ios::trunc);
+  if (!f) {
+    err = "cannot create " + path;
+    return false;
+  }
+  f.write(h.data(), (std::streamsize)h.size());
+  f.write(x.data(), (std::streamsize)x.size());
+  f.write(reinterpret_cast<const char*>(d.data()), (std::streamsize)d.size());
+  if (!f) {
+    err = "write failed for " + path;
+    return false;
+  }
+  return true;
+}
+
+bool fits_read_combined(const std::string& path, CombinedInput& in, std::string& err) {
+  std::vector<FitsImage> hdus;
+  if (!fits_read_all(path, hdus, err)) return false;
+  const FitsImage *tm = nullptr, *vis = nullptr, *rc = nullptr;
+  for (const FitsImage& h : hdus) {
+    if (h.extname == "TRANSFORMATION MATRICES") tm = &h;
+    else if (h.extname == "VISIBILITIES") vis = &h;
+    else if (h.extname == "R-COORDINATES") rc = &h;
+  }
+  if (!tm || !vis || !rc) {
+    err = path + " lacks one of the extensions TRANSFORMATION MATRICES, VISIBILITIES, "
+                 "R-COORDINATES";
+    return false;
+  }
+  if (tm->naxes.size() != 3 || tm->naxes[0] != 3 || tm->naxes[1] != 3 ||
+      vis->naxes.size() != 3 || vis->naxes[0] != 2 || rc->naxes != vis->naxes ||
+      vis->naxes[2] != tm->naxes[2]) {
+    err = "unexpected extension shapes in " + path;
+    return false;
+  }
+  in.snapshots = (size_t)tm->naxes[2];
+  in.samples = (size_t)vis->naxes[1];
+  const size_t ns = in.snapshots * in.samples;
+  in.V = tm->data;
+  in.B = rc->data;
+  in.vis_re.resize(ns);
+  in.vis_im.resize(ns);
+  for (size_t k = 0; k < ns; ++k) {
+    in.vis_re[k] = vis->data[2 * k];
+    in.vis_im[k] = vis->data[2 * k + 1];
   }
   return true;
 }

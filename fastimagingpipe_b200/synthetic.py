@@ -290,3 +290,62 @@ def config_batching(image_size: int = 4096, n_snap: int = 8, n_chan: int = 8, se
                 n_snap=n_snap, freqs_hz=freqs, flag_fraction_max=0.3)
     args.update(kw)
     return make_mfs_snapshots(seed=seed, **args)
+
+
+@dataclasses.dataclass
+class RawSnapshot:
+    """One snapshot before preprocessing: baseline uvw in metres [rows, 3],
+    channel frequencies [chans], and per sample (index row + chan * rows,
+    SVDPreprocessMain.cpp:32-34) polarisations 0 and 3 (XX, YY) with flags and
+    weights, as a Measurement Set holds them."""
+
+    uvw_m: np.ndarray
+    freqs_hz: np.ndarray
+    xx: np.ndarray  # complex64 [rows * chans]
+    yy: np.ndarray
+    flag0: np.ndarray  # uint8
+    flag3: np.ndarray
+    weight0: np.ndarray  # float32
+    weight3: np.ndarray
+    image_size: int
+    cell_size: float
+
+    @property
+    def num_samples(self) -> int:
+        return int(self.xx.shape[0])
+
+
+def make_raw_snapshot(n_ant: int = 64, radius_m: float = 1500.0, image_size: int = 256,
+                      cell_size: float = 6e-5, freqs_hz=(130e6, 140e6, 150e6),
+                      n_sources: int = 10, flag_fraction: float = 0.2,
+                      pol_leak: float = 0.3, noise_sigma: float = 0.1,
+                      dec_deg: float = -30.0, lat_deg: float = -26.7,
+                      hour_angle_h: float = 1.5, seed: int = 7) -> RawSnapshot:
+    """Seeded raw snapshot: Stokes I from point sources, XX = I + Q and
+    YY = I - Q with a random Q of relative size `pol_leak`, independent noise
+    per polarisation, each polarisation flagged with probability
+    `flag_fraction` and weighted uniformly in [0.5, 1.5)."""
+    rng = np.random.default_rng(seed)
+    enu = antenna_layout(n_ant, radius_m, rng)
+    xyz = enu_to_equatorial(baseline_vectors(enu), math.radians(lat_deg))
+    ha = 2.0 * np.pi * hour_angle_h * 3600.0 / SIDEREAL_DAY_S
+    uvw = uvw_from_xyz(xyz, ha, math.radians(dec_deg))
+    fov = image_size * cell_size
+    lm = rng.uniform(-0.2 * fov, 0.2 * fov, size=(n_sources, 2))
+    flux = rng.lognormal(mean=0.0, sigma=1.0, size=n_sources)
+    sources = np.column_stack([lm, flux])
+    freqs = np.asarray(freqs_hz, np.float64)
+    uvw_l = np.concatenate([uvw * (f / C_LIGHT) for f in freqs])  # row + chan * rows
+    stokes_i = point_source_vis(uvw_l, sources)
+    n = stokes_i.shape[0]
+    q = pol_leak * np.abs(stokes_i) * (rng.standard_normal(n) + 1j * rng.standard_normal(n))
+    noise = lambda: noise_sigma * (rng.standard_normal(n) + 1j * rng.standard_normal(n))
+    xx = (stokes_i + q + noise()).astype(np.complex64)
+    yy = (stokes_i - q + noise()).astype(np.complex64)
+    flag0 = (rng.random(n) < flag_fraction).astype(np.uint8)
+    flag3 = (rng.random(n) < flag_fraction).astype(np.uint8)
+    w0 = rng.uniform(0.5, 1.5, n).astype(np.float32)
+    w3 = rng.uniform(0.5, 1.5, n).astype(np.float32)
+    return RawSnapshot(uvw_m=uvw.astype(np.float32), freqs_hz=freqs.astype(np.float32), xx=xx,
+                       yy=yy, flag0=flag0, flag3=flag3, weight0=w0, weight3=w3,
+                       image_size=image_size, cell_size=cell_size)

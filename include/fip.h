@@ -103,6 +103,34 @@ int fip_image_snapshot(fip_imager* im, const float* vis_re, const float* vis_im,
                        const float* V, size_t nb, float* image, float* image_max, void* stream);
 
 /*
+ * Raw two-polarisation samples of one snapshot (device arrays of nb values,
+ * in the preprocessing's sample order, sample = row + channel * rows, the
+ * order fip_plane_project writes B in): polarisations 0 and 3 (XX, YY),
+ * their flags (nonzero = flagged) and weights.
+ */
+typedef struct {
+  const float* v0_re;
+  const float* v0_im;
+  const float* v3_re;
+  const float* v3_im;
+  const uint8_t* flag0;
+  const uint8_t* flag3;
+  const float* weight0;
+  const float* weight3;
+} fip_raw_vis;
+
+/*
+ * fip_image_snapshot from raw polarisations: the flag/weight Stokes-I
+ * collapse (collapse_visibility_kernel, SVDPreprocessKernels.cu:208-237;
+ * SVD_MFS.py:77-95) runs inside the gridder's visibility load, so no
+ * collapsed copy is written or read.  Same image as fip_collapse_visibilities
+ * followed by fip_image_snapshot.
+ */
+int fip_image_snapshot_raw(fip_imager* im, const fip_raw_vis* raw, const float* B,
+                           const float* V, size_t nb, float* image, float* image_max,
+                           void* stream);
+
+/*
  * The gridding stage alone (device): the visibilities of one snapshot,
  * weighted by 1/|V00 V11 - V01 V10| and spread with the ES kernel, as the
  * Hermitian half of the uv grid the reference builds (gridding +
@@ -256,6 +284,39 @@ int fip_batch_check(fip_batch* b, void* stream);
  * (its theta-terms table where the field allows), 1 the exact closed form,
  * 2 the FP32 chain evaluated step by step (no table; the same bits as 0). */
 int fip_pixel_targets(fip_imager* im, const float* V, float* out, int exact, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Trigger post-processing                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* One transient location. */
+typedef struct {
+  int32_t tile_row, tile_col; /* tile of the tLISI minimum (row-major matrix) */
+  float tlisi;                /* its tLISI */
+  float row, col;             /* refined position in image pixels (0-based) */
+  float x, y;                 /* SIN projection-plane offsets of that position
+                                 from the phase centre, radians, in the
+                                 reference's convention (its p2p x0, y0 for a
+                                 destination pixel, FIPkernels.cu:317-322):
+                                 x = -cell (col - N/2 - 1),
+                                 y = cell (row - N/2 - 1) */
+} fip_location;
+
+/*
+ * Transient locations from a tLISI matrix (device, U*U floats row-major, U =
+ * image_size / unit_size), the step the reference's output name
+ * locations.fits promises (README.md:41) but its code leaves to the user: a
+ * tile qualifies when its tLISI is below `threshold` and is the strict
+ * minimum of its 3 x 3 neighbourhood (ties to the lower tile index; NaN tiles
+ * never qualify).  Its position is refined to the centroid of the
+ * neighbourhood's drops max(0, 1 - tLISI).  Up to max_out locations are
+ * written to `out` (host), deepest first; *found gets the number found.  No
+ * counterpart in the reference.  Synchronous on `stream`; uses stream-ordered
+ * scratch (cudaMallocAsync) of 28 bytes per tile.
+ */
+int fip_locate_transients(const float* tlisi, size_t image_size, size_t unit_size,
+                          float cell_size, float threshold, fip_location* out, size_t max_out,
+                          size_t* found, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Plane projection and visibility preparation                               */

@@ -140,6 +140,47 @@ def fipipe(snap, prec="f64", want_images=False):
     return res.reshape(u, u), (imgs.reshape(3, n, n) if imgs is not None else None), mx
 
 
+def locate(tlisi, image_size, unit_size, cell, threshold):
+    """Transient locations of a tLISI matrix (the rule fip_locate_transients
+    states; the reference names its output locations.fits, README.md:41, and
+    leaves the reduction to the user): tiles below `threshold` that are the
+    strict minimum of their 3 x 3 neighbourhood (ties to the lower index),
+    refined to the neighbourhood's centroid of max(0, 1 - tLISI), sorted
+    deepest first.  Plain Python loops over the tiles (small matrices)."""
+    t = np.asarray(tlisi, np.float32)
+    u = t.shape[0]
+    out = []
+    h1 = image_size // 2 + 1
+    for r in range(u):
+        for c in range(u):
+            v = t[r, c]
+            if not v < threshold:
+                continue
+            ws = wr = wc = 0.0
+            ok = True
+            for dr in (-1, 0, 1):
+                for dc in (-1, 0, 1):
+                    rr, cc = r + dr, c + dc
+                    if not (0 <= rr < u and 0 <= cc < u):
+                        continue
+                    w = t[rr, cc]
+                    if (rr, cc) != (r, c) and (w < v or (w == v and rr * u + cc < r * u + c)):
+                        ok = False
+                    d = max(0.0, 1.0 - float(w)) if w == w else 0.0
+                    ws += d
+                    wr += d * dr
+                    wc += d * dc
+            if not ok:
+                continue
+            fr = r + (wr / ws if ws > 0 else 0.0)
+            fc = c + (wc / ws if ws > 0 else 0.0)
+            row = fr * unit_size + 0.5 * (unit_size - 1)
+            col = fc * unit_size + 0.5 * (unit_size - 1)
+            out.append((r, c, float(v), row, col, -cell * (col - h1), cell * (row - h1)))
+    out.sort(key=lambda e: (e[2], e[0] * u + e[1]))
+    return out
+
+
 def plane_fit(uvw_m, freqs_hz):
     """uvw [rows,3] metres, freqs [chans] Hz -> (B [rows*chans,2], V [3,3]) FP64."""
     uvw = _f32(uvw_m).reshape(-1, 3)

@@ -37,3 +37,30 @@ def test_reads_double_and_scaled_integers(tmp_path):
     p = tmp_path / "i.fits"
     p.write_bytes(hdr + body)
     assert np.allclose(fits.read_image(str(p)), [10.5, 9.0, 11.5])
+
+
+def test_binary_table_roundtrip(tmp_path):
+    p = str(tmp_path / "t.fits")
+    cols = [("TILE_ROW", np.array([3, 1], np.int32)), ("TLISI", np.array([0.5, 0.75], np.float32))]
+    fits.write_table(p, cols)
+    raw = open(p, "rb").read()
+    assert len(raw) % 2880 == 0 and b"XTENSION= 'BINTABLE'" in raw
+    t = fits.read_table(p)
+    assert t["TILE_ROW"].tolist() == [3, 1] and t["TLISI"].tolist() == [0.5, 0.75]
+
+
+def test_combined_input_roundtrip(tmp_path):
+    """The preprocessing tool's layout: extensions found by EXTNAME, the
+    visibilities interleaved (real, imaginary) per sample."""
+    rng = np.random.default_rng(1)
+    s, n = 3, 7
+    vr, vi = rng.standard_normal(s * n), rng.standard_normal(s * n)
+    B, V = rng.standard_normal(s * n * 2), rng.standard_normal(s * 9)
+    p = str(tmp_path / "input.fits")
+    fits.write_combined(p, vr, vi, B, V, s)
+    names = [name for name, _ in fits.read_all(p)]
+    assert names == ["", "TRANSFORMATION MATRICES", "VISIBILITIES", "R-COORDINATES"]
+    got = fits.read_combined(p)
+    assert got[4:] == (n, s)
+    for a, b in zip(got[:4], (vr, vi, B, V)):
+        assert np.array_equal(a, np.float32(b))

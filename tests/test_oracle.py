@@ -220,3 +220,20 @@ def test_collapse_matches_reference_formula():
     assert np.allclose(o_re, want_re, atol=1e-6)
     assert np.allclose(o_im, want_im, atol=1e-6)
     assert np.all(o_re[:10] == 0)
+
+
+def test_locate_rule_known_answers():
+    """The locate rule: strict 3 x 3 minima below the threshold, ties to the
+    lower index, NaN never a location; centroid refinement in tile units."""
+    t = np.ones((8, 8), np.float32)
+    t[2, 3] = 0.5
+    t[2, 4] = 0.75   # a neighbour of the minimum, not a location itself
+    t[6, 6] = t[6, 7] = 0.9
+    t[0, 0] = np.nan
+    loc = oracle.locate(t, 128, 16, 1e-3, 0.95)
+    assert [(r, c) for r, c, *_ in loc] == [(2, 3), (6, 6)]
+    r, c, v, row, col, x, y = loc[0]
+    # drops 0.5 at (2,3) and 0.25 at (2,4): the column moves a third of a tile
+    assert v == np.float32(0.5) and row == 2 * 16 + 7.5
+    assert abs(col - ((3 + 0.25 / 0.75) * 16 + 7.5)) < 1e-9
+    assert abs(x + 1e-3 * (col - 65)) < 1e-12 and abs(y - 1e-3 * (row - 65)) < 1e-12
