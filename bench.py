@@ -315,8 +315,18 @@ def run_batching_reference_shape(fip, torch, d, snap, dev, local, plain_value, p
                 ev1.record(stream)
             torch.cuda.synchronize()
             v = per_call * calls / (ev0.elapsed_time(ev1) / 1e3)
+            # Phase breakdown of the same calls (timing events in the graph).
+            b.set_profiling(True)
+            with torch.cuda.stream(stream):
+                for _ in range(calls):
+                    b.image(*a, res, stream=stream)
+            torch.cuda.synchronize()
+            ph = b.phase_times()
+            b.set_profiling(False)
             out[name] = {"value": v, "unit": UNIT, "vs_plain_form": v / plain_value,
                          "autotune": tuning,
+                         "phases_ms_per_snapshot": {k: ms / max(c, 1) / per_call
+                                                    for k, (ms, c) in ph.items()},
                          "config": f"4096^2, 130,816 baselines, tile 32, {per_call} snapshots "
                                    f"per call, {calls} calls, CUDA graph per call"}
     return out
@@ -508,6 +518,16 @@ def main():
             torch.cuda.synchronize()
             forms[name] = {"value": SNAPS_PER_STEP * reps / (ev0.elapsed_time(ev1) / 1e3),
                            "unit": UNIT, "tlisi": res2.cpu().numpy().reshape(u, u)}
+            # Per-stage device times (serialised profiling calls, per launch).
+            im2.set_profiling(True)
+            with torch.cuda.stream(stream):
+                for _ in range(5):
+                    flush.zero_()
+                    im2.pipe_device(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, res2,
+                                    stream=stream)
+            torch.cuda.synchronize()
+            forms[name]["stages_ms_per_launch"] = {
+                k: ms / c for k, (ms, c) in im2.stage_times().items() if c}
             im2.close()
         # Streaming sequence: each new snapshot yields a sliding-window tLISI.
         S = 30
@@ -552,8 +572,24 @@ def main():
             serving.run_poisson(sv, ids, beams, rates, 0.3, seed=1)  # warm-up
             sres = serving.run_poisson(sv, ids, beams, rates, 3.0, seed=2)
             sres["hbm_reserved_gb"] = sv.reserved_bytes / 2**30
+            # Saturation sweep: the same mix at growing offered load, past
+            # what the GPU can serve (throughput flattens, latency grows).
+            sweep = []
+            for factor in (1, 4, 16, 32, 64):
+                st0 = sv.stats()
+                r = serving.run_poisson(sv, ids, beams, [x * factor for x in rates], 1.5,
+                                        seed=10 + factor)
+                st1 = sv.stats()
+                steps = st1["steps"] - st0["steps"]
+                sweep.append({"offered_per_s": sum(rates) * factor,
+                              "throughput": r["throughput"], "p50_ms": r["p50_ms"],
+                              "p99_ms": r["p99_ms"], "refused": r["refused"],
+                              "snapshots_per_launch": (st1["snapshots"] - st0["snapshots"]) /
+                                                      steps if steps else None})
+            sres["saturation_sweep"] = sweep
         sres["config"] = ("beams 1024^2/32,640 bl, 2048^2/130,816, 4096^2/130,816 x2; Poisson "
-                          "200/100/50/20 snapshots/s; HBM budget 150 GB; 4 slots; 3 s")
+                          "200/100/50/20 snapshots/s (x1..x64 in the sweep, 1.5 s each); HBM "
+                          "budget 150 GB; 4 slots; merged launches of up to 8 snapshots")
         forms["serving"] = sres
 
     # ---- CPU baseline and FP64 errors (rank 0, N = 1) ----
@@ -567,6 +603,19 @@ def main():
                 line["tlisi_error_vs_fp64"][name] = float(
                     np.abs(forms[name]["tlisi"] - ref64).max())
         line["tlisi_error_vs_fp64"]["max_1_minus_tlisi_fp64"] = float((1 - ref64).max())
+        # The same shape with the transient in the third snapshot, where it
+        # survives D = ||I1 - I2| - |I2 - I3|| (1 - tLISI = 0.27 at its tile):
+        # errors measured on a matrix whose range can tell right from wrong.
+        import oracle
+        third = synthetic.config_reference(seed=1, transient_snapshot=2)
+        t64, _, _ = oracle.fipipe(third, "f64")
+        disc = {"max_1_minus_tlisi_fp64": float((1 - t64).max())}
+        for name, kw in (("plain", {}),
+                         ("precise_f16", dict(form=fip.FORM_PRECISE, vis_storage=fip.STORE_F16))):
+            with fip.Imager(n, nb, cell, t, device=local, **kw) as im3:
+                got = im3.pipe_host(third.vis_re, third.vis_im, third.B, third.V, nb)
+            disc[name] = float(np.abs(got - t64).max())
+        line["tlisi_error_vs_fp64_transient_third"] = disc
     if line is not None:
         for f in forms.values():
             f.pop("tlisi", None)

@@ -90,6 +90,13 @@ def lib() -> ctypes.CDLL:
         L.fip_imager_image.argtypes = [vp, ctypes.c_int]
         L.fip_imager_image.restype = vp
         L.fip_imager_check.argtypes = [vp, vp]
+        L.fip_server_set_max_step.argtypes = [vp, ctypes.c_int]
+        L.fip_server_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_long),
+                                       ctypes.POINTER(ctypes.c_long)]
+        L.fip_batch_image_slots.argtypes = [vp, vp, vp, vp, vp, vp, sz, vp, vp]
+        L.fip_batch_set_profiling.argtypes = [vp, ctypes.c_int]
+        L.fip_batch_phase_times.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_long)]
         L.fip_locate_transients.argtypes = [vp, sz, sz, fp, fp, vp, sz,
                                              ctypes.POINTER(sz), vp]
         L.fip_image_snapshot_raw.argtypes = [vp, ctypes.POINTER(RawVis), vp, vp, sz, vp, vp, vp]
@@ -379,6 +386,18 @@ class Batch:
     def reset(self):
         _check(lib().fip_batch_reset(self._h))
 
+    PHASES = ("prepare", "grid", "fft_cols", "fft_rows", "reproject", "trigger")
+
+    def set_profiling(self, enable: bool):
+        _check(lib().fip_batch_set_profiling(self._h, 1 if enable else 0))
+
+    def phase_times(self) -> dict:
+        """{phase: (total ms, calls)} of the profiled calls."""
+        arr = (ctypes.c_double * len(self.PHASES))()
+        calls = ctypes.c_long()
+        _check(lib().fip_batch_phase_times(self._h, arr, len(self.PHASES), ctypes.byref(calls)))
+        return {k: (arr[i], calls.value) for i, k in enumerate(self.PHASES)}
+
     def check(self, stream=None):
         """Raises FipError if a gather reprojection since the last check had a
         tile outside its domain (a folding wide-field geometry)."""
@@ -453,12 +472,20 @@ class Server:
     snapshot requests, sliding-window tLISI per beam, HBM-budget admission."""
 
     def __init__(self, hbm_budget_bytes: int, slots: int = 4, max_queue: int = 1024,
-                 device: int = 0):
+                 device: int = 0, max_step: int = None):
         h = ctypes.c_void_p()
         _check(lib().fip_server_create(ctypes.byref(h), device, int(hbm_budget_bytes), slots,
                                        max_queue))
         self._h = h
         self._beams = {}
+        if max_step is not None:
+            _check(lib().fip_server_set_max_step(self._h, int(max_step)))
+
+    def stats(self) -> dict:
+        """Merged launches run so far and the snapshots they imaged."""
+        st, sn = ctypes.c_long(), ctypes.c_long()
+        _check(lib().fip_server_stats(self._h, ctypes.byref(st), ctypes.byref(sn)))
+        return {"steps": st.value, "snapshots": sn.value}
 
     def add_beam(self, image_size: int, max_baselines: int, cell_size: float, unit_size: int,
                  form: int = FORM_PLAIN, vis_storage: int = STORE_F32,

@@ -405,9 +405,10 @@ static void imager_free(fip_imager* im) {
 }
 
 static int validate_sizes(size_t n, size_t t, float cell) {
-  if (n < 8 || n % 4 != 0)
-    return fail(FIP_ERR_ARG, "image_size must be a multiple of 4 and >= 8 (the reference's "
-                             "grid crop is misaligned when ceil(1.5 N) is odd)");
+  if (n < 16 || n % 4 != 0)
+    return fail(FIP_ERR_ARG, "image_size must be a multiple of 4 and >= 16 (the reference's "
+                             "grid crop is misaligned when ceil(1.5 N) is odd; the half-plane "
+                             "grid needs G > 18)");
   if (n > 32768) return fail(FIP_ERR_ARG, "image_size above 32768 is not supported");
   if (t > n) return fail(FIP_ERR_ARG, "unit_size larger than image_size");
   if (!(cell > 0.f) || !(cell < 1.f)) return fail(FIP_ERR_ARG, "cell_size must be in (0, 1) rad");
@@ -1317,6 +1318,14 @@ struct fip_batch {
   cudaStream_t branch[kBranches] = {};
   cudaEvent_t fork = nullptr;
   cudaEvent_t join[kBranches] = {};
+  // Phase timing (fip_batch_set_profiling): timing events captured into the
+  // call's graph at the phase boundaries, read after the call.
+  static constexpr int kPhases = 6;
+  bool profiling = false;
+  cudaEvent_t phase_ev[kPhases + 1] = {};
+  double phase_ms[kPhases] = {};
+  long phase_calls = 0;
+  bool phase_pending = false;
   cudaGraphExec_t exec = nullptr;
   unsigned long long launches = 0;
 
@@ -1353,13 +1362,32 @@ void batch_free(fip_batch* b) {
     if (b->join[k]) cudaEventDestroy(b->join[k]);
   }
   if (b->fork) cudaEventDestroy(b->fork);
+  for (cudaEvent_t e : b->phase_ev)
+    if (e) cudaEventDestroy(e);
   delete b;
 }
 
+// Folds the last profiled call's phase times into the totals (waits for it).
+int batch_collect(fip_batch* b) {
+  if (!b->phase_pending) return FIP_OK;
+  b->phase_pending = false;
+  FIP_CUDA(cudaEventSynchronize(b->phase_ev[fip_batch::kPhases]));
+  for (int k = 0; k < fip_batch::kPhases; ++k) {
+    float ms = 0.f;
+    FIP_CUDA(cudaEventElapsedTime(&ms, b->phase_ev[k], b->phase_ev[k + 1]));
+    b->phase_ms[k] += ms;
+  }
+  b->phase_calls += 1;
+  return FIP_OK;
+}
+
 // Captures the work of one call into a graph (stream s in capture mode).
+// slots (or null): per-snapshot image destinations and trigger predecessors
+// (fip_batch_image_slots) instead of the batch's own sequence ring.
 int batch_record(fip_batch* b, const float* const* vr, const float* const* vi,
                  const float* const* B, const float* const* V, const size_t* nb, int count,
-                 int first_result, float* results, cudaStream_t s) {
+                 int first_result, float* results, cudaStream_t s,
+                 const fip_batch_slot* slots = nullptr) {
   const FipGeom& geo = b->geo;
   const bool precise = b->cfg.form == FIP_FORM_PRECISE;
   const bool reduced = precise && b->cfg.vis_storage != FIP_STORE_F32;
@@ -1367,6 +1395,10 @@ int batch_record(fip_batch* b, const float* const* vr, const float* const* vi,
                           : (b->cfg.vis_storage == FIP_STORE_F16 ? FIP_VIS_F16 : FIP_VIS_BF16);
   const size_t qsz = 2;  // bytes per reduced-storage value
   unsigned long long launches = 0;
+  auto phase = [&](int k) -> cudaError_t {
+    return b->profiling ? cudaEventRecord(b->phase_ev[k], s) : cudaSuccess;
+  };
+  FIP_CUDA(phase(0));
   // Per snapshot, on the branches: storage conversion, binning, pixel mapping.
   FIP_CUDA(cudaEventRecord(b->fork, s));
   for (int i = 0; i < kBranches; ++i) FIP_CUDA(cudaStreamWaitEvent(b->branch[i], b->fork, 0));
@@ -1400,30 +1432,58 @@ int batch_record(fip_batch* b, const float* const* vr, const float* const* vi,
     FIP_CUDA(cudaEventRecord(b->join[i], b->branch[i]));
     FIP_CUDA(cudaStreamWaitEvent(s, b->join[i], 0));
   }
+  FIP_CUDA(phase(1));
   // One persistent gridding launch and one batched transform for the batch.
   FIP_CUDA(fip_launch_grid_batch(geo, in, vt, b->multi, b->ntiles, b->nmulti, b->entries, b->cap,
                                  b->work, b->wcap, b->nwork, b->grid, b->grid_elems,
                                  precise ? 1 : 0, s, b->grid_ctas_per_sm));
+  FIP_CUDA(phase(2));
   FIP_CUDA(fip_launch_fft_cols(geo, b->grid, b->bbox, b->colbuf, b->twiddles, b->fft, s, count,
                                b->grid_elems, b->col_elems));
+  FIP_CUDA(phase(3));
   FIP_CUDA(fip_launch_fft_rows(geo, b->colbuf, b->bbox, b->taper, b->twiddles, b->fft, b->pre, s,
                                count, b->col_elems, b->n2));
+  FIP_CUDA(phase(4));
   launches += 4;
-  // Reprojection per snapshot on the branches, into ring slots 2 .. count+1.
-  FIP_CUDA(cudaMemsetAsync(b->maxima + 2, 0, count * sizeof(float), s));
+  // Reprojection per snapshot on the branches, into ring slots 2 .. count+1
+  // (or the caller's slots).
+  if (slots) {
+    for (int k = 0; k < count; ++k)
+      FIP_CUDA(cudaMemsetAsync(slots[k].image_max, 0, sizeof(float), s));
+  } else {
+    FIP_CUDA(cudaMemsetAsync(b->maxima + 2, 0, count * sizeof(float), s));
+  }
   FIP_CUDA(cudaEventRecord(b->fork, s));
   for (int i = 0; i < kBranches; ++i) FIP_CUDA(cudaStreamWaitEvent(b->branch[i], b->fork, 0));
   for (int k = 0; k < count; ++k) {
     cudaStream_t bs = b->branch[k % kBranches];
+    float* img = slots ? slots[k].image : b->images + (k + 2) * b->n2;
+    float* mx = slots ? slots[k].image_max : b->maxima + k + 2;
     FIP_CUDA(fip_launch_reproject_gather(
         geo, b->pre + k * b->n2, precise ? nullptr : b->targets + k * b->n2, V[k], (int)nb[k],
-        b->bbox + 4 * k + 3, b->images + (k + 2) * b->n2,
-        reinterpret_cast<unsigned*>(b->maxima + k + 2), precise ? 1 : 0, bs, b->gather_err));
+        b->bbox + 4 * k + 3, img, reinterpret_cast<unsigned*>(mx), precise ? 1 : 0, bs,
+        b->gather_err));
     launches += 1;
   }
   for (int i = 0; i < kBranches; ++i) {
     FIP_CUDA(cudaEventRecord(b->join[i], b->branch[i]));
     FIP_CUDA(cudaStreamWaitEvent(s, b->join[i], 0));
+  }
+  FIP_CUDA(phase(5));
+  if (slots) {
+    // Each snapshot with predecessors: the tLISI of (prev 0, prev 1, itself);
+    // predecessors may be images of this call (written above).
+    for (int k = 0; k < count && geo.t > 0; ++k) {
+      const fip_batch_slot& sl = slots[k];
+      if (!sl.prev_image[0]) continue;
+      FIP_CUDA(fip_launch_trigger3(geo, sl.prev_image[0], sl.prev_image[1], sl.image,
+                                   sl.prev_max[0], sl.prev_max[1], sl.image_max, sl.tlisi,
+                                   precise ? 1 : 0, s));
+      launches += 1;
+    }
+    FIP_CUDA(phase(6));
+    b->launches += launches;
+    return FIP_OK;
   }
   // Sliding-window trigger: snapshot k (slot k + 2) with two predecessors.
   const int ntrig = count - first_result;
@@ -1433,6 +1493,7 @@ int batch_record(fip_batch* b, const float* const* vr, const float* const* vi,
                                       precise ? 1 : 0, s));
     launches += 1;
   }
+  FIP_CUDA(phase(6));
   // Carry the last two images (and maxima) to slots 0, 1.
   for (int slot = 0; slot < 2; ++slot) {
     const int from = count + slot;  // slots count, count + 1 (count >= 1)
@@ -1566,6 +1627,31 @@ int fip_batch_reset(fip_batch* b) {
   return FIP_OK;
 }
 
+int fip_batch_set_profiling(fip_batch* b, int enable) {
+  if (!b) return fail(FIP_ERR_ARG, "null batch");
+  DeviceGuard g(b->cfg.device);
+  FIP_TRY(batch_collect(b));
+  if (enable && !b->phase_ev[0])
+    for (cudaEvent_t& e : b->phase_ev) FIP_CUDA(cudaEventCreate(&e));
+  if ((enable != 0) != b->profiling && b->exec) {
+    cudaGraphExecDestroy(b->exec);  // the graph gains or loses its event nodes
+    b->exec = nullptr;
+  }
+  b->profiling = enable != 0;
+  for (double& v : b->phase_ms) v = 0.0;
+  b->phase_calls = 0;
+  return FIP_OK;
+}
+
+int fip_batch_phase_times(fip_batch* b, double* total_ms, int nphases, long* calls) {
+  if (!b || !total_ms) return fail(FIP_ERR_ARG, "null argument");
+  DeviceGuard g(b->cfg.device);
+  FIP_TRY(batch_collect(b));
+  for (int k = 0; k < nphases && k < fip_batch::kPhases; ++k) total_ms[k] = b->phase_ms[k];
+  if (calls) *calls = b->phase_calls;
+  return FIP_OK;
+}
+
 int fip_batch_check(fip_batch* b, void* stream) {
   if (!b) return fail(FIP_ERR_ARG, "null batch");
   DeviceGuard g(b->cfg.device);
@@ -1578,9 +1664,35 @@ int fip_batch_check(fip_batch* b, void* stream) {
   return FIP_OK;
 }
 
+static int batch_run(fip_batch* b, const float* const* vis_re, const float* const* vis_im,
+                     const float* const* B, const float* const* V, const size_t* nb,
+                     size_t count, float* results, size_t* nresults, void* stream,
+                     const fip_batch_slot* slots);
+
+
 int fip_batch_image(fip_batch* b, const float* const* vis_re, const float* const* vis_im,
                     const float* const* B, const float* const* V, const size_t* nb, size_t count,
                     float* results, size_t* nresults, void* stream) {
+  return batch_run(b, vis_re, vis_im, B, V, nb, count, results, nresults, stream, nullptr);
+}
+
+int fip_batch_image_slots(fip_batch* b, const float* const* vis_re, const float* const* vis_im,
+                          const float* const* B, const float* const* V, const size_t* nb,
+                          size_t count, const fip_batch_slot* slots, void* stream) {
+  if (!slots) return fail(FIP_ERR_ARG, "null slots");
+  for (size_t k = 0; k < count; ++k) {
+    const fip_batch_slot& s = slots[k];
+    if (!s.image || !s.image_max) return fail(FIP_ERR_ARG, "null slot image");
+    if (s.prev_image[0] && (!s.prev_image[1] || !s.prev_max[0] || !s.prev_max[1] || !s.tlisi))
+      return fail(FIP_ERR_ARG, "a slot with predecessors needs both, their maxima and tlisi");
+  }
+  return batch_run(b, vis_re, vis_im, B, V, nb, count, nullptr, nullptr, stream, slots);
+}
+
+static int batch_run(fip_batch* b, const float* const* vis_re, const float* const* vis_im,
+                     const float* const* B, const float* const* V, const size_t* nb,
+                     size_t count, float* results, size_t* nresults, void* stream,
+                     const fip_batch_slot* slots) {
   if (!b || !vis_re || !vis_im || !B || !V || !nb) return fail(FIP_ERR_ARG, "null argument");
   if (count < 1 || count > (size_t)b->smax)
     return fail(FIP_ERR_ARG, "count must be in [1, max_snapshots]");
@@ -1591,7 +1703,7 @@ int fip_batch_image(fip_batch* b, const float* const* vis_re, const float* const
   }
   const int first = std::max(0, 2 - b->carried);
   const int ntrig = std::max(0, (int)count - first);
-  if (ntrig > 0 && b->geo.t > 0 && !results) return fail(FIP_ERR_ARG, "null results");
+  if (!slots && ntrig > 0 && b->geo.t > 0 && !results) return fail(FIP_ERR_ARG, "null results");
   DeviceGuard g(b->cfg.device);
   if (!g.ok) return fail(FIP_ERR_CUDA, "cudaSetDevice failed");
   cudaStream_t s = (cudaStream_t)stream;
@@ -1602,9 +1714,10 @@ int fip_batch_image(fip_batch* b, const float* const* vis_re, const float* const
     FIP_CUDA(cudaEventRecord(b->fork, s));
     FIP_CUDA(cudaStreamWaitEvent(cs, b->fork, 0));
   }
+  FIP_TRY(batch_collect(b));  // the previous call's phase times, before its events are reused
   cudaGraph_t graph = nullptr;
   FIP_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-  const int st = batch_record(b, vis_re, vis_im, B, V, nb, (int)count, first, results, cs);
+  const int st = batch_record(b, vis_re, vis_im, B, V, nb, (int)count, first, results, cs, slots);
   cudaError_t e = cudaStreamEndCapture(cs, &graph);
   if (st != FIP_OK) {
     if (graph) cudaGraphDestroy(graph);
@@ -1633,12 +1746,15 @@ int fip_batch_image(fip_batch* b, const float* const* vis_re, const float* const
   }
   cudaGraphDestroy(graph);
   FIP_CUDA(cudaGraphLaunch(b->exec, cs));
+  b->phase_pending = b->profiling;
   if (cs != s) {
     FIP_CUDA(cudaEventRecord(b->fork, cs));
     FIP_CUDA(cudaStreamWaitEvent(s, b->fork, 0));
   }
-  b->carried = std::min(2, b->carried + (int)count);
-  if (nresults) *nresults = (b->geo.t > 0) ? (size_t)ntrig : 0;
+  if (!slots) {
+    b->carried = std::min(2, b->carried + (int)count);
+    if (nresults) *nresults = (b->geo.t > 0) ? (size_t)ntrig : 0;
+  }
   return FIP_OK;
 }
 

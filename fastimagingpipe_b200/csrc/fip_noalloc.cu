@@ -100,10 +100,10 @@ extern "C" int fip_grid_snapshot_noalloc(const float* vis_re, const float* vis_i
     return fip_set_error(FIP_ERR_ARG,
                          "fip_grid_snapshot_noalloc: nb must be in [1, 131072] (fixed scratch "
                          "size); use fip_grid_snapshot for larger snapshots");
-  if (image_size < 8 || image_size % 4 != 0 || image_size > kMaxImage)
+  if (image_size < 16 || image_size % 4 != 0 || image_size > kMaxImage)
     return fip_set_error(FIP_ERR_ARG,
                          "fip_grid_snapshot_noalloc: image_size must be a multiple of 4 in "
-                         "[8, 4096] (fixed scratch size)");
+                         "[16, 4096] (fixed scratch size)");
   if (!(cell_size > 0.f) || !(cell_size < 1.f))
     return fip_set_error(FIP_ERR_ARG, "cell_size must be in (0, 1) rad");
   cudaStream_t s = (cudaStream_t)stream;

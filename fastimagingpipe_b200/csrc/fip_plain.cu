@@ -75,10 +75,20 @@ __device__ __forceinline__ bool footprint(const float* B, int v, float scale, in
 // part h(r) = (g(r) + conj g(-r)) / 2 of the reference's grid g, whose real
 // transform is the real part the reference keeps (FIPkernels.cu:266): the
 // direct copy keeps taps with r2 >= 0 at (r1 mod G, r2), the mirrored copy
-// (conjugated) keeps taps with r2 <= 0 at (-r1 mod G, -r2).
-__device__ __forceinline__ bool half_cols(const Footprint& f, int mir, int& c0, int& c1) {
+// (conjugated) keeps taps with r2 <= 0 at (-r1 mod G, -r2).  Columns are
+// taken modulo G, so for even G a tap at r2 = -G/2 (the reference's first
+// grid column, FIPkernels.cu:202) lies on the Nyquist column G/2 of the
+// direct copy as well as of the mirrored one; a footprint spans 9 columns at
+// most, so for G > 18 that column is then the direct copy's only one.
+__device__ __forceinline__ bool half_cols(const Footprint& f, int mir, int g, int& c0, int& c1) {
   if (!mir) {
-    if (f.b1 < 0) return false;
+    if (f.b1 < 0) {
+      if ((g & 1) == 0 && f.b0 == -(g / 2)) {
+        c0 = c1 = g / 2;
+        return true;
+      }
+      return false;
+    }
     c0 = max(f.b0, 0); c1 = f.b1;
   } else {
     if (f.b0 > 0) return false;
@@ -136,7 +146,7 @@ __global__ void k_bin(const float* __restrict__ B, int nb, float scale, int g, i
   if (ok) k1 = (unsigned)max(abs(f.a0), abs(f.a1));
   for (int mir = 0; mir < 2; ++mir) {
     int c0 = 0, c1 = -1, trs[3], ntr = 0;
-    bool on = ok && half_cols(f, mir, c0, c1);
+    bool on = ok && half_cols(f, mir, g, c0, c1);
     if (on) {
       ntr = tile_rows(f, mir, g, trs);
       k2 = max(k2, (unsigned)c1);
@@ -284,7 +294,7 @@ __device__ __forceinline__ void for_each_entry(const float* B, int v, bool ok, f
   if (ok) k1 = max(k1, (unsigned)max(abs(fp.a0), abs(fp.a1)));
   for (int mir = 0; mir < 2; ++mir) {
     int c0 = 0, c1 = -1, trs[3], ntr = 0;
-    const bool on = ok && half_cols(fp, mir, c0, c1);
+    const bool on = ok && half_cols(fp, mir, g, c0, c1);
     if (on) {
       ntr = tile_rows(fp, mir, g, trs);
       k2 = max(k2, (unsigned)c1);
@@ -578,7 +588,7 @@ __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_ci
     Footprint f;
     footprint(B, v, scale, g, f);
     int c0, c1;
-    half_cols(f, mir, c0, c1);
+    half_cols(f, mir, g, c0, c1);
     // Visibility weighting (FIPkernels.cu:188-195), halved for the
     // Hermitian split, conjugated for the mirrored copy.
     float wr, wi;
@@ -611,7 +621,10 @@ __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_ci
 #pragma unroll
     for (int b = 0; b < 9; ++b)
       if (b < nc) {
-        const int r2 = mir ? -(c0 + b) : c0 + b;
+        // Direct copy: column c holds tap r2 = c, or r2 = -G/2 on the
+        // Nyquist column (r2 never reaches +G/2, FIPkernels.cu:203).
+        const int c = c0 + b;
+        const int r2 = mir ? -c : (2 * c == g ? -c : c);
         S.k2[q][b] = fipref::es((static_cast<float>(r2) - f.p2) * ihs);
       }
   }
@@ -1178,10 +1191,7 @@ __global__ void k_targets(const float* __restrict__ V, int n, float dc,
     const int i = (blockIdx.x * kTargetsPerThread + q) * blockDim.x + threadIdx.x;
     if (i < n) {
       float LL, MM;
-      if (ttab)
-        fipref::pixel_target_fast(fr, i, j, n, LL, MM, ttab);
-      else
-        fipref::pixel_target(fr, i, j, n, LL, MM);
+      fipref::pixel_target(fr, i, j, n, LL, MM, ttab);
       tg[(size_t)j * n + i] = make_float2(LL, MM);
     }
   }
@@ -1287,12 +1297,12 @@ __device__ __forceinline__ void exact_forward(const ExactMap<T>& m, T a, T b, T&
 // Source (a, b), relative to the centre, of an exact target (LL, MM):
 // fixed-point iteration on the slant term, a contraction wherever the map
 // does not fold (the slant part's Jacobian determinant stays positive); it
-// runs until the step is below 1e-3 pixel (or 64 steps).  Returns how far
+// runs until the step is below 1e-3 pixel (or 128 steps).  Returns how far
 // the forward map of the result lands from (LL, MM), in pixels.
 template <typename T>
 __device__ __forceinline__ T exact_inverse(const ExactMap<T>& m, T LL, T MM, T& a, T& b) {
   T P1 = LL, P2 = MM;
-  for (int it = 0; it < 64; ++it) {
+  for (int it = 0; it < 128; ++it) {
     const T zc = slant_over_cell(m, P1, P2);
     const T q1 = LL + m.xi * zc, q2 = MM - m.eta * zc;
     const T step = fmax(fabs(q1 - P1), fabs(q2 - P2));
@@ -1364,10 +1374,13 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
       res = exact_inverse(mf, L, M, a, b);
       s_q[lane][0] = a;
       s_q[lane][1] = b;
-      // Sky offset (X, Y) of the source point in radians, the slant part's
-      // Jacobian determinant there: 1 - xi X / n + eta Y / n, n = sqrt(1 - r2).
-      const float X = cell * (mf.m00 * a + mf.m01 * b - 1.0f);
-      const float Y = cell * (mf.m10 * a + mf.m11 * b - 1.0f);
+      // Sky offset (X, Y) in radians of the source point, held inside the
+      // source image (the candidates are, too), and the slant part's Jacobian
+      // determinant there: 1 - xi X / n + eta Y / n, n = sqrt(1 - r2).
+      const float lim = (float)h + 2.0f;
+      const float ac = fminf(fmaxf(a, -lim), lim), bc = fminf(fmaxf(b, -lim), lim);
+      const float X = cell * (mf.m00 * ac + mf.m01 * bc - 1.0f);
+      const float Y = cell * (mf.m10 * ac + mf.m11 * bc - 1.0f);
       r2 = X * X + Y * Y;
       const float nn = sqrtf(fmaxf(1.0f - r2, 1e-6f));
       det = 1.0f - mf.xi * X / nn + mf.eta * Y / nn;
@@ -1623,10 +1636,7 @@ __global__ void k_pixel_targets(const float* __restrict__ V, int n, float dc, fl
   float LL, MM;
   if (mode != 1) {
     fipref::Frame fr{V[0], V[1], V[3], V[4], V[8], V[6], V[7], dc};
-    if (mode == 0 && ttab)
-      fipref::pixel_target_fast(fr, i, j, n, LL, MM, ttab);  // as k_targets maps
-    else
-      fipref::pixel_target(fr, i, j, n, LL, MM);
+    fipref::pixel_target(fr, i, j, n, LL, MM, mode == 0 ? ttab : nullptr);
   } else {
     const ExactMap<double> m = make_map<double>(V, cell);
     double Ld, Md;

@@ -268,65 +268,4 @@ __device__ __forceinline__ void pixel_target(const Frame& f, int i, int j, int d
   MM = p2 - static_cast<float>(half);
 }
 
-// pixel_target on its common path, taken unless one of the chain's special
-// cases arises: a zero offset (r2 = 0, x0 = 0 or y0 = 0, where the degree
-// arctangent returns a constant), sqrt(r2) = 0 or r2 >= 0.5 (the arccosine's
-// special values, the arcsine branch), phi an exact multiple of 90 degrees
-// (exact sine and cosine), or theta outside the theta-terms table.  On that
-// path the operations are pixel_target's own, in its order and types, with
-// the special-case tests left out, so the bits are the same; any special
-// case evaluates pixel_target in full.  The special cases (a row or column
-// through the phase centre, a handful of pixels) are rare enough that the
-// check costs less than carrying their code on every pixel.
-__device__ __forceinline__ void pixel_target_fast(const Frame& f, int i, int j, int di,
-                                                  float& LL, float& MM,
-                                                  const float2* __restrict__ ttab) {
-  const int half = di / 2;
-  float p1 = (-f.v0 * (static_cast<float>(i) - static_cast<float>(half)) +
-              f.v3 * (static_cast<float>(j) - static_cast<float>(half))) /
-                 fabsf(f.v8) +
-             static_cast<float>(half);
-  float p2 = (-f.v1 * (static_cast<float>(i) - static_cast<float>(half)) +
-              f.v4 * (static_cast<float>(j) - static_cast<float>(half))) /
-                 fabsf(f.v8) +
-             static_cast<float>(half);
-  const float xi = f.v6 / f.v8;
-  const float eta = f.v7 / f.v8;
-  const float dc = f.dc;
-  float x = -dc * (p1 - (static_cast<float>(di) / 2.0f + 1.0f));
-  float y = dc * (p2 - (static_cast<float>(di) / 2.0f + 1.0f));
-  const float r0 = 180.0f / FIP_M_PI;
-  const float x0 = x / r0;
-  const float y0 = y / r0;
-  const float r2 = x0 * x0 + y0 * y0;
-  const float sr = sqrtf(r2);
-  const float phi = rad_to_deg_ret(atan2f(x0, -y0) * 180.0f);
-  const float theta = rad_to_deg_ret(acosf(sr) * 180.0f);
-  const unsigned tb = __float_as_uint(theta) - kThetaTabLo;
-  const bool common = x0 != 0.0f && y0 != 0.0f && r2 != 0.0f && sr != 0.0f && r2 < 0.5f &&
-                      !multiple_of_90(phi) && tb < (unsigned)kThetaTabSize;
-  if (!common) {
-    pixel_target(f, i, j, di, LL, MM, ttab);
-    return;
-  }
-  const float arg = deg_to_rad_arg(phi);
-  const float sinphi = sinf(arg), cosphi = cosf(arg);
-  const float2 q = __ldg(&ttab[tb]);
-  const float r = q.x, zr0 = q.y;
-  const float w = xi * xi + eta * eta;
-  if (w == 0.0f) {
-    x = r * sinphi;
-    y = -r * cosphi;
-  } else {
-    const float z1 = xi * zr0;
-    const float z2 = eta * zr0;
-    x = r * sinphi + z1;
-    y = -r * cosphi + z2;
-  }
-  p1 = -1.0f / static_cast<float>(dc) * x + static_cast<float>(di) / 2.0f + 1.0f;
-  p2 = 1.0f / static_cast<float>(dc) * y + static_cast<float>(di) / 2.0f + 1.0f;
-  LL = p1 - static_cast<float>(half);
-  MM = p2 - static_cast<float>(half);
-}
-
 }  // namespace fipref

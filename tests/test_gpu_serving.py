@@ -2,7 +2,9 @@
 
 Continuous batching must not change results: every beam's sliding-window
 tLISI is the same served alone and served in a mix of beams whose requests
-overlap on the device (tolerance 1e-6: only FP32 summation order differs).
+are merged into shared batched launches and overlap on the device
+(tolerance 1e-6: only FP32 summation order may differ), and the same as the
+per-snapshot imager's.
 """
 import numpy as np
 import pytest
@@ -48,6 +50,10 @@ def test_results_same_alone_and_in_the_mix(cuda):
                 reqs[i].append(sv.submit(i, s.vis_re[k * n:(k + 1) * n], s.vis_im[k * n:(k + 1) * n],
                                          s.B[2 * k * n:2 * (k + 1) * n], s.V[9 * k:9 * k + 9], n))
         mixed = {i: [sv.wait(r) for r in reqs[i]] for i in ids}
+        st = sv.stats()
+    # 20 requests queued at once over two groups of two beams: the steps
+    # merged several snapshots each.
+    assert st["snapshots"] == 20 and st["steps"] < st["snapshots"]
     got = mixed[ids[0]]
     for a, m in zip(alone, got):
         assert a["seq"] == m["seq"]
