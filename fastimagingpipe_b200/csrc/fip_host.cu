@@ -1396,7 +1396,9 @@ int batch_record(fip_batch* b, const float* const* vr, const float* const* vi,
   const size_t qsz = 2;  // bytes per reduced-storage value
   unsigned long long launches = 0;
   auto phase = [&](int k) -> cudaError_t {
-    return b->profiling ? cudaEventRecord(b->phase_ev[k], s) : cudaSuccess;
+    // Inside stream capture only an external record becomes a record node.
+    return b->profiling ? cudaEventRecordWithFlags(b->phase_ev[k], s, cudaEventRecordExternal)
+                        : cudaSuccess;
   };
   FIP_CUDA(phase(0));
   // Per snapshot, on the branches: storage conversion, binning, pixel mapping.

@@ -1334,9 +1334,15 @@ __device__ __forceinline__ T exact_inverse(const ExactMap<T>& m, T LL, T MM, T& 
 constexpr int kAp = 4;
 constexpr int kTW = kDT + 2 * kAp;  // tile side with the apron
 constexpr int kTR = kTW + 1;        // row stride
+// The preimage of a tile's boundary is sampled at kSeg points per edge: a
+// polygon of kPoly vertices, whose chords stay within a small curvature
+// margin of the true preimage even for strongly tilted wide fields.
+constexpr int kSeg = 2;
+constexpr int kPoly = 4 * kSeg;
+static_assert(kPoly <= 32 && (kPoly & (kPoly - 1)) == 0, "one warp's lanes, a power of two");
 
 template <bool EXACT>
-__global__ void __launch_bounds__(kThreads) k_reproject_gather(
+__global__ void __launch_bounds__(kThreads, EXACT ? 5 : 8) k_reproject_gather(
     const float* __restrict__ pre, const float2* __restrict__ tg, const float* __restrict__ V,
     int n, int nb, float cell, float delta, const unsigned* __restrict__ pre_max,
     float* __restrict__ dst, unsigned* img_max, unsigned* err) {
@@ -1344,7 +1350,7 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
   __shared__ int s_base[kMaxRows];  // pixel index of row r's first candidate minus its number
   __shared__ int s_off[kMaxRows + 1];
   __shared__ int s_wsum[kThreads / 32];
-  __shared__ float s_q[4][2];
+  __shared__ float s_q[kPoly][2];
   __shared__ float s_wmax[kThreads / 32];
 
   const int tiles = (n + kDT - 1) / kDT;
@@ -1360,17 +1366,24 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
   // corners and read by every thread after the barrier.
   __shared__ ExactMap<double> s_md;
   if (EXACT && threadIdx.x == 4) s_md = make_map<double>(V, cell);
-  // Preimage corners of the tile widened by the splat reach and delta (lanes
-  // 0-3 of warp 0), the tile's domain check and its curvature margin.
-  __shared__ float s_sag;
+  // Preimage of the tile's boundary, widened by the splat reach and delta:
+  // kPoly points, kSeg per edge, in order around it (lanes of warp 0), the
+  // tile's domain check and its curvature margin.
+  __shared__ float s_sag, s_bmin, s_bmax, s_parea;
   if (warp == 0) {
     const ExactMap<float> mf = make_map_f32(V, cell);
     const float Llo = (float)(c0 - h) - 1.0f - delta, Lhi = (float)(c0 + kDT - h) + delta;
     const float Mlo = (float)(r0 - h) - 1.0f - delta, Mhi = (float)(r0 + kDT - h) + delta;
     float a = 0.f, b = 0.f, res = 0.f, r2 = 0.f, det = 1.f;
-    if (lane < 4) {
-      const float L = (lane == 0 || lane == 3) ? Llo : Lhi;
-      const float M = (lane < 2) ? Mlo : Mhi;
+    if (lane < kPoly) {
+      // Corners (Llo, Mlo), (Lhi, Mlo), (Lhi, Mhi), (Llo, Mhi); point s of
+      // edge e lies s / kSeg of the way from corner e to corner e + 1.
+      const int e = lane / kSeg, sg = lane % kSeg;
+      const float Le = (e == 0 || e == 3) ? Llo : Lhi, Me = (e < 2) ? Mlo : Mhi;
+      const int e1 = (e + 1) & 3;
+      const float Ln = (e1 == 0 || e1 == 3) ? Llo : Lhi, Mn = (e1 < 2) ? Mlo : Mhi;
+      const float w = (float)sg * (1.0f / (float)kSeg);
+      const float L = Le + (Ln - Le) * w, M = Me + (Mn - Me) * w;
       res = exact_inverse(mf, L, M, a, b);
       s_q[lane][0] = a;
       s_q[lane][1] = b;
@@ -1385,34 +1398,41 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
       const float nn = sqrtf(fmaxf(1.0f - r2, 1e-6f));
       det = 1.0f - mf.xi * X / nn + mf.eta * Y / nn;
     }
+    // Row range and shoelace area of the polygon, reduced over its lanes.
+    float bmn = lane < kPoly ? b : 3e38f, bmx = lane < kPoly ? b : -3e38f;
+    const int nxt = (lane + 1) % kPoly;
+    const float an = __shfl_sync(0xffffffffu, a, nxt), bn = __shfl_sync(0xffffffffu, b, nxt);
+    float area = lane < kPoly ? a * bn - an * b : 0.f;
 #pragma unroll
-    for (int o = 1; o < 4; o <<= 1) {
+    for (int o = 1; o < kPoly; o <<= 1) {
       res = fmaxf(res, __shfl_xor_sync(0xffffffffu, res, o));
       r2 = fmaxf(r2, __shfl_xor_sync(0xffffffffu, r2, o));
       det = fminf(det, __shfl_xor_sync(0xffffffffu, det, o));
+      bmn = fminf(bmn, __shfl_xor_sync(0xffffffffu, bmn, o));
+      bmx = fmaxf(bmx, __shfl_xor_sync(0xffffffffu, bmx, o));
+      area += __shfl_xor_sync(0xffffffffu, area, o);
     }
     if (lane == 0) {
       // The candidate bounds hold while the inverse converged, the tile lies
       // well inside the horizon (r2 < 0.98) and the map does not fold
       // (det > 1/4); a tile outside that domain is reported, not skipped.
       if (err && !(res < 0.05f && r2 < 0.98f && det > 0.25f)) atomicOr(err, 1u);
-      // The preimage's edges bow away from the chords between its corners
+      // The preimage's edges bow away from the chords between its points
       // by at most ell^2 / 8 times the slant term's second derivative
-      // (|(xi, eta)| cell / n^3, divided by det for the inverse): widen the
-      // candidate intervals by that (with a 20 % allowance).
+      // (|(xi, eta)| cell / n^3, divided by det for the inverse), ell the
+      // length of one segment: widen the candidate intervals by that (with a
+      // 20 % allowance).
       const float nn = sqrtf(fmaxf(1.0f - r2, 0.02f));
-      const float ell = (float)kDT + 2.0f + 2.0f * delta;
+      const float ell = ((float)kDT + 2.0f + 2.0f * delta) * (1.0f / (float)kSeg);
       s_sag = 0.15f * hypotf(mf.xi, mf.eta) * cell * ell * ell /
               (nn * nn * nn * fmaxf(det, 0.25f));
+      s_bmin = bmn;
+      s_bmax = bmx;
+      s_parea = fabsf(0.5f * area);
     }
   }
   __syncthreads();
-  float bmin = s_q[0][1], bmax = s_q[0][1];
-#pragma unroll
-  for (int k = 1; k < 4; ++k) {
-    bmin = fminf(bmin, s_q[k][1]);
-    bmax = fmaxf(bmax, s_q[k][1]);
-  }
+  const float bmin = s_bmin, bmax = s_bmax;
   const float sag = s_sag + 1e-3f;
   const int jlo = (int)fmaxf(0.f, ceilf(fmaxf(bmin + h - sag, -1.f)));
   const int jhi = (int)fminf((float)(n - 1), floorf(fminf(bmax + h + sag, (float)n)));
@@ -1429,11 +1449,7 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
   // maximum) unless the preimage of the tile, with its margins, covers more
   // than twice the tile's area -- a map that contracts, which only very wide
   // fields with a tilted plane reach -- and then grows by one per doubling.
-  float parea = 0.f;  // preimage quadrilateral's area (shoelace)
-#pragma unroll
-  for (int k = 0; k < 4; ++k)
-    parea += s_q[k][0] * s_q[(k + 1) & 3][1] - s_q[(k + 1) & 3][0] * s_q[k][1];
-  parea = fabsf(0.5f * parea);
+  const float parea = s_parea;  // preimage polygon's area (shoelace)
   int sh = 0;
   while (sh < 12 && parea > (float)(2 * kDT * kDT) * (float)(1 << sh)) ++sh;
   const float pmax = __uint_as_float(*pre_max);
@@ -1452,8 +1468,8 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
     mf.m11 = (float)md.m11; mf.i00 = (float)md.i00; mf.i01 = (float)md.i01;
     mf.i10 = (float)md.i10; mf.i11 = (float)md.i11; mf.xi = (float)md.xi;
     mf.eta = (float)md.eta; mf.cell = (float)md.cell;
-    a0 = (int)rintf(0.25f * (s_q[0][0] + s_q[1][0] + s_q[2][0] + s_q[3][0]));
-    b0 = (int)rintf(0.25f * (s_q[0][1] + s_q[1][1] + s_q[2][1] + s_q[3][1]));
+    a0 = (int)rintf(0.25f * (s_q[0][0] + s_q[kSeg][0] + s_q[2 * kSeg][0] + s_q[3 * kSeg][0]));
+    b0 = (int)rintf(0.25f * (s_q[0][1] + s_q[kSeg][1] + s_q[2 * kSeg][1] + s_q[3 * kSeg][1]));
     const double P1 = md.m00 * a0 + md.m01 * b0, P2 = md.m10 * a0 + md.m11 * b0;
     p10 = (float)P1;
     p20 = (float)P2;
@@ -1517,9 +1533,9 @@ __global__ void __launch_bounds__(kThreads) k_reproject_gather(
         const float b = fminf(fmaxf((float)(cj + r - h), bmin), bmax);
         float alo = 3e38f, ahi = -3e38f;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < kPoly; ++k) {
           const float ax = s_q[k][0], bx = s_q[k][1];
-          const float ay = s_q[(k + 1) & 3][0], by = s_q[(k + 1) & 3][1];
+          const float ay = s_q[(k + 1) % kPoly][0], by = s_q[(k + 1) % kPoly][1];
           if ((bx <= b && b <= by) || (by <= b && b <= bx)) {
             if (by == bx) {
               alo = fminf(alo, fminf(ax, ay));
