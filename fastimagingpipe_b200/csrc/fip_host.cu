@@ -303,6 +303,11 @@ struct fip_imager {
   // host-buffer path; h_err is its pinned copy.
   unsigned* gather_err = nullptr;
   unsigned* h_err = nullptr;
+  // Trigger fused into a three-snapshot call's reprojections (concurrent
+  // lanes, tile gather): a count per 64 x 64 region and the statistics of
+  // every trigger tile.
+  unsigned* fuse_count = nullptr;
+  double* fuse_stats = nullptr;
   // Device and pinned staging of the host-buffer path, 3 snapshot slots.
   // Per snapshot k, one block of 4 nb floats at k * 4 nb: B [2 nb], vis
   // real [nb], vis imaginary [nb], so each snapshot crosses PCIe in one copy.
@@ -379,7 +384,7 @@ static void imager_free(fip_imager* im) {
   for (float* p : im->images)
     if (p) cudaFree(p);
   void* dptrs[] = {im->taper, im->twiddles, im->theta_tab, im->maxima, im->result, im->stats,
-                   im->d_snap, im->d_V, im->gather_err};
+                   im->d_snap, im->d_V, im->gather_err, im->fuse_count, im->fuse_stats};
   for (void* p : dptrs)
     if (p) cudaFree(p);
   void* hptrs[] = {im->h_snap, im->h_V, im->h_result, im->h_err};
@@ -555,6 +560,13 @@ int fip_imager_create(fip_imager** out, const fip_imager_config* cfg) {
                            std::max<size_t>((size_t)geo.u * geo.u, 1) * sizeof(float)));
   FIP_ALLOC(dalloc(&im->gather_err, 1, tot));
   FIP_ALLOC(cudaMemset(im->gather_err, 0, sizeof(unsigned)));
+  // Plain form only: the precision form's compensated statistics cost the
+  // last reprojection more than the separate pass (measured 3 % slower).
+  if (im->lanes > 1 && cfg->reproject == 0 && cfg->form == FIP_FORM_PLAIN &&
+      fip_trigger_fusable(geo)) {
+    FIP_ALLOC(dalloc(&im->fuse_count, fip_trigger_fuse_counts(geo), tot));
+    FIP_ALLOC(dalloc(&im->fuse_stats, 3 * (size_t)geo.u * geo.u, tot));
+  }
   FIP_ALLOC(cudaMallocHost((void**)&im->h_err, sizeof(unsigned)));
   *im->h_err = 0;
 
@@ -593,7 +605,8 @@ static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const f
                                const float* B, const float* V, size_t nb, float* image,
                                float* image_max, cudaStream_t s, bool fork_targets,
                                bool targets_ready = false, cudaEvent_t targets_ev = nullptr,
-                               bool force_scatter = false, const FipRawVis* raw = nullptr) {
+                               bool force_scatter = false, const FipRawVis* raw = nullptr,
+                               const FipFuse* fuse = nullptr) {
   const FipGeom& geo = im->geo;
   if (nb > im->cfg.max_baselines) return fail(FIP_ERR_ARG, "nb exceeds the imager's capacity");
   if (nb == 0) return fail(FIP_ERR_ARG, "nb must be positive");
@@ -679,7 +692,7 @@ static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const f
     k = stage_begin(im, ST_REPROJECT, s);
     FIP_CUDA(fip_launch_reproject_gather(geo, L.pre, L.targets, V, (int)nb, L.bins.bbox + 3,
                                          image, reinterpret_cast<unsigned*>(image_max),
-                                         precise ? 1 : 0, s, im->gather_err));
+                                         precise ? 1 : 0, s, im->gather_err, fuse));
     stage_end(im, k, s);
     im->launches += 1;
   }
@@ -693,19 +706,36 @@ static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const f
 static int image_on_lane(fip_imager* im, int k, const float* vr, const float* vi,
                          const float* B, const float* V, size_t nb, float* image,
                          float* image_max, cudaStream_t s, cudaEvent_t after,
-                         bool targets_ready = false, bool force_scatter = false) {
+                         bool targets_ready = false, bool force_scatter = false,
+                         const FipFuse* fuse = nullptr) {
   if (im->lanes == 1 || im->timer.on) {
     FIP_CUDA(cudaStreamWaitEvent(s, after, 0));
     return image_snapshot_impl(im, im->lane[k % im->lanes], vr, vi, B, V, nb, image, image_max,
-                               s, true, false, nullptr, force_scatter);
+                               s, true, false, nullptr, force_scatter, nullptr, fuse);
   }
   Lane& L = im->lane[k % im->lanes];
   FIP_CUDA(cudaStreamWaitEvent(L.stream, after, 0));
   FIP_TRY(image_snapshot_impl(im, L, vr, vi, B, V, nb, image, image_max, L.stream, false,
                               targets_ready, targets_ready ? L.ev_targets : nullptr,
-                              force_scatter));
+                              force_scatter, nullptr, fuse));
   FIP_CUDA(cudaEventRecord(L.ev_done, L.stream));
   return FIP_OK;
+}
+
+// Whether a three-snapshot call fuses its trigger into the reprojections:
+// the plain form on concurrent lanes (not serialised for profiling, whose
+// stage times keep the trigger apart), the tile gather, a tile side dividing
+// the gather's 64.
+static bool fuse_ok(const fip_imager* im) {
+  return im->fuse_count && !im->timer.on && im->lanes > 1;
+}
+
+static FipFuse fuse_of(const fip_imager* im) {
+  FipFuse f{};
+  for (int k = 0; k < 3; ++k) f.img[k] = im->images[k];
+  f.count = im->fuse_count;
+  f.stats = im->fuse_stats;
+  return f;
 }
 
 // Whether a three-snapshot call maps its pixels ahead on the side stream:
@@ -822,17 +852,27 @@ int fip_pipe_device(fip_imager* im, const float* vr, const float* vi, const floa
   DeviceGuard g(im->cfg.device);
   cudaStream_t s = (cudaStream_t)stream;
   FIP_TRY(call_enter(im, s));
-  // The three snapshots image concurrently on the lanes; the trigger joins them.
+  // The three snapshots image concurrently on the lanes; the trigger joins them
+  // (fused into their reprojections when it can be).
+  const FipFuse fz = fuse_of(im);
+  const bool fused = fuse_ok(im) && result;
+  if (fused) FIP_CUDA(cudaMemsetAsync(im->fuse_count, 0,
+                                      fip_trigger_fuse_counts(im->geo) * sizeof(unsigned), s));
   FIP_CUDA(cudaEventRecord(im->ev_start, s));
   const bool ahead = targets_ahead(im);
   if (ahead) FIP_TRY(launch_targets_ahead(im, V, im->ev_start));
   for (int k = 0; k < 3; ++k)
     FIP_TRY(image_on_lane(im, k, vr + (size_t)k * nb, vi + (size_t)k * nb,
                           B + (size_t)k * nb * 2, V + (size_t)k * 9, nb, im->images[k],
-                          im->maxima + k, s, im->ev_start, ahead));
+                          im->maxima + k, s, im->ev_start, ahead, false,
+                          fused ? &fz : nullptr));
   for (int k = 0; k < 3; ++k) FIP_TRY(wait_lane(im, k, s));
   im->last_lane = 2 % im->lanes;
-  if (im->geo.t > 0 && result) {
+  if (fused) {
+    FIP_CUDA(fip_launch_trigger_combine(im->geo, im->fuse_stats, im->maxima, result,
+                                        im->cfg.form == FIP_FORM_PRECISE ? 1 : 0, s));
+    im->launches += 1;
+  } else if (im->geo.t > 0 && result) {
     const int k = stage_begin(im, ST_TRIGGER, s);
     FIP_CUDA(fip_launch_trigger(im->geo, im->images[0], im->images[1], im->images[2],
                                 im->maxima, im->stats, result,
@@ -896,6 +936,12 @@ int fip_pipe_host(fip_imager* im, const float* vr, const float* vi, const float*
   if (im->cfg.reproject == 0)
     for (int k = 0; k < 3; ++k)
       scatter[k] = !fip_gather_domain_ok(V + 9 * k, im->geo.n, im->cfg.cell_size);
+  // The trigger fuses into the three reprojections when all three gather;
+  // the counts are cleared on the copy stream, ahead of every lane.
+  const FipFuse fz = fuse_of(im);
+  const bool fused = fuse_ok(im) && !scatter[0] && !scatter[1] && !scatter[2];
+  if (fused) FIP_CUDA(cudaMemsetAsync(im->fuse_count, 0,
+                                      fip_trigger_fuse_counts(im->geo) * sizeof(unsigned), cs));
   FIP_CUDA(cudaMemcpyAsync(im->d_V, im->h_V, 27 * sizeof(float), cudaMemcpyHostToDevice, cs));
   const bool early = targets_ahead(im);
   if (early) {
@@ -918,11 +964,15 @@ int fip_pipe_host(fip_imager* im, const float* vr, const float* vi, const float*
     FIP_CUDA(cudaMemcpyAsync(ds, hs, 4 * nb * sizeof(float), cudaMemcpyHostToDevice, cs));
     FIP_CUDA(cudaEventRecord(im->ev_copied[k], cs));
     FIP_TRY(image_on_lane(im, k, dvr, dvi, dB, dV, nb, im->images[k], im->maxima + k, s,
-                          im->ev_copied[k], early, scatter[k]));
+                          im->ev_copied[k], early, scatter[k], fused ? &fz : nullptr));
   }
   for (int k = 0; k < 3; ++k) FIP_TRY(wait_lane(im, k, s));
   im->last_lane = 2 % im->lanes;
-  {
+  if (fused) {
+    FIP_CUDA(fip_launch_trigger_combine(im->geo, im->fuse_stats, im->maxima, im->result,
+                                        im->cfg.form == FIP_FORM_PRECISE ? 1 : 0, s));
+    im->launches += 1;
+  } else {
     const int k = stage_begin(im, ST_TRIGGER, s);
     FIP_CUDA(fip_launch_trigger(im->geo, im->images[0], im->images[1], im->images[2],
                                 im->maxima, im->stats, im->result,
@@ -1316,6 +1366,13 @@ struct fip_batch {
   unsigned* gather_err = nullptr;     // [1] set by a gather tile outside its domain
   int carried = 0;
   cudaStream_t branch[kBranches] = {};
+  cudaStream_t capture = nullptr;  // capture and launch stream (highest priority)
+  // Pixel-mapping branches at the lowest priority: the mappings need only V,
+  // so they run beside the gridding and the transforms and join the call
+  // only before its reprojections.
+  static constexpr int kMapBranches = 2;
+  cudaStream_t map_branch[kMapBranches] = {};
+  cudaEvent_t map_join[kMapBranches] = {};
   cudaEvent_t fork = nullptr;
   cudaEvent_t join[kBranches] = {};
   // Phase timing (fip_batch_set_profiling): timing events captured into the
@@ -1361,6 +1418,11 @@ void batch_free(fip_batch* b) {
     if (b->branch[k]) cudaStreamDestroy(b->branch[k]);
     if (b->join[k]) cudaEventDestroy(b->join[k]);
   }
+  for (int k = 0; k < fip_batch::kMapBranches; ++k) {
+    if (b->map_branch[k]) cudaStreamDestroy(b->map_branch[k]);
+    if (b->map_join[k]) cudaEventDestroy(b->map_join[k]);
+  }
+  if (b->capture) cudaStreamDestroy(b->capture);
   if (b->fork) cudaEventDestroy(b->fork);
   for (cudaEvent_t e : b->phase_ev)
     if (e) cudaEventDestroy(e);
@@ -1401,9 +1463,22 @@ int batch_record(fip_batch* b, const float* const* vr, const float* const* vi,
                         : cudaSuccess;
   };
   FIP_CUDA(phase(0));
-  // Per snapshot, on the branches: storage conversion, binning, pixel mapping.
+  // Per snapshot, on the branches: storage conversion and binning; the pixel
+  // mappings (plain form) on the low-priority mapping branches, joined only
+  // before the reprojections.
   FIP_CUDA(cudaEventRecord(b->fork, s));
   for (int i = 0; i < kBranches; ++i) FIP_CUDA(cudaStreamWaitEvent(b->branch[i], b->fork, 0));
+  if (!precise) {
+    for (int i = 0; i < fip_batch::kMapBranches; ++i)
+      FIP_CUDA(cudaStreamWaitEvent(b->map_branch[i], b->fork, 0));
+    for (int k = 0; k < count; ++k) {
+      FIP_CUDA(fip_launch_targets(geo, V[k], b->theta_tab, b->targets + k * b->n2,
+                                  b->map_branch[k % fip_batch::kMapBranches]));
+      launches += 1;
+    }
+    for (int i = 0; i < fip_batch::kMapBranches; ++i)
+      FIP_CUDA(cudaEventRecord(b->map_join[i], b->map_branch[i]));
+  }
   FipGridBatch in{};
   in.count = count;
   for (int k = 0; k < count; ++k) {
@@ -1425,10 +1500,6 @@ int batch_record(fip_batch* b, const float* const* vr, const float* const* vi,
     FipBins bins = b->bins(k);
     FIP_CUDA(fip_launch_bin(geo, B[k], (int)nb[k], bins, bs));
     launches += fip_bin_launches(geo);
-    if (!precise) {
-      FIP_CUDA(fip_launch_targets(geo, V[k], b->theta_tab, b->targets + k * b->n2, bs));
-      launches += 1;
-    }
   }
   for (int i = 0; i < kBranches; ++i) {
     FIP_CUDA(cudaEventRecord(b->join[i], b->branch[i]));
@@ -1447,6 +1518,9 @@ int batch_record(fip_batch* b, const float* const* vr, const float* const* vi,
                                count, b->col_elems, b->n2));
   FIP_CUDA(phase(4));
   launches += 4;
+  if (!precise)
+    for (int i = 0; i < fip_batch::kMapBranches; ++i)
+      FIP_CUDA(cudaStreamWaitEvent(s, b->map_join[i], 0));
   // Reprojection per snapshot on the branches, into ring slots 2 .. count+1
   // (or the caller's slots).
   if (slots) {
@@ -1601,9 +1675,18 @@ int fip_batch_create(fip_batch** out, const fip_imager_config* cfg, size_t max_s
     FIP_BALLOC(cudaMemcpy(b->twiddles, tw.data(), tw.size() * sizeof(float2),
                           cudaMemcpyHostToDevice));
   }
-  for (int k = 0; k < kBranches; ++k) {
-    FIP_BALLOC(cudaStreamCreateWithFlags(&b->branch[k], cudaStreamNonBlocking));
-    FIP_BALLOC(cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming));
+  {
+    int least = 0, greatest = 0;
+    FIP_BALLOC(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    FIP_BALLOC(cudaStreamCreateWithPriority(&b->capture, cudaStreamNonBlocking, greatest));
+    for (int k = 0; k < kBranches; ++k) {
+      FIP_BALLOC(cudaStreamCreateWithPriority(&b->branch[k], cudaStreamNonBlocking, greatest));
+      FIP_BALLOC(cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming));
+    }
+    for (int k = 0; k < fip_batch::kMapBranches; ++k) {
+      FIP_BALLOC(cudaStreamCreateWithPriority(&b->map_branch[k], cudaStreamNonBlocking, least));
+      FIP_BALLOC(cudaEventCreateWithFlags(&b->map_join[k], cudaEventDisableTiming));
+    }
   }
   FIP_BALLOC(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
   FIP_BALLOC(fip_launch_taper(b->taper, geo, b->branch[0]));
@@ -1709,13 +1792,14 @@ static int batch_run(fip_batch* b, const float* const* vis_re, const float* cons
   DeviceGuard g(b->cfg.device);
   if (!g.ok) return fail(FIP_ERR_CUDA, "cudaSetDevice failed");
   cudaStream_t s = (cudaStream_t)stream;
-  cudaStream_t cs = s;
-  // The legacy default stream cannot be captured: record on a branch then.
-  if (s == nullptr || s == cudaStreamLegacy) cs = b->branch[0];
-  if (cs != s) {
-    FIP_CUDA(cudaEventRecord(b->fork, s));
-    FIP_CUDA(cudaStreamWaitEvent(cs, b->fork, 0));
-  }
+  // The call is captured (and launched) on the batch's own highest-priority
+  // stream, ordered after the caller's stream and joined back to it: its
+  // latency-bound stages then take SM slots ahead of the low-priority pixel
+  // mappings (and the legacy default stream, which cannot be captured, is
+  // never the capture stream).
+  cudaStream_t cs = b->capture;
+  FIP_CUDA(cudaEventRecord(b->fork, s));
+  FIP_CUDA(cudaStreamWaitEvent(cs, b->fork, 0));
   FIP_TRY(batch_collect(b));  // the previous call's phase times, before its events are reused
   cudaGraph_t graph = nullptr;
   FIP_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
@@ -1726,6 +1810,29 @@ static int batch_run(fip_batch* b, const float* const* vis_re, const float* cons
     return st;
   }
   if (e != cudaSuccess) return fail(FIP_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
+  {
+    // Kernel nodes run at the default (lowest) priority unless told: give
+    // the call's latency-bound chain the highest and leave the pixel
+    // mappings at the lowest, so they fill what the chain leaves (as the
+    // lanes' stream priorities do outside graphs).
+    int least = 0, greatest = 0;
+    FIP_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    size_t nn = 0;
+    FIP_CUDA(cudaGraphGetNodes(graph, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (nn) FIP_CUDA(cudaGraphGetNodes(graph, nodes.data(), &nn));
+    const void* mapk = fip_targets_kernel();
+    for (cudaGraphNode_t nd : nodes) {
+      cudaGraphNodeType ty;
+      FIP_CUDA(cudaGraphNodeGetType(nd, &ty));
+      if (ty != cudaGraphNodeTypeKernel) continue;
+      cudaKernelNodeParams kp{};
+      FIP_CUDA(cudaGraphKernelNodeGetParams(nd, &kp));
+      cudaLaunchAttributeValue v{};
+      v.priority = kp.func == mapk ? least : greatest;
+      FIP_CUDA(cudaGraphKernelNodeSetAttribute(nd, cudaLaunchAttributePriority, &v));
+    }
+  }
   // Re-use the executable graph when the call's shape is unchanged (only
   // pointers, sizes and launch extents differ); instantiate otherwise.
   bool updated = false;
@@ -1739,7 +1846,8 @@ static int batch_run(fip_batch* b, const float* const* vis_re, const float* cons
     }
   }
   if (!updated) {
-    e = cudaGraphInstantiate(&b->exec, graph, 0);
+    // Per-node priorities (set above) apply only with this flag.
+    e = cudaGraphInstantiate(&b->exec, graph, cudaGraphInstantiateFlagUseNodePriority);
     if (e != cudaSuccess) {
       cudaGraphDestroy(graph);
       b->exec = nullptr;

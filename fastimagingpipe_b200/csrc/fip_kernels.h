@@ -81,6 +81,8 @@ cudaError_t fip_launch_correct_c2r(const FipGeom& geo, const float* fft_out, con
 // fewer instructions), or null.
 cudaError_t fip_launch_targets(const FipGeom& geo, const float* V, const float2* theta_tab,
                                float2* targets, cudaStream_t s);
+// The pixel-mapping kernel's entry (to tell its graph nodes apart).
+const void* fip_targets_kernel();
 // Entries of the theta-terms table of the pixel mapping, and its fill.
 size_t fip_theta_table_elems();
 cudaError_t fip_launch_theta_table(float2* tab, cudaStream_t s);
@@ -92,13 +94,32 @@ cudaError_t fip_launch_reproject_scatter(const FipGeom& geo, const float* pre, c
 // candidate source pixels, splats in shared memory and is stored once.  Also
 // records the image maximum into *img_max (atomic max, caller zeroes it).
 bool fip_gather_supported(const FipGeom& geo, int exact_targets);
+// The trigger of a three-snapshot call fused into its three reprojections:
+// the images I1, I2, I3 (dst is one of them), a count per 64 x 64 region
+// (fip_trigger_fuse_counts of them, zeroed before the first of the three
+// launches) and the per-tile statistics [U*U][3], which
+// fip_launch_trigger_combine turns into tLISI once the three are done.  The
+// statistics are reduced in k_trigger's order, so the results are the
+// separate trigger's bit for bit.  Needs fip_trigger_fusable(geo).
+struct FipFuse {
+  const float* img[3];
+  unsigned* count;
+  double* stats;
+};
+bool fip_trigger_fusable(const FipGeom& geo);
+size_t fip_trigger_fuse_counts(const FipGeom& geo);
+cudaError_t fip_launch_trigger_combine(const FipGeom& geo, const double* stats,
+                                       const float* max3, float* result, int precise,
+                                       cudaStream_t s);
 // pre_max: maximum of pre (float bits), from the transform's epilogue.
 // err (or null): set to nonzero when a tile lies outside the gather's domain
 // (fip_gather_domain_ok); its image is then not to be trusted.
+// fuse (or null): fuse the call's trigger into this reprojection.
 cudaError_t fip_launch_reproject_gather(const FipGeom& geo, const float* pre,
                                         const float2* targets, const float* V, int nb,
                                         const unsigned* pre_max, float* dst, unsigned* img_max,
-                                        int exact_targets, cudaStream_t s, unsigned* err);
+                                        int exact_targets, cudaStream_t s, unsigned* err,
+                                        const FipFuse* fuse = nullptr);
 // Whether the plane-to-sky map of basis V (host, row-major 3 x 3) stays in
 // the tile gather's domain over an N x N image: well inside the horizon and
 // without folds.  Outside it only the source scatter reprojects correctly.

@@ -1229,6 +1229,117 @@ __global__ void k_reproject_scatter(const float* __restrict__ pre, const float* 
   }
 }
 
+struct Acc {
+  float s, sc, r, rc, m;
+};
+
+template <bool PRECISE>
+__device__ __forceinline__ void acc_add(Acc& a, float d, float q) {
+  if (!PRECISE) {
+    a.s += d;
+    a.r += q;
+  } else {
+    float t = a.s + d;
+    a.sc += (fabsf(a.s) >= fabsf(d)) ? (a.s - t) + d : (d - t) + a.s;
+    a.s = t;
+    t = a.r + q;
+    a.rc += (fabsf(a.r) >= fabsf(q)) ? (a.r - t) + q : (q - t) + a.r;
+    a.r = t;
+  }
+  a.m = fmaxf(a.m, d);
+}
+
+template <bool PRECISE>
+__device__ __forceinline__ void acc_pixel(Acc& a, float i1, float i2, float i3) {
+  const float d = fabs(fabs(i1 - i2) - fabs(i2 - i3));
+  const float s2 = (i2 <= 0) ? FIP_TRIGGER_FLOOR : i2;
+  const float q = d / s2;
+  acc_add<PRECISE>(a, d, (q < 1) ? q : 1.0f);
+}
+
+// Statistics of one trigger tile (FIPkernels.cu:499-552 before the combine),
+// one warp per T x T tile at base: S = sum d, R = sum min(d / I2', 1) (NaN
+// counts as 1), M = max(0, max d), in the lanes' and shuffles' order (valid
+// in lane 0).  Plain form: FP32 sums; precise form: Neumaier-compensated FP32
+// sums combined in FP64.  L2: load through L2 only (data other SMs wrote in
+// the same kernel).
+template <bool PRECISE, bool L2>
+__device__ __forceinline__ void tile_stats(const float* __restrict__ I1,
+                                           const float* __restrict__ I2,
+                                           const float* __restrict__ I3, size_t base, int n,
+                                           int t, int vec, int lane, double& S, double& R,
+                                           float& M) {
+  auto ld4 = [](const float* p) {
+    return L2 ? __ldcg(reinterpret_cast<const float4*>(p)) : *reinterpret_cast<const float4*>(p);
+  };
+  auto ld1 = [](const float* p) { return L2 ? __ldcg(p) : *p; };
+  Acc a{0.f, 0.f, 0.f, 0.f, 0.f};
+  if (vec) {
+    const int q = t / 4;  // float4 per tile row
+    for (int k = lane; k < t * q; k += 32) {
+      const int r = k / q, c = (k % q) * 4;
+      const size_t o = base + (size_t)r * n + c;
+      const float4 x1 = ld4(I1 + o);
+      const float4 x2 = ld4(I2 + o);
+      const float4 x3 = ld4(I3 + o);
+      acc_pixel<PRECISE>(a, x1.x, x2.x, x3.x);
+      acc_pixel<PRECISE>(a, x1.y, x2.y, x3.y);
+      acc_pixel<PRECISE>(a, x1.z, x2.z, x3.z);
+      acc_pixel<PRECISE>(a, x1.w, x2.w, x3.w);
+    }
+  } else {
+    for (int k = lane; k < t * t; k += 32) {
+      const size_t o = base + (size_t)(k / t) * n + (k % t);
+      acc_pixel<PRECISE>(a, ld1(I1 + o), ld1(I2 + o), ld1(I3 + o));
+    }
+  }
+  if (!PRECISE) {
+    for (int o = 16; o > 0; o >>= 1) {
+      a.s += __shfl_xor_sync(0xffffffffu, a.s, o);
+      a.r += __shfl_xor_sync(0xffffffffu, a.r, o);
+      a.m = fmaxf(a.m, __shfl_xor_sync(0xffffffffu, a.m, o));
+    }
+    S = (double)a.s;
+    R = (double)a.r;
+  } else {
+    double s = (double)a.s + (double)a.sc, r = (double)a.r + (double)a.rc;
+    for (int o = 16; o > 0; o >>= 1) {
+      s += __shfl_xor_sync(0xffffffffu, s, o);
+      r += __shfl_xor_sync(0xffffffffu, r, o);
+      a.m = fmaxf(a.m, __shfl_xor_sync(0xffffffffu, a.m, o));
+    }
+    S = s;
+    R = r;
+  }
+  M = a.m;
+}
+
+// The tLISI of one tile from its statistics and the three image maxima
+// (FIPkernels.cu:550): the plain form's FP32 expression, the precise form's
+// FP64 one.
+template <bool PRECISE>
+__device__ __forceinline__ float tlisi_of(double S, double R, float M, const float max3[3], int t) {
+  if (!PRECISE) {
+    const float maxallval = max(max3[0], max(max3[1], max3[2]));
+    const size_t us = (size_t)t;
+    return 1 - ((float)S / us / us) * M * ((float)R / us / us) / maxallval / maxallval;
+  }
+  const double mx = fmax(fmax((double)max3[0], (double)max3[1]), (double)max3[2]);
+  const double tt = (double)t;
+  return (float)(1.0 - (S / tt / tt) * (double)M * (R / tt / tt) / mx / mx);
+}
+
+// The trigger fused into the reprojections of a three-snapshot call: the
+// gather CTA that writes the last of the three images of its 64 x 64 region
+// (a per-region count) computes the region's trigger-tile statistics, and a
+// final one-pass kernel applies the maxima.
+struct FipTriggerFuse {
+  const float* img[3];  // I1, I2, I3
+  unsigned* count;      // [gather tiles], zero at the call's start
+  double* stats;        // [U*U][3]: S, R, M
+  int t, u;
+};
+
 constexpr int kDT = 64;          // destination tile side
 constexpr int kMaxRows = 256;    // candidate source rows per tile (one per thread)
 static_assert(kMaxRows == kThreads, "the gather numbers rows one per thread");
@@ -1345,7 +1456,7 @@ template <bool EXACT>
 __global__ void __launch_bounds__(kThreads, EXACT ? 5 : 8) k_reproject_gather(
     const float* __restrict__ pre, const float2* __restrict__ tg, const float* __restrict__ V,
     int n, int nb, float cell, float delta, const unsigned* __restrict__ pre_max,
-    float* __restrict__ dst, unsigned* img_max, unsigned* err) {
+    float* __restrict__ dst, unsigned* img_max, unsigned* err, const FipTriggerFuse fuse) {
   __shared__ __align__(16) unsigned s_tile[kTW * kTR];
   __shared__ int s_base[kMaxRows];  // pixel index of row r's first candidate minus its number
   __shared__ int s_off[kMaxRows + 1];
@@ -1639,6 +1750,38 @@ __global__ void __launch_bounds__(kThreads, EXACT ? 5 : 8) k_reproject_gather(
     for (int w = 0; w < kThreads / 32; ++w) b = fmaxf(b, s_wmax[w]);
     atomicMax(img_max, __float_as_uint(b));
   }
+  if (fuse.count) {
+    // Fused trigger: every thread's stores made visible device-wide, then one
+    // count per region; the CTA that completes the region's third image
+    // reads all three through L2 and reduces each trigger tile in it.
+    __shared__ unsigned s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const unsigned old = atomicAdd(&fuse.count[blockIdx.x], 1u);
+      s_last = old == 2u;
+      __threadfence();
+    }
+    __syncthreads();
+    if (s_last) {
+      const int per = kDT / fuse.t;
+      const int vec = (fuse.t % 4 == 0) && (n % 4 == 0);
+      for (int k = warp; k < per * per; k += kThreads / 32) {
+        const int ti = r0 / fuse.t + k / per, tj = c0 / fuse.t + k % per;
+        const size_t base = (size_t)ti * fuse.t * n + (size_t)tj * fuse.t;
+        double S, R;
+        float M;
+        tile_stats<EXACT, true>(fuse.img[0], fuse.img[1], fuse.img[2], base, n, fuse.t, vec,
+                                lane, S, R, M);
+        if (lane == 0) {
+          double* o = fuse.stats + 3 * ((size_t)ti * fuse.u + tj);
+          o[0] = S;
+          o[1] = R;
+          o[2] = (double)M;
+        }
+      }
+    }
+  }
 }
 
 // mode 0: the FP32 chain with the theta table (null: evaluated), 2: the
@@ -1680,34 +1823,6 @@ __global__ void k_image_max(const float* __restrict__ img, size_t count, unsigne
 // M = max(0, max D), R = sum min(D/I2c, 1) (NaN counts 1).
 // PRECISE: Neumaier-compensated S and R, FP64 combine.
 // ---------------------------------------------------------------------------
-struct Acc {
-  float s, sc, r, rc, m;
-};
-
-template <bool PRECISE>
-__device__ __forceinline__ void acc_add(Acc& a, float d, float q) {
-  if (!PRECISE) {
-    a.s += d;
-    a.r += q;
-  } else {
-    float t = a.s + d;
-    a.sc += (fabsf(a.s) >= fabsf(d)) ? (a.s - t) + d : (d - t) + a.s;
-    a.s = t;
-    t = a.r + q;
-    a.rc += (fabsf(a.r) >= fabsf(q)) ? (a.r - t) + q : (q - t) + a.r;
-    a.r = t;
-  }
-  a.m = fmaxf(a.m, d);
-}
-
-template <bool PRECISE>
-__device__ __forceinline__ void acc_pixel(Acc& a, float i1, float i2, float i3) {
-  const float d = fabs(fabs(i1 - i2) - fabs(i2 - i3));
-  const float s2 = (i2 <= 0) ? FIP_TRIGGER_FLOOR : i2;
-  const float q = d / s2;
-  acc_add<PRECISE>(a, d, (q < 1) ? q : 1.0f);
-}
-
 template <bool PRECISE>
 __global__ void __launch_bounds__(kThreads) k_trigger(const float* __restrict__ I1,
                                                       const float* __restrict__ I2,
@@ -1729,51 +1844,21 @@ __global__ void __launch_bounds__(kThreads) k_trigger(const float* __restrict__ 
   const int b = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
   if (b >= u * u) return;
   const int ti = b / u, tj = b % u;
-  Acc a{0.f, 0.f, 0.f, 0.f, 0.f};
   const size_t base = (size_t)ti * t * n + (size_t)tj * t;
-  if (vec) {
-    const int q = t / 4;  // float4 per tile row
-    for (int k = lane; k < t * q; k += 32) {
-      const int r = k / q, c = (k % q) * 4;
-      const size_t o = base + (size_t)r * n + c;
-      const float4 x1 = *reinterpret_cast<const float4*>(I1 + o);
-      const float4 x2 = *reinterpret_cast<const float4*>(I2 + o);
-      const float4 x3 = *reinterpret_cast<const float4*>(I3 + o);
-      acc_pixel<PRECISE>(a, x1.x, x2.x, x3.x);
-      acc_pixel<PRECISE>(a, x1.y, x2.y, x3.y);
-      acc_pixel<PRECISE>(a, x1.z, x2.z, x3.z);
-      acc_pixel<PRECISE>(a, x1.w, x2.w, x3.w);
-    }
-  } else {
-    for (int k = lane; k < t * t; k += 32) {
-      const size_t o = base + (size_t)(k / t) * n + (k % t);
-      acc_pixel<PRECISE>(a, I1[o], I2[o], I3[o]);
-    }
-  }
-  if (!PRECISE) {
-    for (int o = 16; o > 0; o >>= 1) {
-      a.s += __shfl_xor_sync(0xffffffffu, a.s, o);
-      a.r += __shfl_xor_sync(0xffffffffu, a.r, o);
-      a.m = fmaxf(a.m, __shfl_xor_sync(0xffffffffu, a.m, o));
-    }
-    if (lane == 0) {
-      const float maxallval = max(max3[0], max(max3[1], max3[2]));
-      const size_t us = (size_t)t;
-      result[b] = 1 - (a.s / us / us) * a.m * (a.r / us / us) / maxallval / maxallval;
-    }
-  } else {
-    double s = (double)a.s + (double)a.sc, r = (double)a.r + (double)a.rc;
-    for (int o = 16; o > 0; o >>= 1) {
-      s += __shfl_xor_sync(0xffffffffu, s, o);
-      r += __shfl_xor_sync(0xffffffffu, r, o);
-      a.m = fmaxf(a.m, __shfl_xor_sync(0xffffffffu, a.m, o));
-    }
-    if (lane == 0) {
-      const double mx = fmax(fmax((double)max3[0], (double)max3[1]), (double)max3[2]);
-      const double tt = (double)t;
-      result[b] = (float)(1.0 - (s / tt / tt) * (double)a.m * (r / tt / tt) / mx / mx);
-    }
-  }
+  double S, R;
+  float M;
+  tile_stats<PRECISE, false>(I1, I2, I3, base, n, t, vec, lane, S, R, M);
+  if (lane == 0) result[b] = tlisi_of<PRECISE>(S, R, M, max3, t);
+}
+
+// Final pass of the fused trigger: tLISI from the statistics and the maxima.
+template <bool PRECISE>
+__global__ void k_trigger_combine(const double* __restrict__ stats, const float* __restrict__ max3p,
+                                  int u, int t, float* __restrict__ result) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= u * u) return;
+  const float max3[3] = {max3p[0], max3p[1], max3p[2]};
+  result[b] = tlisi_of<PRECISE>(stats[3 * b], stats[3 * b + 1], (float)stats[3 * b + 2], max3, t);
 }
 
 inline float cell_degrees(float cell) { return (float)((double)cell / FIP_M_PI * 180); }
@@ -2089,6 +2174,8 @@ cudaError_t fip_launch_correct_c2r(const FipGeom& geo, const float* fft_out, con
   return cudaGetLastError();
 }
 
+const void* fip_targets_kernel() { return reinterpret_cast<const void*>(&k_targets); }
+
 cudaError_t fip_launch_targets(const FipGeom& geo, const float* V, const float2* theta_tab,
                                float2* targets, cudaStream_t s) {
   const int per = kThreads * kTargetsPerThread;
@@ -2115,19 +2202,51 @@ bool fip_gather_supported(const FipGeom& geo, int exact_targets) {
   return exact_targets || chain_delta(geo.cell) <= 40.f;
 }
 
+bool fip_trigger_fusable(const FipGeom& geo) {
+  return geo.t > 0 && kDT % geo.t == 0 && geo.n % kDT == 0;
+}
+
+size_t fip_trigger_fuse_counts(const FipGeom& geo) {
+  const size_t tiles = (geo.n + kDT - 1) / kDT;
+  return tiles * tiles;
+}
+
 cudaError_t fip_launch_reproject_gather(const FipGeom& geo, const float* pre,
                                         const float2* targets, const float* V, int nb,
                                         const unsigned* pre_max, float* dst, unsigned* img_max,
-                                        int exact_targets, cudaStream_t s, unsigned* err) {
+                                        int exact_targets, cudaStream_t s, unsigned* err,
+                                        const FipFuse* fuse) {
   const int tiles = (geo.n + kDT - 1) / kDT;
   const float delta = exact_targets ? 0.25f : chain_delta(geo.cell);
   if (!fip_gather_supported(geo, exact_targets)) return cudaErrorInvalidValue;
+  FipTriggerFuse tf{};
+  if (fuse) {
+    if (!fip_trigger_fusable(geo)) return cudaErrorInvalidValue;
+    for (int k = 0; k < 3; ++k) tf.img[k] = fuse->img[k];
+    tf.count = fuse->count;
+    tf.stats = fuse->stats;
+    tf.t = geo.t;
+    tf.u = geo.u;
+  }
   if (exact_targets)
     k_reproject_gather<true><<<tiles * tiles, kThreads, 0, s>>>(
-        pre, nullptr, V, geo.n, nb, geo.cell, delta, pre_max, dst, img_max, err);
+        pre, nullptr, V, geo.n, nb, geo.cell, delta, pre_max, dst, img_max, err, tf);
   else
     k_reproject_gather<false><<<tiles * tiles, kThreads, 0, s>>>(
-        pre, targets, V, geo.n, nb, geo.cell, delta, pre_max, dst, img_max, err);
+        pre, targets, V, geo.n, nb, geo.cell, delta, pre_max, dst, img_max, err, tf);
+  return cudaGetLastError();
+}
+
+cudaError_t fip_launch_trigger_combine(const FipGeom& geo, const double* stats,
+                                       const float* max3, float* result, int precise,
+                                       cudaStream_t s) {
+  const int tiles = geo.u * geo.u;
+  if (tiles == 0) return cudaSuccess;
+  const int blocks = (tiles + kThreads - 1) / kThreads;
+  if (precise)
+    k_trigger_combine<true><<<blocks, kThreads, 0, s>>>(stats, max3, geo.u, geo.t, result);
+  else
+    k_trigger_combine<false><<<blocks, kThreads, 0, s>>>(stats, max3, geo.u, geo.t, result);
   return cudaGetLastError();
 }
 

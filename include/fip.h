@@ -296,7 +296,8 @@ int fip_batch_tuning(const fip_batch* b, int* fft_values_per_thread, int* fft_sp
 /* Phase timing of batched calls (no counterpart in the reference): when
  * enabled, each call's graph carries timing events at its phase boundaries
  * and the device time of every phase is summed: 0 per-snapshot preparation
- * (storage conversion, binning, pixel mapping), 1 the persistent gridding
+ * (storage conversion, binning; the plain form's pixel mappings run beside
+ * phases 0-3 and a wait for them counts in phase 4), 1 the persistent gridding
  * launch, 2 the batched column transform, 3 the batched row transform, 4 the
  * reprojections, 5 the triggers.  Enabling resets the totals; reading them
  * waits for the last profiled call. */

@@ -326,6 +326,42 @@ def test_host_and_device_entry_points_agree(cuda, tiny):
     assert np.abs(out.cpu().numpy().reshape(u, u) - res).max() <= 1e-6
 
 
+class _DeviceFloats:
+    """A view of n device floats at an address (CUDA array interface)."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f4", "data": (ptr, False),
+                                         "version": 3}
+
+
+@pytest.mark.parametrize("kw", [{}, dict(form=fip.FORM_PRECISE)])
+@pytest.mark.parametrize("cfg", ["small", "reference"])
+def test_fused_trigger_bit_identical_to_separate_trigger(cuda, cfg, kw):
+    """pipe_device (plain form) computes the trigger's tile statistics inside
+    the last reprojection of every 64 x 64 region, in k_trigger's reduction
+    order: its tLISI must equal the separate trigger's on the same images bit
+    for bit (the precision form keeps the separate pass: the same check)."""
+    import torch
+    snap = (synthetic.config_small(transient_snapshot=2) if cfg == "small" else
+            synthetic.config_reference(transient_snapshot=2))
+    n, nb, t = snap.image_size, snap.num_baselines, snap.unit_size
+    u = n // t
+    d = to_dev(snap, cuda)
+    fused = torch.zeros(u * u, device=cuda)
+    sep = torch.zeros(u * u, device=cuda)
+    with fip.Imager(n, nb, snap.cell_size, t, **kw) as im:
+        im.pipe_device(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, fused)
+        torch.cuda.synchronize()
+        ptrs = [im.image_ptr(k) for k in range(3)]
+        imgs = [torch.as_tensor(_DeviceFloats(p, n * n), device=cuda) for p in ptrs]
+        mx = torch.stack([torch.clamp(x.max(), min=0.0) for x in imgs])
+        im.trigger(ptrs[0], ptrs[1], ptrs[2], mx, sep)
+        torch.cuda.synchronize()
+    a, b = fused.cpu().numpy(), sep.cpu().numpy()
+    assert np.array_equal(a.view(np.int32), b.view(np.int32))
+    assert float(1.0 - a.min()) > 0.1  # the transient's tile is in the matrix
+
+
 @pytest.mark.parametrize("kw", [{}, dict(form=fip.FORM_PRECISE, vis_storage=fip.STORE_F16)])
 def test_concurrent_lanes_match_single_snapshot_calls(cuda, small, kw):
     """pipe_device / pipe_host image the three snapshots on concurrent lanes;
