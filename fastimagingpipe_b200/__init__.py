@@ -101,6 +101,8 @@ def lib() -> ctypes.CDLL:
                                              ctypes.POINTER(sz), vp]
         L.fip_image_snapshot_raw.argtypes = [vp, ctypes.POINTER(RawVis), vp, vp, sz, vp, vp, vp]
         L.fip_batch_check.argtypes = [vp, vp]
+        L.fip_set_trigger_streaming.argtypes = [ctypes.c_int]
+        L.fip_trigger_window.argtypes = [vp, vp, vp, sz, vp, vp]
         L.fip_pipe_host.argtypes = [vp, vp, vp, vp, vp, sz, sz, vp]
         L.fip_pixel_targets.argtypes = [vp, vp, vp, ctypes.c_int, vp]
         L.fip_plane_project.argtypes = [vp, vp, sz, sz, vp, vp, vp]
@@ -299,6 +301,12 @@ class Imager:
         _check(lib().fip_trigger(self._h, _ptr(I1), _ptr(I2), _ptr(I3), _ptr(max3), _ptr(result),
                                  _stream(stream)))
 
+    def trigger_window(self, images, maxima, count: int, results, stream=None):
+        """Sliding-window tLISI over `count` consecutive device images ([count][N*N]):
+        triple k -> results[k * U*U:(k + 1) * U*U], k < count - 2."""
+        _check(lib().fip_trigger_window(self._h, _ptr(images), _ptr(maxima), count, _ptr(results),
+                                        _stream(stream)))
+
     def pipe_device(self, vis_re, vis_im, B, V, nb: int, result, stream=None):
         _check(lib().fip_pipe_device(self._h, _ptr(vis_re), _ptr(vis_im), _ptr(B), _ptr(V), nb,
                                      _ptr(result), _stream(stream)))
@@ -427,6 +435,14 @@ class Batch:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def set_trigger_streaming(enable: bool) -> bool:
+    """Plain-form sliding-window triggers (Imager.trigger_window, batches)
+    stream every tile's slices through registers, each image read once (True,
+    the default), or read each triple's three images (False); the tLISI is
+    bit-identical either way.  Process-wide; returns the previous setting."""
+    return bool(lib().fip_set_trigger_streaming(1 if enable else 0))
 
 
 def grid_snapshot_noalloc(vis_re, vis_im, B, V, nb: int, image_size: int, cell_size: float,

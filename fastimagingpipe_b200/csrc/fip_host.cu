@@ -846,6 +846,31 @@ int fip_trigger(fip_imager* im, const float* I1, const float* I2, const float* I
   return FIP_OK;
 }
 
+int fip_trigger_window(fip_imager* im, const float* images, const float* maxima, size_t count,
+                       float* results, void* stream) {
+  if (!im) return fail(FIP_ERR_ARG, "null imager");
+  if (im->geo.t <= 0) return fail(FIP_ERR_ARG, "imager has no trigger tile (unit_size 0)");
+  if (!images || !maxima || !results) return fail(FIP_ERR_ARG, "null device pointer");
+  if (count < 3 || count - 2 > 65535) return fail(FIP_ERR_ARG, "count must be in [3, 65537]");
+  DeviceGuard g(im->cfg.device);
+  FIP_TRY(call_enter(im, (cudaStream_t)stream));
+  const int k = stage_begin(im, ST_TRIGGER, (cudaStream_t)stream);
+  FIP_CUDA(fip_launch_trigger_batch(im->geo, images, maxima, (int)(count - 2), results,
+                                    im->cfg.form == FIP_FORM_PRECISE ? 1 : 0,
+                                    (cudaStream_t)stream));
+  stage_end(im, k, (cudaStream_t)stream);
+  im->launches += 1;
+  FIP_TRY(call_leave(im, (cudaStream_t)stream));
+  if (im->timer.on) stage_collect(im);
+  return FIP_OK;
+}
+
+int fip_set_trigger_streaming(int enable) {
+  const int prev = fip_trigger_stream_enabled();
+  fip_trigger_stream_enable(enable);
+  return prev;
+}
+
 int fip_pipe_device(fip_imager* im, const float* vr, const float* vi, const float* B,
                     const float* V, size_t nb, float* result, void* stream) {
   if (!im) return fail(FIP_ERR_ARG, "null imager");

@@ -135,8 +135,14 @@ cudaError_t fip_launch_trigger3(const FipGeom& geo, const float* I1, const float
                                 const float* m3, float* result, int precise, cudaStream_t s);
 // Batched trigger over a linear ring of images (stride N*N): triple k is
 // images k, k+1, k+2 with maxima[k .. k+2], result k at results + k * U*U.
+// The plain form with count >= 3 and T <= 32 (T % 4 == 0) streams each tile's
+// slices through registers, each image of the ring read once, bit-identical
+// to the per-triple loads.
 cudaError_t fip_launch_trigger_batch(const FipGeom& geo, const float* images, const float* maxima,
                                      int count, float* results, int precise, cudaStream_t s);
+// Process-wide: the streamed window on (default) or off.
+void fip_trigger_stream_enable(int on);
+int fip_trigger_stream_enabled();
 // mode 0: the FP32 chain (theta_tab as in fip_launch_targets), 1: the exact
 // closed form, 2: the FP32 chain evaluated without the table.
 cudaError_t fip_launch_pixel_targets(const FipGeom& geo, const float* V, float* out,

@@ -19,11 +19,16 @@
 //     splats them in shared memory, stores the tile once and reports its
 //     maximum -- no global atomics, no memsets;
 //   * the trigger reads the three images once, in 128-bit loads, with
-//     warp-shuffle tile reductions.
+//     warp-shuffle tile reductions; a batch's sliding window streams each
+//     tile's slices through registers, every image read once for all the
+//     triples it is in.
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
+
+#include <algorithm>
+#include <atomic>
 
 #include "fip_common.cuh"
 #include "fip_fft.cuh"
@@ -1254,7 +1259,31 @@ __device__ __forceinline__ void acc_pixel(Acc& a, float i1, float i2, float i3) 
   const float d = fabs(fabs(i1 - i2) - fabs(i2 - i3));
   const float s2 = (i2 <= 0) ? FIP_TRIGGER_FLOOR : i2;
   const float q = d / s2;
-  acc_add<PRECISE>(a, d, (q < 1) ? q : 1.0f);
+  acc_add<PRECISE>(a, d, fminf(q, 1.0f));  // NaN counts 1, as (q < 1) ? q : 1
+}
+
+// The warp's reduction of its lanes' tile statistics (valid in lane 0).
+template <bool PRECISE>
+__device__ __forceinline__ void warp_stats(Acc a, double& S, double& R, float& M) {
+  if (!PRECISE) {
+    for (int o = 16; o > 0; o >>= 1) {
+      a.s += __shfl_xor_sync(0xffffffffu, a.s, o);
+      a.r += __shfl_xor_sync(0xffffffffu, a.r, o);
+      a.m = fmaxf(a.m, __shfl_xor_sync(0xffffffffu, a.m, o));
+    }
+    S = (double)a.s;
+    R = (double)a.r;
+  } else {
+    double s = (double)a.s + (double)a.sc, r = (double)a.r + (double)a.rc;
+    for (int o = 16; o > 0; o >>= 1) {
+      s += __shfl_xor_sync(0xffffffffu, s, o);
+      r += __shfl_xor_sync(0xffffffffu, r, o);
+      a.m = fmaxf(a.m, __shfl_xor_sync(0xffffffffu, a.m, o));
+    }
+    S = s;
+    R = r;
+  }
+  M = a.m;
 }
 
 // Statistics of one trigger tile (FIPkernels.cu:499-552 before the combine),
@@ -1293,25 +1322,7 @@ __device__ __forceinline__ void tile_stats(const float* __restrict__ I1,
       acc_pixel<PRECISE>(a, ld1(I1 + o), ld1(I2 + o), ld1(I3 + o));
     }
   }
-  if (!PRECISE) {
-    for (int o = 16; o > 0; o >>= 1) {
-      a.s += __shfl_xor_sync(0xffffffffu, a.s, o);
-      a.r += __shfl_xor_sync(0xffffffffu, a.r, o);
-      a.m = fmaxf(a.m, __shfl_xor_sync(0xffffffffu, a.m, o));
-    }
-    S = (double)a.s;
-    R = (double)a.r;
-  } else {
-    double s = (double)a.s + (double)a.sc, r = (double)a.r + (double)a.rc;
-    for (int o = 16; o > 0; o >>= 1) {
-      s += __shfl_xor_sync(0xffffffffu, s, o);
-      r += __shfl_xor_sync(0xffffffffu, r, o);
-      a.m = fmaxf(a.m, __shfl_xor_sync(0xffffffffu, a.m, o));
-    }
-    S = s;
-    R = r;
-  }
-  M = a.m;
+  warp_stats<PRECISE>(a, S, R, M);
 }
 
 // The tLISI of one tile from its statistics and the three image maxima
@@ -1851,6 +1862,77 @@ __global__ void __launch_bounds__(kThreads) k_trigger(const float* __restrict__ 
   if (lane == 0) result[b] = tlisi_of<PRECISE>(S, R, M, max3, t);
 }
 
+// ---------------------------------------------------------------------------
+// Sliding-window trigger streamed through registers: tLISI of triples
+// (k, k+1, k+2) over a linear ring of images.  A warp owns one trigger tile
+// and a chunk of consecutive triples; each lane keeps its float4s of the
+// last three slices in registers and loads the next slice's while it
+// reduces the current triple, so every image of the chunk is read from HBM
+// once instead of once per triple it is in.  Lane k's float4s and the
+// accumulation and shuffle order are k_trigger's (bit-identical results).
+// NV: float4s per lane, >= T*T/128.
+// ---------------------------------------------------------------------------
+constexpr int kStreamThreads = 128;
+
+template <bool PRECISE, int NV>
+__global__ void __launch_bounds__(kStreamThreads) k_trigger_stream(
+    const float* __restrict__ images, size_t img_stride, int count, int chunk,
+    const float* __restrict__ maxima, int n, int t, int u, float* __restrict__ result) {
+  const int lane = threadIdx.x & 31;
+  const int b = blockIdx.x * (kStreamThreads / 32) + (threadIdx.x >> 5);
+  if (b >= u * u) return;
+  const int y0 = blockIdx.y * chunk, y1 = min(count, y0 + chunk);
+  const int q = t / 4, nv = t * q;  // float4s per tile row, per tile
+  const float* base = images + (size_t)(b / u) * t * n + (size_t)(b % u) * t;
+  unsigned off[NV];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    const int k = lane + 32 * i;
+    off[i] = (unsigned)((k / q) * n + (k % q) * 4);
+  }
+  auto load = [&](float4(&v)[NV], int sl) {
+    const float* img = base + (size_t)sl * img_stride;
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+      if (lane + 32 * i < nv) v[i] = __ldcs(reinterpret_cast<const float4*>(img + off[i]));
+  };
+  // Triple y from slices (P0, P1, P2); slice y + 3 is loaded into NX first
+  // so that its latency hides behind the reduction.
+  auto step = [&](float4(&P0)[NV], float4(&P1)[NV], float4(&P2)[NV], float4(&NX)[NV], int y) {
+    if (y + 1 < y1) load(NX, y + 3);
+    Acc a{0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+      if (lane + 32 * i < nv) {
+        acc_pixel<PRECISE>(a, P0[i].x, P1[i].x, P2[i].x);
+        acc_pixel<PRECISE>(a, P0[i].y, P1[i].y, P2[i].y);
+        acc_pixel<PRECISE>(a, P0[i].z, P1[i].z, P2[i].z);
+        acc_pixel<PRECISE>(a, P0[i].w, P1[i].w, P2[i].w);
+      }
+    double S, R;
+    float M;
+    warp_stats<PRECISE>(a, S, R, M);
+    if (lane == 0) {
+      const float max3[3] = {maxima[y], maxima[y + 1], maxima[y + 2]};
+      result[(size_t)y * u * u + b] = tlisi_of<PRECISE>(S, R, M, max3, t);
+    }
+  };
+  // Four slice buffers whose roles rotate with the triple (no copies).
+  float4 s0[NV], s1[NV], s2[NV], s3[NV];
+  load(s0, y0);
+  load(s1, y0 + 1);
+  load(s2, y0 + 2);
+  for (int y = y0; y < y1; y += 4) {
+    step(s0, s1, s2, s3, y);
+    if (y + 1 >= y1) break;
+    step(s1, s2, s3, s0, y + 1);
+    if (y + 2 >= y1) break;
+    step(s2, s3, s0, s1, y + 2);
+    if (y + 3 >= y1) break;
+    step(s3, s0, s1, s2, y + 3);
+  }
+}
+
 // Final pass of the fused trigger: tLISI from the statistics and the maxima.
 template <bool PRECISE>
 __global__ void k_trigger_combine(const double* __restrict__ stats, const float* __restrict__ max3p,
@@ -2278,6 +2360,42 @@ cudaError_t fip_launch_image_max(const float* img, size_t count, unsigned* out, 
   return cudaGetLastError();
 }
 
+// ---- The streamed sliding-window trigger ----------------------------------
+static std::atomic<int> g_trigger_stream{1};
+
+void fip_trigger_stream_enable(int on) { g_trigger_stream.store(on ? 1 : 0); }
+int fip_trigger_stream_enabled() { return g_trigger_stream.load(); }
+
+template <bool PRECISE>
+static cudaError_t launch_stream_window(const FipGeom& geo, const float* images, int count,
+                                        const float* maxima, float* results, cudaStream_t s) {
+  const int tiles = geo.u * geo.u;
+  const int bx = (tiles + kStreamThreads / 32 - 1) / (kStreamThreads / 32);
+  // Chunks of triples: enough warps to fill the device (about eight waves
+  // of 12 warps per SM), each chunk re-reading only its first two slices.
+  const int want = 8 * 12 * sm_count();
+  int chunks = std::max(1, std::min(count, want / std::max(1, tiles)));
+  const int chunk = (count + chunks - 1) / chunks;
+  chunks = (count + chunk - 1) / chunk;
+  if (chunks > 65535) return cudaErrorInvalidValue;
+  const dim3 grid(bx, chunks);
+  const size_t n2 = (size_t)geo.n * geo.n;
+  const int nv = (geo.t * geo.t / 4 + 31) / 32;
+#define FIP_STREAM(NV)                                                                         \
+  k_trigger_stream<PRECISE, NV><<<grid, kStreamThreads, 0, s>>>(                               \
+      images, n2, count, chunk, maxima, geo.n, geo.t, geo.u, results)
+  if (nv <= 1)
+    FIP_STREAM(1);
+  else if (nv <= 2)
+    FIP_STREAM(2);
+  else if (nv <= 4)
+    FIP_STREAM(4);
+  else
+    FIP_STREAM(8);
+#undef FIP_STREAM
+  return cudaGetLastError();
+}
+
 cudaError_t fip_launch_trigger(const FipGeom& geo, const float* I1, const float* I2,
                                const float* I3, const float* max3, float* stats, float* result,
                                int precise, cudaStream_t s) {
@@ -2307,6 +2425,12 @@ cudaError_t fip_launch_trigger_batch(const FipGeom& geo, const float* images, co
   const int tiles = geo.u * geo.u;
   if (tiles == 0 || count <= 0) return cudaSuccess;
   if (count > 65535) return cudaErrorInvalidValue;
+  // Plain form, three or more triples: the register stream (each image read
+  // once).  The precision form's compensated sums make it issue-bound; its
+  // triples keep the plain loads, which hide latency with more warps.
+  if (g_trigger_stream.load() && !precise && count >= 3 && geo.t % 4 == 0 && geo.t <= 32 &&
+      geo.n % 4 == 0 && ((uintptr_t)images & 15) == 0)
+    return launch_stream_window<false>(geo, images, count, maxima, results, s);
   const size_t n2 = (size_t)geo.n * geo.n;
   const dim3 blocks((tiles + kThreads / 32 - 1) / (kThreads / 32), count);
   const int vec = (geo.t % 4 == 0) && (geo.n % 4 == 0) && ((uintptr_t)images & 15) == 0;

@@ -174,6 +174,29 @@ int fip_trigger(fip_imager* im, const float* I1, const float* I2, const float* I
                 const float* max3, float* result, void* stream);
 
 /*
+ * How sliding-window triggers (fip_trigger_window, batches) read their tiles
+ * (no counterpart in the reference): enable = 1 (the default) streams every
+ * tile's slices through registers in the plain form, each image read once
+ * for the (up to three) triples it is in; 0 reads each triple's three images.
+ * Both give bit-identical tLISI.  Windows of fewer than three triples, unit
+ * sizes above 32 and the precision form (whose compensated sums are
+ * issue-bound) always read per triple.  Process-wide; returns the previous
+ * setting.
+ */
+int fip_set_trigger_streaming(int enable);
+
+/*
+ * Sliding-window tLISI over `count` consecutive device images (no
+ * counterpart in the reference, which triggers on one triple per call):
+ * images [count][N*N] contiguous, maxima [count] as produced by
+ * fip_image_snapshot; triple k (images k, k+1, k+2) -> results + k*U*U for
+ * k < count - 2.  The imager's form and unit size; in the plain form each
+ * image is read once (fip_set_trigger_streaming).  count >= 3.
+ */
+int fip_trigger_window(fip_imager* im, const float* images, const float* maxima, size_t count,
+                       float* results, void* stream);
+
+/*
  * FIpipe on device buffers with the imager's persistent state: snapshots
  * 0..2 of the concatenated device inputs -> result [U*U] (device).  The
  * three images and their maxima stay in the imager (fip_imager_image).
