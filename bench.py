@@ -215,12 +215,13 @@ def run_reference(args, rank):
     return line
 
 
-def run_batching(fip, synthetic, torch, dev, local, per_call=16, calls_per_size=2,
-                 distinct=4):
-    """Times the batching form: for each image size (4096^2 and 2048^2) a Batch of
-    `per_call` snapshots per call, `calls_per_size` calls, the two sizes on two
-    streams at once (64 snapshots in all).  `distinct` seeded snapshots per size are
-    generated and cycled (input generation on the host is the slow part)."""
+def run_batching(fip, synthetic, torch, dev, local, per_size=16, calls=2, distinct=4):
+    """Times the batching form on configuration 4: one Batch of two sequences
+    (4096^2 and 2048^2, cell scaled for one field of view), each call imaging
+    `per_size` snapshots of each size interleaved (one persistent gridding launch
+    for both sizes, one batched transform per size, one CUDA graph), `calls` calls
+    (64 snapshots in all).  `distinct` seeded snapshots per size are generated and
+    cycled (input generation on the host is the slow part)."""
     out = {}
     sizes = (4096, 2048)
     data = {}
@@ -229,58 +230,50 @@ def run_batching(fip, synthetic, torch, dev, local, per_call=16, calls_per_size=
         d = [{k: torch.tensor(getattr(x, k), device=dev) for k in ("vis_re", "vis_im", "B", "V")}
              for x in snaps]
         data[n] = (snaps, d)
-    total = len(sizes) * per_call * calls_per_size
+    total = len(sizes) * per_size * calls
+    # One call: snapshot j of each size in turn.
+    order = [(c, j % distinct) for j in range(per_size) for c in range(len(sizes))]
+    seq = [c for c, _ in order]
+    args = tuple([data[sizes[c]][1][i][key] for c, i in order]
+                 for key in ("vis_re", "vis_im", "B", "V"))
+    nbs = [data[sizes[c]][0][i].nb for c, i in order]
+    spec = [(n, max(x.nb for x in data[n][0]), data[n][0][0].cell_size, 32) for n in sizes]
     for name, kw in (("batching_plain", {}),
                      ("batching_precise_f16", dict(form=fip.FORM_PRECISE,
                                                    vis_storage=fip.STORE_F16))):
-        batches, streams, res, args_of = {}, {}, {}, {}
-        for n in sizes:
-            snaps, d = data[n]
-            idx = [k % distinct for k in range(per_call)]
-            a = ([d[i]["vis_re"] for i in idx], [d[i]["vis_im"] for i in idx],
-                 [d[i]["B"] for i in idx], [d[i]["V"] for i in idx], [snaps[i].nb for i in idx])
-            nbmax = max(x.nb for x in snaps)
-            b = fip.Batch(n, nbmax, snaps[0].cell_size, 32, per_call, device=local, **kw)
-            tuning = b.autotune(*a)
-            u = n // 32
-            batches[n], args_of[n] = b, a
-            streams[n] = torch.cuda.Stream(device=dev)
-            res[n] = torch.zeros((per_call * calls_per_size, u * u), device=dev)
-            out.setdefault("autotune", {})[f"{name}_{n}"] = tuning
+        b = fip.Batch.of_sequences(spec, per_size, device=local, **kw)
+        tunes = b.autotune_sequences(seq, *args, nbs)
+        for n, tn in zip(sizes, tunes):
+            out.setdefault("autotune", {})[f"{name}_{n}"] = tn
+        res = [torch.zeros((per_size * calls, (n // 32) ** 2), device=dev) for n in sizes]
+
         def run_all():
-            got = {}
-            for c in range(calls_per_size):
-                for n in sizes:
-                    with torch.cuda.stream(streams[n]):
-                        got[n] = got.get(n, 0) + batches[n].image(
-                            *args_of[n], res[n][got.get(n, 0):], stream=streams[n])
+            got = [0] * len(sizes)
+            for _ in range(calls):
+                counts = b.image_sequences(seq, *args, nbs, [r[g:] for r, g in zip(res, got)])
+                got = [g + k for g, k in zip(got, counts)]
             return got
-        for n in sizes:
-            batches[n].reset()
-        run_all()  # warm-up: instantiates the graphs
+        b.reset()
+        run_all()  # warm-up: instantiates the graph
         torch.cuda.synchronize()
-        for n in sizes:
-            batches[n].reset()
-        l0 = sum(b.kernel_launches for b in batches.values())
+        b.reset()
+        l0 = b.kernel_launches
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         ev0.record()
-        for n in sizes:
-            streams[n].wait_event(ev0)
         run_all()
-        for n in sizes:
-            torch.cuda.current_stream().wait_stream(streams[n])
         ev1.record()
         torch.cuda.synchronize()
+        b.check()
         ms = ev0.elapsed_time(ev1)
         out[name] = {"value": total / (ms / 1e3), "unit": UNIT, "snapshots": total,
-                     "gpu_launches": sum(b.kernel_launches for b in batches.values()) - l0,
-                     "hbm_gb": sum(b.device_bytes for b in batches.values()) / 2**30,
+                     "gpu_launches": b.kernel_launches - l0,
+                     "hbm_gb": b.device_bytes / 2**30,
                      "config": f"{total} snapshots x 8 channels (130-150 MHz), 0-30 % flagged, "
-                               f"half 4096^2 / half 2048^2, tile 32, {per_call} per call, "
-                               "two sizes on two streams, CUDA graph per call"}
-        for b in batches.values():
-            b.close()
+                               f"half 4096^2 / half 2048^2 interleaved in each call, tile 32, "
+                               f"{per_size} of each size per call, one persistent gridding "
+                               "launch for both sizes, CUDA graph per call"}
+        b.close()
     return out
 
 

@@ -101,6 +101,10 @@ def lib() -> ctypes.CDLL:
                                              ctypes.POINTER(sz), vp]
         L.fip_image_snapshot_raw.argtypes = [vp, ctypes.POINTER(RawVis), vp, vp, sz, vp, vp, vp]
         L.fip_batch_check.argtypes = [vp, vp]
+        L.fip_batch_create_sequences.argtypes = [ctypes.POINTER(vp), vp, sz, sz]
+        L.fip_batch_image_sequences.argtypes = [vp, vp, vp, vp, vp, vp, vp, sz, vp, vp, vp]
+        L.fip_batch_autotune_sequences.argtypes = [vp, vp, vp, vp, vp, vp, vp, sz, vp]
+        L.fip_batch_sequence_tuning.argtypes = [vp, ctypes.c_int] + [ctypes.POINTER(ctypes.c_int)] * 4
         L.fip_set_trigger_streaming.argtypes = [ctypes.c_int]
         L.fip_trigger_window.argtypes = [vp, vp, vp, sz, vp, vp]
         L.fip_pipe_host.argtypes = [vp, vp, vp, vp, vp, sz, sz, vp]
@@ -346,7 +350,9 @@ class Batch:
     """Batching form (fip_batch): many snapshots of one power-of-two image size per
     call, one persistent gridding launch and one batched transform per call,
     replayed as a CUDA graph; the batch carries the sequence's last two images so
-    every snapshot with two predecessors yields a tLISI matrix."""
+    every snapshot with two predecessors yields a tLISI matrix.  Batch.of_sequences
+    makes a batch of several sequences of different image sizes, imaged together
+    (image_sequences)."""
 
     def __init__(self, image_size: int, max_baselines: int, cell_size: float, unit_size: int,
                  max_snapshots: int, form: int = FORM_PLAIN, vis_storage: int = STORE_F32,
@@ -359,6 +365,28 @@ class Batch:
         self.image_size = image_size
         self.unit_size = unit_size
         self.max_snapshots = max_snapshots
+        self.sequences = [(image_size, max_baselines, cell_size, unit_size)]
+
+    @classmethod
+    def of_sequences(cls, sequences, max_snapshots: int, form: int = FORM_PLAIN,
+                     vis_storage: int = STORE_F32, device: int = 0) -> "Batch":
+        """A batch of several sequences (fip_batch_create_sequences): `sequences` holds
+        (image_size, max_baselines, cell_size, unit_size) per sequence; up to
+        max_snapshots of each sequence per call."""
+        self = cls.__new__(cls)
+        seqs = [tuple(x) for x in sequences]
+        cfgs = (ImagerConfig * len(seqs))(*[
+            ImagerConfig(n, nb, t, cell, form, vis_storage, device, REPROJECT_GATHER)
+            for (n, nb, cell, t) in seqs])
+        h = ctypes.c_void_p()
+        _check(lib().fip_batch_create_sequences(ctypes.byref(h), ctypes.cast(cfgs, ctypes.c_void_p),
+                                                len(seqs), max_snapshots))
+        self._h = h
+        self.cfg = cfgs[0]
+        self.image_size, _, _, self.unit_size = seqs[0]
+        self.max_snapshots = max_snapshots
+        self.sequences = seqs
+        return self
 
     @staticmethod
     def _arrays(vis_re, vis_im, B, V, nb):
@@ -379,15 +407,39 @@ class Batch:
                                      _stream(stream)))
         return int(nr.value)
 
+    def image_sequences(self, sequence, vis_re, vis_im, B, V, nb, results, stream=None) -> list:
+        """Images len(nb) snapshots of several sequences in one call: snapshot k
+        belongs to sequence sequence[k]; sequence c's tLISI matrices go to results[c]
+        (U_c * U_c floats each, in order).  Returns the number per sequence."""
+        a = self._arrays(vis_re, vis_im, B, V, nb)
+        count = a[-1]
+        if len(sequence) != count:
+            raise ValueError("one sequence index per snapshot")
+        ns = len(self.sequences)
+        seq = (ctypes.c_int * count)(*[int(c) for c in sequence])
+        res = (ctypes.c_void_p * ns)(*[_ptr(r) if r is not None else None for r in results])
+        nr = (ctypes.c_size_t * ns)()
+        _check(lib().fip_batch_image_sequences(self._h, seq, *a, res, nr, _stream(stream)))
+        return [int(x) for x in nr]
+
     def autotune(self, vis_re, vis_im, B, V, nb, stream=None) -> dict:
         _check(lib().fip_batch_autotune(self._h, *self._arrays(vis_re, vis_im, B, V, nb),
                                         _stream(stream)))
         return self.tuning()
 
-    def tuning(self) -> dict:
+    def autotune_sequences(self, sequence, vis_re, vis_im, B, V, nb, stream=None) -> list:
+        """Autotunes on a representative call of several sequences; returns each
+        sequence's tuning."""
+        a = self._arrays(vis_re, vis_im, B, V, nb)
+        seq = (ctypes.c_int * a[-1])(*[int(c) for c in sequence])
+        _check(lib().fip_batch_autotune_sequences(self._h, seq, *a, _stream(stream)))
+        return [self.tuning(c) for c in range(len(self.sequences))]
+
+    def tuning(self, sequence: int = 0) -> dict:
         e, sp, dr, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        _check(lib().fip_batch_tuning(self._h, ctypes.byref(e), ctypes.byref(sp),
-                                      ctypes.byref(dr), ctypes.byref(c)))
+        _check(lib().fip_batch_sequence_tuning(self._h, sequence, ctypes.byref(e),
+                                               ctypes.byref(sp), ctypes.byref(dr),
+                                               ctypes.byref(c)))
         return {"fft_values_per_thread": int(e.value), "fft_split": int(sp.value),
                 "fft_direct": int(dr.value), "grid_ctas_per_sm": int(c.value)}
 

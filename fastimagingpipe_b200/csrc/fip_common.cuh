@@ -65,15 +65,30 @@ __device__ __forceinline__ void fip_collapse_sample(const FipRawVis& r, size_t s
   }
 }
 
-// Batched launches: at most FIP_MAX_BATCH snapshots of one image size.
+// Batched launches: at most FIP_MAX_BATCH snapshots, of one or several
+// image sizes.
 #define FIP_MAX_BATCH 64
 
-// Per-snapshot inputs of a batched gridding launch (a kernel parameter).
+// One snapshot of a batched gridding launch: its inputs, bins and grid, and
+// its grid geometry (snapshots of a launch may differ in image size).
+struct FipGridSnap {
+  const float* B;           // [nb][2]
+  const void* vr;           // float, or half/bf16 for reduced storage
+  const void* vi;
+  const float* V;           // [9]
+  const float* vis_scale;   // reduced-storage scale, or null
+  const unsigned* entries;  // the snapshot's bins (FipBins)
+  const int4* work;
+  const unsigned* nwork;
+  float2* grid;             // its half-plane grid
+  float scale;              // cell * G
+  int g, hp, tiles_c;
+};
+
+// The snapshots of one batched gridding launch (a kernel parameter of
+// about 5.6 KB).
 struct FipGridBatch {
   int count;
-  const float* B[FIP_MAX_BATCH];          // [nb][2]
-  const void* vr[FIP_MAX_BATCH];          // float, or half/bf16 for reduced storage
-  const void* vi[FIP_MAX_BATCH];
-  const float* V[FIP_MAX_BATCH];          // [9]
-  const float* vis_scale[FIP_MAX_BATCH];  // reduced-storage scale, or null
+  int layout;
+  FipGridSnap s[FIP_MAX_BATCH];
 };

@@ -1346,27 +1346,27 @@ int fip_pipe(const float* vis_re, const float* vis_im, const float* B, const flo
 
 
 // ---------------------------------------------------------------------------
-// Batching form: many snapshots of one image size per call, imaged with one
-// persistent gridding launch and one batched transform for the whole batch,
-// the per-snapshot stages (binning, pixel mapping, reprojection) on parallel
-// branches, the trigger batched over the sequence, all captured as one CUDA
-// graph per call shape.
+// Batching form: many snapshots per call, of one or several sequences (each
+// with its own image size, cell and tile), imaged with one persistent
+// gridding launch for the whole call and one batched transform per image
+// size, the per-snapshot stages (binning, pixel mapping, reprojection) on
+// parallel branches, each sequence's trigger batched over its sliding window,
+// all captured as one CUDA graph per call shape.
 // ---------------------------------------------------------------------------
 namespace {
 constexpr int kBranches = 4;
+constexpr int kMaxSequences = 8;
 }  // namespace
 
-struct fip_batch {
+// One sequence of a batch: its configuration, transform plan and tables, the
+// scratch of up to smax snapshots per call (the call's j-th snapshot of the
+// sequence at base + j * stride) and its image ring.
+struct BatchSeq {
   fip_imager_config cfg{};
   FipGeom geo{};
-  int smax = 0;                       // snapshots per call at most
-  size_t device_bytes = 0;
   fipfft::Plan fft{};
-  int grid_ctas_per_sm = 0;
   float2* twiddles = nullptr;
-  float2* theta_tab = nullptr;  // theta terms of the pixel mapping (plain form)
   float* taper = nullptr;
-  // Per-snapshot scratch, snapshot k at base + k * stride.
   size_t ntiles = 0, cap = 0, wcap = 0, n2 = 0, grid_elems = 0, col_elems = 0;
   unsigned* count = nullptr;          // [smax][ntiles]
   unsigned* offset = nullptr;         // [smax][ntiles + 1]
@@ -1388,8 +1388,39 @@ struct fip_batch {
   // snapshots go to slots 2 .. count + 1.
   float* images = nullptr;            // [smax + 2][N N]
   float* maxima = nullptr;            // [smax + 2]
-  unsigned* gather_err = nullptr;     // [1] set by a gather tile outside its domain
   int carried = 0;
+
+  FipBins bins(int k) const {
+    FipBins b{};
+    b.count = count + k * ntiles;
+    b.offset = offset + k * (ntiles + 1);
+    b.cursor = cursor + k * ntiles;
+    b.entries = entries + k * cap;
+    b.work = work + k * wcap;
+    b.nwork = nwork + k;
+    b.bbox = bbox + 4 * k;
+    b.multi = multi + k * ntiles;
+    b.nmulti = nmulti + k;
+    b.cap = cap;
+    b.wcap = wcap;
+    return b;
+  }
+  void free_all() {
+    void* ptrs[] = {twiddles, taper, count, offset, cursor, entries, work, nwork, bbox, multi,
+                    nmulti, grid, colbuf, pre, targets, q_re, q_im, q_scale, images, maxima};
+    for (void* p : ptrs)
+      if (p) cudaFree(p);
+  }
+};
+
+struct fip_batch {
+  fip_imager_config cfg{};  // sequence 0's; form, storage and device are every sequence's
+  int smax = 0;             // snapshots of one sequence per call at most
+  size_t device_bytes = 0;
+  int grid_ctas_per_sm = 0;
+  float2* theta_tab = nullptr;  // theta terms of the pixel mapping (plain form)
+  std::vector<BatchSeq> seq;
+  unsigned* gather_err = nullptr;     // [1] set by a gather tile outside its domain
   cudaStream_t branch[kBranches] = {};
   cudaStream_t capture = nullptr;  // capture and launch stream (highest priority)
   // Pixel-mapping branches at the lowest priority: the mappings need only V,
@@ -1410,22 +1441,6 @@ struct fip_batch {
   bool phase_pending = false;
   cudaGraphExec_t exec = nullptr;
   unsigned long long launches = 0;
-
-  FipBins bins(int k) const {
-    FipBins b{};
-    b.count = count + k * ntiles;
-    b.offset = offset + k * (ntiles + 1);
-    b.cursor = cursor + k * ntiles;
-    b.entries = entries + k * cap;
-    b.work = work + k * wcap;
-    b.nwork = nwork + k;
-    b.bbox = bbox + 4 * k;
-    b.multi = multi + k * ntiles;
-    b.nmulti = nmulti + k;
-    b.cap = cap;
-    b.wcap = wcap;
-    return b;
-  }
 };
 
 namespace {
@@ -1433,12 +1448,9 @@ void batch_free(fip_batch* b) {
   if (!b) return;
   DeviceGuard g(b->cfg.device);
   if (b->exec) cudaGraphExecDestroy(b->exec);
-  void* ptrs[] = {b->twiddles, b->theta_tab, b->taper, b->count, b->offset, b->cursor, b->entries, b->work,
-                  b->nwork, b->bbox, b->multi, b->nmulti, b->grid, b->colbuf, b->pre,
-                  b->targets, b->q_re, b->q_im, b->q_scale, b->images, b->maxima,
-                  b->gather_err};
-  for (void* p : ptrs)
-    if (p) cudaFree(p);
+  for (BatchSeq& q : b->seq) q.free_all();
+  if (b->theta_tab) cudaFree(b->theta_tab);
+  if (b->gather_err) cudaFree(b->gather_err);
   for (int k = 0; k < kBranches; ++k) {
     if (b->branch[k]) cudaStreamDestroy(b->branch[k]);
     if (b->join[k]) cudaEventDestroy(b->join[k]);
@@ -1468,19 +1480,72 @@ int batch_collect(fip_batch* b) {
   return FIP_OK;
 }
 
+int batch_vis_type(const fip_batch* b) {
+  const bool reduced = b->cfg.form == FIP_FORM_PRECISE && b->cfg.vis_storage != FIP_STORE_F32;
+  return !reduced ? FIP_VIS_F32
+                  : (b->cfg.vis_storage == FIP_STORE_F16 ? FIP_VIS_F16 : FIP_VIS_BF16);
+}
+
+// The snapshots of a call by sequence: snapshot k is the loc[k]-th of
+// sequence sq[k] in this call, which holds per[c] snapshots of sequence c.
+struct CallLayout {
+  int sq[FIP_MAX_BATCH];
+  int loc[FIP_MAX_BATCH];
+  int per[kMaxSequences];
+};
+
+CallLayout call_layout(const int* seq_of, int count) {
+  CallLayout l{};
+  for (int k = 0; k < count; ++k) {
+    l.sq[k] = seq_of ? seq_of[k] : 0;
+    l.loc[k] = l.per[l.sq[k]]++;
+  }
+  return l;
+}
+
+// Snapshot k's entry of the batched gridding launch (its bins in place).
+FipGridSnap grid_snap(const fip_batch* b, const CallLayout& l, int k, const float* B,
+                      const float* V, const void* vr, const void* vi) {
+  const BatchSeq& q = b->seq[l.sq[k]];
+  const int j = l.loc[k];
+  const bool reduced = batch_vis_type(b) != FIP_VIS_F32;
+  FipGridSnap g{};
+  g.B = B;
+  g.V = V;
+  g.vr = reduced ? static_cast<const void*>(static_cast<char*>(q.q_re) +
+                                            j * q.cfg.max_baselines * 2)
+                 : vr;
+  g.vi = reduced ? static_cast<const void*>(static_cast<char*>(q.q_im) +
+                                            j * q.cfg.max_baselines * 2)
+                 : vi;
+  g.vis_scale = reduced ? q.q_scale + j : nullptr;
+  const FipBins bins = q.bins(j);
+  g.entries = bins.entries;
+  g.work = bins.work;
+  g.nwork = bins.nwork;
+  g.grid = q.grid + j * q.grid_elems;
+  g.scale = q.geo.cell * (float)(size_t)q.geo.g;
+  g.g = q.geo.g;
+  g.hp = q.geo.hp;
+  g.tiles_c = q.geo.tiles_c;
+  return g;
+}
+
 // Captures the work of one call into a graph (stream s in capture mode).
-// slots (or null): per-snapshot image destinations and trigger predecessors
-// (fip_batch_image_slots) instead of the batch's own sequence ring.
-int batch_record(fip_batch* b, const float* const* vr, const float* const* vi,
-                 const float* const* B, const float* const* V, const size_t* nb, int count,
-                 int first_result, float* results, cudaStream_t s,
-                 const fip_batch_slot* slots = nullptr) {
-  const FipGeom& geo = b->geo;
+// seq_of (or null: all sequence 0): each snapshot's sequence; first[c] and
+// results[c]: sequence c's first snapshot with two predecessors and where
+// its tLISI matrices go.  slots (or null): per-snapshot image destinations
+// and trigger predecessors (fip_batch_image_slots) instead of the sequences'
+// rings.
+int batch_record(fip_batch* b, const int* seq_of, const float* const* vr,
+                 const float* const* vi, const float* const* B, const float* const* V,
+                 const size_t* nb, int count, const int* first, float* const* results,
+                 cudaStream_t s, const fip_batch_slot* slots = nullptr) {
   const bool precise = b->cfg.form == FIP_FORM_PRECISE;
-  const bool reduced = precise && b->cfg.vis_storage != FIP_STORE_F32;
-  const int vt = !reduced ? FIP_VIS_F32
-                          : (b->cfg.vis_storage == FIP_STORE_F16 ? FIP_VIS_F16 : FIP_VIS_BF16);
-  const size_t qsz = 2;  // bytes per reduced-storage value
+  const int vt = batch_vis_type(b);
+  const bool reduced = vt != FIP_VIS_F32;
+  const int nseq = (int)b->seq.size();
+  const CallLayout l = call_layout(seq_of, count);
   unsigned long long launches = 0;
   auto phase = [&](int k) -> cudaError_t {
     // Inside stream capture only an external record becomes a record node.
@@ -1497,7 +1562,8 @@ int batch_record(fip_batch* b, const float* const* vr, const float* const* vi,
     for (int i = 0; i < fip_batch::kMapBranches; ++i)
       FIP_CUDA(cudaStreamWaitEvent(b->map_branch[i], b->fork, 0));
     for (int k = 0; k < count; ++k) {
-      FIP_CUDA(fip_launch_targets(geo, V[k], b->theta_tab, b->targets + k * b->n2,
+      const BatchSeq& q = b->seq[l.sq[k]];
+      FIP_CUDA(fip_launch_targets(q.geo, V[k], b->theta_tab, q.targets + l.loc[k] * q.n2,
                                   b->map_branch[k % fip_batch::kMapBranches]));
       launches += 1;
     }
@@ -1506,63 +1572,79 @@ int batch_record(fip_batch* b, const float* const* vr, const float* const* vi,
   }
   FipGridBatch in{};
   in.count = count;
+  in.layout = 1;
   for (int k = 0; k < count; ++k) {
+    const BatchSeq& q = b->seq[l.sq[k]];
+    const int j = l.loc[k];
     cudaStream_t bs = b->branch[k % kBranches];
-    in.B[k] = B[k];
-    in.V[k] = V[k];
-    in.vr[k] = vr[k];
-    in.vi[k] = vi[k];
-    in.vis_scale[k] = nullptr;
     if (reduced) {
-      void* qr = static_cast<char*>(b->q_re) + k * b->cfg.max_baselines * qsz;
-      void* qi = static_cast<char*>(b->q_im) + k * b->cfg.max_baselines * qsz;
-      FIP_CUDA(fip_launch_quantize(vr[k], vi[k], nb[k], vt, qr, qi, b->q_scale + k, bs));
-      in.vr[k] = qr;
-      in.vi[k] = qi;
-      in.vis_scale[k] = b->q_scale + k;
+      void* qr = static_cast<char*>(q.q_re) + j * q.cfg.max_baselines * 2;
+      void* qi = static_cast<char*>(q.q_im) + j * q.cfg.max_baselines * 2;
+      FIP_CUDA(fip_launch_quantize(vr[k], vi[k], nb[k], vt, qr, qi, q.q_scale + j, bs));
       launches += 3;
     }
-    FipBins bins = b->bins(k);
-    FIP_CUDA(fip_launch_bin(geo, B[k], (int)nb[k], bins, bs));
-    launches += fip_bin_launches(geo);
+    FipBins bins = q.bins(j);
+    FIP_CUDA(fip_launch_bin(q.geo, B[k], (int)nb[k], bins, bs));
+    launches += fip_bin_launches(q.geo);
+    in.s[k] = grid_snap(b, l, k, B[k], V[k], vr[k], vi[k]);
   }
   for (int i = 0; i < kBranches; ++i) {
     FIP_CUDA(cudaEventRecord(b->join[i], b->branch[i]));
     FIP_CUDA(cudaStreamWaitEvent(s, b->join[i], 0));
   }
   FIP_CUDA(phase(1));
-  // One persistent gridding launch and one batched transform for the batch.
-  FIP_CUDA(fip_launch_grid_batch(geo, in, vt, b->multi, b->ntiles, b->nmulti, b->entries, b->cap,
-                                 b->work, b->wcap, b->nwork, b->grid, b->grid_elems,
-                                 precise ? 1 : 0, s, b->grid_ctas_per_sm));
+  // One persistent gridding launch for the whole call (after each sequence's
+  // split tiles are zeroed), one batched transform per sequence.
+  for (int c = 0; c < nseq; ++c) {
+    const BatchSeq& q = b->seq[c];
+    if (l.per[c] == 0) continue;
+    FIP_CUDA(fip_launch_zero_batch(q.geo, q.multi, q.ntiles, q.nmulti, q.grid, q.grid_elems,
+                                   l.per[c], s));
+    launches += 1;
+  }
+  FIP_CUDA(fip_launch_grid_batch(in, vt, precise ? 1 : 0, s, b->grid_ctas_per_sm));
+  launches += 1;
   FIP_CUDA(phase(2));
-  FIP_CUDA(fip_launch_fft_cols(geo, b->grid, b->bbox, b->colbuf, b->twiddles, b->fft, s, count,
-                               b->grid_elems, b->col_elems));
+  for (int c = 0; c < nseq; ++c) {
+    const BatchSeq& q = b->seq[c];
+    if (l.per[c] == 0) continue;
+    FIP_CUDA(fip_launch_fft_cols(q.geo, q.grid, q.bbox, q.colbuf, q.twiddles, q.fft, s, l.per[c],
+                                 q.grid_elems, q.col_elems));
+    launches += 1;
+  }
   FIP_CUDA(phase(3));
-  FIP_CUDA(fip_launch_fft_rows(geo, b->colbuf, b->bbox, b->taper, b->twiddles, b->fft, b->pre, s,
-                               count, b->col_elems, b->n2));
+  for (int c = 0; c < nseq; ++c) {
+    const BatchSeq& q = b->seq[c];
+    if (l.per[c] == 0) continue;
+    FIP_CUDA(fip_launch_fft_rows(q.geo, q.colbuf, q.bbox, q.taper, q.twiddles, q.fft, q.pre, s,
+                                 l.per[c], q.col_elems, q.n2));
+    launches += 1;
+  }
   FIP_CUDA(phase(4));
-  launches += 4;
   if (!precise)
     for (int i = 0; i < fip_batch::kMapBranches; ++i)
       FIP_CUDA(cudaStreamWaitEvent(s, b->map_join[i], 0));
   // Reprojection per snapshot on the branches, into ring slots 2 .. count+1
-  // (or the caller's slots).
+  // of its sequence (or the caller's slots).
   if (slots) {
     for (int k = 0; k < count; ++k)
       FIP_CUDA(cudaMemsetAsync(slots[k].image_max, 0, sizeof(float), s));
   } else {
-    FIP_CUDA(cudaMemsetAsync(b->maxima + 2, 0, count * sizeof(float), s));
+    for (int c = 0; c < nseq; ++c)
+      if (l.per[c] > 0)
+        FIP_CUDA(cudaMemsetAsync(b->seq[c].maxima + 2, 0, l.per[c] * sizeof(float), s));
   }
   FIP_CUDA(cudaEventRecord(b->fork, s));
   for (int i = 0; i < kBranches; ++i) FIP_CUDA(cudaStreamWaitEvent(b->branch[i], b->fork, 0));
   for (int k = 0; k < count; ++k) {
+    const BatchSeq& q = b->seq[l.sq[k]];
+    const int j = l.loc[k];
     cudaStream_t bs = b->branch[k % kBranches];
-    float* img = slots ? slots[k].image : b->images + (k + 2) * b->n2;
-    float* mx = slots ? slots[k].image_max : b->maxima + k + 2;
+    float* img = slots ? slots[k].image : q.images + (j + 2) * q.n2;
+    float* mx = slots ? slots[k].image_max : q.maxima + j + 2;
     FIP_CUDA(fip_launch_reproject_gather(
-        geo, b->pre + k * b->n2, precise ? nullptr : b->targets + k * b->n2, V[k], (int)nb[k],
-        b->bbox + 4 * k + 3, img, reinterpret_cast<unsigned*>(mx), precise ? 1 : 0, bs,
+        q.geo, q.pre + j * q.n2, precise ? nullptr : q.targets + j * q.n2, V[k], (int)nb[k],
+        q.bbox + 4 * j + 3, img, reinterpret_cast<unsigned*>(mx), precise ? 1 : 0, bs,
         b->gather_err));
     launches += 1;
   }
@@ -1574,9 +1656,10 @@ int batch_record(fip_batch* b, const float* const* vr, const float* const* vi,
   if (slots) {
     // Each snapshot with predecessors: the tLISI of (prev 0, prev 1, itself);
     // predecessors may be images of this call (written above).
-    for (int k = 0; k < count && geo.t > 0; ++k) {
+    for (int k = 0; k < count; ++k) {
       const fip_batch_slot& sl = slots[k];
-      if (!sl.prev_image[0]) continue;
+      const FipGeom& geo = b->seq[l.sq[k]].geo;
+      if (!sl.prev_image[0] || geo.t <= 0) continue;
       FIP_CUDA(fip_launch_trigger3(geo, sl.prev_image[0], sl.prev_image[1], sl.image,
                                    sl.prev_max[0], sl.prev_max[1], sl.image_max, sl.tlisi,
                                    precise ? 1 : 0, s));
@@ -1586,73 +1669,138 @@ int batch_record(fip_batch* b, const float* const* vr, const float* const* vi,
     b->launches += launches;
     return FIP_OK;
   }
-  // Sliding-window trigger: snapshot k (slot k + 2) with two predecessors.
-  const int ntrig = count - first_result;
-  if (ntrig > 0 && geo.t > 0) {
-    FIP_CUDA(fip_launch_trigger_batch(geo, b->images + first_result * b->n2,
-                                      b->maxima + first_result, ntrig, results,
-                                      precise ? 1 : 0, s));
-    launches += 1;
+  // Each sequence's sliding-window trigger: its snapshot j (slot j + 2) with
+  // two predecessors.
+  for (int c = 0; c < nseq; ++c) {
+    const BatchSeq& q = b->seq[c];
+    const int ntrig = l.per[c] - first[c];
+    if (ntrig > 0 && q.geo.t > 0) {
+      FIP_CUDA(fip_launch_trigger_batch(q.geo, q.images + first[c] * q.n2, q.maxima + first[c],
+                                        ntrig, results[c], precise ? 1 : 0, s));
+      launches += 1;
+    }
   }
   FIP_CUDA(phase(6));
-  // Carry the last two images (and maxima) to slots 0, 1.
-  for (int slot = 0; slot < 2; ++slot) {
-    const int from = count + slot;  // slots count, count + 1 (count >= 1)
-    if (from == slot) continue;
-    FIP_CUDA(cudaMemcpyAsync(b->images + slot * b->n2, b->images + from * b->n2,
-                             b->n2 * sizeof(float), cudaMemcpyDeviceToDevice, s));
-    FIP_CUDA(cudaMemcpyAsync(b->maxima + slot, b->maxima + from, sizeof(float),
-                             cudaMemcpyDeviceToDevice, s));
+  // Carry each sequence's last two images (and maxima) to its slots 0, 1.
+  for (int c = 0; c < nseq; ++c) {
+    const BatchSeq& q = b->seq[c];
+    if (l.per[c] == 0) continue;
+    for (int slot = 0; slot < 2; ++slot) {
+      const int from = l.per[c] + slot;  // slots per, per + 1 (per >= 1)
+      if (from == slot) continue;
+      FIP_CUDA(cudaMemcpyAsync(q.images + slot * q.n2, q.images + from * q.n2,
+                               q.n2 * sizeof(float), cudaMemcpyDeviceToDevice, s));
+      FIP_CUDA(cudaMemcpyAsync(q.maxima + slot, q.maxima + from, sizeof(float),
+                               cudaMemcpyDeviceToDevice, s));
+    }
   }
   b->launches += launches;
+  return FIP_OK;
+}
+
+// Allocates sequence q's scratch for smax snapshots per call.
+int seq_alloc(BatchSeq& q, size_t smax, size_t& tot) {
+  const fip_imager_config& cfg = q.cfg;
+  FipGeom& geo = q.geo;
+  geo.n = (int)cfg.image_size;
+  geo.g = (int)ceilf(1.5f * (float)cfg.image_size);  // FIPkernels.cu:583
+  geo.hp = geo.g / 2 + 1;
+  geo.t = (int)cfg.unit_size;
+  geo.u = geo.t > 0 ? geo.n / geo.t : 0;
+  geo.tiles_r = (geo.g + FIP_GTILE - 1) / FIP_GTILE;
+  geo.tiles_c = (geo.hp + FIP_GTILE - 1) / FIP_GTILE;
+  geo.cell = cfg.cell_size;
+  geo.layout = 1;
+  if (!fip_fft_plan(geo.g, q.fft))
+    return fail(FIP_ERR_ARG, "the batching form needs a power-of-two image size "
+                             "(band-pruned transform)");
+  if (!fip_gather_supported(geo, cfg.form == FIP_FORM_PRECISE))
+    return fail(FIP_ERR_ARG, "cell_size too small for the tile-gather reprojection");
+#define FIP_SALLOC(call)                                                                     \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(e_ == cudaErrorMemoryAllocation ? FIP_ERR_NOMEM : FIP_ERR_CUDA,            \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                       \
+  } while (0)
+  const size_t S = smax, nb = cfg.max_baselines;
+  q.ntiles = (size_t)geo.tiles_r * geo.tiles_c;
+  q.cap = 12 * nb;
+  q.wcap = q.ntiles + q.cap / FIP_GCHUNK + 1;
+  q.n2 = (size_t)geo.n * geo.n;
+  q.grid_elems = (size_t)geo.g * geo.hp;
+  q.col_elems = (size_t)geo.hp * geo.n;
+  FIP_SALLOC(dalloc(&q.count, S * q.ntiles, tot));
+  FIP_SALLOC(dalloc(&q.offset, S * (q.ntiles + 1), tot));
+  FIP_SALLOC(dalloc(&q.cursor, S * q.ntiles, tot));
+  FIP_SALLOC(dalloc(&q.entries, S * q.cap, tot));
+  FIP_SALLOC(dalloc(&q.work, S * q.wcap, tot));
+  FIP_SALLOC(dalloc(&q.nwork, S, tot));
+  FIP_SALLOC(dalloc(&q.bbox, 4 * S, tot));
+  FIP_SALLOC(dalloc(&q.multi, S * q.ntiles, tot));
+  FIP_SALLOC(dalloc(&q.nmulti, S, tot));
+  FIP_SALLOC(dalloc(&q.grid, S * q.grid_elems, tot));
+  FIP_SALLOC(dalloc(&q.colbuf, S * q.col_elems, tot));
+  FIP_SALLOC(dalloc(&q.pre, S * q.n2, tot));
+  if (cfg.form == FIP_FORM_PLAIN) FIP_SALLOC(dalloc(&q.targets, S * q.n2, tot));
+  if (cfg.form == FIP_FORM_PRECISE && cfg.vis_storage != FIP_STORE_F32) {
+    FIP_SALLOC(dalloc((uint16_t**)&q.q_re, S * nb, tot));
+    FIP_SALLOC(dalloc((uint16_t**)&q.q_im, S * nb, tot));
+    FIP_SALLOC(dalloc(&q.q_scale, S, tot));
+  }
+  FIP_SALLOC(dalloc(&q.images, (S + 2) * q.n2, tot));
+  FIP_SALLOC(dalloc(&q.maxima, S + 2, tot));
+  FIP_SALLOC(dalloc(&q.taper, 2 * ((size_t)geo.n / 2 + 1), tot));
+  {
+    const std::vector<float2> tw = fft_twiddles(geo.g);
+    FIP_SALLOC(dalloc(&q.twiddles, tw.size(), tot));
+    FIP_SALLOC(cudaMemcpy(q.twiddles, tw.data(), tw.size() * sizeof(float2),
+                          cudaMemcpyHostToDevice));
+  }
+#undef FIP_SALLOC
   return FIP_OK;
 }
 }  // namespace
 
 extern "C" {
 
-int fip_batch_create(fip_batch** out, const fip_imager_config* cfg, size_t max_snapshots) {
-  if (!out || !cfg) return fail(FIP_ERR_ARG, "null argument");
+int fip_batch_create_sequences(fip_batch** out, const fip_imager_config* cfgs, size_t nseq,
+                               size_t max_snapshots) {
+  if (!out || !cfgs) return fail(FIP_ERR_ARG, "null argument");
   *out = nullptr;
-  FIP_TRY(validate_sizes(cfg->image_size, cfg->unit_size, cfg->cell_size));
+  if (nseq < 1 || nseq > (size_t)kMaxSequences)
+    return fail(FIP_ERR_ARG, "the number of sequences must be in [1, 8]");
   if (max_snapshots < 1 || max_snapshots > FIP_MAX_BATCH)
     return fail(FIP_ERR_ARG, "max_snapshots must be in [1, 64]");
-  if (cfg->max_baselines == 0 || cfg->max_baselines > (1u << 24))
-    return fail(FIP_ERR_ARG, "max_baselines must be in [1, 2^24]");
-  if (cfg->form != FIP_FORM_PLAIN && cfg->form != FIP_FORM_PRECISE)
-    return fail(FIP_ERR_ARG, "unknown form");
-  if (cfg->vis_storage < 0 || cfg->vis_storage > 2) return fail(FIP_ERR_ARG, "unknown storage");
-  if (cfg->reproject != 0) return fail(FIP_ERR_ARG, "the batching form reprojects by tile gather");
+  for (size_t c = 0; c < nseq; ++c) {
+    const fip_imager_config* cfg = cfgs + c;
+    FIP_TRY(validate_sizes(cfg->image_size, cfg->unit_size, cfg->cell_size));
+    if (cfg->max_baselines == 0 || cfg->max_baselines > (1u << 24))
+      return fail(FIP_ERR_ARG, "max_baselines must be in [1, 2^24]");
+    if (cfg->form != FIP_FORM_PLAIN && cfg->form != FIP_FORM_PRECISE)
+      return fail(FIP_ERR_ARG, "unknown form");
+    if (cfg->vis_storage < 0 || cfg->vis_storage > 2) return fail(FIP_ERR_ARG, "unknown storage");
+    if (cfg->reproject != 0) return fail(FIP_ERR_ARG, "the batching form reprojects by tile gather");
+    if (cfg->form != cfgs[0].form || cfg->vis_storage != cfgs[0].vis_storage ||
+        cfg->device != cfgs[0].device)
+      return fail(FIP_ERR_ARG, "the sequences of a batch share form, storage and device");
+  }
   int ndev = 0;
   FIP_CUDA(cudaGetDeviceCount(&ndev));
-  if (cfg->device < 0 || cfg->device >= ndev) return fail(FIP_ERR_ARG, "no such device");
-  DeviceGuard guard(cfg->device);
+  if (cfgs[0].device < 0 || cfgs[0].device >= ndev) return fail(FIP_ERR_ARG, "no such device");
+  DeviceGuard guard(cfgs[0].device);
   if (!guard.ok) return fail(FIP_ERR_CUDA, "cudaSetDevice failed");
 
   fip_batch* b = new fip_batch();
-  b->cfg = *cfg;
+  b->cfg = cfgs[0];
   b->smax = (int)max_snapshots;
-  FipGeom& geo = b->geo;
-  geo.n = (int)cfg->image_size;
-  geo.g = (int)ceilf(1.5f * (float)cfg->image_size);  // FIPkernels.cu:583
-  geo.hp = geo.g / 2 + 1;
-  geo.t = (int)cfg->unit_size;
-  geo.u = geo.t > 0 ? geo.n / geo.t : 0;
-  geo.tiles_r = (geo.g + FIP_GTILE - 1) / FIP_GTILE;
-  geo.tiles_c = (geo.hp + FIP_GTILE - 1) / FIP_GTILE;
-  geo.cell = cfg->cell_size;
-  geo.layout = 1;
+  b->seq.resize(nseq);
   auto cleanup = [&](int code) {
     std::string msg = g_last_error;
     batch_free(b);
     g_last_error = msg;
     return code;
   };
-  if (!fip_fft_plan(geo.g, b->fft))
-    return cleanup(fail(FIP_ERR_ARG, "the batching form needs a power-of-two image size "
-                                     "(band-pruned transform)"));
-  if (!fip_gather_supported(geo, cfg->form == FIP_FORM_PRECISE))
-    return cleanup(fail(FIP_ERR_ARG, "cell_size too small for the tile-gather reprojection"));
 #define FIP_BALLOC(call)                                                                     \
   do {                                                                                       \
     cudaError_t e_ = (call);                                                                 \
@@ -1660,46 +1808,16 @@ int fip_batch_create(fip_batch** out, const fip_imager_config* cfg, size_t max_s
       return cleanup(fail(e_ == cudaErrorMemoryAllocation ? FIP_ERR_NOMEM : FIP_ERR_CUDA,    \
                           std::string(#call) + ": " + cudaGetErrorString(e_)));              \
   } while (0)
-  const size_t S = max_snapshots, nb = cfg->max_baselines;
   size_t& tot = b->device_bytes;
-  b->ntiles = (size_t)geo.tiles_r * geo.tiles_c;
-  b->cap = 12 * nb;
-  b->wcap = b->ntiles + b->cap / FIP_GCHUNK + 1;
-  b->n2 = (size_t)geo.n * geo.n;
-  b->grid_elems = (size_t)geo.g * geo.hp;
-  b->col_elems = (size_t)geo.hp * geo.n;
-  FIP_BALLOC(dalloc(&b->count, S * b->ntiles, tot));
-  FIP_BALLOC(dalloc(&b->offset, S * (b->ntiles + 1), tot));
-  FIP_BALLOC(dalloc(&b->cursor, S * b->ntiles, tot));
-  FIP_BALLOC(dalloc(&b->entries, S * b->cap, tot));
-  FIP_BALLOC(dalloc(&b->work, S * b->wcap, tot));
-  FIP_BALLOC(dalloc(&b->nwork, S, tot));
-  FIP_BALLOC(dalloc(&b->bbox, 4 * S, tot));
-  FIP_BALLOC(dalloc(&b->multi, S * b->ntiles, tot));
-  FIP_BALLOC(dalloc(&b->nmulti, S, tot));
-  FIP_BALLOC(dalloc(&b->grid, S * b->grid_elems, tot));
-  FIP_BALLOC(dalloc(&b->colbuf, S * b->col_elems, tot));
-  FIP_BALLOC(dalloc(&b->pre, S * b->n2, tot));
-  if (cfg->form == FIP_FORM_PLAIN) {
-    FIP_BALLOC(dalloc(&b->targets, S * b->n2, tot));
+  for (size_t c = 0; c < nseq; ++c) {
+    b->seq[c].cfg = cfgs[c];
+    const int st = seq_alloc(b->seq[c], max_snapshots, tot);
+    if (st != FIP_OK) return cleanup(st);
+  }
+  if (b->cfg.form == FIP_FORM_PLAIN)
     FIP_BALLOC(dalloc(&b->theta_tab, fip_theta_table_elems(), tot));
-  }
-  if (cfg->form == FIP_FORM_PRECISE && cfg->vis_storage != FIP_STORE_F32) {
-    FIP_BALLOC(dalloc((uint16_t**)&b->q_re, S * nb, tot));
-    FIP_BALLOC(dalloc((uint16_t**)&b->q_im, S * nb, tot));
-    FIP_BALLOC(dalloc(&b->q_scale, S, tot));
-  }
-  FIP_BALLOC(dalloc(&b->images, (S + 2) * b->n2, tot));
-  FIP_BALLOC(dalloc(&b->maxima, S + 2, tot));
   FIP_BALLOC(dalloc(&b->gather_err, 1, tot));
   FIP_BALLOC(cudaMemset(b->gather_err, 0, sizeof(unsigned)));
-  FIP_BALLOC(dalloc(&b->taper, 2 * ((size_t)geo.n / 2 + 1), tot));
-  {
-    const std::vector<float2> tw = fft_twiddles(geo.g);
-    FIP_BALLOC(dalloc(&b->twiddles, tw.size(), tot));
-    FIP_BALLOC(cudaMemcpy(b->twiddles, tw.data(), tw.size() * sizeof(float2),
-                          cudaMemcpyHostToDevice));
-  }
   {
     int least = 0, greatest = 0;
     FIP_BALLOC(cudaDeviceGetStreamPriorityRange(&least, &greatest));
@@ -1714,12 +1832,17 @@ int fip_batch_create(fip_batch** out, const fip_imager_config* cfg, size_t max_s
     }
   }
   FIP_BALLOC(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
-  FIP_BALLOC(fip_launch_taper(b->taper, geo, b->branch[0]));
+  for (BatchSeq& q : b->seq) FIP_BALLOC(fip_launch_taper(q.taper, q.geo, b->branch[0]));
   if (b->theta_tab) FIP_BALLOC(fip_launch_theta_table(b->theta_tab, b->branch[0]));
   FIP_BALLOC(cudaStreamSynchronize(b->branch[0]));
 #undef FIP_BALLOC
   *out = b;
   return FIP_OK;
+}
+
+int fip_batch_create(fip_batch** out, const fip_imager_config* cfg, size_t max_snapshots) {
+  if (!out || !cfg) return fail(FIP_ERR_ARG, "null argument");
+  return fip_batch_create_sequences(out, cfg, 1, max_snapshots);
 }
 
 int fip_batch_destroy(fip_batch* b) {
@@ -1733,7 +1856,7 @@ unsigned long long fip_batch_kernel_launches(const fip_batch* b) { return b ? b-
 
 int fip_batch_reset(fip_batch* b) {
   if (!b) return fail(FIP_ERR_ARG, "null batch");
-  b->carried = 0;
+  for (BatchSeq& q : b->seq) q.carried = 0;
   return FIP_OK;
 }
 
@@ -1774,16 +1897,25 @@ int fip_batch_check(fip_batch* b, void* stream) {
   return FIP_OK;
 }
 
-static int batch_run(fip_batch* b, const float* const* vis_re, const float* const* vis_im,
-                     const float* const* B, const float* const* V, const size_t* nb,
-                     size_t count, float* results, size_t* nresults, void* stream,
-                     const fip_batch_slot* slots);
-
+static int batch_run(fip_batch* b, const int* seq_of, const float* const* vis_re,
+                     const float* const* vis_im, const float* const* B, const float* const* V,
+                     const size_t* nb, size_t count, float* const* results, size_t* nresults,
+                     void* stream, const fip_batch_slot* slots);
 
 int fip_batch_image(fip_batch* b, const float* const* vis_re, const float* const* vis_im,
                     const float* const* B, const float* const* V, const size_t* nb, size_t count,
                     float* results, size_t* nresults, void* stream) {
-  return batch_run(b, vis_re, vis_im, B, V, nb, count, results, nresults, stream, nullptr);
+  return batch_run(b, nullptr, vis_re, vis_im, B, V, nb, count, &results, nresults, stream,
+                   nullptr);
+}
+
+int fip_batch_image_sequences(fip_batch* b, const int* sequence, const float* const* vis_re,
+                              const float* const* vis_im, const float* const* B,
+                              const float* const* V, const size_t* nb, size_t count,
+                              float* const* results, size_t* nresults, void* stream) {
+  if (!sequence || !results) return fail(FIP_ERR_ARG, "null argument");
+  return batch_run(b, sequence, vis_re, vis_im, B, V, nb, count, results, nresults, stream,
+                   nullptr);
 }
 
 int fip_batch_image_slots(fip_batch* b, const float* const* vis_re, const float* const* vis_im,
@@ -1796,24 +1928,34 @@ int fip_batch_image_slots(fip_batch* b, const float* const* vis_re, const float*
     if (s.prev_image[0] && (!s.prev_image[1] || !s.prev_max[0] || !s.prev_max[1] || !s.tlisi))
       return fail(FIP_ERR_ARG, "a slot with predecessors needs both, their maxima and tlisi");
   }
-  return batch_run(b, vis_re, vis_im, B, V, nb, count, nullptr, nullptr, stream, slots);
+  return batch_run(b, nullptr, vis_re, vis_im, B, V, nb, count, nullptr, nullptr, stream, slots);
 }
 
-static int batch_run(fip_batch* b, const float* const* vis_re, const float* const* vis_im,
-                     const float* const* B, const float* const* V, const size_t* nb,
-                     size_t count, float* results, size_t* nresults, void* stream,
-                     const fip_batch_slot* slots) {
+static int batch_run(fip_batch* b, const int* seq_of, const float* const* vis_re,
+                     const float* const* vis_im, const float* const* B, const float* const* V,
+                     const size_t* nb, size_t count, float* const* results, size_t* nresults,
+                     void* stream, const fip_batch_slot* slots) {
   if (!b || !vis_re || !vis_im || !B || !V || !nb) return fail(FIP_ERR_ARG, "null argument");
-  if (count < 1 || count > (size_t)b->smax)
-    return fail(FIP_ERR_ARG, "count must be in [1, max_snapshots]");
+  const int nseq = (int)b->seq.size();
+  if (count < 1 || count > (size_t)FIP_MAX_BATCH)
+    return fail(FIP_ERR_ARG, "count must be in [1, 64]");
+  int per[kMaxSequences] = {};
   for (size_t k = 0; k < count; ++k) {
+    const int c = seq_of ? seq_of[k] : 0;
+    if (c < 0 || c >= nseq) return fail(FIP_ERR_ARG, "no such sequence");
+    if (++per[c] > b->smax)
+      return fail(FIP_ERR_ARG, "more snapshots of one sequence than max_snapshots");
     if (!vis_re[k] || !vis_im[k] || !B[k] || !V[k]) return fail(FIP_ERR_ARG, "null device pointer");
-    if (nb[k] == 0 || nb[k] > b->cfg.max_baselines)
+    if (nb[k] == 0 || nb[k] > b->seq[c].cfg.max_baselines)
       return fail(FIP_ERR_ARG, "nb must be in [1, max_baselines]");
   }
-  const int first = std::max(0, 2 - b->carried);
-  const int ntrig = std::max(0, (int)count - first);
-  if (!slots && ntrig > 0 && b->geo.t > 0 && !results) return fail(FIP_ERR_ARG, "null results");
+  int first[kMaxSequences] = {}, ntrig[kMaxSequences] = {};
+  for (int c = 0; c < nseq; ++c) {
+    first[c] = std::max(0, 2 - b->seq[c].carried);
+    ntrig[c] = std::max(0, per[c] - first[c]);
+    if (!slots && ntrig[c] > 0 && b->seq[c].geo.t > 0 && !results[c])
+      return fail(FIP_ERR_ARG, "null results");
+  }
   DeviceGuard g(b->cfg.device);
   if (!g.ok) return fail(FIP_ERR_CUDA, "cudaSetDevice failed");
   cudaStream_t s = (cudaStream_t)stream;
@@ -1828,7 +1970,8 @@ static int batch_run(fip_batch* b, const float* const* vis_re, const float* cons
   FIP_TRY(batch_collect(b));  // the previous call's phase times, before its events are reused
   cudaGraph_t graph = nullptr;
   FIP_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-  const int st = batch_record(b, vis_re, vis_im, B, V, nb, (int)count, first, results, cs, slots);
+  const int st = batch_record(b, seq_of, vis_re, vis_im, B, V, nb, (int)count, first, results, cs,
+                              slots);
   cudaError_t e = cudaStreamEndCapture(cs, &graph);
   if (st != FIP_OK) {
     if (graph) cudaGraphDestroy(graph);
@@ -1887,47 +2030,56 @@ static int batch_run(fip_batch* b, const float* const* vis_re, const float* cons
     FIP_CUDA(cudaStreamWaitEvent(s, b->fork, 0));
   }
   if (!slots) {
-    b->carried = std::min(2, b->carried + (int)count);
-    if (nresults) *nresults = (b->geo.t > 0) ? (size_t)ntrig : 0;
+    for (int c = 0; c < nseq; ++c) {
+      BatchSeq& q = b->seq[c];
+      q.carried = std::min(2, q.carried + per[c]);
+      if (nresults) nresults[seq_of ? c : 0] = q.geo.t > 0 ? (size_t)ntrig[c] : 0;
+      if (!seq_of) break;  // fip_batch_image: sequence 0 only
+    }
   }
   return FIP_OK;
 }
 
-int fip_batch_autotune(fip_batch* b, const float* const* vis_re, const float* const* vis_im,
-                       const float* const* B, const float* const* V, const size_t* nb,
-                       size_t count, void* stream) {
+static int batch_autotune(fip_batch* b, const int* seq_of, const float* const* vis_re,
+                          const float* const* vis_im, const float* const* B,
+                          const float* const* V, const size_t* nb, size_t count, void* stream) {
   if (!b) return fail(FIP_ERR_ARG, "null batch");
-  const int first = std::max(0, 2 - b->carried);
-  float* res = nullptr;
-  const int ntrig = std::max(0, (int)count - first);
-  if (ntrig > 0 && b->geo.t > 0) {
-    FIP_CUDA(cudaMalloc(&res, (size_t)ntrig * b->geo.u * b->geo.u * sizeof(float)));
+  if (!vis_re || !vis_im || !B || !V || !nb) return fail(FIP_ERR_ARG, "null argument");
+  const int nseq = (int)b->seq.size();
+  std::vector<float*> res(nseq, nullptr);
+  for (int c = 0; c < nseq; ++c) {
+    const BatchSeq& q = b->seq[c];
+    int per = 0;
+    for (size_t k = 0; k < count; ++k) per += (seq_of ? seq_of[k] : 0) == c;
+    const int ntrig = std::max(0, per - std::max(0, 2 - q.carried));
+    if (ntrig > 0 && q.geo.t > 0) {
+      cudaError_t e = cudaMalloc(&res[c], (size_t)ntrig * q.geo.u * q.geo.u * sizeof(float));
+      if (e != cudaSuccess) {
+        for (float* p : res)
+          if (p) cudaFree(p);
+        return fail(FIP_ERR_NOMEM, "autotune results");
+      }
+    }
   }
-  size_t nr = 0;
-  int st = fip_batch_image(b, vis_re, vis_im, B, V, nb, count, res, &nr, stream);
+  std::vector<size_t> nr(nseq, 0);
+  int st = batch_run(b, seq_of, vis_re, vis_im, B, V, nb, count, res.data(), nr.data(), stream,
+                     nullptr);
   DeviceGuard g(b->cfg.device);
   cudaStream_t s = (cudaStream_t)stream;
   if (st == FIP_OK) st = cudaStreamSynchronize(s) == cudaSuccess ? FIP_OK : fail(FIP_ERR_CUDA, "sync");
-  if (res) cudaFree(res);
+  for (float* p : res)
+    if (p) cudaFree(p);
   if (st != FIP_OK) return st;
   // The bins, bands and grids of these snapshots are now in place: time the
   // launch shapes on them.
-  const FipGeom& geo = b->geo;
   const bool precise = b->cfg.form == FIP_FORM_PRECISE;
-  const bool reduced = precise && b->cfg.vis_storage != FIP_STORE_F32;
-  const int vt = !reduced ? FIP_VIS_F32
-                          : (b->cfg.vis_storage == FIP_STORE_F16 ? FIP_VIS_F16 : FIP_VIS_BF16);
+  const int vt = batch_vis_type(b);
+  const CallLayout l = call_layout(seq_of, (int)count);
   FipGridBatch in{};
   in.count = (int)count;
-  for (size_t k = 0; k < count; ++k) {
-    in.B[k] = B[k];
-    in.V[k] = V[k];
-    in.vr[k] = reduced ? static_cast<const void*>(static_cast<char*>(b->q_re) + k * b->cfg.max_baselines * 2)
-                       : vis_re[k];
-    in.vi[k] = reduced ? static_cast<const void*>(static_cast<char*>(b->q_im) + k * b->cfg.max_baselines * 2)
-                       : vis_im[k];
-    in.vis_scale[k] = reduced ? b->q_scale + k : nullptr;
-  }
+  in.layout = 1;
+  for (size_t k = 0; k < count; ++k)
+    in.s[k] = grid_snap(b, l, (int)k, B[k], V[k], vis_re[k], vis_im[k]);
   EventPair ev;
   FIP_CUDA(cudaEventCreate(&ev.a));
   FIP_CUDA(cudaEventCreate(&ev.b));
@@ -1944,23 +2096,25 @@ int fip_batch_autotune(fip_batch* b, const float* const* vis_re, const float* co
     }
     return FIP_OK;
   };
-  {
+  for (int c = 0; c < nseq; ++c) {
+    BatchSeq& q = b->seq[c];
+    if (l.per[c] == 0) continue;
     float best = 1e30f;
-    fipfft::Plan chosen = b->fft;
+    fipfft::Plan chosen = q.fft;
     // Values per thread 8 or 16 x {joint, split, joint with a direct first pass}.
     for (int shape = 0; shape < 6; ++shape) {
       fipfft::Plan p{};
-      if (!fip_fft_plan(geo.g, p, shape & 1 ? 16 : 8)) continue;
+      if (!fip_fft_plan(q.geo.g, p, shape & 1 ? 16 : 8)) continue;
       p.split = (shape >> 1) == 1;
       p.direct = (shape >> 1) == 2;
       float ms = 0.f;
       FIP_TRY(timed(
           [&]() -> cudaError_t {
-            cudaError_t e = fip_launch_fft_cols(geo, b->grid, b->bbox, b->colbuf, b->twiddles, p,
-                                                s, (int)count, b->grid_elems, b->col_elems);
+            cudaError_t e = fip_launch_fft_cols(q.geo, q.grid, q.bbox, q.colbuf, q.twiddles, p, s,
+                                                l.per[c], q.grid_elems, q.col_elems);
             if (e != cudaSuccess) return e;
-            return fip_launch_fft_rows(geo, b->colbuf, b->bbox, b->taper, b->twiddles, p, b->pre,
-                                       s, (int)count, b->col_elems, b->n2);
+            return fip_launch_fft_rows(q.geo, q.colbuf, q.bbox, q.taper, q.twiddles, p, q.pre, s,
+                                       l.per[c], q.col_elems, q.n2);
           },
           ms));
       if (ms < best) {
@@ -1968,20 +2122,15 @@ int fip_batch_autotune(fip_batch* b, const float* const* vis_re, const float* co
         chosen = p;
       }
     }
-    b->fft = chosen;
+    q.fft = chosen;
   }
   {
     float best = 1e30f;
     int chosen = 0;
     for (int c = 1; c <= fip_grid_max_ctas_per_sm(precise ? 1 : 0); ++c) {
       float ms = 0.f;
-      FIP_TRY(timed(
-          [&]() -> cudaError_t {
-            return fip_launch_grid_batch(geo, in, vt, b->multi, b->ntiles, b->nmulti, b->entries,
-                                         b->cap, b->work, b->wcap, b->nwork, b->grid,
-                                         b->grid_elems, precise ? 1 : 0, s, c);
-          },
-          ms));
+      FIP_TRY(timed([&]() -> cudaError_t { return fip_launch_grid_batch(in, vt, precise ? 1 : 0, s, c); },
+                    ms));
       if (ms < best) {
         best = ms;
         chosen = c;
@@ -1994,16 +2143,32 @@ int fip_batch_autotune(fip_batch* b, const float* const* vis_re, const float* co
     cudaGraphExecDestroy(b->exec);
     b->exec = nullptr;
   }
-  b->carried = 0;
+  for (BatchSeq& q : b->seq) q.carried = 0;
   return FIP_OK;
 }
 
-int fip_batch_tuning(const fip_batch* b, int* fft_values_per_thread, int* fft_split,
-                     int* fft_direct, int* grid_ctas_per_sm) {
+int fip_batch_autotune(fip_batch* b, const float* const* vis_re, const float* const* vis_im,
+                       const float* const* B, const float* const* V, const size_t* nb,
+                       size_t count, void* stream) {
+  return batch_autotune(b, nullptr, vis_re, vis_im, B, V, nb, count, stream);
+}
+
+int fip_batch_autotune_sequences(fip_batch* b, const int* sequence, const float* const* vis_re,
+                                 const float* const* vis_im, const float* const* B,
+                                 const float* const* V, const size_t* nb, size_t count,
+                                 void* stream) {
+  if (!sequence) return fail(FIP_ERR_ARG, "null argument");
+  return batch_autotune(b, sequence, vis_re, vis_im, B, V, nb, count, stream);
+}
+
+int fip_batch_sequence_tuning(const fip_batch* b, int sequence, int* fft_values_per_thread,
+                              int* fft_split, int* fft_direct, int* grid_ctas_per_sm) {
   if (!b) return fail(FIP_ERR_ARG, "null batch");
-  if (fft_values_per_thread) *fft_values_per_thread = b->fft.e;
-  if (fft_split) *fft_split = b->fft.split;
-  if (fft_direct) *fft_direct = b->fft.direct;
+  if (sequence < 0 || sequence >= (int)b->seq.size()) return fail(FIP_ERR_ARG, "no such sequence");
+  const BatchSeq& q = b->seq[sequence];
+  if (fft_values_per_thread) *fft_values_per_thread = q.fft.e;
+  if (fft_split) *fft_split = q.fft.split;
+  if (fft_direct) *fft_direct = q.fft.direct;
   if (grid_ctas_per_sm)
     *grid_ctas_per_sm = b->grid_ctas_per_sm > 0
                             ? b->grid_ctas_per_sm
@@ -2011,7 +2176,14 @@ int fip_batch_tuning(const fip_batch* b, int* fft_values_per_thread, int* fft_sp
   return FIP_OK;
 }
 
+int fip_batch_tuning(const fip_batch* b, int* fft_values_per_thread, int* fft_split,
+                     int* fft_direct, int* grid_ctas_per_sm) {
+  return fip_batch_sequence_tuning(b, 0, fft_values_per_thread, fft_split, fft_direct,
+                                   grid_ctas_per_sm);
+}
+
 }  // extern "C"
+
 
 int FIpipe(float* Visreal, float* Visimag, float* Bin, float* Vin, float* result_array,
            size_t num_baselines, size_t image_size, size_t num_snapshots, float cell_size,

@@ -48,15 +48,15 @@ cudaError_t fip_launch_grid(const FipGeom& geo, const float* B, const void* vr, 
                             const FipBins& bins, float2* grid, int compensated, cudaStream_t s,
                             int ctas_per_sm = 0, const FipRawVis* raw = nullptr);
 int fip_grid_max_ctas_per_sm(int compensated);
-// One persistent gridding launch over a batch of snapshots (plus the zeroing
-// of their split tiles): snapshot k's inputs in in.*[k], its bins and grid at
-// base + k * stride, its item count nwork[k] and split-tile count nmulti[k].
-cudaError_t fip_launch_grid_batch(const FipGeom& geo, const FipGridBatch& in, int vis_type,
-                                  const unsigned* multi, size_t multi_stride,
-                                  const unsigned* nmulti, const unsigned* entries,
-                                  size_t entries_stride, const int4* work, size_t work_stride,
-                                  const unsigned* nwork, float2* grid, size_t grid_stride,
-                                  int compensated, cudaStream_t s, int ctas_per_sm = 0);
+// Zeroes the split tiles of `count` snapshots of one geometry (their grids
+// and split-tile lists at base + k * stride) before a batched gridding launch.
+cudaError_t fip_launch_zero_batch(const FipGeom& geo, const unsigned* multi, size_t multi_stride,
+                                  const unsigned* nmulti, float2* grid, size_t grid_stride,
+                                  int count, cudaStream_t s);
+// One persistent gridding launch over the work items of all the batch's
+// snapshots (in.s[k]: inputs, bins, grid and geometry of snapshot k).
+cudaError_t fip_launch_grid_batch(const FipGridBatch& in, int vis_type, int compensated,
+                                  cudaStream_t s, int ctas_per_sm = 0);
 // values_per_thread: 8 or 16 (0 = the default for the length).
 bool fip_fft_plan(int g, fipfft::Plan& p, int values_per_thread = 0);
 // Band-pruned inverse FFT: column pass (band grid -> colbuf [G/2+1][N]) and

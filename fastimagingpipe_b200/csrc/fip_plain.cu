@@ -767,18 +767,10 @@ __global__ void __launch_bounds__(kThreads) k_grid(const float* __restrict__ B, 
 }
 
 // Persistent gridder over the work items of a batch of snapshots (one launch
-// for the batch): snapshot k reads in.*[k] and its bins and grid at
-// base + k * stride.
+// for the batch, whatever their image sizes): snapshot k's inputs, bins,
+// grid and geometry are in.s[k].
 template <int VT, bool COMP>
-__global__ void __launch_bounds__(kThreads) k_grid_batch(const FipGridBatch in, float scale,
-                                                         int g, int hp, int tiles_c, int layout,
-                                                         const unsigned* __restrict__ entries,
-                                                         size_t entries_stride,
-                                                         const int4* __restrict__ work,
-                                                         size_t work_stride,
-                                                         const unsigned* __restrict__ nwork,
-                                                         float2* __restrict__ grid,
-                                                         size_t grid_stride) {
+__global__ void __launch_bounds__(kThreads) k_grid_batch(const __grid_constant__ FipGridBatch in) {
   extern __shared__ float4 s_raw[];
   __shared__ unsigned s_first[FIP_MAX_BATCH + 1];  // prefix of the snapshots' item counts
   GridSmem& S = *reinterpret_cast<GridSmem*>(s_raw);
@@ -788,7 +780,7 @@ __global__ void __launch_bounds__(kThreads) k_grid_batch(const FipGridBatch in, 
     unsigned acc = 0;
     for (int k = 0; k < in.count; ++k) {
       s_first[k] = acc;
-      acc += nwork[k];
+      acc += *in.s[k].nwork;
     }
     s_first[in.count] = acc;
   }
@@ -798,11 +790,12 @@ __global__ void __launch_bounds__(kThreads) k_grid_batch(const FipGridBatch in, 
   int k = 0;
   for (unsigned w = blockIdx.x; w < total; w += gridDim.x) {
     while (s_first[k + 1] <= w) ++k;  // items are visited in increasing order
-    const float inten = plane_intensity(in.V[k]);
-    const float vis_scale = in.vis_scale[k] ? *in.vis_scale[k] : 1.0f;
-    grid_item<VT, COMP>(S, s_cre, s_cim, in.B[k], in.vr[k], in.vi[k], vis_scale, inten, scale,
-                        g, hp, tiles_c, layout, entries + k * entries_stride,
-                        work[k * work_stride + (w - s_first[k])], grid + k * grid_stride);
+    const FipGridSnap& sn = in.s[k];
+    const float inten = plane_intensity(sn.V);
+    const float vis_scale = sn.vis_scale ? *sn.vis_scale : 1.0f;
+    grid_item<VT, COMP>(S, s_cre, s_cim, sn.B, sn.vr, sn.vi, vis_scale, inten, sn.scale, sn.g,
+                        sn.hp, sn.tiles_c, in.layout, sn.entries, sn.work[w - s_first[k]],
+                        sn.grid);
   }
 }
 
@@ -2070,18 +2063,20 @@ cudaError_t fip_launch_grid(const FipGeom& geo, const float* B, const void* vr, 
   return cudaGetLastError();
 }
 
-cudaError_t fip_launch_grid_batch(const FipGeom& geo, const FipGridBatch& in, int vis_type,
-                                  const unsigned* multi, size_t multi_stride,
-                                  const unsigned* nmulti, const unsigned* entries,
-                                  size_t entries_stride, const int4* work, size_t work_stride,
-                                  const unsigned* nwork, float2* grid, size_t grid_stride,
-                                  int compensated, cudaStream_t s, int ctas_per_sm) {
+cudaError_t fip_launch_zero_batch(const FipGeom& geo, const unsigned* multi, size_t multi_stride,
+                                  const unsigned* nmulti, float2* grid, size_t grid_stride,
+                                  int count, cudaStream_t s) {
+  if (count < 1 || count > 65535) return cudaErrorInvalidValue;
+  k_zero_tiles<<<dim3(sm_count(), count), kThreads, 0, s>>>(multi, nmulti, geo.tiles_c, geo.g,
+                                                            geo.hp, geo.layout, grid,
+                                                            multi_stride, grid_stride);
+  return cudaGetLastError();
+}
+
+cudaError_t fip_launch_grid_batch(const FipGridBatch& in, int vis_type, int compensated,
+                                  cudaStream_t s, int ctas_per_sm) {
   if (in.count < 1 || in.count > FIP_MAX_BATCH) return cudaErrorInvalidValue;
-  const float scale = geo.cell * (float)(size_t)geo.g;
   const int sms = sm_count();
-  k_zero_tiles<<<dim3(sms, in.count), kThreads, 0, s>>>(multi, nmulti, geo.tiles_c, geo.g,
-                                                         geo.hp, geo.layout, grid, multi_stride,
-                                                         grid_stride);
   const size_t smem = sizeof(GridSmem) + (compensated ? 2 * FIP_GTILE * kTS * sizeof(float) : 0);
   const int most = fip_grid_max_ctas_per_sm(compensated);
   const int blocks = sms * (ctas_per_sm > 0 ? min(ctas_per_sm, most) : most);
@@ -2089,9 +2084,7 @@ cudaError_t fip_launch_grid_batch(const FipGeom& geo, const FipGridBatch& in, in
   do {                                                                                         \
     auto kern = k_grid_batch<VT, C>;                                                           \
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);        \
-    kern<<<blocks, kThreads, smem, s>>>(in, scale, geo.g, geo.hp, geo.tiles_c, geo.layout,     \
-                                        entries, entries_stride, work, work_stride, nwork,     \
-                                        grid, grid_stride);                                    \
+    kern<<<blocks, kThreads, smem, s>>>(in);                                                   \
   } while (0)
   if (vis_type == FIP_VIS_F32) {
     if (compensated) FIP_GRID_CASE(FIP_VIS_F32, true); else FIP_GRID_CASE(FIP_VIS_F32, false);

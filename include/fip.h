@@ -316,6 +316,34 @@ int fip_batch_autotune(fip_batch* b, const float* const* vis_re, const float* co
                        size_t count, void* stream);
 int fip_batch_tuning(const fip_batch* b, int* fft_values_per_thread, int* fft_split,
                      int* fft_direct, int* grid_ctas_per_sm);
+
+/* ---- Batches of several sequences (mixed image sizes) -------------------
+ * A batch of nseq (1..8) sequences, sequence c with configuration cfgs[c]
+ * (its own image size, cell, unit size and max_baselines; form, storage and
+ * device shared): each call images up to 64 snapshots, at most max_snapshots
+ * of any one sequence, with one persistent gridding launch for all of them
+ * and one batched transform per sequence, in one CUDA graph.  Snapshot k
+ * belongs to sequence sequence[k] (its snapshots in call order); each
+ * sequence keeps its own last two images, and its tLISI matrices (U_c * U_c
+ * floats each, in order) go to results[c], their number to nresults[c].
+ * fip_batch_image on such a batch images everything into sequence 0;
+ * fip_batch_create is the one-sequence case.  Asynchronous on `stream`. */
+int fip_batch_create_sequences(fip_batch** out, const fip_imager_config* cfgs, size_t nseq,
+                               size_t max_snapshots);
+int fip_batch_image_sequences(fip_batch* b, const int* sequence, const float* const* vis_re,
+                              const float* const* vis_im, const float* const* B,
+                              const float* const* V, const size_t* nb, size_t count,
+                              float* const* results, size_t* nresults, void* stream);
+/* Autotuner over a representative mixed call: each sequence's transform
+ * shape on its own snapshots, the gridder's CTAs per SM on the whole launch;
+ * synchronous; resets every sequence. */
+int fip_batch_autotune_sequences(fip_batch* b, const int* sequence, const float* const* vis_re,
+                                 const float* const* vis_im, const float* const* B,
+                                 const float* const* V, const size_t* nb, size_t count,
+                                 void* stream);
+/* The launch shapes of sequence `sequence` (fip_batch_tuning: sequence 0). */
+int fip_batch_sequence_tuning(const fip_batch* b, int sequence, int* fft_values_per_thread,
+                              int* fft_split, int* fft_direct, int* grid_ctas_per_sm);
 /* Phase timing of batched calls (no counterpart in the reference): when
  * enabled, each call's graph carries timing events at its phase boundaries
  * and the device time of every phase is summed: 0 per-snapshot preparation

@@ -144,3 +144,81 @@ def test_batch_rejects_bad_arguments(cuda):
             b.image([z] * 3, [z] * 3, [z] * 3, [z] * 3, [5] * 3, z)  # count > max_snapshots
         with pytest.raises(fip.FipError):
             b.image([z], [z], [z], [z], [11], z)  # nb > max_baselines
+
+
+def mfs_n(n, n_snap, seed):
+    return synthetic.config_batching(n, n_snap=n_snap, n_chan=2, n_ant=64, radius_m=1500.0,
+                                     core_fraction=0.0, transient_snapshot=2, seed=seed)
+
+
+@pytest.mark.parametrize("kw", [{}, dict(form=fip.FORM_PRECISE, vis_storage=fip.STORE_F16)])
+@pytest.mark.parametrize("calls", [[11], [4, 7]])
+def test_mixed_sizes_in_one_batch(cuda, kw, calls):
+    """Two sequences of different image sizes (512^2 and 256^2, the cell scaled
+    for the same field) imaged together: one persistent gridding launch per
+    call over both; each sequence's sliding-window tLISI must equal its
+    per-snapshot path's."""
+    import torch
+    big, small = mfs_n(512, 6, 5), mfs_n(256, 5, 7)
+    db, ds = dev(big, cuda), dev(small, cuda)
+    ref = [per_snapshot(big, db, cuda, **kw), per_snapshot(small, ds, cuda, **kw)]
+    # Interleaved call order: 512, 256, 512, 256, ...
+    order = []
+    ib = is_ = 0
+    while ib < len(big) or is_ < len(small):
+        if ib < len(big):
+            order.append((0, ib))
+            ib += 1
+        if is_ < len(small):
+            order.append((1, is_))
+            is_ += 1
+    seqs = [big, small]
+    devs = [db, ds]
+    spec = [(s[0].image_size, max(x.nb for x in s), s[0].cell_size, s[0].unit_size) for s in seqs]
+    us = [x[0] // x[3] for x in spec]
+    res = [torch.zeros((len(s), u * u), device=cuda) for s, u in zip(seqs, us)]
+    got = [0, 0]
+    with fip.Batch.of_sequences(spec, 6, **kw) as b:
+        tunes = b.autotune_sequences([c for c, _ in order[:6]],
+                                     *[[devs[c][i][key] for c, i in order[:6]]
+                                       for key in ("vis_re", "vis_im", "B", "V")],
+                                     [seqs[c][i].nb for c, i in order[:6]])
+        assert len(tunes) == 2
+        k = 0
+        for n_call in calls:
+            part = order[k:k + n_call]
+            k += n_call
+            counts = b.image_sequences(
+                [c for c, _ in part],
+                *[[devs[c][i][key] for c, i in part] for key in ("vis_re", "vis_im", "B", "V")],
+                [seqs[c][i].nb for c, i in part],
+                [res[0][got[0]:], res[1][got[1]:]])
+            got = [g + n for g, n in zip(got, counts)]
+        torch.cuda.synchronize()
+        b.check()
+        assert b.kernel_launches > 0
+    assert got == [len(big) - 2, len(small) - 2]
+    for c in range(2):
+        out = res[c][:got[c]].cpu().numpy().reshape(got[c], us[c], us[c])
+        assert np.abs(out - ref[c]).max() <= 1e-5
+
+
+def test_sequences_reject_bad_arguments(cuda):
+    import torch
+    spec = [(64, 10, 1e-3, 16), (128, 10, 5e-4, 16)]
+    with pytest.raises(fip.FipError):
+        fip.Batch.of_sequences(spec * 5, 2)  # more than 8 sequences
+    z = torch.zeros(64, device=cuda)
+    with fip.Batch.of_sequences(spec, 2) as b:
+        with pytest.raises(fip.FipError):
+            b.image_sequences([2], [z], [z], [z], [z], [5], [z, z])  # no such sequence
+        with pytest.raises(fip.FipError):
+            b.image_sequences([1, 1, 1], [z] * 3, [z] * 3, [z] * 3, [z] * 3, [5] * 3,
+                              [z, z])  # more than max_snapshots of one sequence
+    lib = fip.lib()
+    import ctypes
+    cfgs = (fip.ImagerConfig * 2)(fip.ImagerConfig(64, 10, 16, 1e-3, fip.FORM_PLAIN, 0, 0, 0),
+                                  fip.ImagerConfig(128, 10, 16, 5e-4, fip.FORM_PRECISE, 0, 0, 0))
+    h = ctypes.c_void_p()
+    assert lib.fip_batch_create_sequences(ctypes.byref(h), ctypes.cast(cfgs, ctypes.c_void_p),
+                                          2, 2) == 1  # forms differ
