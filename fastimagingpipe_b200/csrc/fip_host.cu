@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -273,7 +274,8 @@ struct fip_imager {
   size_t device_bytes = 0;
   cudaStream_t stream = nullptr;     // compute stream of the host-buffer path
   cudaStream_t copy_stream = nullptr;
-  cudaEvent_t ev_copied[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ev_copied[3] = {nullptr, nullptr, nullptr};  // host path: snapshot k's B
+  cudaEvent_t ev_vis[3] = {nullptr, nullptr, nullptr};     // host path: its visibilities
   cudaEvent_t ev_used[3] = {nullptr, nullptr, nullptr};
   // Pixel-mapping stream (overlaps gridding + FFT), at the lowest priority:
   // the lanes' latency-bound stages take SM slots first and the
@@ -392,6 +394,7 @@ static void imager_free(fip_imager* im) {
     if (p) cudaFreeHost(p);
   for (int k = 0; k < 3; ++k) {
     if (im->ev_copied[k]) cudaEventDestroy(im->ev_copied[k]);
+    if (im->ev_vis[k]) cudaEventDestroy(im->ev_vis[k]);
     if (im->ev_used[k]) cudaEventDestroy(im->ev_used[k]);
   }
   for (int k = 0; k < kMaxPending; ++k)
@@ -501,6 +504,7 @@ int fip_imager_create(fip_imager** out, const fip_imager_config* cfg) {
     for (int e = 0; e < 2; ++e) FIP_ALLOC(cudaEventCreate(&im->timer.ev[k][e]));
   for (int k = 0; k < 3; ++k) {
     FIP_ALLOC(cudaEventCreateWithFlags(&im->ev_copied[k], cudaEventDisableTiming));
+    FIP_ALLOC(cudaEventCreateWithFlags(&im->ev_vis[k], cudaEventDisableTiming));
     FIP_ALLOC(cudaEventCreateWithFlags(&im->ev_used[k], cudaEventDisableTiming));
   }
   if (cfg->reproject != 0 && cfg->reproject != 1) return cleanup(fail(FIP_ERR_ARG, "unknown reproject mode"));
@@ -606,7 +610,8 @@ static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const f
                                float* image_max, cudaStream_t s, bool fork_targets,
                                bool targets_ready = false, cudaEvent_t targets_ev = nullptr,
                                bool force_scatter = false, const FipRawVis* raw = nullptr,
-                               const FipFuse* fuse = nullptr) {
+                               const FipFuse* fuse = nullptr,
+                               const std::function<int(cudaEvent_t*)>* before_grid = nullptr) {
   const FipGeom& geo = im->geo;
   if (nb > im->cfg.max_baselines) return fail(FIP_ERR_ARG, "nb exceeds the imager's capacity");
   if (nb == 0) return fail(FIP_ERR_ARG, "nb must be positive");
@@ -619,18 +624,6 @@ static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const f
   // load (or inside the reduced-storage conversion).
   int vt = raw ? FIP_VIS_RAW : FIP_VIS_F32;
   int k;
-  if (precise && im->cfg.vis_storage != FIP_STORE_F32) {
-    vt = im->cfg.vis_storage == FIP_STORE_F16 ? FIP_VIS_F16 : FIP_VIS_BF16;
-    k = stage_begin(im, ST_GRID, s);
-    if (raw)
-      FIP_CUDA(fip_launch_quantize_raw(*raw, nb, vt, L.q_re, L.q_im, L.q_scale, s));
-    else
-      FIP_CUDA(fip_launch_quantize(vr, vi, nb, vt, L.q_re, L.q_im, L.q_scale, s));
-    stage_end(im, k, s);
-    im->launches += 3;
-    gvr = L.q_re;
-    gvi = L.q_im;
-  }
   // force_scatter: the snapshot's geometry lies outside the gather's domain
   // (checked on the host where V is a host array): the reference's scheme.
   const bool gather = im->cfg.reproject == 0 && !force_scatter;
@@ -654,6 +647,25 @@ static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const f
   k = stage_begin(im, ST_BIN, s);
   FIP_CUDA(fip_launch_bin(geo, B, (int)nb, L.bins, s));
   stage_end(im, k, s);
+  // The host path stages the visibilities while the binning runs: the
+  // gridding (and the reduced-storage conversion) wait for them.
+  if (before_grid && *before_grid) {
+    cudaEvent_t ready = nullptr;
+    FIP_TRY((*before_grid)(&ready));
+    if (ready) FIP_CUDA(cudaStreamWaitEvent(s, ready, 0));
+  }
+  if (precise && im->cfg.vis_storage != FIP_STORE_F32) {
+    vt = im->cfg.vis_storage == FIP_STORE_F16 ? FIP_VIS_F16 : FIP_VIS_BF16;
+    k = stage_begin(im, ST_GRID, s);
+    if (raw)
+      FIP_CUDA(fip_launch_quantize_raw(*raw, nb, vt, L.q_re, L.q_im, L.q_scale, s));
+    else
+      FIP_CUDA(fip_launch_quantize(vr, vi, nb, vt, L.q_re, L.q_im, L.q_scale, s));
+    stage_end(im, k, s);
+    im->launches += 3;
+    gvr = L.q_re;
+    gvi = L.q_im;
+  }
   k = stage_begin(im, ST_GRID, s);
   FIP_CUDA(fip_launch_grid(geo, B, gvr, gvi, vt, L.q_scale, V, (int)nb, L.bins, L.grid,
                            precise ? 1 : 0, s, im->grid_ctas_per_sm, raw));
@@ -707,17 +719,19 @@ static int image_on_lane(fip_imager* im, int k, const float* vr, const float* vi
                          const float* B, const float* V, size_t nb, float* image,
                          float* image_max, cudaStream_t s, cudaEvent_t after,
                          bool targets_ready = false, bool force_scatter = false,
-                         const FipFuse* fuse = nullptr) {
+                         const FipFuse* fuse = nullptr,
+                         const std::function<int(cudaEvent_t*)>* before_grid = nullptr) {
   if (im->lanes == 1 || im->timer.on) {
     FIP_CUDA(cudaStreamWaitEvent(s, after, 0));
     return image_snapshot_impl(im, im->lane[k % im->lanes], vr, vi, B, V, nb, image, image_max,
-                               s, true, false, nullptr, force_scatter, nullptr, fuse);
+                               s, true, false, nullptr, force_scatter, nullptr, fuse,
+                               before_grid);
   }
   Lane& L = im->lane[k % im->lanes];
   FIP_CUDA(cudaStreamWaitEvent(L.stream, after, 0));
   FIP_TRY(image_snapshot_impl(im, L, vr, vi, B, V, nb, image, image_max, L.stream, false,
                               targets_ready, targets_ready ? L.ev_targets : nullptr,
-                              force_scatter, nullptr, fuse));
+                              force_scatter, nullptr, fuse, before_grid));
   FIP_CUDA(cudaEventRecord(L.ev_done, L.stream));
   return FIP_OK;
 }
@@ -955,8 +969,15 @@ int fip_pipe_host(fip_imager* im, const float* vr, const float* vi, const float*
   // only V, so with concurrent lanes it starts on every lane while the host
   // still stages the visibilities.
   std::memcpy(im->h_V, V, 27 * sizeof(float));
+  FIP_CUDA(cudaMemcpyAsync(im->d_V, im->h_V, 27 * sizeof(float), cudaMemcpyHostToDevice, cs));
+  const bool early = targets_ahead(im);
+  if (early) {
+    FIP_CUDA(cudaEventRecord(im->ev_start, cs));
+    FIP_TRY(launch_targets_ahead(im, im->d_V, im->ev_start));
+  }
   // Snapshots whose plane-to-sky map leaves the gather's domain (very wide,
   // strongly tilted fields) reproject with the reference's scatter instead.
+  // Checked on the host while the GPU already runs the pixel mappings.
   bool scatter[3] = {false, false, false};
   if (im->cfg.reproject == 0)
     for (int k = 0; k < 3; ++k)
@@ -967,29 +988,30 @@ int fip_pipe_host(fip_imager* im, const float* vr, const float* vi, const float*
   const bool fused = fuse_ok(im) && !scatter[0] && !scatter[1] && !scatter[2];
   if (fused) FIP_CUDA(cudaMemsetAsync(im->fuse_count, 0,
                                       fip_trigger_fuse_counts(im->geo) * sizeof(unsigned), cs));
-  FIP_CUDA(cudaMemcpyAsync(im->d_V, im->h_V, 27 * sizeof(float), cudaMemcpyHostToDevice, cs));
-  const bool early = targets_ahead(im);
-  if (early) {
-    FIP_CUDA(cudaEventRecord(im->ev_start, cs));
-    FIP_TRY(launch_targets_ahead(im, im->d_V, im->ev_start));
-  }
-  // Per snapshot: host copy into pinned slot k (CPU), async H2D on the copy
-  // stream, then the snapshot's lane images it while the CPU stages k+1.
+  // Per snapshot: host copy of its B into pinned slot k (CPU), async H2D on
+  // the copy stream, the snapshot's lane enqueued up to its binning; then
+  // the same for its visibilities, which only the gridding waits for.  The
+  // lanes thus start binning while the CPU still stages.
   for (int k = 0; k < 3; ++k) {
     float* hs = im->h_snap + (size_t)k * 4 * nb;
     float* ds = im->d_snap + (size_t)k * 4 * nb;
-    const CopyPool::Seg segs[3] = {{hs, B + (size_t)k * nb * 2, nb * 2 * sizeof(float)},
-                                   {hs + 2 * nb, vr + (size_t)k * nb, nb * sizeof(float)},
-                                   {hs + 3 * nb, vi + (size_t)k * nb, nb * sizeof(float)}};
-    CopyPool::get().copy(segs, 3);
-    float* dB = ds;
-    float* dvr = ds + 2 * nb;
-    float* dvi = ds + 3 * nb;
-    float* dV = im->d_V + (size_t)k * 9;
-    FIP_CUDA(cudaMemcpyAsync(ds, hs, 4 * nb * sizeof(float), cudaMemcpyHostToDevice, cs));
+    const CopyPool::Seg seg_b = {hs, B + (size_t)k * nb * 2, nb * 2 * sizeof(float)};
+    CopyPool::get().copy(&seg_b, 1);
+    FIP_CUDA(cudaMemcpyAsync(ds, hs, 2 * nb * sizeof(float), cudaMemcpyHostToDevice, cs));
     FIP_CUDA(cudaEventRecord(im->ev_copied[k], cs));
-    FIP_TRY(image_on_lane(im, k, dvr, dvi, dB, dV, nb, im->images[k], im->maxima + k, s,
-                          im->ev_copied[k], early, scatter[k], fused ? &fz : nullptr));
+    const std::function<int(cudaEvent_t*)> stage_vis = [&, k, hs, ds](cudaEvent_t* ready) -> int {
+      const CopyPool::Seg segs[2] = {{hs + 2 * nb, vr + (size_t)k * nb, nb * sizeof(float)},
+                                     {hs + 3 * nb, vi + (size_t)k * nb, nb * sizeof(float)}};
+      CopyPool::get().copy(segs, 2);
+      FIP_CUDA(cudaMemcpyAsync(ds + 2 * nb, hs + 2 * nb, 2 * nb * sizeof(float),
+                               cudaMemcpyHostToDevice, cs));
+      FIP_CUDA(cudaEventRecord(im->ev_vis[k], cs));
+      *ready = im->ev_vis[k];
+      return FIP_OK;
+    };
+    FIP_TRY(image_on_lane(im, k, ds + 2 * nb, ds + 3 * nb, ds, im->d_V + (size_t)k * 9, nb,
+                          im->images[k], im->maxima + k, s, im->ev_copied[k], early, scatter[k],
+                          fused ? &fz : nullptr, &stage_vis));
   }
   for (int k = 0; k < 3; ++k) FIP_TRY(wait_lane(im, k, s));
   im->last_lane = 2 % im->lanes;
