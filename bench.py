@@ -266,8 +266,17 @@ def run_batching(fip, synthetic, torch, dev, local, per_size=16, calls=2, distin
         torch.cuda.synchronize()
         b.check()
         ms = ev0.elapsed_time(ev1)
+        launches = b.kernel_launches - l0
+        # Phase breakdown of the same calls (timing events in the graph).
+        b.set_profiling(True)
+        b.reset()
+        run_all()
+        torch.cuda.synchronize()
+        ph = b.phase_times()
+        b.set_profiling(False)
         out[name] = {"value": total / (ms / 1e3), "unit": UNIT, "snapshots": total,
-                     "gpu_launches": b.kernel_launches - l0,
+                     "gpu_launches": launches,
+                     "phases_ms_per_snapshot": {k: v / total for k, (v, c) in ph.items()},
                      "hbm_gb": b.device_bytes / 2**30,
                      "config": f"{total} snapshots x 8 channels (130-150 MHz), 0-30 % flagged, "
                                f"half 4096^2 / half 2048^2 interleaved in each call, tile 32, "

@@ -542,9 +542,13 @@ constexpr int kTS = FIP_GTILE + 8;  // padded row stride: 4 tap rows x 8 columns
 struct GridSmem {
   float re[FIP_GTILE * kTS], im[FIP_GTILE * kTS];
   float wr[FIP_GCHUNK], wi[FIP_GCHUNK];
-  int row0[FIP_GCHUNK];   // r1 of the first tap row (negated when mirrored)
-  int col0[FIP_GCHUNK];   // half-plane column of the first kept tap column
-  int meta[FIP_GCHUNK];   // nr | nc << 4 | mirrored << 8
+  // The entry's taps inside the tile: rows ia in [ia_lo, ia_hi), columns ib
+  // in [ib_lo, ib_hi) of its footprint, as ia_lo | ia_hi << 4 | ib_lo << 8 |
+  // ib_hi << 12 | (rows run upwards) << 16; cell0 is the tile cell of tap
+  // (ia_lo, ib_lo).  An empty span has ib_lo == ib_hi.
+  int span[FIP_GCHUNK];
+  int cell0[FIP_GCHUNK];
+  int r1[FIP_GCHUNK];  // r1 of tap row ia_lo (grids of one tile row only)
   float k1[FIP_GCHUNK][9], k2[FIP_GCHUNK][9];  // stride 9: conflict-free both ways
   float bound[kThreads / 32];
 };
@@ -614,18 +618,39 @@ __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_ci
     S.wi[q] = mir ? -0.5f * wi : 0.5f * wi;
     bound += 0.5f * fmaxf(fabsf(wr), fabsf(wi));
     const int nr = f.a1 - f.a0 + 1, nc = c1 - c0 + 1;
-    S.row0[q] = mir ? -f.a0 : f.a0;
-    S.col0[q] = c0;
-    S.meta[q] = nr | (nc << 4) | (mir << 8);
+    // Tap row ia is grid row wrap(r1), r1 = a0 + ia (mirrored: -(a0 + ia)).
+    // Unless the grid is one tile high, no tile holds the wrap point inside
+    // it (it falls on a tile edge), so a tile's rows of the footprint are
+    // one run of ia along which the tile row moves by +1 (mirrored: -1).
+    int ia_lo = 9, ia_hi = 0, lr_first = 0;
+#pragma unroll
+    for (int a = 0; a < 9; ++a)
+      if (a < nr) {
+        const int lr = wrap_row(mir ? -(f.a0 + a) : f.a0 + a, g) - trow0;
+        if ((unsigned)lr < (unsigned)FIP_GTILE) {
+          if (a < ia_lo) {
+            ia_lo = a;
+            lr_first = lr;
+          }
+          ia_hi = a + 1;
+        }
+      }
+    const int ib_lo = max(0, tcol0 - c0), ib_hi = min(nc, tcol0 + FIP_GTILE - c0);
+    const bool empty = ia_lo >= ia_hi || ib_lo >= ib_hi;
+    S.span[q] = empty ? 0
+                      : ia_lo | (ia_hi << 4) | (ib_lo << 8) | (ib_hi << 12) | (mir << 16);
+    S.cell0[q] = lr_first * kTS + (c0 + ib_lo - tcol0);
+    S.r1[q] = mir ? -(f.a0 + ia_lo) : f.a0 + ia_lo;
     const float ihs = 1 / static_cast<float>(FIP_SUPPORT / 2);
 #pragma unroll
     for (int a = 0; a < 9; ++a)
-      if (a < nr) S.k1[q][a] = fipref::es((static_cast<float>(f.a0 + a) - f.p1) * ihs);
+      if (a >= ia_lo && a < ia_hi)
+        S.k1[q][a] = fipref::es((static_cast<float>(f.a0 + a) - f.p1) * ihs);
     // Column taps in half-plane order c0..c1: original r2 = c (direct) or
     // -c (mirrored).
 #pragma unroll
     for (int b = 0; b < 9; ++b)
-      if (b < nc) {
+      if (b >= ib_lo && b < ib_hi) {
         // Direct copy: column c holds tap r2 = c, or r2 = -G/2 on the
         // Nyquist column (r2 never reaches +G/2, FIPkernels.cu:203).
         const int c = c0 + b;
@@ -673,38 +698,61 @@ __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_ci
     hi = __float_as_int(hf + 12582912.0f) - 0x4B400000;  // |hf| < 2^22: exact
     lo = __float_as_uint(lf + 8388608.0f) - 0x4B000000u;  // round to integer
   };
-  // Phase 2.
+  // Phase 2: a warp per entry, its in-tile taps over the lanes (a column
+  // per lane, 32 / columns rows per step); each lane's column factor is
+  // folded into the weights once, so a tap is one product per component.
   for (int q = warp; q < cnt; q += kThreads / 32) {
-    const int meta = S.meta[q];
-    const int nr = meta & 15, nc = (meta >> 4) & 15, mir = (meta >> 8) & 1;
-    const int map = s_lane_map[nc][lane];  // (lane / nc) | (lane % nc) << 8 | (32 / nc) << 16
-    const int ia0 = map & 255, ib = (map >> 8) & 255, per = map >> 16;  // tap rows per warp step
-    if (ia0 >= per) continue;
-    const float wr = S.wr[q], wi = S.wi[q];
-    const int rbase = S.row0[q], col = S.col0[q] + ib;
-    const int lc = col - tcol0;
-    if ((unsigned)lc >= (unsigned)FIP_GTILE) continue;
-    const float k2 = S.k2[q][ib];
-    for (int ia = ia0; ia < nr; ia += per) {
-      const int row = wrap_row(mir ? rbase - ia : rbase + ia, g);
-      const int lr = row - trow0;
-      if ((unsigned)lr >= (unsigned)FIP_GTILE) continue;
-      const float kval = S.k1[q][ia] * k2;
-      const float cr = wr * kval, ci = wi * kval;
-      const int cell = lr * kTS + lc;
-      if (!COMP) {
-        const int qr = __float2int_rn(cr * fx), qi = __float2int_rn(ci * fx);
-        if (qr) atomicAdd(&s_qre[cell], qr);
-        if (qi) atomicAdd(&s_qim[cell], qi);
-      } else {
+    const int span = S.span[q];
+    const int ia_lo = span & 15, ia_hi = (span >> 4) & 15;
+    const int ib_lo = (span >> 8) & 15, ncw = ((span >> 12) & 15) - ib_lo;
+    const int map = s_lane_map[ncw][lane];  // (lane / n) | (lane % n) << 8 | (32 / n) << 16
+    const int ia0 = map & 255, ibo = (map >> 8) & 255, per = map >> 16;  // rows per warp step
+    if (ia0 >= per) continue;  // idle lane, or an empty span (per == 0)
+    const float k2 = S.k2[q][ib_lo + ibo];
+    const float wrk = S.wr[q] * k2, wik = S.wi[q] * k2;
+    const int dstep = (span >> 16) & 1 ? -kTS : kTS;  // tile-row step per tap row
+    int cell = S.cell0[q] + ibo + ia0 * dstep;
+    const int cstep = per * dstep;
+    if (g <= FIP_GTILE) {
+      // One tile row holds the whole grid: the wrap point may lie inside the
+      // footprint, so each tap row is wrapped on its own.
+      const int r1f = S.r1[q], dir = (span >> 16) & 1 ? -1 : 1;
+      const int lcb = S.cell0[q] - (wrap_row(r1f, g) - trow0) * kTS + ibo;
+      for (int ia = ia_lo + ia0; ia < ia_hi; ia += per) {
+        const int c = (wrap_row(r1f + (ia - ia_lo) * dir, g) - trow0) * kTS + lcb;
+        const float k1 = S.k1[q][ia];
+        if (!COMP) {
+          atomicAdd(&s_qre[c], __float2int_rn(wrk * fx * k1));
+          atomicAdd(&s_qim[c], __float2int_rn(wik * fx * k1));
+        } else {
+          int hr, hi;
+          unsigned lr2, li2;
+          limbs(wrk * k1, hr, lr2);
+          limbs(wik * k1, hi, li2);
+          atomicAdd(&s_qre[c], hr);
+          atomicAdd(&s_lre[c], lr2);
+          atomicAdd(&s_qim[c], hi);
+          atomicAdd(&s_lim[c], li2);
+        }
+      }
+    } else if (!COMP) {
+      const float wrf = wrk * fx, wif = wik * fx;
+      for (int ia = ia_lo + ia0; ia < ia_hi; ia += per, cell += cstep) {
+        const float k1 = S.k1[q][ia];
+        atomicAdd(&s_qre[cell], __float2int_rn(wrf * k1));
+        atomicAdd(&s_qim[cell], __float2int_rn(wif * k1));
+      }
+    } else {
+      for (int ia = ia_lo + ia0; ia < ia_hi; ia += per, cell += cstep) {
+        const float k1 = S.k1[q][ia];
         int hr, hi;
         unsigned lr2, li2;
-        limbs(cr, hr, lr2);
-        limbs(ci, hi, li2);
-        if (hr) atomicAdd(&s_qre[cell], hr);
-        if (lr2) atomicAdd(&s_lre[cell], lr2);
-        if (hi) atomicAdd(&s_qim[cell], hi);
-        if (li2) atomicAdd(&s_lim[cell], li2);
+        limbs(wrk * k1, hr, lr2);
+        limbs(wik * k1, hi, li2);
+        atomicAdd(&s_qre[cell], hr);
+        atomicAdd(&s_lre[cell], lr2);
+        atomicAdd(&s_qim[cell], hi);
+        atomicAdd(&s_lim[cell], li2);
       }
     }
   }
