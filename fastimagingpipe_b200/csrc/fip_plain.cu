@@ -5,10 +5,12 @@
 // reproduces the reference's FP32 arithmetic (fip_refmath.cuh).  Data
 // movement is B200-native:
 //   * gridding bins every visibility by 64x64 tile of the Hermitian half-plane
-//     uv grid, prefetches each work item's visibilities into shared memory,
-//     accumulates the tile there and commits it once (plain stores for tiles
-//     owned by one work item, vector reductions for the few dense tiles split
-//     over several); only tiles inside the occupied uv band are written;
+//     uv grid; a thread per visibility of a work item takes its footprint
+//     and kernel values into registers and adds its in-tile taps into the
+//     tile in shared memory (int32 fixed point), which is committed once
+//     (plain stores for tiles owned by one work item, vector reductions for
+//     the few dense tiles split over several); only tiles inside the
+//     occupied uv band are written;
 //   * the 2-D inverse FFT is band-pruned: column transforms run only over the
 //     occupied half-plane columns and keep only the N needed outputs; row
 //     transforms pack two real image rows into one complex transform and
@@ -537,47 +539,125 @@ __device__ __forceinline__ float load_vis(const void* p, int v) {
   return __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(p)[v]);
 }
 
-// Shared-memory layout of one gridding work item.
+// Shared-memory layout of one gridding work item: the tile (int32 fixed
+// point) and the bound reduction; the precision form adds the tile's low
+// limbs.
 constexpr int kTS = FIP_GTILE + 8;  // padded row stride: 4 tap rows x 8 columns hit 32 banks
 struct GridSmem {
   float re[FIP_GTILE * kTS], im[FIP_GTILE * kTS];
-  float wr[FIP_GCHUNK], wi[FIP_GCHUNK];
-  // The entry's taps inside the tile: rows ia in [ia_lo, ia_hi), columns ib
-  // in [ib_lo, ib_hi) of its footprint, as ia_lo | ia_hi << 4 | ib_lo << 8 |
-  // ib_hi << 12 | (rows run upwards) << 16; cell0 is the tile cell of tap
-  // (ia_lo, ib_lo).  An empty span has ib_lo == ib_hi.
-  int span[FIP_GCHUNK];
-  int cell0[FIP_GCHUNK];
-  int r1[FIP_GCHUNK];  // r1 of tap row ia_lo (grids of one tile row only)
-  float k1[FIP_GCHUNK][9], k2[FIP_GCHUNK][9];  // stride 9: conflict-free both ways
   float bound[kThreads / 32];
 };
+// Dynamic shared memory of a gridding CTA.
+__host__ __device__ constexpr size_t grid_smem_bytes(bool comp) {
+  return sizeof(GridSmem) + (comp ? 2 * FIP_GTILE * kTS * sizeof(float) : 0);
+}
 
-// Lane -> (tap row, tap column) of a warp step for nc tap columns, without a
-// division per visibility: s_lane_map[nc][lane] = (lane / nc) | (lane % nc)
-// << 8 | (32 / nc) << 16, filled once per CTA (init_lane_map + a barrier).
-__shared__ int s_lane_map[10][32];
-__device__ __forceinline__ void init_lane_map() {
-  for (int t = threadIdx.x; t < 10 * 32; t += blockDim.x) {
-    const int nc = t >> 5, l = t & 31;
-    s_lane_map[nc][l] = nc ? (l / nc) | ((l % nc) << 8) | ((32 / nc) << 16) : 0;
+// One entry's taps inside a tile: its weights (halved for the Hermitian
+// split, conjugated for the mirrored copy), its in-tile rows ia in [ia_lo,
+// ia_hi) and columns ib in [ib_lo, ib_hi) of the footprint, the tile cell
+// cell0 of tap (ia_lo, ib_lo), the row direction and the separable kernel
+// values of the in-tile rows and columns.
+struct EntryTaps {
+  float wr, wi;
+  int ia_lo, ia_hi, ib_lo, ib_hi, cell0, r1, mir;
+  float k1[9], k2[9];
+  __device__ bool empty() const { return ia_lo >= ia_hi || ib_lo >= ib_hi; }
+};
+
+template <int VT>
+__device__ __forceinline__ void entry_taps(const float* __restrict__ B, const void* vr,
+                                           const void* vi, float vis_scale, float inten,
+                                           float scale, int g, unsigned ent, int trow0,
+                                           int tcol0, const FipRawVis& raw, EntryTaps& e) {
+  const int v = (int)(ent >> 1), mir = (int)(ent & 1);
+  Footprint f;
+  footprint(B, v, scale, g, f);
+  int c0, c1;
+  half_cols(f, mir, g, c0, c1);
+  // Visibility weighting (FIPkernels.cu:188-195).
+  float wr, wi;
+  if constexpr (VT == FIP_VIS_RAW) {
+    // Stokes-I collapse fused into the load: no collapsed copy in memory.
+    float cr, ci;
+    fip_collapse_sample(raw, (size_t)v, cr, ci);
+    wr = cr / inten;
+    wi = ci / inten;
+  } else if constexpr (VT == FIP_VIS_F32) {
+    wr = load_vis<VT>(vr, v) / inten;
+    wi = load_vis<VT>(vi, v) / inten;
+  } else {
+    wr = (load_vis<VT>(vr, v) * vis_scale) / inten;
+    wi = (load_vis<VT>(vi, v) * vis_scale) / inten;
+  }
+  e.wr = 0.5f * wr;
+  e.wi = mir ? -0.5f * wi : 0.5f * wi;
+  e.mir = mir;
+  const int nr = f.a1 - f.a0 + 1, nc = c1 - c0 + 1;
+  // Tap row ia is grid row wrap(r1), r1 = a0 + ia (mirrored: -(a0 + ia)).
+  // Unless the grid is one tile high, no tile holds the wrap point inside
+  // it (it falls on a tile edge), so a tile's rows of the footprint are one
+  // run of ia along which the tile row moves by +1 (mirrored: -1).
+  int ia_lo = 9, ia_hi = 0, lr_first = 0;
+#pragma unroll
+  for (int a = 0; a < 9; ++a)
+    if (a < nr) {
+      const int lr = wrap_row(mir ? -(f.a0 + a) : f.a0 + a, g) - trow0;
+      if ((unsigned)lr < (unsigned)FIP_GTILE) {
+        if (a < ia_lo) {
+          ia_lo = a;
+          lr_first = lr;
+        }
+        ia_hi = a + 1;
+      }
+    }
+  e.ia_lo = ia_lo;
+  e.ia_hi = ia_hi;
+  e.ib_lo = max(0, tcol0 - c0);
+  e.ib_hi = min(nc, tcol0 + FIP_GTILE - c0);
+  e.cell0 = lr_first * kTS + (c0 + e.ib_lo - tcol0);
+  e.r1 = mir ? -(f.a0 + ia_lo) : f.a0 + ia_lo;
+  const float ihs = 1 / static_cast<float>(FIP_SUPPORT / 2);
+#pragma unroll
+  for (int a = 0; a < 9; ++a)
+    e.k1[a] = (a >= ia_lo && a < ia_hi)
+                  ? fipref::es((static_cast<float>(f.a0 + a) - f.p1) * ihs)
+                  : 0.f;
+  // Column taps in half-plane order c0..c1: original r2 = c (direct) or -c
+  // (mirrored); on the Nyquist column a direct tap is r2 = -G/2 (r2 never
+  // reaches +G/2, FIPkernels.cu:203).
+#pragma unroll
+  for (int b = 0; b < 9; ++b) {
+    const int c = c0 + b;
+    const int r2 = mir ? -c : (2 * c == g ? -c : c);
+    e.k2[b] = (b >= e.ib_lo && b < e.ib_hi)
+                  ? fipref::es((static_cast<float>(r2) - f.p2) * ihs)
+                  : 0.f;
   }
 }
 
-// One gridding work item (tile, entry range) of one snapshot.  Phase 1
-// loads the item's visibilities and their separable kernel values into
-// shared memory (all loads in flight at once); phase 2 lets each warp spread
-// one visibility's taps over its lanes into the shared tile; phase 3 commits.
-// COMP: compensated tile sums of the precision form (exact two-limb fixed
-// point, below).
+// One gridding work item (tile, entry range) of one snapshot, a thread per
+// entry (at most one per thread: FIP_GCHUNK <= kThreads).  Phase 1 takes the
+// thread's entry footprint and kernel values into registers and reduces the
+// item's bound, phase 2 walks the entry's in-tile taps into the shared
+// tile, phase 3 commits.  The tile sums are fixed point, so the shared-memory
+// sums are native integer atomics: exact and independent of their order.
+// Plain form: q = round(tap * 2^30 / bound) in one int32, `bound` (the
+// item's summed weights) bounding every cell sum.
+// Precision form (COMP): t = tap * 2^e, 2^e = the power of two with
+// bound * 2^e < 2^45, is exact in FP32 and is split exactly into
+// hi * 2^23 + lo (hi < 2^22 in magnitude, 0 <= lo <= 2^23), two int32 limbs
+// summed separately (at most 256 taps per cell per item: no overflow), so a
+// cell holds the exact sum of its FP32 taps to 2^-45 of the bound and is
+// rounded once at the commit.
 template <int VT, bool COMP>
 __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_cim,
-                                          const float* __restrict__ B, const void* vr,
-                                          const void* vi, float vis_scale, float inten,
-                                          float scale, int g, int hp, int tiles_c, int layout,
-                                          const unsigned* __restrict__ entries, int4 item,
-                                          float2* __restrict__ grid,
+                                          const float* __restrict__ B,
+                                          const void* vr, const void* vi, float vis_scale,
+                                          float inten, float scale, int g, int hp, int tiles_c,
+                                          int layout, const unsigned* __restrict__ entries,
+                                          int4 item, float2* __restrict__ grid,
                                           const FipRawVis& raw = FipRawVis{}) {
+  static_assert(FIP_GCHUNK <= kThreads, "one entry per thread at most");
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int tile = item.x, cnt = item.z - item.y;
   const int trow0 = (tile / tiles_c) * FIP_GTILE, tcol0 = (tile % tiles_c) * FIP_GTILE;
@@ -589,86 +669,16 @@ __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_ci
       s_cim[k] = 0.f;
     }
   }
-  // Phase 1.
+  // Phase 1: this thread's entry.
+  const int q = threadIdx.x;
+  const bool have = q < cnt;
+  EntryTaps et;
   float bound = 0.f;  // sum over the item of max(|wr|, |wi|): bounds every cell sum
-  for (int q = threadIdx.x; q < cnt; q += kThreads) {
-    const unsigned ent = entries[item.y + q];
-    const int v = (int)(ent >> 1), mir = (int)(ent & 1);
-    Footprint f;
-    footprint(B, v, scale, g, f);
-    int c0, c1;
-    half_cols(f, mir, g, c0, c1);
-    // Visibility weighting (FIPkernels.cu:188-195), halved for the
-    // Hermitian split, conjugated for the mirrored copy.
-    float wr, wi;
-    if constexpr (VT == FIP_VIS_RAW) {
-      // Stokes-I collapse fused into the load: no collapsed copy in memory.
-      float cr, ci;
-      fip_collapse_sample(raw, (size_t)v, cr, ci);
-      wr = cr / inten;
-      wi = ci / inten;
-    } else if constexpr (VT == FIP_VIS_F32) {
-      wr = load_vis<VT>(vr, v) / inten;
-      wi = load_vis<VT>(vi, v) / inten;
-    } else {
-      wr = (load_vis<VT>(vr, v) * vis_scale) / inten;
-      wi = (load_vis<VT>(vi, v) * vis_scale) / inten;
-    }
-    S.wr[q] = 0.5f * wr;
-    S.wi[q] = mir ? -0.5f * wi : 0.5f * wi;
-    bound += 0.5f * fmaxf(fabsf(wr), fabsf(wi));
-    const int nr = f.a1 - f.a0 + 1, nc = c1 - c0 + 1;
-    // Tap row ia is grid row wrap(r1), r1 = a0 + ia (mirrored: -(a0 + ia)).
-    // Unless the grid is one tile high, no tile holds the wrap point inside
-    // it (it falls on a tile edge), so a tile's rows of the footprint are
-    // one run of ia along which the tile row moves by +1 (mirrored: -1).
-    int ia_lo = 9, ia_hi = 0, lr_first = 0;
-#pragma unroll
-    for (int a = 0; a < 9; ++a)
-      if (a < nr) {
-        const int lr = wrap_row(mir ? -(f.a0 + a) : f.a0 + a, g) - trow0;
-        if ((unsigned)lr < (unsigned)FIP_GTILE) {
-          if (a < ia_lo) {
-            ia_lo = a;
-            lr_first = lr;
-          }
-          ia_hi = a + 1;
-        }
-      }
-    const int ib_lo = max(0, tcol0 - c0), ib_hi = min(nc, tcol0 + FIP_GTILE - c0);
-    const bool empty = ia_lo >= ia_hi || ib_lo >= ib_hi;
-    S.span[q] = empty ? 0
-                      : ia_lo | (ia_hi << 4) | (ib_lo << 8) | (ib_hi << 12) | (mir << 16);
-    S.cell0[q] = lr_first * kTS + (c0 + ib_lo - tcol0);
-    S.r1[q] = mir ? -(f.a0 + ia_lo) : f.a0 + ia_lo;
-    const float ihs = 1 / static_cast<float>(FIP_SUPPORT / 2);
-#pragma unroll
-    for (int a = 0; a < 9; ++a)
-      if (a >= ia_lo && a < ia_hi)
-        S.k1[q][a] = fipref::es((static_cast<float>(f.a0 + a) - f.p1) * ihs);
-    // Column taps in half-plane order c0..c1: original r2 = c (direct) or
-    // -c (mirrored).
-#pragma unroll
-    for (int b = 0; b < 9; ++b)
-      if (b >= ib_lo && b < ib_hi) {
-        // Direct copy: column c holds tap r2 = c, or r2 = -G/2 on the
-        // Nyquist column (r2 never reaches +G/2, FIPkernels.cu:203).
-        const int c = c0 + b;
-        const int r2 = mir ? -c : (2 * c == g ? -c : c);
-        S.k2[q][b] = fipref::es((static_cast<float>(r2) - f.p2) * ihs);
-      }
+  if (have) {
+    entry_taps<VT>(B, vr, vi, vis_scale, inten, scale, g, entries[item.y + q], trow0, tcol0,
+                   raw, et);
+    bound = fmaxf(fabsf(et.wr), fabsf(et.wi));
   }
-  // The tile sums are fixed point, so the shared-memory sums are native
-  // integer atomics: exact and independent of their order.  `bound` (the
-  // item's summed weights) bounds every cell sum.
-  // Plain form: q = round(tap * 2^30 / bound) in one int32; resolution 2^-30
-  // of the bound.
-  // Precision form (compensated sums): t = tap * 2^e, 2^e = the power of two
-  // with bound * 2^e < 2^45, is exact in FP32 and is split exactly into
-  // hi * 2^23 + lo (hi < 2^22 in magnitude, 0 <= lo <= 2^23), two int32 limbs
-  // summed separately (at most 256 taps per cell per item: no overflow), so a
-  // cell holds the exact sum of its FP32 taps to 2^-45 of the bound and is
-  // rounded once at the commit.
   for (int o = 16; o > 0; o >>= 1) bound += __shfl_xor_sync(0xffffffffu, bound, o);
   if (lane == 0) S.bound[warp] = bound;
   __syncthreads();
@@ -690,7 +700,7 @@ __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_ci
   int* s_qim = reinterpret_cast<int*>(S.im);
   unsigned* s_lre = reinterpret_cast<unsigned*>(s_cre);
   unsigned* s_lim = reinterpret_cast<unsigned*>(s_cim);
-  // Exact limbs of t = x * 2^e (see above).
+  // Exact limbs of t = x * 2^e (precision form, see above).
   auto limbs = [&](float x, int& hi, unsigned& lo) {
     const float t = x * fx;
     const float hf = floorf(t * (1.0f / 8388608.0f));
@@ -698,61 +708,38 @@ __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_ci
     hi = __float_as_int(hf + 12582912.0f) - 0x4B400000;  // |hf| < 2^22: exact
     lo = __float_as_uint(lf + 8388608.0f) - 0x4B000000u;  // round to integer
   };
-  // Phase 2: a warp per entry, its in-tile taps over the lanes (a column
-  // per lane, 32 / columns rows per step); each lane's column factor is
-  // folded into the weights once, so a tap is one product per component.
-  for (int q = warp; q < cnt; q += kThreads / 32) {
-    const int span = S.span[q];
-    const int ia_lo = span & 15, ia_hi = (span >> 4) & 15;
-    const int ib_lo = (span >> 8) & 15, ncw = ((span >> 12) & 15) - ib_lo;
-    const int map = s_lane_map[ncw][lane];  // (lane / n) | (lane % n) << 8 | (32 / n) << 16
-    const int ia0 = map & 255, ibo = (map >> 8) & 255, per = map >> 16;  // rows per warp step
-    if (ia0 >= per) continue;  // idle lane, or an empty span (per == 0)
-    const float k2 = S.k2[q][ib_lo + ibo];
-    const float wrk = S.wr[q] * k2, wik = S.wi[q] * k2;
-    const int dstep = (span >> 16) & 1 ? -kTS : kTS;  // tile-row step per tap row
-    int cell = S.cell0[q] + ibo + ia0 * dstep;
-    const int cstep = per * dstep;
-    if (g <= FIP_GTILE) {
-      // One tile row holds the whole grid: the wrap point may lie inside the
-      // footprint, so each tap row is wrapped on its own.
-      const int r1f = S.r1[q], dir = (span >> 16) & 1 ? -1 : 1;
-      const int lcb = S.cell0[q] - (wrap_row(r1f, g) - trow0) * kTS + ibo;
-      for (int ia = ia_lo + ia0; ia < ia_hi; ia += per) {
-        const int c = (wrap_row(r1f + (ia - ia_lo) * dir, g) - trow0) * kTS + lcb;
-        const float k1 = S.k1[q][ia];
+  // Phase 2: the thread walks its entry's in-tile taps.
+  if (have && !et.empty()) {
+    const float wrf = COMP ? et.wr : et.wr * fx, wif = COMP ? et.wi : et.wi * fx;
+    const int dstep = et.mir ? -kTS : kTS;
+    const int lc0 = et.cell0 - (wrap_row(et.r1, g) - trow0) * kTS;
+#pragma unroll
+    for (int a = 0; a < 9; ++a) {
+      if (a < et.ia_lo || a >= et.ia_hi) continue;
+      // One tile row holding the whole grid may hold the wrap point: each
+      // tap row is then wrapped on its own.
+      const int rc = g > FIP_GTILE
+                         ? et.cell0 + (a - et.ia_lo) * dstep
+                         : (wrap_row(et.r1 + (et.mir ? et.ia_lo - a : a - et.ia_lo), g) - trow0) *
+                                   kTS + lc0;
+      const float ra = wrf * et.k1[a], rb = wif * et.k1[a];
+#pragma unroll
+      for (int b = 0; b < 9; ++b) {
+        if (b < et.ib_lo || b >= et.ib_hi) continue;
+        const int c = rc + (b - et.ib_lo);
         if (!COMP) {
-          atomicAdd(&s_qre[c], __float2int_rn(wrk * fx * k1));
-          atomicAdd(&s_qim[c], __float2int_rn(wik * fx * k1));
+          atomicAdd(&s_qre[c], __float2int_rn(ra * et.k2[b]));
+          atomicAdd(&s_qim[c], __float2int_rn(rb * et.k2[b]));
         } else {
           int hr, hi;
           unsigned lr2, li2;
-          limbs(wrk * k1, hr, lr2);
-          limbs(wik * k1, hi, li2);
+          limbs(ra * et.k2[b], hr, lr2);
+          limbs(rb * et.k2[b], hi, li2);
           atomicAdd(&s_qre[c], hr);
           atomicAdd(&s_lre[c], lr2);
           atomicAdd(&s_qim[c], hi);
           atomicAdd(&s_lim[c], li2);
         }
-      }
-    } else if (!COMP) {
-      const float wrf = wrk * fx, wif = wik * fx;
-      for (int ia = ia_lo + ia0; ia < ia_hi; ia += per, cell += cstep) {
-        const float k1 = S.k1[q][ia];
-        atomicAdd(&s_qre[cell], __float2int_rn(wrf * k1));
-        atomicAdd(&s_qim[cell], __float2int_rn(wif * k1));
-      }
-    } else {
-      for (int ia = ia_lo + ia0; ia < ia_hi; ia += per, cell += cstep) {
-        const float k1 = S.k1[q][ia];
-        int hr, hi;
-        unsigned lr2, li2;
-        limbs(wrk * k1, hr, lr2);
-        limbs(wik * k1, hi, li2);
-        atomicAdd(&s_qre[cell], hr);
-        atomicAdd(&s_lre[cell], lr2);
-        atomicAdd(&s_qim[cell], hi);
-        atomicAdd(&s_lim[cell], li2);
       }
     }
   }
@@ -767,6 +754,8 @@ __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_ci
       float2 val;
       if (COMP) {
         const int at = lr * kTS + lc;
+        const unsigned* s_lre = reinterpret_cast<const unsigned*>(s_cre);
+        const unsigned* s_lim = reinterpret_cast<const unsigned*>(s_cim);
         val = make_float2((float)(((double)s_qre[at] * 8388608.0 + (double)s_lre[at]) * fx_inv),
                           (float)(((double)s_qim[at] * 8388608.0 + (double)s_lim[at]) * fx_inv));
       } else {
@@ -807,7 +796,6 @@ __global__ void __launch_bounds__(kThreads) k_grid(const float* __restrict__ B, 
   const float inten = plane_intensity(V);
   const float vis_scale = vis_scale_p ? *vis_scale_p : 1.0f;
   const unsigned nw = *nwork;
-  init_lane_map();
   __syncthreads();
   for (unsigned w = blockIdx.x; w < nw; w += gridDim.x)
     grid_item<VT, COMP>(S, s_cre, s_cim, B, vr, vi, vis_scale, inten, scale, g, hp, tiles_c,
@@ -832,7 +820,6 @@ __global__ void __launch_bounds__(kThreads) k_grid_batch(const __grid_constant__
     }
     s_first[in.count] = acc;
   }
-  init_lane_map();
   __syncthreads();
   const unsigned total = s_first[in.count];
   int k = 0;
@@ -2074,7 +2061,9 @@ cudaError_t fip_launch_bin(const FipGeom& geo, const float* B, int nb, FipBins& 
   return cudaGetLastError();
 }
 
-int fip_grid_max_ctas_per_sm(int compensated) { return compensated ? 2 : 3; }
+// CTAs per SM that fit: the precision form's shared memory (the tile and its
+// low limbs) allows three, the plain form's registers four.
+int fip_grid_max_ctas_per_sm(int compensated) { return compensated ? 3 : 4; }
 
 cudaError_t fip_launch_grid(const FipGeom& geo, const float* B, const void* vr, const void* vi,
                             int vis_type, const float* vis_scale, const float* V, int nb,
@@ -2086,7 +2075,7 @@ cudaError_t fip_launch_grid(const FipGeom& geo, const float* B, const void* vr, 
   const int sms = sm_count();
   k_zero_tiles<<<sms, kThreads, 0, s>>>(bins.multi, bins.nmulti, geo.tiles_c, geo.g, geo.hp,
                                         geo.layout, grid, 0, 0);
-  const size_t smem = sizeof(GridSmem) + (compensated ? 2 * FIP_GTILE * kTS * sizeof(float) : 0);
+  const size_t smem = grid_smem_bytes(compensated != 0);
   const int most = fip_grid_max_ctas_per_sm(compensated);
   const int blocks = sms * (ctas_per_sm > 0 ? min(ctas_per_sm, most) : most);
 #define FIP_GRID_CASE(VT, C)                                                                    \
@@ -2125,7 +2114,7 @@ cudaError_t fip_launch_grid_batch(const FipGridBatch& in, int vis_type, int comp
                                   cudaStream_t s, int ctas_per_sm) {
   if (in.count < 1 || in.count > FIP_MAX_BATCH) return cudaErrorInvalidValue;
   const int sms = sm_count();
-  const size_t smem = sizeof(GridSmem) + (compensated ? 2 * FIP_GTILE * kTS * sizeof(float) : 0);
+  const size_t smem = grid_smem_bytes(compensated != 0);
   const int most = fip_grid_max_ctas_per_sm(compensated);
   const int blocks = sms * (ctas_per_sm > 0 ? min(ctas_per_sm, most) : most);
 #define FIP_GRID_CASE(VT, C)                                                                   \

@@ -482,7 +482,7 @@ def test_profiling_and_launch_count(cuda, tiny):
 
 
 @pytest.mark.parametrize("vpt,split,direct,ctas", [(8, 0, 0, 3), (16, 0, 0, 2), (8, 1, 0, 1),
-                                                   (16, 1, 0, 3), (8, 0, 1, 2), (16, 0, 1, 3)])
+                                                   (16, 1, 0, 4), (8, 0, 1, 2), (16, 0, 1, 3)])
 def test_every_launch_shape_gives_the_same_results(cuda, small, vpt, split, direct, ctas):
     """Transform values per thread, split/joint transform and gridder CTAs per SM
     change rounding only."""
@@ -514,7 +514,7 @@ def test_autotune_keeps_results(cuda, small, form):
         im.pipe_device(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, before)
         choice = im.autotune(d["vis_re"], d["vis_im"], d["B"], d["V"], nb)
         assert choice["fft_values_per_thread"] in (8, 16)
-        assert 1 <= choice["grid_ctas_per_sm"] <= 3
+        assert 1 <= choice["grid_ctas_per_sm"] <= (4 if form == "plain" else 3)
         im.pipe_device(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, after)
         torch.cuda.synchronize()
     assert np.abs(after.cpu().numpy() - before.cpu().numpy()).max() <= 1e-5
