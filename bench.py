@@ -551,6 +551,23 @@ def main():
         forms["sequence_plain"] = {
             "value": S / (ev0.elapsed_time(ev1) / 1e3), "unit": UNIT,
             "note": "30 snapshots, sliding-window tLISI per snapshot (28 matrices)"}
+        # The same sequence in the precision form (FP16 storage): the per-call
+        # counterpart of the batched precision form, which also yields a
+        # tLISI matrix per snapshot.
+        with fip.Imager(n, nb, cell, t, form=fip.FORM_PRECISE, vis_storage=fip.STORE_F16,
+                        device=local) as imp:
+            imp.autotune(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, stream=stream)
+            with torch.cuda.stream(stream):
+                imp.image_sequence(vre, vim, Bs, Vs, nbs, nb, seq_res, stream=stream)
+            torch.cuda.synchronize()
+            with torch.cuda.stream(stream):
+                ev0.record(stream)
+                imp.image_sequence(vre, vim, Bs, Vs, nbs, nb, seq_res, stream=stream)
+                ev1.record(stream)
+            torch.cuda.synchronize()
+        forms["sequence_precise_f16"] = {
+            "value": S / (ev0.elapsed_time(ev1) / 1e3), "unit": UNIT,
+            "note": "30 snapshots, sliding-window tLISI per snapshot (28 matrices)"}
 
     # ---- batching form: 64 snapshots x 8 channels (130-150 MHz), 0-30 % flagged,
     # half at 2048^2 and half at 4096^2 (fixed field of view), tile 32 ----
