@@ -37,7 +37,9 @@ struct Plan {
   int e;   // values per thread
   int nt;  // threads = 3 M / e
   int split;  // 1: one CTA per sub-transform (grid.y = s), 0: one CTA per transform
-  int direct;  // 1: the first pass reads the band from global memory (no staging)
+  int direct;  // 1: the first pass reads the band from global memory (no staging);
+               // 2 (row pass): from a shared-memory band copy, brought in by bulk
+               // tensor copies one row pair ahead
 };
 
 // Padded shared-memory index.
@@ -403,9 +405,15 @@ __device__ __forceinline__ void passes(float2 (&v)[1 << LE], float2* base,
 // use group barriers, and one buffer (sm holds direct_smem_elems(G)) serves
 // all passes.  pt: the thread's pass twiddles (loaded for lane
 // sub_lane(threadIdx.x)).
-template <int LM, int LE, bool DIRECT = false, class Load>
+// loaded(): called by every thread once its band values are in registers
+// (before the first pass's stores), e.g. to release a staging buffer.
+struct NoHook {
+  __device__ void operator()() const {}
+};
+template <int LM, int LE, bool DIRECT = false, class Load, class Loaded = NoHook>
 __device__ __forceinline__ void run(float2* sm, const float2* __restrict__ tw,
-                                    const PassTw<LM, LE>& pt, int lo, int hi, Load& load) {
+                                    const PassTw<LM, LE>& pt, int lo, int hi, Load& load,
+                                    const Loaded& loaded = Loaded{}) {
   constexpr int E = 1 << LE, M = 1 << LM, TS = M / E;
   constexpr int R0 = 1 << pass_lr<LM, LE>(0);
   const int tid = threadIdx.x;
@@ -416,6 +424,7 @@ __device__ __forceinline__ void run(float2* sm, const float2* __restrict__ tw,
     first_load<R0, E, M, true>(v, s, lt, lo, hi, tw, load);
   else
     first_load<R0, E, M, false>(v, s, lt, lo, hi, tw, load);
+  loaded();
   passes<LM, LE, 0, DIRECT ? 0 : stage_offset(3 * M), DIRECT>(v, sm + s * sub_stride(M), pt,
                                                                  lt, s);
 }

@@ -1146,12 +1146,13 @@ int fip_imager_autotune(fip_imager* im, const float* vr, const float* vi, const 
   if (im->custom_fft) {
     float best = 1e30f;
     fipfft::Plan chosen = im->fft;
-    // Values per thread 8 or 16 x {joint, split, joint with a direct first pass}.
-    for (int shape = 0; shape < 6; ++shape) {
+    // Values per thread 8 or 16 x {joint, split, joint with a direct first
+    // pass, joint with the row pass's band copied by bulk tensor copies}.
+    for (int shape = 0; shape < 8; ++shape) {
       fipfft::Plan p{};
       if (!fip_fft_plan(geo.g, p, shape & 1 ? 16 : 8)) continue;
       p.split = (shape >> 1) == 1;
-      p.direct = (shape >> 1) == 2;
+      p.direct = (shape >> 1) == 2 ? 1 : ((shape >> 1) == 3 ? 2 : 0);
       float ms = 0.f;
       FIP_TRY(timed(
           [&]() -> cudaError_t {
@@ -1202,7 +1203,7 @@ int fip_imager_set_tuning(fip_imager* im, int fft_values_per_thread, int fft_spl
     if (!fip_fft_plan(im->geo.g, p, fft_values_per_thread))
       return fail(FIP_ERR_ARG, "no transform with these values per thread for this size");
     p.split = fft_split ? 1 : 0;
-    p.direct = fft_direct && !fft_split ? 1 : 0;
+    p.direct = fft_split ? 0 : std::max(0, std::min(fft_direct, 2));
     im->fft = p;
   }
   im->grid_ctas_per_sm = grid_ctas_per_sm;
@@ -2123,12 +2124,13 @@ static int batch_autotune(fip_batch* b, const int* seq_of, const float* const* v
     if (l.per[c] == 0) continue;
     float best = 1e30f;
     fipfft::Plan chosen = q.fft;
-    // Values per thread 8 or 16 x {joint, split, joint with a direct first pass}.
-    for (int shape = 0; shape < 6; ++shape) {
+    // Values per thread 8 or 16 x {joint, split, joint with a direct first
+    // pass, joint with the row pass's band copied by bulk tensor copies}.
+    for (int shape = 0; shape < 8; ++shape) {
       fipfft::Plan p{};
       if (!fip_fft_plan(q.geo.g, p, shape & 1 ? 16 : 8)) continue;
       p.split = (shape >> 1) == 1;
-      p.direct = (shape >> 1) == 2;
+      p.direct = (shape >> 1) == 2 ? 1 : ((shape >> 1) == 3 ? 2 : 0);
       float ms = 0.f;
       FIP_TRY(timed(
           [&]() -> cudaError_t {

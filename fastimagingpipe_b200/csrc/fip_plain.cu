@@ -24,9 +24,11 @@
 //     warp-shuffle tile reductions; a batch's sliding window streams each
 //     tile's slices through registers, every image read once for all the
 //     triples it is in.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
 #include <stdint.h>
 
 #include <algorithm>
@@ -938,6 +940,63 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
   }
 }
 
+// Bulk tensor copies (TMA) with an mbarrier, for the row pass's band copy.
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// Bounded wait for phase `parity` of *bar: false if it did not complete
+// within kMbarSpin polls.
+constexpr unsigned kMbarSpin = 1u << 20;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+  const unsigned a = smem_u32(bar);
+  for (unsigned it = 0; it < kMbarSpin; ++it) {
+    unsigned done = 0;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y,
+                                            int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+// The row pass's band copy: columns 0 .. K2 (at most kBandCap; wider bands
+// read global memory) of a row pair, kBandBox columns per bulk copy, 16
+// bytes (rows yy1, yy1 + 1 of one column) each.
+constexpr int kBandCap = 1024;
+constexpr int kBandBox = 256;
+// The copy's buffer follows the direct form's pass buffer; a bulk tensor
+// copy's shared-memory destination must be 128-byte aligned, and dynamic
+// shared memory starts after the kernel's static shared memory (not on a
+// 128-byte boundary), so the buffer is aligned at run time within 128 bytes
+// of slack.
+template <int LM>
+__host__ __device__ constexpr size_t band_offset() {  // bytes
+  return (size_t)fipfft::direct_smem_elems(3 << LM) * sizeof(float2);
+}
+template <int LM>
+__host__ __device__ constexpr size_t band_smem_bytes() {
+  return band_offset<LM>() + 128 + (size_t)kBandCap * 16;
+}
+
 // Row pass for image rows yy1 = 2b, yy2 = 2b+1: their Hermitian spectra
 // X1, X2 (the column-pass output, extended by X(-c) = conj X(c)) are packed as
 // Z = X1 + i X2 so one complex transform yields both real rows.  The epilogue
@@ -945,11 +1004,18 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
 // is |out| / (taper|x| taper|y| norm^2) (the checkerboard signs cancel
 // against the centred grid origin), applied as a product of the reciprocal
 // table rck[t] = 1 / (taper[t] norm).
-template <int LM, int LE, bool DIRECT>
+// BAND (with DIRECT, persistent over row pairs): the first pass reads the
+// row pair's band from a shared-memory copy that bulk tensor copies bring in
+// one row pair ahead (band_map: the column-pass output as floats [batch][G/2
+// + 1][2 N]); a copy that does not arrive within the wait limit switches the
+// CTA to global reads (same results).
+template <int LM, int LE, bool DIRECT, bool BAND = false>
 __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE, DIRECT>()))
     k_fft_rows(const float2* __restrict__ P, unsigned* bbox,
                const float* __restrict__ rck, float* __restrict__ pre,
-               const float2* __restrict__ tw, size_t col_stride, size_t pre_stride) {
+               const float2* __restrict__ tw, size_t col_stride, size_t pre_stride,
+               const __grid_constant__ CUtensorMap band_map) {
+  static_assert(!BAND || DIRECT, "the band copy replaces the direct form's global reads");
   constexpr int M = 1 << LM, g = 3 * M, half = g / 2, n = 2 * M, h = M, NT = fft_threads<LM, LE>();
   extern __shared__ float2 s_fft[];
   // Batched launches: snapshot blockIdx.y.
@@ -982,9 +1048,44 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
     const int c = threadIdx.x + m * NT;
     if (!DIRECT && c <= k2) pf[m] = col_load(c, 2 * blockIdx.x);
   }
+  // BAND: the copy's buffer, its mbarrier, and the parity of a copy issued
+  // but not yet consumed (-1: none).
+  char* band_raw = reinterpret_cast<char*>(s_fft) + band_offset<LM>();
+  float4* sband =
+      reinterpret_cast<float4*>(band_raw + ((128u - (smem_u32(band_raw) & 127u)) & 127u));
+  __shared__ uint64_t s_bandbar;
+  // Uniform over the CTA; a misaligned buffer (not expected) reads global
+  // memory instead.
+  bool band = BAND && k2 + 1 <= kBandCap && (smem_u32(sband) & 127u) == 0;
+  int pend = -1;
+  const int nbox = (k2 + kBandBox) / kBandBox;  // boxes covering columns 0 .. k2
+  auto issue = [&](int rpair) {  // one thread
+    mbar_expect_tx(&s_bandbar, (unsigned)(nbox * kBandBox * 16));
+    for (int b = 0; b < nbox; ++b)
+      tma_load_3d(sband + b * kBandBox, &band_map, 4 * rpair, b * kBandBox, (int)blockIdx.y,
+                  &s_bandbar);
+  };
+  if (BAND && band) {
+    if (threadIdx.x == 0) {
+      mbar_init(&s_bandbar, 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (blockIdx.x < n / 2) {
+      if (threadIdx.x == 0) issue(blockIdx.x);
+      pend = 0;
+    }
+  }
   float vmax = 0.f;
-  for (int rp = blockIdx.x; rp < n / 2; rp += gridDim.x) {
+  int it = 0;
+  for (int rp = blockIdx.x; rp < n / 2; rp += gridDim.x, ++it) {
     const int yy1 = 2 * rp;
+    if (BAND && band) {
+      const bool got = mbar_wait(&s_bandbar, (unsigned)(it & 1));
+      band = __syncthreads_and(got) != 0;
+      if (band) pend = -1;  // else the copy stays pending: drained at the end
+    }
     if (!DIRECT) {
       fipfft::StageTw w(tw, g, threadIdx.x, NT);
       auto stage = [&](int c, const float4& ab) {
@@ -1025,7 +1126,7 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
     // DIRECT: Z[c] straight from the column-pass output (L2-resident).
     auto zval = [&](int c) -> float2 {
       const int a = c < 0 ? -c : c;
-      const float4 ab = col_load(a, yy1);
+      const float4 ab = (BAND && band) ? sband[a] : col_load(a, yy1);
       float ay = ab.y, by = ab.w;
       if (a == 0 || a == half) {
         ay = 0.f;
@@ -1034,10 +1135,27 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
       return c >= 0 ? make_float2(ab.x - by, ay + ab.z) : make_float2(ab.x + by, ab.z - ay);
     };
     auto load = [&](int c) -> float2 { return DIRECT ? zval(c) : st[c - lo]; };
-    if (fold)
+    if (fold) {
       fipfft::run_pre<LM, LE>(s_fft, pt);
-    else
+    } else if constexpr (BAND) {
+      // Once every thread holds its band values, the next row pair's copy
+      // goes into the buffer (it lands during this pair's passes).
+      auto loaded = [&]() {
+        if (!band) return;
+        __syncthreads();
+        const int nx = rp + (int)gridDim.x;
+        if (nx < n / 2) {
+          if (threadIdx.x == 0) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue(nx);
+          }
+          pend = (it + 1) & 1;
+        }
+      };
+      fipfft::run<LM, LE, DIRECT>(s_fft, tw, pt, lo, hi, load, loaded);
+    } else {
       fipfft::run<LM, LE, DIRECT>(s_fft, tw, pt, lo, hi, load);
+    }
     const float ry1 = rck[abs(yy1 - h)], ry2 = rck[abs(yy1 + 1 - h)];
     float4* row1 = reinterpret_cast<float4*>(pre + (size_t)yy1 * n);
     float4* row2 = reinterpret_cast<float4*>(pre + (size_t)(yy1 + 1) * n);
@@ -1074,6 +1192,9 @@ __global__ void __launch_bounds__(fft_threads<LM, LE>(), (fft_min_blocks<LM, LE,
     // its outputs there, every thread must be done reading them.
     if constexpr (!DIRECT && ((fipfft::pass_count<LM, LE>() - 1) & 1)) __syncthreads();
   }
+  // A copy still pending (its wait ran out) lands before the CTA's shared
+  // memory goes away (bounded, like every wait here).
+  if (BAND && pend >= 0 && threadIdx.x == 0) mbar_wait(&s_bandbar, (unsigned)pend);
   // Image maximum (bbox[3], float bits; zeroed by the binning), which
   // scales the reprojection's fixed-point sums.
   block_max_to(vmax, &bbox[3]);
@@ -2167,7 +2288,7 @@ static cudaError_t launch_cols(const FipGeom& geo, const float2* grid, const uns
         grid, bbox, colbuf, tw, grid_stride, col_stride);
     return cudaGetLastError();
   }
-  if (direct) {
+  if (direct == 1) {  // (2: the row pass's band copy; the column pass stays staged)
     smem = (size_t)fipfft::direct_smem_elems(geo.g) * sizeof(float2);
     e = fft_smem_attr((const void*)k_fft_cols<LM, LE, true>, smem);
     if (e != cudaSuccess) return e;
@@ -2193,6 +2314,39 @@ static cudaError_t launch_cols(const FipGeom& geo, const float2* grid, const uns
   return cudaGetLastError();
 }
 
+// The driver's tensor-map encoder (cuTensorMapEncodeTiled), or null.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault,
+                                         &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// The column-pass output of a batch as floats [batch][G/2 + 1][2 N], in boxes
+// of 4 floats (rows yy1, yy1 + 1 of a column) x kBandBox columns.
+static bool encode_band_map(CUtensorMap* m, const float2* colbuf, const FipGeom& geo, int batch,
+                            size_t col_stride) {
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc || ((uintptr_t)colbuf & 15) != 0 || batch < 1) return false;
+  const cuuint64_t dims[3] = {2 * (cuuint64_t)geo.n, (cuuint64_t)geo.hp, (cuuint64_t)batch};
+  const cuuint64_t strides[2] = {2 * (cuuint64_t)geo.n * 4,
+                                 (cuuint64_t)(batch > 1 ? col_stride : (size_t)geo.hp * geo.n) * 8};
+  const cuuint32_t box[3] = {4, (cuuint32_t)kBandBox, 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float2*>(colbuf), dims, strides,
+             box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
 template <int LM, int LE>
 static cudaError_t launch_rows(const FipGeom& geo, const float2* colbuf, unsigned* bbox,
                                const float* taper, const float2* tw, float* pre,
@@ -2200,6 +2354,7 @@ static cudaError_t launch_rows(const FipGeom& geo, const float2* colbuf, unsigne
                                size_t pre_stride, int split, int direct) {
   size_t smem;
   cudaError_t e;
+  const CUtensorMap no_map{};
   if (split) {
     smem = 2 * (size_t)fipfft::sub_stride(1 << LM) * sizeof(float2);
     if ((e = fft_smem_attr((const void*)k_fft_rows_split<LM, LE>, smem)) != cudaSuccess)
@@ -2208,12 +2363,32 @@ static cudaError_t launch_rows(const FipGeom& geo, const float2* colbuf, unsigne
         colbuf, bbox, taper + geo.n / 2 + 1, pre, tw, col_stride, pre_stride);
     return cudaGetLastError();
   }
+  CUtensorMap band_map{};
+  if (direct == 2 && encode_band_map(&band_map, colbuf, geo, batch, col_stride)) {
+    // Persistent over row pairs (the CTAs that fit at once), the band copy
+    // one row pair ahead.
+    smem = band_smem_bytes<LM>();
+    e = fft_smem_attr((const void*)k_fft_rows<LM, LE, true, true>, smem);
+    if (e != cudaSuccess) return e;
+    static const int per_sm = [&] {
+      int v = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_fft_rows<LM, LE, true, true>,
+                                                        fft_threads<LM, LE>(), smem) !=
+          cudaSuccess)
+        v = 1;
+      return std::max(v, 1);
+    }();
+    const int ctas = std::max(1, std::min(geo.n / 2, per_sm * sm_count()));
+    k_fft_rows<LM, LE, true, true><<<dim3(ctas, batch), fft_threads<LM, LE>(), smem, s>>>(
+        colbuf, bbox, taper + geo.n / 2 + 1, pre, tw, col_stride, pre_stride, band_map);
+    return cudaGetLastError();
+  }
   if (direct) {
     smem = (size_t)fipfft::direct_smem_elems(geo.g) * sizeof(float2);
     e = fft_smem_attr((const void*)k_fft_rows<LM, LE, true>, smem);
     if (e != cudaSuccess) return e;
     k_fft_rows<LM, LE, true><<<dim3(geo.n / 2, batch), fft_threads<LM, LE>(), smem, s>>>(
-        colbuf, bbox, taper + geo.n / 2 + 1, pre, tw, col_stride, pre_stride);
+        colbuf, bbox, taper + geo.n / 2 + 1, pre, tw, col_stride, pre_stride, no_map);
     return cudaGetLastError();
   }
   smem = (size_t)fipfft::smem_elems(geo.g) * sizeof(float2);
@@ -2230,7 +2405,7 @@ static cudaError_t launch_rows(const FipGeom& geo, const float2* colbuf, unsigne
   }();
   const int ctas = std::max(1, std::min(geo.n / 2, per_sm * sm_count()));
   k_fft_rows<LM, LE, false><<<dim3(ctas, batch), fft_threads<LM, LE>(), smem, s>>>(
-      colbuf, bbox, taper + geo.n / 2 + 1, pre, tw, col_stride, pre_stride);
+      colbuf, bbox, taper + geo.n / 2 + 1, pre, tw, col_stride, pre_stride, no_map);
   return cudaGetLastError();
 }
 

@@ -251,8 +251,9 @@ int fip_imager_grid_side(const fip_imager* im);
  * once (device buffers, as fip_image_snapshot), then times the launch shapes
  * that do not change the arithmetic beyond rounding -- the transform's complex
  * values per thread (8 or 16), one CTA per transform or one per sub-transform
- * (fft_split), the first pass reading a staged band or global memory
- * (fft_direct), and the persistent gridder's CTAs per SM -- on
+ * (fft_split), the first pass reading a staged band, global memory, or (row
+ * pass) a band copy brought in by bulk tensor copies one row pair ahead
+ * (fft_direct 0, 1, 2), and the persistent gridder's CTAs per SM -- on
  * that snapshot's band and bins, and keeps the fastest for later calls.
  * Synchronous; overwrites the imager's trigger ring, so call it before a run
  * of snapshots, not inside one.  fip_imager_tuning reports the choice. */
@@ -261,8 +262,8 @@ int fip_imager_autotune(fip_imager* im, const float* vis_re, const float* vis_im
 int fip_imager_tuning(const fip_imager* im, int* fft_values_per_thread, int* fft_split,
                       int* fft_direct, int* grid_ctas_per_sm);
 /* Pins the launch shapes instead (values per thread 8 or 16, or 0 for the
- * default; split 0 or 1; direct first pass 0 or 1 (joint form only); gridder
- * CTAs per SM, 0 for the most that fit). */
+ * default; split 0 or 1; direct first pass 0, 1 or 2 (joint form only);
+ * gridder CTAs per SM, 0 for the most that fit). */
 int fip_imager_set_tuning(fip_imager* im, int fft_values_per_thread, int fft_split,
                           int fft_direct, int grid_ctas_per_sm);
 

@@ -482,7 +482,8 @@ def test_profiling_and_launch_count(cuda, tiny):
 
 
 @pytest.mark.parametrize("vpt,split,direct,ctas", [(8, 0, 0, 3), (16, 0, 0, 2), (8, 1, 0, 1),
-                                                   (16, 1, 0, 4), (8, 0, 1, 2), (16, 0, 1, 3)])
+                                                   (16, 1, 0, 4), (8, 0, 1, 2), (16, 0, 1, 3),
+                                                   (16, 0, 2, 4), (8, 0, 2, 1)])
 def test_every_launch_shape_gives_the_same_results(cuda, small, vpt, split, direct, ctas):
     """Transform values per thread, split/joint transform and gridder CTAs per SM
     change rounding only."""
@@ -499,6 +500,29 @@ def test_every_launch_shape_gives_the_same_results(cuda, small, vpt, split, dire
         im.pipe_device(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, got)
         torch.cuda.synchronize()
     assert np.abs(got.cpu().numpy() - ref.cpu().numpy()).max() <= 1e-5
+
+
+@pytest.mark.parametrize("direct", [1, 2])
+def test_row_pass_band_copy_at_reference_shape(cuda, direct):
+    """The row pass's first pass reading global memory (1) or a band copy brought
+    in by bulk tensor copies (2) gives the staged form's images up to rounding,
+    at 4096^2 (a persistent launch over 2048 row pairs)."""
+    import torch
+    snap = synthetic.config_reference(transient_snapshot=2)
+    n, nb, t = snap.image_size, snap.num_baselines, snap.unit_size
+    d = to_dev(snap, cuda)
+    with fip.Imager(n, nb, snap.cell_size, t) as im:
+        imgs = []
+        for dr in (0, direct):
+            im.set_tuning(16, 0, 4, dr)
+            assert im.tuning()["fft_direct"] == dr
+            img = torch.zeros(n * n, device=cuda)
+            mx = torch.zeros(1, device=cuda)
+            im.image_snapshot(d["vis_re"][:nb], d["vis_im"][:nb], d["B"][:2 * nb], d["V"][:9], nb,
+                              img, mx)
+            torch.cuda.synchronize()
+            imgs.append(img.cpu().numpy())
+    assert relrms(imgs[1], imgs[0]) <= 1e-6
 
 
 @pytest.mark.parametrize("form", ["plain", "precise"])
