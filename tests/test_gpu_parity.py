@@ -464,6 +464,12 @@ def test_invalid_sizes_raise(cuda):
         z = torch.zeros(1000, device=cuda)
         with pytest.raises(fip.FipError):
             im.image_snapshot(z, z, z, z, 11, z)
+        # The host-buffer path checks nb against the imager's capacity before
+        # it stages anything into its pinned block.
+        h = np.zeros(3 * 2 * 11, np.float32)
+        for bad in (11, 0):
+            with pytest.raises(fip.FipError):
+                im.pipe_host(h, h, h, np.zeros(27, np.float32), bad)
 
 
 def test_profiling_and_launch_count(cuda, tiny):
