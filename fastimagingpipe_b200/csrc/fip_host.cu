@@ -265,6 +265,8 @@ struct Lane {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev_done = nullptr;
   cudaEvent_t ev_targets = nullptr;  // pixel mapping of the lane's snapshot written
+  cufftHandle plan = 0;              // cuFFT C2R fallback: the lane's own plan and work area
+  bool plan_ok = false;
 };
 constexpr int kLanes = 3;
 
@@ -282,8 +284,6 @@ struct fip_imager {
   // issue-bound mapping fills what they leave.
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  cufftHandle plan = 0;              // cuFFT C2R fallback (grid side not 3 * 2^k)
-  bool plan_ok = false;
   bool custom_fft = false;           // band-pruned FFT (fip_fft.cuh)
   fipfft::Plan fft{};
   int grid_ctas_per_sm = 0;          // persistent gridder CTAs per SM (0 = most that fit)
@@ -371,9 +371,9 @@ static void imager_free(fip_imager* im) {
   if (im->stream) cudaStreamSynchronize(im->stream);
   if (im->copy_stream) cudaStreamSynchronize(im->copy_stream);
   if (im->side) cudaStreamSynchronize(im->side);
-  if (im->plan_ok) cufftDestroy(im->plan);
   for (Lane& L : im->lane) {
     if (L.stream) cudaStreamSynchronize(L.stream);
+    if (L.plan_ok) cufftDestroy(L.plan);
     void* lp[] = {L.grid, L.bins.count, L.bins.offset, L.bins.cursor, L.bins.entries,
                   L.bins.work, L.bins.nwork, L.bins.bbox, L.bins.multi, L.bins.nmulti,
                   L.colbuf, L.pre, L.targets, L.q_re, L.q_im, L.q_scale};
@@ -516,8 +516,9 @@ int fip_imager_create(fip_imager** out, const fip_imager_config* cfg) {
     FIP_ALLOC(dalloc(&im->theta_tab, fip_theta_table_elems(), tot));
     FIP_ALLOC(fip_launch_theta_table(im->theta_tab, im->stream));
   }
-  // The cuFFT fallback shares one plan (and its work area): one lane.
-  im->lanes = im->custom_fft ? kLanes : 1;
+  // Three lanes; with the cuFFT fallback each lane has its own plan and work
+  // area (a plan's work area serves one stream at a time).
+  im->lanes = kLanes;
   for (int l = 0; l < im->lanes; ++l) {
     Lane& L = im->lane[l];
     FIP_ALLOC(cudaStreamCreateWithPriority(&L.stream, cudaStreamNonBlocking, prio_greatest));
@@ -574,12 +575,13 @@ int fip_imager_create(fip_imager** out, const fip_imager_config* cfg) {
   FIP_ALLOC(cudaMallocHost((void**)&im->h_err, sizeof(unsigned)));
   *im->h_err = 0;
 
-  if (!im->custom_fft) {
-    cufftResult r = cufftCreate(&im->plan);
+  for (int l = 0; l < im->lanes && !im->custom_fft; ++l) {
+    Lane& L = im->lane[l];
+    cufftResult r = cufftCreate(&L.plan);
     if (r != CUFFT_SUCCESS) return cleanup(fail(FIP_ERR_CUFFT, "cufftCreate failed"));
-    im->plan_ok = true;
+    L.plan_ok = true;
     size_t work = 0;
-    r = cufftMakePlan2d(im->plan, geo.g, geo.g, CUFFT_C2R, &work);
+    r = cufftMakePlan2d(L.plan, geo.g, geo.g, CUFFT_C2R, &work);
     if (r != CUFFT_SUCCESS)
       return cleanup(fail(r == CUFFT_ALLOC_FAILED ? FIP_ERR_NOMEM : FIP_ERR_CUFFT,
                           "cufftMakePlan2d(C2R) failed: " + std::to_string((int)r)));
@@ -681,8 +683,8 @@ static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const f
     im->launches += 2;
   } else {
     k = stage_begin(im, ST_FFT_ROWS, s);
-    FIP_CUFFT(cufftSetStream(im->plan, s));
-    FIP_CUFFT(cufftExecC2R(im->plan, reinterpret_cast<cufftComplex*>(L.grid),
+    FIP_CUFFT(cufftSetStream(L.plan, s));
+    FIP_CUFFT(cufftExecC2R(L.plan, reinterpret_cast<cufftComplex*>(L.grid),
                            reinterpret_cast<cufftReal*>(L.grid)));
     FIP_CUDA(fip_launch_correct_c2r(geo, reinterpret_cast<const float*>(L.grid), im->taper,
                                     L.pre, L.bins.bbox + 3, s));

@@ -262,6 +262,30 @@ def test_cufft_fallback_size_vs_fp64(cuda):
     assert np.abs(res - r64).max() <= 1e-4
 
 
+@pytest.mark.parametrize("kw", [{}, dict(form=fip.FORM_PRECISE)])
+@pytest.mark.parametrize("n,cell,t", [(100, 1.5e-4, 20), (1000, 1.5e-5, 20)])
+def test_cufft_fallback_lanes_match_single_snapshot_calls(cuda, n, cell, t, kw):
+    """Image sides whose grid is not 3 * 2^k transform with cuFFT; each of the
+    three concurrent lanes has its own plan, so the three snapshots of a
+    pipe_device / pipe_host call must still give the one-at-a-time results."""
+    import torch
+    snap = synthetic.config_tiny(image_size=n, cell_size=cell, unit_size=t, transient_snapshot=2)
+    nb, u = snap.num_baselines, n // t
+    ref, _, _ = run(snap, cuda, **kw)
+    d = to_dev(snap, cuda)
+    got = torch.zeros(u * u, device=cuda)
+    with fip.Imager(n, nb, cell, t, **kw) as im:
+        for _ in range(2):
+            im.pipe_device(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, got)
+        host = im.pipe_host(snap.vis_re, snap.vis_im, snap.B, snap.V, nb)
+        torch.cuda.synchronize()
+    assert np.abs(got.cpu().numpy().reshape(u, u) - ref).max() <= 1e-5
+    assert np.abs(host - ref).max() <= 1e-5
+    if n == 1000 and kw:  # the precision form's bar against the FP64 oracle
+        r64, _, _ = oracle.fipipe(snap, "f64")
+        assert np.abs(ref - r64).max() <= 1e-4
+
+
 def hermitian_half_grid(snap, k=0):
     """The oracle's checkerboarded grid (FIPkernels.cu:197-245) as the
     half-plane Hermitian grid fip_grid_snapshot returns."""
