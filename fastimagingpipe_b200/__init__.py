@@ -347,7 +347,7 @@ class Imager:
 
 
 class Batch:
-    """Batching form (fip_batch): many snapshots of one power-of-two image size per
+    """Batching form (fip_batch): many snapshots of one image size per
     call, one persistent gridding launch and one batched transform per call,
     replayed as a CUDA graph; the batch carries the sequence's last two images so
     every snapshot with two predecessors yields a tLISI matrix.  Batch.of_sequences

@@ -83,12 +83,12 @@ struct FipGridSnap {
   float2* grid;             // its half-plane grid
   float scale;              // cell * G
   int g, hp, tiles_c;
+  int layout;               // grid layout (FipGeom::layout)
 };
 
 // The snapshots of one batched gridding launch (a kernel parameter of
 // about 5.6 KB).
 struct FipGridBatch {
   int count;
-  int layout;
   FipGridSnap s[FIP_MAX_BATCH];
 };

@@ -1389,7 +1389,11 @@ constexpr int kMaxSequences = 8;
 struct BatchSeq {
   fip_imager_config cfg{};
   FipGeom geo{};
+  bool custom_fft = true;  // band-pruned transform; else batched cuFFT C2R plans
   fipfft::Plan fft{};
+  // cuFFT C2R plans by number of snapshots per call (grid sides not 3 * 2^k),
+  // created before the call's capture.
+  std::vector<std::pair<int, cufftHandle>> plans;
   float2* twiddles = nullptr;
   float* taper = nullptr;
   size_t ntiles = 0, cap = 0, wcap = 0, n2 = 0, grid_elems = 0, col_elems = 0;
@@ -1430,7 +1434,14 @@ struct BatchSeq {
     b.wcap = wcap;
     return b;
   }
+  cufftHandle plan_for(int count) const {
+    for (const auto& p : plans)
+      if (p.first == count) return p.second;
+    return 0;
+  }
   void free_all() {
+    for (auto& p : plans) cufftDestroy(p.second);
+    plans.clear();
     void* ptrs[] = {twiddles, taper, count, offset, cursor, entries, work, nwork, bbox, multi,
                     nmulti, grid, colbuf, pre, targets, q_re, q_im, q_scale, images, maxima};
     for (void* p : ptrs)
@@ -1553,6 +1564,7 @@ FipGridSnap grid_snap(const fip_batch* b, const CallLayout& l, int k, const floa
   g.g = q.geo.g;
   g.hp = q.geo.hp;
   g.tiles_c = q.geo.tiles_c;
+  g.layout = q.geo.layout;
   return g;
 }
 
@@ -1597,7 +1609,6 @@ int batch_record(fip_batch* b, const int* seq_of, const float* const* vr,
   }
   FipGridBatch in{};
   in.count = count;
-  in.layout = 1;
   for (int k = 0; k < count; ++k) {
     const BatchSeq& q = b->seq[l.sq[k]];
     const int j = l.loc[k];
@@ -1630,20 +1641,38 @@ int batch_record(fip_batch* b, const int* seq_of, const float* const* vr,
   FIP_CUDA(fip_launch_grid_batch(in, vt, precise ? 1 : 0, s, b->grid_ctas_per_sm));
   launches += 1;
   FIP_CUDA(phase(2));
+  // Grid sides not 3 * 2^k: one batched cuFFT C2R (in place, phase 2) and the
+  // crop + correction per snapshot (phase 3).
   for (int c = 0; c < nseq; ++c) {
     const BatchSeq& q = b->seq[c];
     if (l.per[c] == 0) continue;
-    FIP_CUDA(fip_launch_fft_cols(q.geo, q.grid, q.bbox, q.colbuf, q.twiddles, q.fft, s, l.per[c],
-                                 q.grid_elems, q.col_elems));
+    if (q.custom_fft) {
+      FIP_CUDA(fip_launch_fft_cols(q.geo, q.grid, q.bbox, q.colbuf, q.twiddles, q.fft, s,
+                                   l.per[c], q.grid_elems, q.col_elems));
+    } else {
+      const cufftHandle plan = q.plan_for(l.per[c]);
+      if (!plan) return fail(FIP_ERR_STATE, "no cuFFT plan for this call size");
+      FIP_CUFFT(cufftSetStream(plan, s));
+      FIP_CUFFT(cufftExecC2R(plan, reinterpret_cast<cufftComplex*>(q.grid),
+                             reinterpret_cast<cufftReal*>(q.grid)));
+    }
     launches += 1;
   }
   FIP_CUDA(phase(3));
   for (int c = 0; c < nseq; ++c) {
     const BatchSeq& q = b->seq[c];
     if (l.per[c] == 0) continue;
-    FIP_CUDA(fip_launch_fft_rows(q.geo, q.colbuf, q.bbox, q.taper, q.twiddles, q.fft, q.pre, s,
-                                 l.per[c], q.col_elems, q.n2));
-    launches += 1;
+    if (q.custom_fft) {
+      FIP_CUDA(fip_launch_fft_rows(q.geo, q.colbuf, q.bbox, q.taper, q.twiddles, q.fft, q.pre, s,
+                                   l.per[c], q.col_elems, q.n2));
+      launches += 1;
+    } else {
+      for (int j = 0; j < l.per[c]; ++j)
+        FIP_CUDA(fip_launch_correct_c2r(q.geo, reinterpret_cast<const float*>(
+                                                   q.grid + (size_t)j * q.grid_elems),
+                                        q.taper, q.pre + (size_t)j * q.n2, q.bbox + 4 * j + 3, s));
+      launches += l.per[c];
+    }
   }
   FIP_CUDA(phase(4));
   if (!precise)
@@ -1735,10 +1764,10 @@ int seq_alloc(BatchSeq& q, size_t smax, size_t& tot) {
   geo.tiles_r = (geo.g + FIP_GTILE - 1) / FIP_GTILE;
   geo.tiles_c = (geo.hp + FIP_GTILE - 1) / FIP_GTILE;
   geo.cell = cfg.cell_size;
-  geo.layout = 1;
-  if (!fip_fft_plan(geo.g, q.fft))
-    return fail(FIP_ERR_ARG, "the batching form needs a power-of-two image size "
-                             "(band-pruned transform)");
+  // The band-pruned transform (grid side 3 * 2^k, power-of-two images) works
+  // on the band layout; other sides on the full grid with cuFFT.
+  q.custom_fft = fip_fft_plan(geo.g, q.fft);
+  geo.layout = q.custom_fft ? 1 : 0;
   if (!fip_gather_supported(geo, cfg.form == FIP_FORM_PRECISE))
     return fail(FIP_ERR_ARG, "cell_size too small for the tile-gather reprojection");
 #define FIP_SALLOC(call)                                                                     \
@@ -1765,7 +1794,7 @@ int seq_alloc(BatchSeq& q, size_t smax, size_t& tot) {
   FIP_SALLOC(dalloc(&q.multi, S * q.ntiles, tot));
   FIP_SALLOC(dalloc(&q.nmulti, S, tot));
   FIP_SALLOC(dalloc(&q.grid, S * q.grid_elems, tot));
-  FIP_SALLOC(dalloc(&q.colbuf, S * q.col_elems, tot));
+  if (q.custom_fft) FIP_SALLOC(dalloc(&q.colbuf, S * q.col_elems, tot));
   FIP_SALLOC(dalloc(&q.pre, S * q.n2, tot));
   if (cfg.form == FIP_FORM_PLAIN) FIP_SALLOC(dalloc(&q.targets, S * q.n2, tot));
   if (cfg.form == FIP_FORM_PRECISE && cfg.vis_storage != FIP_STORE_F32) {
@@ -1776,7 +1805,7 @@ int seq_alloc(BatchSeq& q, size_t smax, size_t& tot) {
   FIP_SALLOC(dalloc(&q.images, (S + 2) * q.n2, tot));
   FIP_SALLOC(dalloc(&q.maxima, S + 2, tot));
   FIP_SALLOC(dalloc(&q.taper, 2 * ((size_t)geo.n / 2 + 1), tot));
-  {
+  if (q.custom_fft) {
     const std::vector<float2> tw = fft_twiddles(geo.g);
     FIP_SALLOC(dalloc(&q.twiddles, tw.size(), tot));
     FIP_SALLOC(cudaMemcpy(q.twiddles, tw.data(), tw.size() * sizeof(float2),
@@ -1990,6 +2019,27 @@ static int batch_run(fip_batch* b, const int* seq_of, const float* const* vis_re
   // mappings (and the legacy default stream, which cannot be captured, is
   // never the capture stream).
   cudaStream_t cs = b->capture;
+  // cuFFT sequences: the batched C2R plan of this call's size, made before
+  // the capture (making a plan allocates its work area).
+  for (int c = 0; c < nseq; ++c) {
+    BatchSeq& q = b->seq[c];
+    if (q.custom_fft || per[c] == 0 || q.plan_for(per[c])) continue;
+    cufftHandle plan = 0;
+    if (cufftCreate(&plan) != CUFFT_SUCCESS) return fail(FIP_ERR_CUFFT, "cufftCreate failed");
+    int nn[2] = {q.geo.g, q.geo.g}, inembed[2] = {q.geo.g, q.geo.hp},
+        onembed[2] = {q.geo.g, 2 * q.geo.hp};
+    size_t work = 0;
+    const cufftResult r = cufftMakePlanMany(plan, 2, nn, inembed, 1, q.geo.g * q.geo.hp,
+                                            onembed, 1, 2 * q.geo.g * q.geo.hp, CUFFT_C2R,
+                                            per[c], &work);
+    if (r != CUFFT_SUCCESS) {
+      cufftDestroy(plan);
+      return fail(r == CUFFT_ALLOC_FAILED ? FIP_ERR_NOMEM : FIP_ERR_CUFFT,
+                  "cufftMakePlanMany(C2R) failed: " + std::to_string((int)r));
+    }
+    q.plans.emplace_back(per[c], plan);
+    b->device_bytes += work;
+  }
   FIP_CUDA(cudaEventRecord(b->fork, s));
   FIP_CUDA(cudaStreamWaitEvent(cs, b->fork, 0));
   FIP_TRY(batch_collect(b));  // the previous call's phase times, before its events are reused
@@ -2019,8 +2069,13 @@ static int batch_run(fip_batch* b, const int* seq_of, const float* const* vis_re
       cudaGraphNodeType ty;
       FIP_CUDA(cudaGraphNodeGetType(nd, &ty));
       if (ty != cudaGraphNodeTypeKernel) continue;
+      // Library kernels (cuFFT's) are not the runtime's to describe: such
+      // nodes keep their default priority.
       cudaKernelNodeParams kp{};
-      FIP_CUDA(cudaGraphKernelNodeGetParams(nd, &kp));
+      if (cudaGraphKernelNodeGetParams(nd, &kp) != cudaSuccess) {
+        cudaGetLastError();
+        continue;
+      }
       cudaLaunchAttributeValue v{};
       v.priority = kp.func == mapk ? least : greatest;
       FIP_CUDA(cudaGraphKernelNodeSetAttribute(nd, cudaLaunchAttributePriority, &v));
@@ -2102,7 +2157,6 @@ static int batch_autotune(fip_batch* b, const int* seq_of, const float* const* v
   const CallLayout l = call_layout(seq_of, (int)count);
   FipGridBatch in{};
   in.count = (int)count;
-  in.layout = 1;
   for (size_t k = 0; k < count; ++k)
     in.s[k] = grid_snap(b, l, (int)k, B[k], V[k], vis_re[k], vis_im[k]);
   EventPair ev;
@@ -2123,7 +2177,7 @@ static int batch_autotune(fip_batch* b, const int* seq_of, const float* const* v
   };
   for (int c = 0; c < nseq; ++c) {
     BatchSeq& q = b->seq[c];
-    if (l.per[c] == 0) continue;
+    if (l.per[c] == 0 || !q.custom_fft) continue;
     float best = 1e30f;
     fipfft::Plan chosen = q.fft;
     // Values per thread 8 or 16 x {joint, split, joint with a direct first

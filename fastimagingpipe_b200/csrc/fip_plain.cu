@@ -831,7 +831,7 @@ __global__ void __launch_bounds__(kThreads) k_grid_batch(const __grid_constant__
     const float inten = plane_intensity(sn.V);
     const float vis_scale = sn.vis_scale ? *sn.vis_scale : 1.0f;
     grid_item<VT, COMP>(S, s_cre, s_cim, sn.B, sn.vr, sn.vi, vis_scale, inten, sn.scale, sn.g,
-                        sn.hp, sn.tiles_c, in.layout, sn.entries, sn.work[w - s_first[k]],
+                        sn.hp, sn.tiles_c, sn.layout, sn.entries, sn.work[w - s_first[k]],
                         sn.grid);
   }
 }

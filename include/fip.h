@@ -278,8 +278,10 @@ int fip_imager_set_tuning(fip_imager* im, int fft_values_per_thread, int fft_spl
  * visibilities dropped).  The batch keeps the sequence's last two images, so
  * every snapshot with two predecessors (in this call or the previous ones)
  * yields a tLISI matrix (U*U floats, in order, at results); *nresults gets
- * their number.  Asynchronous on `stream`.  The image size must be a power of
- * two (the band-pruned transform); cfg->reproject must be 0. */
+ * their number.  Asynchronous on `stream`.  Power-of-two images use the
+ * band-pruned transform; other sizes one batched cuFFT C2R plan per call
+ * size (made before the call's capture, kept for later calls).
+ * cfg->reproject must be 0. */
 typedef struct fip_batch fip_batch;
 int fip_batch_create(fip_batch** out, const fip_imager_config* cfg, size_t max_snapshots);
 int fip_batch_destroy(fip_batch* b);

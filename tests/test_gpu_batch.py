@@ -6,6 +6,8 @@ Tolerances: batch vs the per-snapshot path 1e-5 absolute in tLISI (the same
 kernels; float-atomic gridding sums may round in another order); precision
 form vs FP64 1e-4 absolute (the parity bar of the precision form).
 """
+from types import SimpleNamespace
+
 import numpy as np
 import pytest
 
@@ -135,7 +137,7 @@ def test_batch_precision_form_vs_fp64(cuda):
 def test_batch_rejects_bad_arguments(cuda):
     import torch
     with pytest.raises(fip.FipError):
-        fip.Batch(100, 10, 1e-3, 10, 4)  # not a power of two
+        fip.Batch(102, 10, 1e-3, 17, 4)  # not a multiple of 4
     with pytest.raises(fip.FipError):
         fip.Batch(64, 10, 1e-3, 16, 65)  # above the batch limit
     z = torch.zeros(64, device=cuda)
@@ -222,3 +224,43 @@ def test_sequences_reject_bad_arguments(cuda):
     h = ctypes.c_void_p()
     assert lib.fip_batch_create_sequences(ctypes.byref(h), ctypes.cast(cfgs, ctypes.c_void_p),
                                           2, 2) == 1  # forms differ
+
+
+@pytest.mark.parametrize("kw", [{}, dict(form=fip.FORM_PRECISE, vis_storage=fip.STORE_F16)])
+def test_batch_of_cufft_and_pruned_sizes(cuda, kw):
+    """A 100^2 sequence (grid side 150: a batched cuFFT C2R plan) and a 128^2
+    sequence (band-pruned transform) imaged together, over calls of two
+    sizes (two cuFFT plans): each sequence's tLISI equals its per-snapshot
+    path's."""
+    import torch
+    odd = [synthetic.config_tiny(image_size=100, cell_size=1.5e-4, unit_size=20,
+                                 transient_snapshot=2, n_snap=5, seed=31)]
+    pow2 = [synthetic.config_tiny(transient_snapshot=2, n_snap=5, seed=32)]
+    seqs = []
+    for s in (odd[0], pow2[0]):
+        nb = s.num_baselines
+        seqs.append([SimpleNamespace(vis_re=s.vis_re[k * nb:(k + 1) * nb],
+                                     vis_im=s.vis_im[k * nb:(k + 1) * nb],
+                                     B=s.B[2 * k * nb:2 * (k + 1) * nb], V=s.V[9 * k:9 * k + 9],
+                                     nb=nb, image_size=s.image_size, unit_size=s.unit_size,
+                                     cell_size=s.cell_size) for k in range(5)])
+    devs = [dev(x, cuda) for x in seqs]
+    ref = [per_snapshot(x, d, cuda, **kw) for x, d in zip(seqs, devs)]
+    spec = [(x[0].image_size, x[0].nb, x[0].cell_size, x[0].unit_size) for x in seqs]
+    us = [x[0] // x[3] for x in spec]
+    res = [torch.zeros((5, u * u), device=cuda) for u in us]
+    order = [(c, k) for k in range(5) for c in range(2)]
+    got = [0, 0]
+    with fip.Batch.of_sequences(spec, 5, **kw) as b:
+        for part in (order[:4], order[4:]):
+            counts = b.image_sequences(
+                [c for c, _ in part],
+                *[[devs[c][k][key] for c, k in part] for key in ("vis_re", "vis_im", "B", "V")],
+                [seqs[c][k].nb for c, k in part], [res[0][got[0]:], res[1][got[1]:]])
+            got = [g + n for g, n in zip(got, counts)]
+        torch.cuda.synchronize()
+        b.check()
+    assert got == [3, 3]
+    for c in range(2):
+        out = res[c][:3].cpu().numpy().reshape(3, us[c], us[c])
+        assert np.abs(out - ref[c]).max() <= 1e-5
