@@ -9,6 +9,10 @@
         the sliding-window trigger over 18 seeded 4096^2 images (16 triples,
         tile 32), streamed and per-triple (fip_set_trigger_streaming).
 
+    python -m fastimagingpipe_b200.cases fipipe [plain|precise]
+        three device-resident three-snapshot calls (fip_pipe_device) at
+        4096^2, 130,816 baselines, tile 32 (precise: FP16 storage).
+
 Each prints one line and exits 0; inputs are seeded synthetic data.
 """
 import sys
@@ -58,7 +62,25 @@ def trigger_window(form: str) -> str:
     return f"trigger-window {form}: {count - 2} triples, min tLISI {float(out.min()):.4f}"
 
 
-CASES = {"batch-mfs": batch_mfs, "trigger-window": trigger_window}
+def fipipe(form: str) -> str:
+    import torch
+    import fastimagingpipe_b200 as fip
+    from fastimagingpipe_b200 import synthetic
+    dev = torch.device("cuda:0")
+    snap = synthetic.config_reference(transient_snapshot=2)
+    n, nb, t = snap.image_size, snap.num_baselines, snap.unit_size
+    d = {k: torch.tensor(getattr(snap, k), device=dev) for k in ("vis_re", "vis_im", "B", "V")}
+    out = torch.zeros((n // t) ** 2, device=dev)
+    kw = {} if form == "plain" else dict(form=fip.FORM_PRECISE, vis_storage=fip.STORE_F16)
+    with fip.Imager(n, nb, snap.cell_size, t, **kw) as im:
+        for _ in range(3):
+            im.pipe_device(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, out)
+        torch.cuda.synchronize()
+        im.check()
+    return f"fipipe {form}: min tLISI {float(out.min()):.4f}"
+
+
+CASES = {"batch-mfs": batch_mfs, "trigger-window": trigger_window, "fipipe": fipipe}
 
 
 def main(argv=None) -> int:

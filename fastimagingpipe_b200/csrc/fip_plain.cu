@@ -1530,23 +1530,23 @@ __device__ __forceinline__ ExactMap<T> make_map(const float* V, float cell) {
   return m;
 }
 
-// The same map in FP32 arithmetic throughout (no FP64 divisions): for the
+// The same map in FP32 arithmetic throughout (three reciprocals): for the
 // gather's candidate bounds, whose margins (a quarter pixel at least) dwarf
 // its rounding (~1e-4 pixel at 4096^2).
 __device__ __forceinline__ ExactMap<float> make_map_f32(const float* V, float cell) {
   ExactMap<float> m;
-  const float a22 = fabsf(V[8]);
-  m.m00 = -V[0] / a22;
-  m.m01 = V[3] / a22;
-  m.m10 = -V[1] / a22;
-  m.m11 = V[4] / a22;
-  const float det = m.m00 * m.m11 - m.m01 * m.m10;
-  m.i00 = m.m11 / det;
-  m.i01 = -m.m01 / det;
-  m.i10 = -m.m10 / det;
-  m.i11 = m.m00 / det;
-  m.xi = V[6] / V[8];
-  m.eta = V[7] / V[8];
+  const float ia = 1.0f / fabsf(V[8]), iv = 1.0f / V[8];
+  m.m00 = -V[0] * ia;
+  m.m01 = V[3] * ia;
+  m.m10 = -V[1] * ia;
+  m.m11 = V[4] * ia;
+  const float idet = 1.0f / (m.m00 * m.m11 - m.m01 * m.m10);
+  m.i00 = m.m11 * idet;
+  m.i01 = -m.m01 * idet;
+  m.i10 = -m.m10 * idet;
+  m.i11 = m.m00 * idet;
+  m.xi = V[6] * iv;
+  m.eta = V[7] * iv;
   m.cell = cell;
   return m;
 }
@@ -1555,6 +1555,16 @@ template <typename T>
 __device__ __forceinline__ T slant_over_cell(const ExactMap<T>& m, T P1, T P2) {
   const T rho = m.cell * m.cell * ((P1 - 1) * (P1 - 1) + (P2 - 1) * (P2 - 1));
   return rho <= 1 ? (rho / (1 + sqrt(1 - rho))) / m.cell : (T)0;
+}
+
+// FP32, for the gather's candidate bounds only: rsqrtf and __fdividef (a few
+// ulp), whose rounding the bounds' margins dwarf.
+__device__ __forceinline__ float slant_over_cell(const ExactMap<float>& m, float P1, float P2) {
+  const float rho = m.cell * m.cell * ((P1 - 1) * (P1 - 1) + (P2 - 1) * (P2 - 1));
+  if (!(rho <= 1.f)) return 0.f;
+  const float u = 1.f - rho;
+  const float s = u > 0.f ? u * rsqrtf(u) : 0.f;
+  return __fdividef(rho, m.cell * (1.f + s));
 }
 
 template <typename T>
@@ -1586,6 +1596,68 @@ __device__ __forceinline__ T exact_inverse(const ExactMap<T>& m, T LL, T MM, T& 
   T L2, M2;
   exact_forward(m, a, b, L2, M2);
   return fmax(fabs(L2 - LL), fabs(M2 - MM));
+}
+
+// The exact map around a per-tile origin (a0, b0) of source offsets, for the
+// precision form's splats.  With Q = P - 1 the vector whose squared length,
+// times cell^2, is rho, and Q0 its value at the origin, a source d = M (a -
+// a0, b - b0) away has
+//   rho - rho0 = cell^2 g,   g = 2 Q0.d + d.d,
+//   z(rho) - z(rho0) = cell g / (sqrt(1 - rho0) + sqrt(1 - rho))
+// (z = slant over cell), so its target relative to the destination tile is
+//   L = l0 + d1 - xi dz,  M = m0 + d2 + eta dz,
+// with l0, m0 the origin's target in tile coordinates (FP64).  Every FP32
+// quantity is then a tile-sized offset or a relative correction: rsqrtf and
+// __fdividef (a few ulp) move a target by ~1e-5 pixel, well inside the
+// FP64 tolerance, where the slant term in absolute form rounds at its own
+// magnitude (hundreds of pixels on wide fields).  Beyond the horizon
+// (rho > 1) the slant term is 0, as in the closed form; the relative form
+// needs the origin inside it, which every tile in the gather's domain has.
+struct TileMap {
+  float m00, m01, m10, m11;  // M / |V22|
+  float xi, eta, cell, c2;   // c2 = cell^2
+  float q1, q2;              // 2 Q0
+  float u0, s0, z0;          // 1 - rho0, its square root, the slant term at the origin
+  float l0, m0;              // the origin's target relative to the tile's corner
+  int a0, b0;
+};
+
+__device__ __forceinline__ TileMap tile_map(const ExactMap<double>& md, const float (*q)[2],
+                                            int seg, int cl, int rl) {
+  TileMap t;
+  // Origin: the rounded mean of the preimage polygon's four corners.
+  t.a0 = (int)rintf(0.25f * (q[0][0] + q[seg][0] + q[2 * seg][0] + q[3 * seg][0]));
+  t.b0 = (int)rintf(0.25f * (q[0][1] + q[seg][1] + q[2 * seg][1] + q[3 * seg][1]));
+  const double P1 = md.m00 * t.a0 + md.m01 * t.b0, P2 = md.m10 * t.a0 + md.m11 * t.b0;
+  const double Q1 = P1 - 1.0, Q2 = P2 - 1.0;
+  const double rho = md.cell * md.cell * (Q1 * Q1 + Q2 * Q2);
+  const double u0 = 1.0 - rho;
+  const double s0 = u0 > 0.0 ? sqrt(u0) : 0.0;
+  const double z0 = rho <= 1.0 ? (rho / (1.0 + s0)) / md.cell : 0.0;
+  t.m00 = (float)md.m00; t.m01 = (float)md.m01; t.m10 = (float)md.m10; t.m11 = (float)md.m11;
+  t.xi = (float)md.xi; t.eta = (float)md.eta;
+  t.cell = (float)md.cell; t.c2 = (float)(md.cell * md.cell);
+  t.q1 = (float)(2.0 * Q1); t.q2 = (float)(2.0 * Q2);
+  t.u0 = (float)u0; t.s0 = (float)s0; t.z0 = (float)z0;
+  t.l0 = (float)(P1 - md.xi * z0 - (double)cl);
+  t.m0 = (float)(P2 + md.eta * z0 - (double)rl);
+  return t;
+}
+
+// Target (L, M), relative to the tile's corner, of the source at offsets
+// (a, b) from the image centre.
+__device__ __forceinline__ void tile_target(const TileMap& t, int a, int b, float& L, float& M) {
+  const float da = (float)(a - t.a0), db = (float)(b - t.b0);
+  const float d1 = t.m00 * da + t.m01 * db, d2 = t.m10 * da + t.m11 * db;
+  const float g = d1 * (t.q1 + d1) + d2 * (t.q2 + d2);
+  const float u = t.u0 - t.c2 * g;
+  float dz = -t.z0;
+  if (u >= 0.f) {
+    const float s = u > 0.f ? u * rsqrtf(u) : 0.f;
+    dz = __fdividef(t.cell * g, t.s0 + s);
+  }
+  L = t.l0 + d1 - t.xi * dz;
+  M = t.m0 + d2 + t.eta * dz;
 }
 
 // Destination-tile-major reprojection.  The candidate source pixels of a
@@ -1633,10 +1705,12 @@ __global__ void __launch_bounds__(kThreads, EXACT ? 5 : 8) k_reproject_gather(
   static_assert((kTW * kTR) % 4 == 0, "the tile is zeroed in 16-byte stores");
   for (int k = threadIdx.x; k < kTW * kTR / 4; k += kThreads)
     reinterpret_cast<uint4*>(s_tile)[k] = make_uint4(0u, 0u, 0u, 0u);
-  // Precision form: the FP64 map, formed once per CTA (thread 4) beside the
-  // corners and read by every thread after the barrier.
+  // Precision form: the FP64 map, formed once per CTA by a lane of warp 1
+  // while warp 0 traces the preimage, and turned into the tile's FP32
+  // constants (TileMap) by one thread after the barrier.
   __shared__ ExactMap<double> s_md;
-  if (EXACT && threadIdx.x == 4) s_md = make_map<double>(V, cell);
+  __shared__ TileMap s_tm;
+  if (EXACT && threadIdx.x == 32) s_md = make_map<double>(V, cell);
   // Preimage of the tile's boundary, widened by the splat reach and delta:
   // kPoly points, kSeg per edge, in order around it (lanes of warp 0), the
   // tile's domain check and its curvature margin.
@@ -1710,6 +1784,11 @@ __global__ void __launch_bounds__(kThreads, EXACT ? 5 : 8) k_reproject_gather(
   const float inv_nb = 1.0f / static_cast<float>(nb);
   const size_t half = n / 2;
   const float lim = half - 1;  // the reference compares |LL| with size_t (N/2 - 1)
+  // A candidate that reaches the tile has LL in [c0 - h - 1, c0 - h + kDT)
+  // (MM likewise): for tiles at least two pixels inside that range check on
+  // both axes, every such candidate passes it, and a candidate that would fail
+  // it lands beyond the tile, so the check is left out there.
+  const bool inner = c0 >= 4 && c0 + kDT + 4 <= 2 * h && r0 >= 4 && r0 + kDT + 4 <= 2 * h;
   // Fixed-point tile sums: a source's splat value v / nb is carried as
   // v * 2^(28 - sh) / max(pre).  Every contribution is <= 2^(28 - sh), and
   // the bilinear weights landing on one pixel sum to about the density of
@@ -1726,33 +1805,17 @@ __global__ void __launch_bounds__(kThreads, EXACT ? 5 : 8) k_reproject_gather(
   const float pmax = __uint_as_float(*pre_max);
   const float qk = pmax > 0.f ? 268435456.0f / (pmax * (float)(1 << sh)) : 0.f;
   const float deq = pmax * inv_nb * ((float)(1 << sh) / 268435456.0f);
-  // Precision form: exact targets in FP32 around a per-tile origin (a0, b0),
-  // so offsets stay small; P at the origin and the destination-tile offset
-  // come from FP64.
-  ExactMap<float> mf;
-  float p10 = 0.f, p20 = 0.f, off1 = 0.f, off2 = 0.f;
-  int a0 = 0, b0 = 0;
-  if (EXACT) {
-    const ExactMap<double> md = s_md;
-    // make_map<float>: the FP64 map's coefficients rounded to FP32.
-    mf.m00 = (float)md.m00; mf.m01 = (float)md.m01; mf.m10 = (float)md.m10;
-    mf.m11 = (float)md.m11; mf.i00 = (float)md.i00; mf.i01 = (float)md.i01;
-    mf.i10 = (float)md.i10; mf.i11 = (float)md.i11; mf.xi = (float)md.xi;
-    mf.eta = (float)md.eta; mf.cell = (float)md.cell;
-    a0 = (int)rintf(0.25f * (s_q[0][0] + s_q[kSeg][0] + s_q[2 * kSeg][0] + s_q[3 * kSeg][0]));
-    b0 = (int)rintf(0.25f * (s_q[0][1] + s_q[kSeg][1] + s_q[2 * kSeg][1] + s_q[3 * kSeg][1]));
-    const double P1 = md.m00 * a0 + md.m01 * b0, P2 = md.m10 * a0 + md.m11 * b0;
-    p10 = (float)P1;
-    p20 = (float)P2;
-    off1 = (float)(P1 - (double)(c0 - h));
-    off2 = (float)(P2 - (double)(r0 - h));
-  }
+  // Precision form: the tile's constants, from FP64 by a thread of the last
+  // warp (idle in the row-interval step unless a chunk has 256 rows); every
+  // thread reads them after the chunk's barriers, before its first splat.
+  if (EXACT && threadIdx.x == kThreads - 1) s_tm = tile_map(s_md, s_q, kSeg, c0 - h, r0 - h);
+  TileMap tm;
   auto splat = [&](int i, int j, float vq, float2 t) {
     int fl, fm;
     float wl1, wm1, wl0, wm0;
     if (!EXACT) {
       const float LL = t.x, MM = t.y;
-      if (!(fabsf(LL) < lim && fabsf(MM) < lim)) return;
+      if (!inner && !(fabsf(LL) < lim && fabsf(MM) < lim)) return;
       const float flf = floorf(LL), fmf = floorf(MM);
       // The reference's weight expressions (FIPkernels.cu:397-409).  Its far
       // pixel is ceil(LL), equal to floor(LL) + 1 except on exact integers,
@@ -1763,11 +1826,10 @@ __global__ void __launch_bounds__(kThreads, EXACT ? 5 : 8) k_reproject_gather(
       fl = (int)flf + (h - c0);
       fm = (int)fmf + (h - r0);
     } else {
-      const float da = (float)(i - h - a0), db = (float)(j - h - b0);
-      const float d1 = mf.m00 * da + mf.m01 * db, d2 = mf.m10 * da + mf.m11 * db;
-      const float zc = slant_over_cell(mf, p10 + d1, p20 + d2);
-      const float Lr = off1 + d1 - mf.xi * zc, Mr = off2 + d2 + mf.eta * zc;
-      if (!(fabsf(Lr + (float)(c0 - h)) < lim && fabsf(Mr + (float)(r0 - h)) < lim)) return;
+      float Lr, Mr;
+      tile_target(tm, i - h, j - h, Lr, Mr);
+      if (!inner && !(fabsf(Lr + (float)(c0 - h)) < lim && fabsf(Mr + (float)(r0 - h)) < lim))
+        return;
       const float flr = floorf(Lr), fmr = floorf(Mr);
       fl = (int)flr;
       fm = (int)fmr;
@@ -1844,6 +1906,7 @@ __global__ void __launch_bounds__(kThreads, EXACT ? 5 : 8) k_reproject_gather(
     }
     __syncthreads();
     const int total = s_off[kMaxRows];
+    if (EXACT) tm = s_tm;
     // Rows past nrows have no candidates: their offsets equal total.
     // Each warp takes a contiguous eighth of the candidates, so a lane's row
     // cursor moves about half a row per candidate; its start is found by
