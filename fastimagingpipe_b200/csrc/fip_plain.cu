@@ -2177,8 +2177,10 @@ bool fip_fft_plan(int g, fipfft::Plan& p, int values_per_thread) {
   int lm = 0;
   while ((1 << lm) < m) ++lm;
   // Instantiated: 8 values per thread for M = 2^4..2^11, 16 for 2^5..2^12
-  // (<= 768 threads).  Default: 8 up to M = 2048 (N = 4096), 16 beyond.
-  int le = (lm <= 11) ? 3 : 4;
+  // (<= 768 threads).  Default: 8 up to M = 1024 (N = 2048), 16 beyond -- at
+  // M = 2048 the 16-value row pass takes about two thirds of the 8-value one's
+  // time on B200, and the autotuner picks it there.
+  int le = (lm <= 10) ? 3 : 4;
   if (values_per_thread == 8) le = 3;
   if (values_per_thread == 16) le = 4;
   if (le == 3 && (lm < 4 || lm > 11)) return false;
