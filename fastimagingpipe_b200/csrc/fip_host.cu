@@ -664,7 +664,7 @@ static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const f
     else
       FIP_CUDA(fip_launch_quantize(vr, vi, nb, vt, L.q_re, L.q_im, L.q_scale, s));
     stage_end(im, k, s);
-    im->launches += 3;
+    im->launches += 2;
     gvr = L.q_re;
     gvi = L.q_im;
   }
@@ -832,7 +832,7 @@ int fip_grid_snapshot(fip_imager* im, const float* vis_re, const float* vis_im, 
   if (precise && im->cfg.vis_storage != FIP_STORE_F32) {
     vt = im->cfg.vis_storage == FIP_STORE_F16 ? FIP_VIS_F16 : FIP_VIS_BF16;
     FIP_CUDA(fip_launch_quantize(vis_re, vis_im, nb, vt, L.q_re, L.q_im, L.q_scale, s));
-    im->launches += 3;
+    im->launches += 2;
     gvr = L.q_re;
     gvi = L.q_im;
   }
@@ -1617,7 +1617,7 @@ int batch_record(fip_batch* b, const int* seq_of, const float* const* vr,
       void* qr = static_cast<char*>(q.q_re) + j * q.cfg.max_baselines * 2;
       void* qi = static_cast<char*>(q.q_im) + j * q.cfg.max_baselines * 2;
       FIP_CUDA(fip_launch_quantize(vr[k], vi[k], nb[k], vt, qr, qi, q.q_scale + j, bs));
-      launches += 3;
+      launches += 2;
     }
     FipBins bins = q.bins(j);
     FIP_CUDA(fip_launch_bin(q.geo, B[k], (int)nb[k], bins, bs));

@@ -284,17 +284,17 @@ __global__ void __launch_bounds__(kScanThreads) k_bin_scan(
 // ---------------------------------------------------------------------------
 // Binning with per-CTA shared-memory histograms (grids of up to
 // kMaxSmemTiles tiles).  Each CTA takes a contiguous range of visibilities,
-// counts their tile entries in shared memory (native integer atomics,
-// warp-aggregated), and adds its non-zero counts to the global ones; the last
-// CTA to finish scans the tiles.  The scatter pass recounts its range,
+// counts their tile entries in shared memory (native integer atomics, one
+// per entry: the hardware serialises lanes that hit one counter, cheaper
+// than matching the lanes first), and adds its non-zero counts to the global
+// ones; one CTA then scans the tiles.  The scatter pass recounts its range,
 // reserves one slice of each tile's list with one global atomic per
 // (CTA, tile), and fills it through shared-memory cursors.
 // ---------------------------------------------------------------------------
 constexpr int kBinThreads = 256;
 constexpr int kMaxSmemTiles = 12288;  // 48 KB of counters
 
-// Visits every tile entry (tile, code) of visibility v (ok = v is valid);
-// all lanes of the warp must call it together.
+// Visits every tile entry (tile, code) of visibility v (ok = v is valid).
 template <class F>
 __device__ __forceinline__ void for_each_entry(const float* B, int v, bool ok, float scale, int g,
                                                int tiles_c, unsigned& k1, unsigned& k2, F&& f) {
@@ -309,12 +309,9 @@ __device__ __forceinline__ void for_each_entry(const float* B, int v, bool ok, f
       k2 = max(k2, (unsigned)c1);
     }
     const int tc0 = on ? c0 / FIP_GTILE : 0, tc1 = on ? c1 / FIP_GTILE : -1;
-    for (int s = 0; s < 6; ++s) {
-      const int kr = s >> 1, kc = s & 1;
-      const bool act = on && kr < ntr && tc0 + kc <= tc1;
-      const unsigned mask = __ballot_sync(0xffffffffu, act);
-      if (act) f((unsigned)(trs[kr] * tiles_c + tc0 + kc), ((unsigned)v << 1) | (unsigned)mir, mask);
-    }
+    for (int kr = 0; kr < ntr; ++kr)
+      for (int tc = tc0; tc <= tc1; ++tc)
+        f((unsigned)(trs[kr] * tiles_c + tc), ((unsigned)v << 1) | (unsigned)mir);
   }
 }
 
@@ -447,7 +444,7 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_count(
   for (int base = v0; base < v1; base += kBinThreads) {
     const int v = base + threadIdx.x;
     for_each_entry(B, v, v < v1, scale, g, tiles_c, k1, k2,
-                   [&](unsigned tile, unsigned, unsigned mask) { agg_inc(s_hist, tile, mask); });
+                   [&](unsigned tile, unsigned) { atomicAdd(&s_hist[tile], 1u); });
   }
   for (int o = 16; o > 0; o >>= 1) {
     k1 = max(k1, __shfl_xor_sync(0xffffffffu, k1, o));
@@ -492,7 +489,7 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(
   for (int base = v0; base < v1; base += kBinThreads) {
     const int v = base + threadIdx.x;
     for_each_entry(B, v, v < v1, scale, g, tiles_c, k1, k2,
-                   [&](unsigned tile, unsigned, unsigned mask) { agg_inc(s_hist, tile, mask); });
+                   [&](unsigned tile, unsigned) { atomicAdd(&s_hist[tile], 1u); });
   }
   __syncthreads();
   for (int t = threadIdx.x; t < ntiles; t += kBinThreads) {
@@ -503,8 +500,8 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(
   for (int base = v0; base < v1; base += kBinThreads) {
     const int v = base + threadIdx.x;
     for_each_entry(B, v, v < v1, scale, g, tiles_c, k1, k2,
-                   [&](unsigned tile, unsigned code, unsigned mask) {
-                     entries[agg_inc(s_hist, tile, mask)] = code;
+                   [&](unsigned tile, unsigned code) {
+                     entries[atomicAdd(&s_hist[tile], 1u)] = code;
                    });
   }
 }
@@ -796,7 +793,7 @@ __global__ void __launch_bounds__(kThreads) k_grid(const float* __restrict__ B, 
   float* s_cre = reinterpret_cast<float*>(reinterpret_cast<char*>(s_raw) + sizeof(GridSmem));
   float* s_cim = s_cre + FIP_GTILE * kTS;
   const float inten = plane_intensity(V);
-  const float vis_scale = vis_scale_p ? *vis_scale_p : 1.0f;
+  const float vis_scale = fip_vis_scale(vis_scale_p);
   const unsigned nw = *nwork;
   __syncthreads();
   for (unsigned w = blockIdx.x; w < nw; w += gridDim.x)
@@ -829,7 +826,7 @@ __global__ void __launch_bounds__(kThreads) k_grid_batch(const __grid_constant__
     while (s_first[k + 1] <= w) ++k;  // items are visited in increasing order
     const FipGridSnap& sn = in.s[k];
     const float inten = plane_intensity(sn.V);
-    const float vis_scale = sn.vis_scale ? *sn.vis_scale : 1.0f;
+    const float vis_scale = fip_vis_scale(sn.vis_scale);
     grid_item<VT, COMP>(S, s_cre, s_cim, sn.B, sn.vr, sn.vi, vis_scale, inten, sn.scale, sn.g,
                         sn.hp, sn.tiles_c, sn.layout, sn.entries, sn.work[w - s_first[k]],
                         sn.grid);

@@ -196,12 +196,12 @@ __global__ void k_maxabs(const L load, size_t nb, unsigned* out) {
 }
 
 // Scaled storage: the maximum maps to 2^14 (FP16 keeps 2^-24..65504), the
-// stored value is v / scale and the gridder multiplies by scale.
+// stored value is v / scale and the gridder multiplies by scale; the scale
+// buffer keeps the maximum, from which both sides form the scale
+// (fip_vis_scale).
 template <int VT, class L>
-__global__ void k_quantize(const L load, size_t nb, void* qr, void* qi, float* scale_io) {
-  const float mx = scale_io[0];  // max-abs bits written by k_maxabs
-  const float scale = mx > 0.f ? mx / 16384.0f : 1.0f;
-  const float inv = 1.0f / scale;
+__global__ void k_quantize(const L load, size_t nb, void* qr, void* qi, const float* max_abs) {
+  const float inv = 1.0f / fip_vis_scale(max_abs);
   for (size_t k = blockIdx.x * (size_t)kThreads + threadIdx.x; k < nb;
        k += (size_t)gridDim.x * kThreads) {
     float re, im;
@@ -214,11 +214,6 @@ __global__ void k_quantize(const L load, size_t nb, void* qr, void* qi, float* s
       reinterpret_cast<__nv_bfloat16*>(qi)[k] = __float2bfloat16_rn(im * inv);
     }
   }
-}
-
-__global__ void k_store_scale(float* scale_io) {
-  const float mx = scale_io[0];
-  scale_io[0] = mx > 0.f ? mx / 16384.0f : 1.0f;
 }
 
 }  // namespace
@@ -274,7 +269,6 @@ static cudaError_t launch_quantize(const L& load, size_t nb, int vis_type, void*
     k_quantize<FIP_VIS_F16><<<blocks, kThreads, 0, s>>>(load, nb, out_re, out_im, scale_out);
   else
     k_quantize<FIP_VIS_BF16><<<blocks, kThreads, 0, s>>>(load, nb, out_re, out_im, scale_out);
-  k_store_scale<<<1, 1, 0, s>>>(scale_out);
   return cudaGetLastError();
 }
 
