@@ -65,13 +65,15 @@ __device__ __forceinline__ void fip_collapse_sample(const FipRawVis& r, size_t s
   }
 }
 
-// Reduced (FP16/BF16) visibility storage keeps v / scale, with the scale
-// formed from the snapshot's max-abs (stored by the conversion pass) so that
-// the maximum maps to 2^14; null: FP32 storage, scale 1.
-__device__ __forceinline__ float fip_vis_scale(const float* max_abs) {
-  if (!max_abs) return 1.0f;
-  const float mx = *max_abs;
-  return mx > 0.f ? mx / 16384.0f : 1.0f;
+// Reduced (FP16/BF16) visibility storage keeps v / scale with one
+// power-of-two scale per block of 2^FIP_QBLOCK_SHIFT samples, which puts the
+// block's max-abs in [2^14, 2^15): a power of two leaves the FP16/BF16
+// rounding of every normal value as it would be unscaled, and a block scale
+// needs no pass over the whole snapshot before the conversion.
+#define FIP_QBLOCK_SHIFT 10
+#define FIP_QBLOCK (1 << FIP_QBLOCK_SHIFT)
+__host__ __device__ constexpr size_t fip_qblocks(size_t nb) {
+  return (nb + FIP_QBLOCK - 1) / FIP_QBLOCK;
 }
 
 // Batched launches: at most FIP_MAX_BATCH snapshots, of one or several
@@ -85,7 +87,7 @@ struct FipGridSnap {
   const void* vr;           // float, or half/bf16 for reduced storage
   const void* vi;
   const float* V;           // [9]
-  const float* vis_scale;   // reduced storage: the max-abs (fip_vis_scale), or null
+  const float* vis_scale;   // reduced storage: the block scales (fip_qblocks), or null
   const unsigned* entries;  // the snapshot's bins (FipBins)
   const int4* work;
   const unsigned* nwork;

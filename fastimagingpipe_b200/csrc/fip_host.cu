@@ -542,7 +542,7 @@ int fip_imager_create(fip_imager** out, const fip_imager_config* cfg) {
     if (cfg->form == FIP_FORM_PRECISE && cfg->vis_storage != FIP_STORE_F32) {
       FIP_ALLOC(dalloc((uint16_t**)&L.q_re, nb, tot));
       FIP_ALLOC(dalloc((uint16_t**)&L.q_im, nb, tot));
-      FIP_ALLOC(dalloc(&L.q_scale, 1, tot));
+      FIP_ALLOC(dalloc(&L.q_scale, fip_qblocks(nb), tot));
     }
   }
   if (im->custom_fft) {
@@ -664,7 +664,7 @@ static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const f
     else
       FIP_CUDA(fip_launch_quantize(vr, vi, nb, vt, L.q_re, L.q_im, L.q_scale, s));
     stage_end(im, k, s);
-    im->launches += 2;
+    im->launches += 1;
     gvr = L.q_re;
     gvi = L.q_im;
   }
@@ -832,7 +832,7 @@ int fip_grid_snapshot(fip_imager* im, const float* vis_re, const float* vis_im, 
   if (precise && im->cfg.vis_storage != FIP_STORE_F32) {
     vt = im->cfg.vis_storage == FIP_STORE_F16 ? FIP_VIS_F16 : FIP_VIS_BF16;
     FIP_CUDA(fip_launch_quantize(vis_re, vis_im, nb, vt, L.q_re, L.q_im, L.q_scale, s));
-    im->launches += 2;
+    im->launches += 1;
     gvr = L.q_re;
     gvi = L.q_im;
   }
@@ -1412,7 +1412,7 @@ struct BatchSeq {
   float2* targets = nullptr;          // [smax][N N] (plain form)
   void* q_re = nullptr;               // [smax][max_baselines] (reduced storage)
   void* q_im = nullptr;
-  float* q_scale = nullptr;           // [smax]
+  float* q_scale = nullptr;           // [smax][fip_qblocks(max_baselines)]
   // Linear ring: slots 0, 1 carry the sequence's last two images, the call's
   // snapshots go to slots 2 .. count + 1.
   float* images = nullptr;            // [smax + 2][N N]
@@ -1554,7 +1554,7 @@ FipGridSnap grid_snap(const fip_batch* b, const CallLayout& l, int k, const floa
   g.vi = reduced ? static_cast<const void*>(static_cast<char*>(q.q_im) +
                                             j * q.cfg.max_baselines * 2)
                  : vi;
-  g.vis_scale = reduced ? q.q_scale + j : nullptr;
+  g.vis_scale = reduced ? q.q_scale + j * fip_qblocks(q.cfg.max_baselines) : nullptr;
   const FipBins bins = q.bins(j);
   g.entries = bins.entries;
   g.work = bins.work;
@@ -1616,8 +1616,9 @@ int batch_record(fip_batch* b, const int* seq_of, const float* const* vr,
     if (reduced) {
       void* qr = static_cast<char*>(q.q_re) + j * q.cfg.max_baselines * 2;
       void* qi = static_cast<char*>(q.q_im) + j * q.cfg.max_baselines * 2;
-      FIP_CUDA(fip_launch_quantize(vr[k], vi[k], nb[k], vt, qr, qi, q.q_scale + j, bs));
-      launches += 2;
+      FIP_CUDA(fip_launch_quantize(vr[k], vi[k], nb[k], vt, qr, qi,
+                                   q.q_scale + j * fip_qblocks(q.cfg.max_baselines), bs));
+      launches += 1;
     }
     FipBins bins = q.bins(j);
     FIP_CUDA(fip_launch_bin(q.geo, B[k], (int)nb[k], bins, bs));
@@ -1800,7 +1801,7 @@ int seq_alloc(BatchSeq& q, size_t smax, size_t& tot) {
   if (cfg.form == FIP_FORM_PRECISE && cfg.vis_storage != FIP_STORE_F32) {
     FIP_SALLOC(dalloc((uint16_t**)&q.q_re, S * nb, tot));
     FIP_SALLOC(dalloc((uint16_t**)&q.q_im, S * nb, tot));
-    FIP_SALLOC(dalloc(&q.q_scale, S, tot));
+    FIP_SALLOC(dalloc(&q.q_scale, S * fip_qblocks(q.cfg.max_baselines), tot));
   }
   FIP_SALLOC(dalloc(&q.images, (S + 2) * q.n2, tot));
   FIP_SALLOC(dalloc(&q.maxima, S + 2, tot));

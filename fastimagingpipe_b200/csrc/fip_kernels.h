@@ -156,11 +156,11 @@ cudaError_t fip_launch_collapse(const float* v0r, const float* v0i, const float*
                                 const float* v3i, const unsigned char* f0,
                                 const unsigned char* f3, const float* w0, const float* w3,
                                 float* out_re, float* out_im, size_t ns, cudaStream_t s);
-// FP16/BF16 storage of a snapshot's visibilities (two launches): scale_out
-// receives the max-abs, from which the gridder forms the scale
-// (fip_vis_scale), and out_re/out_im the values divided by that scale.
+// FP16/BF16 storage of a snapshot's visibilities (one launch): scales
+// receives one power-of-two scale per block of FIP_QBLOCK samples
+// ([fip_qblocks(nb)]), out_re/out_im the values divided by their block's.
 cudaError_t fip_launch_quantize(const float* vr, const float* vi, size_t nb, int vis_type,
-                                void* out_re, void* out_im, float* scale_out, cudaStream_t s);
+                                void* out_re, void* out_im, float* scales, cudaStream_t s);
 // The same from raw two-polarisation samples, collapsed to Stokes I on load.
 cudaError_t fip_launch_quantize_raw(const FipRawVis& raw, size_t nb, int vis_type, void* out_re,
-                                    void* out_im, float* scale_out, cudaStream_t s);
+                                    void* out_im, float* scales, cudaStream_t s);

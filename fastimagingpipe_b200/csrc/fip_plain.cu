@@ -565,7 +565,7 @@ struct EntryTaps {
 
 template <int VT>
 __device__ __forceinline__ void entry_taps(const float* __restrict__ B, const void* vr,
-                                           const void* vi, float vis_scale, float inten,
+                                           const void* vi, const float* vis_scale, float inten,
                                            float scale, int g, unsigned ent, int trow0,
                                            int tcol0, const FipRawVis& raw, EntryTaps& e) {
   const int v = (int)(ent >> 1), mir = (int)(ent & 1);
@@ -585,8 +585,10 @@ __device__ __forceinline__ void entry_taps(const float* __restrict__ B, const vo
     wr = load_vis<VT>(vr, v) / inten;
     wi = load_vis<VT>(vi, v) / inten;
   } else {
-    wr = (load_vis<VT>(vr, v) * vis_scale) / inten;
-    wi = (load_vis<VT>(vi, v) * vis_scale) / inten;
+    // Reduced storage: the value over its block's power-of-two scale.
+    const float sc = vis_scale[v >> FIP_QBLOCK_SHIFT];
+    wr = (load_vis<VT>(vr, v) * sc) / inten;
+    wi = (load_vis<VT>(vi, v) * sc) / inten;
   }
   e.wr = 0.5f * wr;
   e.wi = mir ? -0.5f * wi : 0.5f * wi;
@@ -651,8 +653,9 @@ __device__ __forceinline__ void entry_taps(const float* __restrict__ B, const vo
 template <int VT, bool COMP>
 __device__ __forceinline__ void grid_item(GridSmem& S, float* s_cre, float* s_cim,
                                           const float* __restrict__ B,
-                                          const void* vr, const void* vi, float vis_scale,
-                                          float inten, float scale, int g, int hp, int tiles_c,
+                                          const void* vr, const void* vi,
+                                          const float* vis_scale, float inten, float scale,
+                                          int g, int hp, int tiles_c,
                                           int layout, const unsigned* __restrict__ entries,
                                           int4 item, float2* __restrict__ grid,
                                           const FipRawVis& raw = FipRawVis{}) {
@@ -793,11 +796,10 @@ __global__ void __launch_bounds__(kThreads) k_grid(const float* __restrict__ B, 
   float* s_cre = reinterpret_cast<float*>(reinterpret_cast<char*>(s_raw) + sizeof(GridSmem));
   float* s_cim = s_cre + FIP_GTILE * kTS;
   const float inten = plane_intensity(V);
-  const float vis_scale = fip_vis_scale(vis_scale_p);
   const unsigned nw = *nwork;
   __syncthreads();
   for (unsigned w = blockIdx.x; w < nw; w += gridDim.x)
-    grid_item<VT, COMP>(S, s_cre, s_cim, B, vr, vi, vis_scale, inten, scale, g, hp, tiles_c,
+    grid_item<VT, COMP>(S, s_cre, s_cim, B, vr, vi, vis_scale_p, inten, scale, g, hp, tiles_c,
                         layout, entries, work[w], grid, raw);
 }
 
@@ -826,8 +828,7 @@ __global__ void __launch_bounds__(kThreads) k_grid_batch(const __grid_constant__
     while (s_first[k + 1] <= w) ++k;  // items are visited in increasing order
     const FipGridSnap& sn = in.s[k];
     const float inten = plane_intensity(sn.V);
-    const float vis_scale = fip_vis_scale(sn.vis_scale);
-    grid_item<VT, COMP>(S, s_cre, s_cim, sn.B, sn.vr, sn.vi, vis_scale, inten, sn.scale, sn.g,
+    grid_item<VT, COMP>(S, s_cre, s_cim, sn.B, sn.vr, sn.vi, sn.vis_scale, inten, sn.scale, sn.g,
                         sn.hp, sn.tiles_c, sn.layout, sn.entries, sn.work[w - s_first[k]],
                         sn.grid);
   }

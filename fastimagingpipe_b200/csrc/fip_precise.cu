@@ -181,37 +181,49 @@ struct RawVis {
   }
 };
 
-// Per-snapshot max-abs of the visibilities (as float bits, values >= 0).
-template <class L>
-__global__ void k_maxabs(const L load, size_t nb, unsigned* out) {
+// One block of FIP_QBLOCK samples per CTA (kThreads threads, four samples
+// each): the block's max-abs, its power-of-two scale 2^(e - 14) for a max-abs
+// in [2^e, 2^(e+1)) (so the max lands in [2^14, 2^15), inside FP16's range,
+// and the division by the scale is exact), then the values divided by it.
+template <int VT, class L>
+__global__ void __launch_bounds__(kThreads) k_quantize(const L load, size_t nb, void* qr,
+                                                       void* qi, float* scales) {
+  static_assert(FIP_QBLOCK == 4 * kThreads, "four samples per thread");
+  __shared__ float s_max[kThreads / 32];
+  const size_t base = (size_t)blockIdx.x * FIP_QBLOCK;
+  float re[4], im[4];
   float m = 0.f;
-  for (size_t k = blockIdx.x * (size_t)kThreads + threadIdx.x; k < nb;
-       k += (size_t)gridDim.x * kThreads) {
-    float re, im;
-    load(k, re, im);
-    m = fmaxf(m, fmaxf(fabsf(re), fabsf(im)));
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const size_t i = base + (size_t)k * kThreads + threadIdx.x;
+    re[k] = 0.f;
+    im[k] = 0.f;
+    if (i < nb) load(i, re[k], im[k]);
+    m = fmaxf(m, fmaxf(fabsf(re[k]), fabsf(im[k])));
   }
   for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
-}
-
-// Scaled storage: the maximum maps to 2^14 (FP16 keeps 2^-24..65504), the
-// stored value is v / scale and the gridder multiplies by scale; the scale
-// buffer keeps the maximum, from which both sides form the scale
-// (fip_vis_scale).
-template <int VT, class L>
-__global__ void k_quantize(const L load, size_t nb, void* qr, void* qi, const float* max_abs) {
-  const float inv = 1.0f / fip_vis_scale(max_abs);
-  for (size_t k = blockIdx.x * (size_t)kThreads + threadIdx.x; k < nb;
-       k += (size_t)gridDim.x * kThreads) {
-    float re, im;
-    load(k, re, im);
+  if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = m;
+  __syncthreads();
+  m = s_max[0];
+#pragma unroll
+  for (int w = 1; w < kThreads / 32; ++w) m = fmaxf(m, s_max[w]);
+  // The max's biased exponent E gives scale 2^(E - 141) (bits E - 14) and
+  // inverse 2^(141 - E) (bits 268 - E).  E is held >= 15 so both are normal:
+  // a block whose max is below 2^-112 (zero included) takes scale 2^-126.
+  const int eb = max((int)((__float_as_uint(m) >> 23) & 0xffu), 15);
+  const float scale = __uint_as_float((unsigned)(eb - 14) << 23);
+  const float inv = __uint_as_float((unsigned)(268 - eb) << 23);
+  if (threadIdx.x == 0) scales[blockIdx.x] = scale;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const size_t i = base + (size_t)k * kThreads + threadIdx.x;
+    if (i >= nb) continue;
     if (VT == FIP_VIS_F16) {
-      reinterpret_cast<__half*>(qr)[k] = __float2half_rn(re * inv);
-      reinterpret_cast<__half*>(qi)[k] = __float2half_rn(im * inv);
+      reinterpret_cast<__half*>(qr)[i] = __float2half_rn(re[k] * inv);
+      reinterpret_cast<__half*>(qi)[i] = __float2half_rn(im[k] * inv);
     } else {
-      reinterpret_cast<__nv_bfloat16*>(qr)[k] = __float2bfloat16_rn(re * inv);
-      reinterpret_cast<__nv_bfloat16*>(qi)[k] = __float2bfloat16_rn(im * inv);
+      reinterpret_cast<__nv_bfloat16*>(qr)[i] = __float2bfloat16_rn(re[k] * inv);
+      reinterpret_cast<__nv_bfloat16*>(qi)[i] = __float2bfloat16_rn(im[k] * inv);
     }
   }
 }
@@ -260,24 +272,24 @@ cudaError_t fip_launch_collapse(const float* v0r, const float* v0i, const float*
 
 template <class L>
 static cudaError_t launch_quantize(const L& load, size_t nb, int vis_type, void* out_re,
-                                  void* out_im, float* scale_out, cudaStream_t s) {
-  cudaError_t e = cudaMemsetAsync(scale_out, 0, sizeof(float), s);
-  if (e != cudaSuccess) return e;
-  const int blocks = (int)std::min<size_t>(4 * 148, (nb + kThreads - 1) / kThreads + 1);
-  k_maxabs<<<blocks, kThreads, 0, s>>>(load, nb, reinterpret_cast<unsigned*>(scale_out));
+                                  void* out_im, float* scales, cudaStream_t s) {
+  const size_t blocks = fip_qblocks(nb);
+  if (blocks == 0) return cudaSuccess;
+  if (blocks > 0x7fffffffu) return cudaErrorInvalidValue;
   if (vis_type == FIP_VIS_F16)
-    k_quantize<FIP_VIS_F16><<<blocks, kThreads, 0, s>>>(load, nb, out_re, out_im, scale_out);
+    k_quantize<FIP_VIS_F16><<<(unsigned)blocks, kThreads, 0, s>>>(load, nb, out_re, out_im, scales);
   else
-    k_quantize<FIP_VIS_BF16><<<blocks, kThreads, 0, s>>>(load, nb, out_re, out_im, scale_out);
+    k_quantize<FIP_VIS_BF16><<<(unsigned)blocks, kThreads, 0, s>>>(load, nb, out_re, out_im,
+                                                                   scales);
   return cudaGetLastError();
 }
 
 cudaError_t fip_launch_quantize(const float* vr, const float* vi, size_t nb, int vis_type,
-                                void* out_re, void* out_im, float* scale_out, cudaStream_t s) {
-  return launch_quantize(F32Vis{vr, vi}, nb, vis_type, out_re, out_im, scale_out, s);
+                                void* out_re, void* out_im, float* scales, cudaStream_t s) {
+  return launch_quantize(F32Vis{vr, vi}, nb, vis_type, out_re, out_im, scales, s);
 }
 
 cudaError_t fip_launch_quantize_raw(const FipRawVis& raw, size_t nb, int vis_type, void* out_re,
-                                    void* out_im, float* scale_out, cudaStream_t s) {
-  return launch_quantize(RawVis{raw}, nb, vis_type, out_re, out_im, scale_out, s);
+                                    void* out_im, float* scales, cudaStream_t s) {
+  return launch_quantize(RawVis{raw}, nb, vis_type, out_re, out_im, scales, s);
 }
