@@ -1,9 +1,11 @@
-"""ctypes front end of the reference's own CUDA build (oracle/_ref/libfipref.so).
+"""ctypes front end of the reference's own CUDA build (oracle/_ref/libfipref.so,
+and its GPU preprocessing in oracle/_ref/libfippre.so).
 
-TEST INFRASTRUCTURE ONLY: the reference's FIPkernels.cu recompiled for sm_100a
-by `make -C oracle ref` (the sources are read where they lie at build time; the
-built library travels with the repository).  Used by the GPU parity tests and
-by bench.py's reference arm; never by the product.
+TEST INFRASTRUCTURE ONLY: the reference's FIPkernels.cu and
+SVDPreprocessKernels.cu recompiled for sm_100a by `make -C oracle ref` (the
+sources are read where they lie at build time; the built libraries travel with
+the repository).  Used by the GPU parity tests and by bench.py's reference
+arm; never by the product.
 """
 from __future__ import annotations
 
@@ -14,7 +16,9 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_ref", "libfipref.so")
+PRE_LIB_PATH = os.path.join(_HERE, "_ref", "libfippre.so")
 _LIB = None
+_PRE = None
 
 
 def available() -> bool:
@@ -82,3 +86,40 @@ def pixel_targets(V, n, cell) -> np.ndarray:
         raise RuntimeError(f"ref_pixel_targets failed ({st})")
     oi = oi.reshape(n, n, 2)  # [i][j][2] (FIPkernels.cu:296)
     return np.ascontiguousarray(oi.transpose(1, 0, 2)) - np.float32(n // 2)
+
+
+def preprocess_available() -> bool:
+    return os.path.exists(PRE_LIB_PATH)
+
+
+def preprocess(uvw_m, freqs_hz, v0, v3, flag0, flag3, weight0, weight3):
+    """The reference's GPU preprocessing (SVDPreprocessKernels.cu:255-500):
+    uvw [rows][3] metres, freqs [chans] Hz, complex polarisations 0 and 3,
+    uint8 flags and weights [rows * chans] (sample row + chan * rows).
+    Returns B [samples][2], V [3][3], and the collapsed visibilities
+    (real, imaginary)."""
+    global _PRE
+    if _PRE is None:
+        L = ctypes.CDLL(PRE_LIB_PATH)
+        vp, sz = ctypes.c_void_p, ctypes.c_size_t
+        L.ref_preprocess.argtypes = [sz, sz] + [vp] * 14
+        L.ref_preprocess.restype = ctypes.c_int
+        _PRE = L
+    uvw = _f(uvw_m).reshape(-1, 3)
+    freqs = _f(freqs_hz)
+    rows, chans = uvw.shape[0], freqs.shape[0]
+    ns = rows * chans
+    arrs = [_f(np.real(v0)), _f(np.imag(v0)), _f(np.real(v3)), _f(np.imag(v3))]
+    flags = [np.ascontiguousarray(f, dtype=np.uint8) for f in (flag0, flag3)]
+    weights = [_f(w) for w in (weight0, weight3)]
+    B = np.zeros((ns, 2), np.float32)
+    V = np.zeros(9, np.float32)
+    vr = np.zeros(ns, np.float32)
+    vi = np.zeros(ns, np.float32)
+    rc = _PRE.ref_preprocess(rows, chans, uvw.ctypes.data, freqs.ctypes.data,
+                             *(a.ctypes.data for a in arrs), *(f.ctypes.data for f in flags),
+                             *(w.ctypes.data for w in weights), B.ctypes.data, V.ctypes.data,
+                             vr.ctypes.data, vi.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("the reference's preprocessing failed")
+    return B, V.reshape(3, 3), vr, vi

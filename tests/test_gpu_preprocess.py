@@ -9,6 +9,11 @@
   rows) and the fused collapse into the image -- against the FP64 oracle's
   plane fit, collapse and imager: images within 1e-4 relative RMS (precision
   form; the device fit's FP32 outputs against the FP64 fit).
+* The device plane fit and collapse against the reference's own GPU
+  preprocessing (SVDPreprocessKernels.cu recompiled for sm_100a,
+  oracle/_ref/libfippre.so: FP32 moments with atomics, a cuSOLVER
+  eigensolve, its PCA sign rule), run live: V and B within the FP32
+  covariance's rounding, the collapsed visibilities within 1e-6.
 """
 import numpy as np
 import pytest
@@ -16,8 +21,11 @@ import pytest
 import fastimagingpipe_b200 as fip
 from fastimagingpipe_b200 import synthetic
 import oracle
+from oracle import reference as ref
 
 pytestmark = pytest.mark.gpu
+needs_pre = pytest.mark.skipif(not ref.preprocess_available(),
+                               reason="oracle/_ref/libfippre.so not built")
 
 
 def relrms(a, b):
@@ -97,3 +105,35 @@ def test_raw_entry_point_rejects_null_arrays(cuda):
     with fip.Imager(64, 64, 1e-3, 16) as im:
         with pytest.raises(fip.FipError):
             im.image_snapshot_raw(z, z, z, z, u8, None, z, z, z, z, 64, z)
+
+
+@needs_pre
+@pytest.mark.parametrize("seed,ha,chans", [(7, 1.5, (130e6, 140e6, 150e6)),
+                                           (12, -2.0, (142e6,)),
+                                           (5, 0.3, tuple(130e6 + 2.5e6 * k for k in range(8)))])
+def test_plane_fit_and_collapse_vs_reference_gpu_preprocessing(cuda, seed, ha, chans):
+    import torch
+    raw = synthetic.make_raw_snapshot(seed=seed, hour_angle_h=ha, freqs_hz=chans)
+    ns = raw.num_samples
+    B, V = plane(raw, cuda)
+    d = raw_device(raw, cuda)
+    cre, cim = torch.zeros(ns, device=cuda), torch.zeros(ns, device=cuda)
+    fip.collapse_visibilities(d["v0_re"], d["v0_im"], d["v3_re"], d["v3_im"], d["flag0"],
+                              d["flag3"], d["weight0"], d["weight3"], cre, cim, ns)
+    torch.cuda.synchronize()
+    Br, Vr, vr, vi = ref.preprocess(raw.uvw_m, raw.freqs_hz, raw.xx, raw.yy, raw.flag0,
+                                    raw.flag3, raw.weight0, raw.weight3)
+    got_V = V.cpu().numpy().reshape(3, 3)
+    # Same rows, signs and handedness (the sign rule picks each row's sign
+    # from its largest component; the third row is their cross product).
+    assert np.abs(got_V - Vr).max() <= 2e-5, (got_V, Vr)
+    got_B = B.cpu().numpy().reshape(-1, 2)
+    scale = float(np.abs(Br).max())
+    assert np.abs(got_B - Br).max() <= 3e-5 * scale
+    assert np.allclose(cre.cpu().numpy(), vr, rtol=1e-6, atol=1e-6)
+    assert np.allclose(cim.cpu().numpy(), vi, rtol=1e-6, atol=1e-6)
+    # The oracle's FP64 fit (the checker of the tests above) against the
+    # reference's, pinning its sign rule and sample order.
+    Bo, Vo = oracle.plane_fit(raw.uvw_m, raw.freqs_hz)
+    assert np.abs(Vo - Vr).max() <= 2e-5
+    assert np.abs(Bo - Br).max() <= 3e-5 * scale
