@@ -1664,8 +1664,9 @@ __device__ __forceinline__ void tile_target(const TileMap& t, int a, int b, floa
 // from the exact map): per source row, one column interval.  Each candidate
 // is splatted (bilinear weights of FIPkernels.cu:394-410) into shared memory;
 // the tile is stored once and its maximum folded into *img_max.
-// EXACT: targets from the closed form in FP64 (precision form) instead of
-// the precomputed reference-chain targets.
+// EXACT: targets from the closed form (precision form), in FP32 relative to
+// a per-tile origin whose terms are FP64 (TileMap), instead of the
+// precomputed reference-chain targets.
 // The shared tile carries an apron of kAp pixels on every side, so the four
 // pixels of any candidate's splat land inside it without per-pixel checks
 // (apron pixels belong to the neighbouring tiles, which splat them
