@@ -450,6 +450,32 @@ def test_identical_snapshots_give_unit_tlisi(cuda):
     assert np.abs(res - 1.0).max() <= 1e-6
 
 
+@pytest.mark.parametrize("storage,tol", [(fip.STORE_F16, 1e-3), (fip.STORE_BF16, 8e-3)])
+def test_reduced_storage_block_scales_at_extreme_blocks(cuda, storage, tol):
+    """Reduced storage keeps one power-of-two scale per 1,024 visibilities:
+    a block of zeros (the smallest scale), a block 1e12 brighter and one
+    1e-12 fainter than the rest, and a partial last block (2,145 samples
+    per snapshot here) image as with FP32 storage within the storage's
+    rounding, in the precision form."""
+    snap = synthetic.config_small(n_ant=66, transient_snapshot=2)
+    nb = snap.num_baselines
+    assert nb % 1024 != 0 and nb > 2048
+    for k in range(3):
+        v = slice(k * nb, (k + 1) * nb)
+        for arr in (snap.vis_re, snap.vis_im):
+            a = arr[v]
+            a[:1024] = 0.0
+            a[1024:2048] *= 1e12 if k != 1 else 1e-12
+    want, wimg, _ = run(snap, cuda, form=fip.FORM_PRECISE, vis_storage=fip.STORE_F32)
+    got, gimg, _ = run(snap, cuda, form=fip.FORM_PRECISE, vis_storage=storage)
+    assert np.isfinite(gimg).all()
+    for k in range(3):
+        assert relrms(gimg[k], wimg[k]) <= tol
+    both = np.isfinite(want) & np.isfinite(got)
+    assert np.array_equal(np.isfinite(want), np.isfinite(got))
+    assert np.abs(got - want)[both].max() <= 50 * tol
+
+
 def test_zero_visibilities_give_nan_like_reference(cuda):
     snap = synthetic.config_tiny()
     snap.vis_re[:] = 0
