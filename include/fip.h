@@ -56,6 +56,10 @@ typedef enum {
   FIP_FORM_PRECISE = 1
 } fip_form;
 
+/* Device storage of a snapshot's visibilities in the precision form: FP32,
+ * or FP16/BF16 with one power-of-two scale per 1,024 visibilities (the
+ * block's max-abs lands in [2^14, 2^15)), converted in one pass per call;
+ * the gridder multiplies each value by its block's scale. */
 typedef enum { FIP_STORE_F32 = 0, FIP_STORE_F16 = 1, FIP_STORE_BF16 = 2 } fip_vis_storage;
 
 const char* fip_last_error(void);
