@@ -24,9 +24,11 @@
 // engine takes it into a step; until then it waits in the host queue, which
 // holds max_queue requests (FIP_ERR_NOT_READY beyond that).
 //
-// Beams the batch engine cannot serve (image sizes that are not powers of
-// two, or the scatter reprojection) get an imager of their own and are served
-// one snapshot at a time.  Latency is measured per request from submit to
+// Beams of image sizes that are not powers of two, or with the scatter
+// reprojection, get an imager of their own and are served one snapshot at a
+// time: the batch engine transforms such sizes with cuFFT, whose plan and
+// work area per step size are made on first use, outside the memory that the
+// group's HBM admission sizes.  Latency is measured per request from submit to
 // result.
 #include <cuda_runtime.h>
 
