@@ -412,6 +412,17 @@ static void imager_free(fip_imager* im) {
   delete im;
 }
 
+// The gridder's sums: the precision form's two-limb compensated sums for
+// FP32 (or raw) visibilities; one int32 limb (2^-30 of a work item's summed
+// weights, 2^19 below the rounding of the stored values) for FP16/BF16
+// storage, whose own rounding the compensation could not recover.
+static int grid_compensated(bool precise, int vt) {
+  return precise && vt != FIP_VIS_F16 && vt != FIP_VIS_BF16 ? 1 : 0;
+}
+static int grid_compensated(const fip_imager_config& c) {
+  return c.form == FIP_FORM_PRECISE && c.vis_storage == FIP_STORE_F32 ? 1 : 0;
+}
+
 static int validate_sizes(size_t n, size_t t, float cell) {
   if (n < 16 || n % 4 != 0)
     return fail(FIP_ERR_ARG, "image_size must be a multiple of 4 and >= 16 (the reference's "
@@ -670,7 +681,7 @@ static int image_snapshot_impl(fip_imager* im, Lane& L, const float* vr, const f
   }
   k = stage_begin(im, ST_GRID, s);
   FIP_CUDA(fip_launch_grid(geo, B, gvr, gvi, vt, L.q_scale, V, (int)nb, L.bins, L.grid,
-                           precise ? 1 : 0, s, im->grid_ctas_per_sm, raw));
+                           grid_compensated(precise, vt), s, im->grid_ctas_per_sm, raw));
   stage_end(im, k, s);
   im->launches += fip_bin_launches(geo) + 2;  // binning, zero tiles, grid
   if (im->custom_fft) {
@@ -838,7 +849,7 @@ int fip_grid_snapshot(fip_imager* im, const float* vis_re, const float* vis_im, 
   }
   FIP_CUDA(fip_launch_bin(geo, B, (int)nb, L.bins, s));
   FIP_CUDA(fip_launch_grid(geo, B, gvr, gvi, vt, L.q_scale, V, (int)nb, L.bins,
-                           reinterpret_cast<float2*>(grid), precise ? 1 : 0, s,
+                           reinterpret_cast<float2*>(grid), grid_compensated(precise, vt), s,
                            im->grid_ctas_per_sm));
   im->last_lane = 0;
   im->launches += fip_bin_launches(geo) + 2;
@@ -1175,12 +1186,12 @@ int fip_imager_autotune(fip_imager* im, const float* vr, const float* vi, const 
   {
     float best = 1e30f;
     int chosen = 0;
-    for (int c = 1; c <= fip_grid_max_ctas_per_sm(precise ? 1 : 0); ++c) {
+    for (int c = 1; c <= fip_grid_max_ctas_per_sm(grid_compensated(precise, vt)); ++c) {
       float ms = 0.f;
       FIP_TRY(timed(
           [&]() -> cudaError_t {
             return fip_launch_grid(geo, B, gvr, gvi, vt, L.q_scale, V, (int)nb, L.bins,
-                                   L.grid, precise ? 1 : 0, s, c);
+                                   L.grid, grid_compensated(precise, vt), s, c);
           },
           ms));
       if (ms < best) {
@@ -1221,7 +1232,7 @@ int fip_imager_tuning(const fip_imager* im, int* fft_values_per_thread, int* fft
   if (grid_ctas_per_sm)
     *grid_ctas_per_sm = im->grid_ctas_per_sm > 0
                             ? im->grid_ctas_per_sm
-                            : fip_grid_max_ctas_per_sm(im->cfg.form == FIP_FORM_PRECISE ? 1 : 0);
+                            : fip_grid_max_ctas_per_sm(grid_compensated(im->cfg));
   return FIP_OK;
 }
 
@@ -1639,7 +1650,7 @@ int batch_record(fip_batch* b, const int* seq_of, const float* const* vr,
                                    l.per[c], s));
     launches += 1;
   }
-  FIP_CUDA(fip_launch_grid_batch(in, vt, precise ? 1 : 0, s, b->grid_ctas_per_sm));
+  FIP_CUDA(fip_launch_grid_batch(in, vt, grid_compensated(precise, vt), s, b->grid_ctas_per_sm));
   launches += 1;
   FIP_CUDA(phase(2));
   // Grid sides not 3 * 2^k: one batched cuFFT C2R (in place, phase 2) and the
@@ -2208,9 +2219,10 @@ static int batch_autotune(fip_batch* b, const int* seq_of, const float* const* v
   {
     float best = 1e30f;
     int chosen = 0;
-    for (int c = 1; c <= fip_grid_max_ctas_per_sm(precise ? 1 : 0); ++c) {
+    const int comp = grid_compensated(precise, vt);
+    for (int c = 1; c <= fip_grid_max_ctas_per_sm(comp); ++c) {
       float ms = 0.f;
-      FIP_TRY(timed([&]() -> cudaError_t { return fip_launch_grid_batch(in, vt, precise ? 1 : 0, s, c); },
+      FIP_TRY(timed([&]() -> cudaError_t { return fip_launch_grid_batch(in, vt, comp, s, c); },
                     ms));
       if (ms < best) {
         best = ms;
@@ -2253,7 +2265,7 @@ int fip_batch_sequence_tuning(const fip_batch* b, int sequence, int* fft_values_
   if (grid_ctas_per_sm)
     *grid_ctas_per_sm = b->grid_ctas_per_sm > 0
                             ? b->grid_ctas_per_sm
-                            : fip_grid_max_ctas_per_sm(b->cfg.form == FIP_FORM_PRECISE ? 1 : 0);
+                            : fip_grid_max_ctas_per_sm(grid_compensated(b->cfg));
   return FIP_OK;
 }
 

@@ -644,7 +644,8 @@ __device__ __forceinline__ void entry_taps(const float* __restrict__ B, const vo
 // sums are native integer atomics: exact and independent of their order.
 // Plain form: q = round(tap * 2^30 / bound) in one int32, `bound` (the
 // item's summed weights) bounding every cell sum.
-// Precision form (COMP): t = tap * 2^e, 2^e = the power of two with
+// Precision form with FP32 visibilities (COMP; with FP16/BF16 storage the
+// precision form sums as the plain form does): t = tap * 2^e, 2^e = the power of two with
 // bound * 2^e < 2^45, is exact in FP32 and is split exactly into
 // hi * 2^23 + lo (hi < 2^22 in magnitude, 0 <= lo <= 2^23), two int32 limbs
 // summed separately (at most 256 taps per cell per item: no overflow), so a

@@ -52,7 +52,9 @@ typedef enum {
    * pixel mapping, FP32 sums), B200 data movement. */
   FIP_FORM_PLAIN = 0,
   /* Precision form: exact closed-form reprojection, compensated FP32 grid
-   * and tLISI sums, FP64 tLISI combine; visibility storage per vis_storage. */
+   * sums (FP32 storage; one int32 fixed-point limb with FP16/BF16 storage,
+   * whose rounding dominates) and tLISI sums, FP64 tLISI combine;
+   * visibility storage per vis_storage. */
   FIP_FORM_PRECISE = 1
 } fip_form;
 

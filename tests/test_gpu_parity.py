@@ -581,11 +581,13 @@ def test_row_pass_band_copy_at_reference_shape(cuda, direct):
     assert relrms(imgs[1], imgs[0]) <= 1e-6
 
 
-@pytest.mark.parametrize("form", ["plain", "precise"])
+@pytest.mark.parametrize("form", ["plain", "precise", "precise_f32"])
 def test_autotune_keeps_results(cuda, small, form):
     """The autotuner only picks launch shapes: results stay within rounding."""
     import torch
-    kw = {} if form == "plain" else dict(form=fip.FORM_PRECISE, vis_storage=fip.STORE_F16)
+    kw = ({} if form == "plain" else
+          dict(form=fip.FORM_PRECISE,
+               vis_storage=fip.STORE_F32 if form == "precise_f32" else fip.STORE_F16))
     n, nb, t = small.image_size, small.num_baselines, small.unit_size
     u = n // t
     d = to_dev(small, cuda)
@@ -594,7 +596,9 @@ def test_autotune_keeps_results(cuda, small, form):
         im.pipe_device(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, before)
         choice = im.autotune(d["vis_re"], d["vis_im"], d["B"], d["V"], nb)
         assert choice["fft_values_per_thread"] in (8, 16)
-        assert 1 <= choice["grid_ctas_per_sm"] <= (4 if form == "plain" else 3)
+        # Two-limb compensated sums (FP32 storage) fit 3 gridder CTAs per SM,
+        # one-limb sums (plain form, FP16/BF16 storage) 4.
+        assert 1 <= choice["grid_ctas_per_sm"] <= (3 if form == "precise_f32" else 4)
         im.pipe_device(d["vis_re"], d["vis_im"], d["B"], d["V"], nb, after)
         torch.cuda.synchronize()
     assert np.abs(after.cpu().numpy() - before.cpu().numpy()).max() <= 1e-5
